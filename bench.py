@@ -1,0 +1,332 @@
+"""MCSA benchmark: time-to-1e-8 and walk-steps/s on one B200 per rank.
+
+Workload (default): 3D 7-point variable-coefficient diffusion on 128^3
+(2,097,152 unknowns; D log-uniform in [0.1, 10] per cell, absorption 0.01,
+b ~ U(0,1), seed 0), point-Jacobi MCSA with the expected-value estimator,
+FP32 walks/records/tallies, FP64 residual and update, 2^22 histories per
+iteration (Sample Ratio 2), History Length 10, stop at |rp|/|PL b| <= 1e-8.
+
+One step = one full MCSA solve from x = 0 on the same seed (identical work
+each step).  `value` = walk steps / device time of the solves with b and x
+resident in HBM (CUDA events on the library stream); `e2e` = the same solves
+through the host-buffer C-ABI call (H2D of b and x0, D2H of x inside the
+timed region).  Inputs are larger than L2 (working set ~0.4 GB).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mcls_b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MCSA time-to-1e-8 residual, learned vs Jacobi precond, one B200; walk-steps/sec"
+UNIT = "walk-steps/s"
+CONFIGS = {
+    "c2": dict(workload="3D 7-pt variable-coefficient diffusion 128^3, Jacobi MCSA, expected-value "
+                        "estimator, FP32 walks / FP64 residual, 2^22 histories per iteration",
+               n=128, sample_ratio=2.0, estimator=1, history_length=10),
+    "c1": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, collision estimator, FP64 walks, "
+                        "N histories per iteration",
+               n=100, sample_ratio=1.0, estimator=0, history_length=10),
+}
+# Algorithmic bytes of one walk step for a k-entry row record: k * (4 B CDF +
+# 4 B column|sign) + 4 B row weight + 8 B FP32 tally read-modify-write.
+K_ENTRIES = {"c2": 6, "c1": 4}
+
+
+def step_bytes(cfg):
+    k = K_ENTRIES[cfg]
+    return 8 * k + 12
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def make_system(cfg):
+    from mcls_b200 import problems as P
+
+    c = CONFIGS[cfg]
+    if cfg == "c2":
+        A, b = P.diffusion3d_varcoef(c["n"], seed=0)
+    else:
+        A = P.poisson2d(c["n"])
+        b = np.ones(A.shape[0])
+    return A, b
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        import torch
+
+        pg.barrier()
+        torch.cuda.synchronize()
+
+
+def allmax(pg, v):
+    if pg is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(pg, v):
+    if pg is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t)
+    return float(t.item())
+
+
+def cpu_baseline(cfg, A, b, seconds_target=15.0):
+    """Oracle port: multi-threaded adjoint walks on the same domain."""
+    from oracle import oracle as O
+
+    c = CONFIGS[cfg]
+    Ao = O.Csr.from_scipy(A)
+    mc = O.MC(Ao, PL=O.point_jacobi(Ao), history_length=c["history_length"], rng_mode=1)
+    threads = os.cpu_count() or 1
+    src = (1.0 / A.diagonal()) * b
+    nh = 1 << 18
+    steps, secs, _ = mc.bench_walks(src, nh, threads)
+    # scale the sample to ~seconds_target of CPU work
+    nh2 = int(min(1 << 26, nh * max(1.0, seconds_target / max(secs, 1e-3))))
+    steps, secs, _ = mc.bench_walks(src, nh2, threads)
+    return {"value": steps / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nh2} adjoint histories x {c['history_length']} steps on the "
+                      f"{A.shape[0]}-row Jacobi domain, {secs:.1f} s"}
+
+
+def run_reference(args, world, rank, pg):
+    if rank != 0:
+        return
+    A, b = make_system(args.config)
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args.config, A, b, seconds_target=max(2.0, 60.0 / (args.warmup + args.steps)))
+        if i >= args.warmup:
+            vals.append(cb["value"])
+        base = cb
+    v = float(np.mean(vals))
+    base["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": CONFIGS[args.config]["workload"], "l2": "inputs larger than L2"},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mcls_b200", choices=["mcls_b200", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-iters", type=int, default=20000)
+    args = ap.parse_args()
+    world, rank, local, pg = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import torch
+
+    from mcls_b200 import capi
+
+    cfgd = CONFIGS[args.config]
+    torch.cuda.set_device(local)
+    A, b = make_system(args.config)
+    n = A.shape[0]
+    fp = capi.FP32 if args.config == "c2" else capi.FP64
+    ctx = capi.Context(local)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    seed = 1234 + rank
+    dom = capi.Domain(ctx, op, pc, precision=fp, rng_mode=capi.RNG_COUNTER, seed=seed,
+                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
+                      history_length=cfgd["history_length"])
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
+    bt = torch.tensor(b, device=f"cuda:{local}", dtype=torch.float64)
+    xt = torch.zeros_like(bt)
+
+    def device_step():
+        dom.reseed(seed)
+        xt.zero_()
+        torch.cuda.synchronize()
+        return dom.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
+
+    for _ in range(args.warmup):
+        st = device_step()
+    clocks = ClockSampler(local)
+    barrier(pg)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = time.perf_counter()
+    stats = [device_step() for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(pg)
+    clk = clocks.stop()
+    dev_ms = sum(s["solve_ms"] for s in stats)
+    steps_total = sum(s["walk_steps"] for s in stats)
+    dev_ms_max = allmax(pg, dev_ms)
+    steps_all = allsum(pg, steps_total)
+    value = steps_all / (dev_ms_max * 1e-3)
+
+    # End to end through the host-buffer call: H2D(b, x0) + solve + D2H(x).
+    bh = np.ascontiguousarray(b)
+    e2e_ms = 0.0
+    e2e_steps = 0
+    barrier(pg)
+    for _ in range(args.steps):
+        dom.reseed(seed)
+        x0 = np.zeros(n)
+        t1 = time.perf_counter()
+        x, st = dom.mcsa_solve(bh, x0, params=mp)
+        e2e_ms += (time.perf_counter() - t1) * 1e3
+        e2e_steps += st["walk_steps"]
+    barrier(pg)
+    e2e_ms = allmax(pg, e2e_ms)
+    e2e_value = allsum(pg, e2e_steps) / (e2e_ms * 1e-3)
+
+    s0 = stats[-1]
+    rel = float(np.linalg.norm(b - A @ xt.cpu().numpy()) / np.linalg.norm(b))
+    peak, peak_kind = load_peaks()
+    walk_ms = sum(s["walk_ms"] for s in stats)
+    walk_launches = sum(s["walk_launches"] for s in stats)
+    per_launch_ms = walk_ms / max(walk_launches, 1)
+    bytes_per_launch = step_bytes(args.config) * steps_total / max(walk_launches, 1)
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fp == capi.FP32 else "f64",
+        "data": "synthetic",
+        "config": {"workload": cfgd["workload"], "n": n, "nnz": int(A.nnz),
+                   "histories_per_iteration": int(s0["histories"] // max(s0["iterations"], 1)),
+                   "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+                   "l2": "inputs larger than L2 (no flush)",
+                   "time_to_1e-8_s": dev_ms_max / args.steps / 1e3,
+                   "iterations": s0["iterations"], "achieved_tol": s0["achieved_tol"],
+                   "rel_residual_b_minus_Ax": rel},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "kernel": "walk32", "peak_kind": peak_kind,
+                     "bytes_per_step": step_bytes(args.config),
+                     "walk_ms_per_launch": per_launch_ms,
+                     "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
+        "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.config, A, b)
+    if rank == 0:
+        print(json.dumps(line))
+    dom.close()
+    pc.close()
+    op.close()
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,257 @@
+/*
+ * mclsgpu.h -- C ABI of the B200 MCSA library (libmclsgpu.so).
+ *
+ * This is the drop-in boundary under the MCLS solver managers: the C++
+ * facade (include/MCLS_*.hpp) and any FFI binding call only these entry
+ * points.  Plain pointers and sizes; no CUDA or C++ types in signatures.
+ * Every entry point returns an mclsgpu_status and never throws; the message
+ * of the last failure on a context is available through mclsgpu_last_error.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the MCLS source tree).
+ *
+ * Threading: one context owns one CUDA stream; calls on one context must be
+ * serialised by the caller (the reference is single-threaded per rank).
+ * Distinct contexts may be used from distinct host threads.
+ * Ownership: host arrays are borrowed for the duration of a call and copied;
+ * the *_dev variants borrow caller device memory for the duration of the
+ * call.  Handles are owned by the caller and released with *_destroy.
+ */
+#ifndef MCLSGPU_H
+#define MCLSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCLSGPU_ABI_VERSION 1
+
+typedef enum {
+    MCLSGPU_OK = 0,
+    MCLSGPU_ERR_INVALID_ARG = 1,  /* bad argument (MCLS_REQUIRE analogue)        */
+    MCLSGPU_ERR_CUDA = 2,         /* CUDA runtime error                           */
+    MCLSGPU_ERR_DIVERGED = 3,     /* non-finite residual or weight                */
+    MCLSGPU_ERR_TIMEOUT = 4,      /* a bounded device wait gave up                */
+    MCLSGPU_ERR_NOT_CONVERGED = 5,/* informational: max iterations reached        */
+    MCLSGPU_ERR_DEGENERATE = 6,   /* empty or zero-weight domain row (MCLS_CHECK) */
+    MCLSGPU_ERR_NO_DEVICE = 7,    /* no usable CUDA device                        */
+    MCLSGPU_ERR_UNSUPPORTED = 8   /* configuration outside this build's limits    */
+} mclsgpu_status;
+
+/* Monte Carlo direction (MonteCarloTag of the reference managers). */
+enum { MCLSGPU_ADJOINT = 0, MCLSGPU_FORWARD = 1 };
+/* Estimator: "Estimator Type" = "Collision" | "Expected Value". */
+enum { MCLSGPU_COLLISION = 0, MCLSGPU_EXPECTED_VALUE = 1 };
+/* "Source Sampling Type" = "Random" | "Stratified". */
+enum { MCLSGPU_SOURCE_RANDOM = 0, MCLSGPU_SOURCE_STRATIFIED = 1 };
+/* Walk precision: FP64 records/uniforms/weights/tallies (bit-exact parity
+ * mode) or FP32 packed records, uniforms, weights and tallies. */
+enum { MCLSGPU_FP64 = 0, MCLSGPU_FP32 = 1 };
+/* Random stream: the reference's single Xorshift stream reproduced exactly
+ * (GF(2) jump-ahead per history) or the counter-based per-history stream. */
+enum { MCLSGPU_RNG_REFERENCE = 0, MCLSGPU_RNG_COUNTER = 1 };
+/* Preconditioner kinds. */
+enum {
+    MCLSGPU_PREC_NONE = 0,
+    MCLSGPU_PREC_POINT_JACOBI = 1,
+    MCLSGPU_PREC_BLOCK_JACOBI = 2,
+    MCLSGPU_PREC_LEARNED_SPAI = 3,
+    MCLSGPU_PREC_USER_CSR = 4
+};
+
+typedef struct mclsgpu_context mclsgpu_context;
+typedef struct mclsgpu_operator mclsgpu_operator;
+typedef struct mclsgpu_precond mclsgpu_precond;
+typedef struct mclsgpu_domain mclsgpu_domain;
+
+/* Monte Carlo parameters.  Field <-> ParameterList key:
+ *   history_length      "History Length" (src/MCLS_AlmostOptimalDomain_impl.hpp:88-91)
+ *   weight_cutoff       "Weight Cutoff", relative to |starting weight|; 0 = off
+ *   sample_ratio        "Sample Ratio"; <= 0 means the key is absent
+ *                       (src/MCLS_UniformAdjointSource_impl.hpp:82-86)
+ *   source_sampling     "Source Sampling Type" (:90-101)
+ *   neumann_relaxation  "Neumann Relaxation"; <= 0 means absent
+ *   composite_threshold "Composite Operator Threshold"
+ *   rng_mode            "Reproducible MC Mode" = true selects REFERENCE
+ *   seed                Xorshift seed (REFERENCE) or stream key (COUNTER)
+ */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_mc_params) */
+    int32_t direction;
+    int32_t estimator;
+    int32_t history_length;
+    double weight_cutoff;
+    double sample_ratio;
+    int32_t source_sampling;
+    int32_t precision;
+    double neumann_relaxation;
+    double composite_threshold;
+    int32_t rng_mode;
+    int32_t reserved0;
+    uint64_t seed;
+} mclsgpu_mc_params;
+
+/* MCSA parameters (src/MCLS_MCSASolverManager_impl.hpp:290-343). */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_mcsa_params) */
+    int32_t max_iters;        /* "Maximum Iterations" (1000)        */
+    double tolerance;         /* "Convergence Tolerance" (1.0)      */
+    int32_t check_freq;       /* "Iteration Check Frequency" (1)    */
+    int32_t smoother_steps;   /* "Smoother Steps" (1)               */
+    double richardson_omega;  /* "Richardson Relaxation" (1.0)      */
+    int32_t print_freq;       /* "Iteration Print Frequency" (10)   */
+    int32_t verbose;          /* print the reference's banner lines */
+    int32_t batch_iters;      /* iterations launched per host check (0 = auto) */
+    int32_t reserved0;
+} mclsgpu_mcsa_params;
+
+/* Preconditioner parameters. */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_precond_params) */
+    int32_t kind;             /* MCLSGPU_PREC_*                                 */
+    int32_t block_size;       /* "Jacobi Block Size" for BLOCK_JACOBI           */
+    int32_t reserved0;
+    /* USER_CSR: a host CSR matrix used as the left preconditioner. */
+    int64_t user_n;
+    const int64_t* user_rowptr;
+    const int64_t* user_colind;
+    const double* user_values;
+    /* LEARNED_SPAI: network handle from mclsgpu_spai_* (may be NULL) and the
+     * spectral-radius threshold at which Jacobi is used instead (0.95). */
+    const void* spai_net;
+    double rho_fallback;
+} mclsgpu_precond_params;
+
+/* Statistics of the last solve. */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_stats) */
+    int32_t iterations;
+    int32_t converged;
+    int32_t fallback_taken;   /* learned preconditioner replaced by Jacobi */
+    double achieved_tol;      /* |rp|_2 / |PL b|_2 (MCSASolverManager::achievedTol) */
+    double residual_norm;     /* final |rp|_2 */
+    int64_t histories;        /* histories transported (all iterations) */
+    int64_t walk_steps;       /* transitions performed (all iterations) */
+    double solve_ms;          /* device time of the solve (CUDA events) */
+    double walk_ms;           /* FP32 walk kernels: summed device duration */
+    double rho;               /* spectral radius estimate (when computed) */
+    int64_t walk_launches;    /* FP32 walk kernel launches in the solve */
+    int64_t kernel_launches;  /* library kernels launched by the solve */
+} mclsgpu_stats;
+
+/* ---- version / device --------------------------------------------------- */
+int mclsgpu_abi_version(void);
+/* Library build information (architecture, options). */
+const char* mclsgpu_build_info(void);
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces the Teuchos::Comm / rank plumbing of the managers: one context per
+ * device.  `device` < 0 selects the current device. */
+int mclsgpu_context_create(int device, mclsgpu_context** out);
+int mclsgpu_context_destroy(mclsgpu_context* ctx);
+const char* mclsgpu_last_error(const mclsgpu_context* ctx);
+/* Synchronise the context stream and report any pending device error. */
+int mclsgpu_context_sync(mclsgpu_context* ctx);
+
+/* ---- operator (LinearProblem's A) --------------------------------------- */
+/* Replaces LinearProblem(A, x, b)'s operator handle
+ * (src/MCLS_LinearProblem.hpp:73-80): a square FP64 CSR matrix with sorted
+ * column indices, copied to the device. */
+int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n,
+                            const int64_t* rowptr, const int64_t* colind,
+                            const double* values, mclsgpu_operator** out);
+int mclsgpu_operator_destroy(mclsgpu_operator* op);
+int64_t mclsgpu_operator_rows(const mclsgpu_operator* op);
+int64_t mclsgpu_operator_nnz(const mclsgpu_operator* op);
+/* y = A x with host vectors (MatrixTraits::apply,
+ * tpetra/src/MCLS_TpetraCrsMatrixAdapter.hpp:366-371). */
+int mclsgpu_operator_apply(mclsgpu_operator* op, const double* x, double* y);
+
+/* ---- preconditioner ------------------------------------------------------ */
+/* Replaces Preconditioner<Matrix>::buildPreconditioner / getLeftPreconditioner
+ * (src/MCLS_Preconditioner.hpp:75-100;
+ *  tpetra/src/MCLS_TpetraPointJacobiPreconditioner_impl.hpp:104-139;
+ *  tpetra/src/MCLS_TpetraBlockJacobiPreconditioner_impl.hpp:122-223). */
+int mclsgpu_precond_build(mclsgpu_context* ctx, mclsgpu_operator* op,
+                          const mclsgpu_precond_params* params,
+                          mclsgpu_precond** out);
+int mclsgpu_precond_destroy(mclsgpu_precond* pc);
+/* Copies the preconditioner's CSR to host arrays (NULL arrays query sizes:
+ * *nnz_out receives the entry count). */
+int mclsgpu_precond_export(mclsgpu_precond* pc, int64_t* nnz_out,
+                           int64_t* rowptr, int64_t* colind, double* values);
+
+/* ---- Monte Carlo domain --------------------------------------------------- */
+/* Replaces MonteCarloSolverManager::buildMonteCarloDomain + the
+ * AlmostOptimalDomain constructor (src/MCLS_MonteCarloSolverManager_impl.hpp:
+ * 308-340, src/MCLS_AlmostOptimalDomain_impl.hpp:70-366): builds the
+ * (transposed, for ADJOINT) composite operator PL*A*PR, the iteration matrix
+ * H = I - w*M on its pattern, the per-row CDFs and weights, and the packed
+ * FP32 walk records.  `right` may be NULL (no right preconditioner). */
+int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op,
+                         mclsgpu_precond* left, mclsgpu_precond* right,
+                         const mclsgpu_mc_params* params,
+                         mclsgpu_domain** out);
+int mclsgpu_domain_destroy(mclsgpu_domain* dom);
+/* Copies the FP64 domain (rowptr[n+1], col[nnz], h[nnz], cdf[nnz],
+ * weights[n]) to host arrays; NULL arrays query *nnz_out only. */
+int mclsgpu_domain_export(mclsgpu_domain* dom, int64_t* nnz_out,
+                          int64_t* rowptr, int64_t* col, double* h,
+                          double* cdf, double* weights);
+/* Replace the stream seed/position (restart the reproducible stream). */
+int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed);
+/* Per-rank Xorshift seed as PRNG<RNG>(rank) derives it
+ * (src/MCLS_PRNG_impl.hpp:56-75) with std::random_device replaced by
+ * `master_seed`. */
+uint64_t mclsgpu_rank_seed(uint64_t master_seed, int rank);
+
+/* ---- Monte Carlo solve ---------------------------------------------------- */
+/* Replaces MonteCarloSolverManager::solve (src/MCLS_MonteCarloSolverManager_
+ * impl.hpp:199-235) and MCSolver::solve (src/MCLS_MCSolver_impl.hpp:82-112):
+ * x = MC estimate of (I-H)^-1 (PL rhs, x w).  `internal` = 1 skips the left
+ * preconditioning of the source and the right recovery (the MCSA inner
+ * solve).  Host vectors of length n. */
+int mclsgpu_mc_solve(mclsgpu_domain* dom, const double* rhs, double* x,
+                     int internal, mclsgpu_stats* stats);
+/* Same with device vectors. */
+int mclsgpu_mc_solve_dev(mclsgpu_domain* dom, const double* rhs_dev,
+                         double* x_dev, int internal, mclsgpu_stats* stats);
+/* Parity instrument: one MC solve recording, per history in emission order
+ * (up to max_trace histories), the state before each step
+ * (states[e*(L+1)+k], -1 after termination), the final weight, the
+ * termination event (2 = CUTOFF) and the starting state. */
+int mclsgpu_mc_trace(mclsgpu_domain* dom, const double* rhs, double* x,
+                     int internal, int64_t max_trace, int64_t* states,
+                     double* final_weight, int32_t* events,
+                     int64_t* start_state, int64_t* num_histories);
+
+/* ---- MCSA solve ------------------------------------------------------------ */
+/* Replaces MCSASolverManager::solve (src/MCLS_MCSASolverManager_impl.hpp:
+ * 278-432) including RichardsonIteration::doOneIteration
+ * (src/MCLS_RichardsonIteration_impl.hpp:134-147) and
+ * LinearProblem::updatePrecResidual (src/MCLS_LinearProblem_impl.hpp:
+ * 410-442).  x is updated in place.  Returns MCLSGPU_OK whether or not the
+ * tolerance was met; stats->converged carries the converged status. */
+int mclsgpu_mcsa_solve(mclsgpu_domain* dom, const double* b, double* x,
+                       const mclsgpu_mcsa_params* params,
+                       mclsgpu_stats* stats);
+int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev,
+                           double* x_dev, const mclsgpu_mcsa_params* params,
+                           mclsgpu_stats* stats);
+
+/* ---- spectral radius ------------------------------------------------------- */
+/* Replaces AlmostOptimalDomain::computeConvergenceCriteria
+ * (src/MCLS_AlmostOptimalDomain_impl.hpp:437-635): FP64 power iteration
+ * estimates of rho(H) (which = 0), rho(|H|) (which = 1) and rho(H*)
+ * (which = 2, |h_ij| * W_i). */
+int mclsgpu_domain_spectral_radius(mclsgpu_domain* dom, int which,
+                                   int max_iters, double tol, uint64_t seed,
+                                   double* rho);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCLSGPU_H */

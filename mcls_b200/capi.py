@@ -1,0 +1,389 @@
+"""ctypes binding of libmclsgpu.so (the C ABI in include/mclsgpu.h).
+
+This is what the tests and bench.py call: every solve goes through the same
+extern "C" entry points a C++, cgo or JNI caller would bind.  Loading fails
+loudly when the library is missing -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import scipy.sparse as sp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmclsgpu.so")
+
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_DIVERGED, ERR_TIMEOUT, ERR_NOT_CONVERGED, \
+    ERR_DEGENERATE, ERR_NO_DEVICE, ERR_UNSUPPORTED = range(9)
+ADJOINT, FORWARD = 0, 1
+COLLISION, EXPECTED_VALUE = 0, 1
+SOURCE_RANDOM, SOURCE_STRATIFIED = 0, 1
+FP64, FP32 = 0, 1
+RNG_REFERENCE, RNG_COUNTER = 0, 1
+PREC_NONE, PREC_POINT_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED_SPAI, PREC_USER_CSR = range(5)
+
+
+class McParams(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("direction", C.c_int32),
+        ("estimator", C.c_int32),
+        ("history_length", C.c_int32),
+        ("weight_cutoff", C.c_double),
+        ("sample_ratio", C.c_double),
+        ("source_sampling", C.c_int32),
+        ("precision", C.c_int32),
+        ("neumann_relaxation", C.c_double),
+        ("composite_threshold", C.c_double),
+        ("rng_mode", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("seed", C.c_uint64),
+    ]
+
+
+class McsaParams(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("max_iters", C.c_int32),
+        ("tolerance", C.c_double),
+        ("check_freq", C.c_int32),
+        ("smoother_steps", C.c_int32),
+        ("richardson_omega", C.c_double),
+        ("print_freq", C.c_int32),
+        ("verbose", C.c_int32),
+        ("batch_iters", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+class PrecondParams(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("kind", C.c_int32),
+        ("block_size", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("user_n", C.c_int64),
+        ("user_rowptr", C.c_void_p),
+        ("user_colind", C.c_void_p),
+        ("user_values", C.c_void_p),
+        ("spai_net", C.c_void_p),
+        ("rho_fallback", C.c_double),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("fallback_taken", C.c_int32),
+        ("achieved_tol", C.c_double),
+        ("residual_norm", C.c_double),
+        ("histories", C.c_int64),
+        ("walk_steps", C.c_int64),
+        ("solve_ms", C.c_double),
+        ("walk_ms", C.c_double),
+        ("rho", C.c_double),
+        ("walk_launches", C.c_int64),
+        ("kernel_launches", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "size"}
+
+
+#: Every entry point declared in include/mclsgpu.h.
+EXPORTS = [
+    "mclsgpu_abi_version", "mclsgpu_build_info", "mclsgpu_context_create",
+    "mclsgpu_context_destroy", "mclsgpu_last_error", "mclsgpu_context_sync",
+    "mclsgpu_operator_upload", "mclsgpu_operator_destroy", "mclsgpu_operator_rows",
+    "mclsgpu_operator_nnz", "mclsgpu_operator_apply", "mclsgpu_precond_build",
+    "mclsgpu_precond_destroy", "mclsgpu_precond_export", "mclsgpu_domain_build",
+    "mclsgpu_domain_destroy", "mclsgpu_domain_export", "mclsgpu_domain_reseed",
+    "mclsgpu_rank_seed", "mclsgpu_mc_solve", "mclsgpu_mc_solve_dev", "mclsgpu_mc_trace",
+    "mclsgpu_mcsa_solve", "mclsgpu_mcsa_solve_dev", "mclsgpu_domain_spectral_radius",
+]
+
+_LIB = None
+
+
+class MclsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mclsgpu error {code}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Load libmclsgpu.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} not built: run `python -m mcls_b200.build`")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    PP = C.POINTER(C.c_void_p)
+    d = C.c_double
+    i64 = C.c_int64
+    L.mclsgpu_abi_version.restype = C.c_int
+    L.mclsgpu_build_info.restype = C.c_char_p
+    L.mclsgpu_context_create.argtypes = [C.c_int, PP]
+    L.mclsgpu_context_destroy.argtypes = [P]
+    L.mclsgpu_last_error.argtypes = [P]
+    L.mclsgpu_last_error.restype = C.c_char_p
+    L.mclsgpu_context_sync.argtypes = [P]
+    L.mclsgpu_operator_upload.argtypes = [P, i64, P, P, P, PP]
+    L.mclsgpu_operator_destroy.argtypes = [P]
+    L.mclsgpu_operator_rows.argtypes = [P]
+    L.mclsgpu_operator_rows.restype = i64
+    L.mclsgpu_operator_nnz.argtypes = [P]
+    L.mclsgpu_operator_nnz.restype = i64
+    L.mclsgpu_operator_apply.argtypes = [P, P, P]
+    L.mclsgpu_precond_build.argtypes = [P, P, C.POINTER(PrecondParams), PP]
+    L.mclsgpu_precond_destroy.argtypes = [P]
+    L.mclsgpu_precond_export.argtypes = [P, C.POINTER(i64), P, P, P]
+    L.mclsgpu_domain_build.argtypes = [P, P, P, P, C.POINTER(McParams), PP]
+    L.mclsgpu_domain_destroy.argtypes = [P]
+    L.mclsgpu_domain_export.argtypes = [P, C.POINTER(i64), P, P, P, P, P]
+    L.mclsgpu_domain_reseed.argtypes = [P, C.c_uint64]
+    L.mclsgpu_rank_seed.argtypes = [C.c_uint64, C.c_int]
+    L.mclsgpu_rank_seed.restype = C.c_uint64
+    L.mclsgpu_mc_solve.argtypes = [P, P, P, C.c_int, C.POINTER(Stats)]
+    L.mclsgpu_mc_solve_dev.argtypes = [P, P, P, C.c_int, C.POINTER(Stats)]
+    L.mclsgpu_mc_trace.argtypes = [P, P, P, C.c_int, i64, P, P, P, P, C.POINTER(i64)]
+    L.mclsgpu_mcsa_solve.argtypes = [P, P, P, C.POINTER(McsaParams), C.POINTER(Stats)]
+    L.mclsgpu_mcsa_solve_dev.argtypes = [P, P, P, C.POINTER(McsaParams), C.POINTER(Stats)]
+    L.mclsgpu_domain_spectral_radius.argtypes = [P, C.c_int, C.c_int, d, C.c_uint64,
+                                                 C.POINTER(d)]
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None else None
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        rc = self.L.mclsgpu_context_create(device, C.byref(h))
+        if rc != OK:
+            raise MclsError(rc, "context create failed")
+        self.h = h
+
+    def check(self, rc):
+        if rc != OK:
+            raise MclsError(rc, self.L.mclsgpu_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mclsgpu_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def _csr64(A):
+    A = sp.csr_matrix(A)
+    rp = np.ascontiguousarray(A.indptr, np.int64)
+    ci = np.ascontiguousarray(A.indices, np.int64)
+    v = np.ascontiguousarray(A.data, np.float64)
+    return A.shape[0], rp, ci, v
+
+
+class Operator:
+    def __init__(self, ctx: Context, A):
+        self.ctx = ctx
+        n, rp, ci, v = _csr64(A)
+        self.n = n
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_operator_upload(ctx.h, n, _ptr(rp), _ptr(ci), _ptr(v), C.byref(h)))
+        self.h = h
+
+    def apply(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        self.ctx.check(self.ctx.L.mclsgpu_operator_apply(self.h, _ptr(x), _ptr(y)))
+        return y
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_operator_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Precond:
+    def __init__(self, ctx: Context, op: Operator, kind: int, block_size: int = 1, user=None,
+                 rho_fallback: float = 0.95, net=None):
+        self.ctx = ctx
+        p = PrecondParams()
+        p.size = C.sizeof(PrecondParams)
+        p.kind = kind
+        p.block_size = block_size
+        p.rho_fallback = rho_fallback
+        keep = []
+        if user is not None:
+            n, rp, ci, v = _csr64(user)
+            keep = [rp, ci, v]
+            p.user_n = n
+            p.user_rowptr, p.user_colind, p.user_values = _ptr(rp), _ptr(ci), _ptr(v)
+        if net is not None:
+            p.spai_net = net
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_precond_build(ctx.h, op.h, C.byref(p), C.byref(h)))
+        del keep
+        self.h = h
+
+    def to_scipy(self, n):
+        nnz = C.c_int64()
+        L = self.ctx.L
+        self.ctx.check(L.mclsgpu_precond_export(self.h, C.byref(nnz), None, None, None))
+        rp = np.empty(n + 1, np.int64)
+        ci = np.empty(max(nnz.value, 1), np.int64)
+        v = np.empty(max(nnz.value, 1), np.float64)
+        self.ctx.check(L.mclsgpu_precond_export(self.h, C.byref(nnz), _ptr(rp), _ptr(ci), _ptr(v)))
+        return sp.csr_matrix((v[: nnz.value], ci[: nnz.value], rp), shape=(n, n))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_precond_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def mc_params(direction=ADJOINT, estimator=COLLISION, history_length=10, weight_cutoff=0.0,
+              sample_ratio=-1.0, source_sampling=SOURCE_RANDOM, precision=FP32,
+              neumann_relaxation=-1.0, composite_threshold=0.0, rng_mode=RNG_COUNTER, seed=1):
+    p = McParams()
+    p.size = C.sizeof(McParams)
+    p.direction = direction
+    p.estimator = estimator
+    p.history_length = history_length
+    p.weight_cutoff = weight_cutoff
+    p.sample_ratio = sample_ratio
+    p.source_sampling = source_sampling
+    p.precision = precision
+    p.neumann_relaxation = neumann_relaxation
+    p.composite_threshold = composite_threshold
+    p.rng_mode = rng_mode
+    p.seed = seed
+    return p
+
+
+def mcsa_params(tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
+                richardson_omega=1.0, print_freq=10, verbose=0):
+    p = McsaParams()
+    p.size = C.sizeof(McsaParams)
+    p.tolerance = tolerance
+    p.max_iters = max_iters
+    p.check_freq = check_freq
+    p.smoother_steps = smoother_steps
+    p.richardson_omega = richardson_omega
+    p.print_freq = print_freq
+    p.verbose = verbose
+    return p
+
+
+class Domain:
+    def __init__(self, ctx: Context, op: Operator, left: Precond | None = None,
+                 right: Precond | None = None, params: McParams | None = None, **kw):
+        self.ctx = ctx
+        self.op = op
+        self.left = left
+        self.right = right
+        self.p = params if params is not None else mc_params(**kw)
+        self.n = op.n
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_domain_build(ctx.h, op.h, left.h if left else None,
+                                             right.h if right else None, C.byref(self.p),
+                                             C.byref(h)))
+        self.h = h
+
+    def export(self):
+        L = self.ctx.L
+        nnz = C.c_int64()
+        self.ctx.check(L.mclsgpu_domain_export(self.h, C.byref(nnz), None, None, None, None, None))
+        k = nnz.value
+        rp = np.empty(self.n + 1, np.int64)
+        col = np.empty(max(k, 1), np.int64)
+        h = np.empty(max(k, 1), np.float64)
+        cdf = np.empty(max(k, 1), np.float64)
+        w = np.empty(self.n, np.float64)
+        self.ctx.check(L.mclsgpu_domain_export(self.h, C.byref(nnz), _ptr(rp), _ptr(col), _ptr(h),
+                                               _ptr(cdf), _ptr(w)))
+        return dict(rowptr=rp, col=col[:k], h=h[:k], cdf=cdf[:k], weights=w)
+
+    def reseed(self, seed):
+        self.ctx.check(self.ctx.L.mclsgpu_domain_reseed(self.h, seed))
+
+    def mc_solve(self, rhs, internal=False):
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        x = np.empty_like(rhs)
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_mc_solve(self.h, _ptr(rhs), _ptr(x), int(internal),
+                                                   C.byref(st)))
+        return x, st.as_dict()
+
+    def mc_trace(self, rhs, max_trace, internal=False):
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        x = np.empty_like(rhs)
+        L = self.p.history_length
+        states = np.empty(max(max_trace, 1) * (L + 1), np.int64)
+        fw = np.empty(max(max_trace, 1), np.float64)
+        ev = np.empty(max(max_trace, 1), np.int32)
+        st = np.empty(max(max_trace, 1), np.int64)
+        nh = C.c_int64()
+        self.ctx.check(self.ctx.L.mclsgpu_mc_trace(self.h, _ptr(rhs), _ptr(x), int(internal),
+                                                   max_trace, _ptr(states), _ptr(fw), _ptr(ev),
+                                                   _ptr(st), C.byref(nh)))
+        k = min(nh.value, max_trace)
+        return x, nh.value, dict(states=states.reshape(-1, L + 1)[:k], final_weight=fw[:k],
+                                 events=ev[:k], start=st[:k])
+
+    def mcsa_solve(self, b, x0=None, params: McsaParams | None = None, **kw):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+        p = params if params is not None else mcsa_params(**kw)
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_solve(self.h, _ptr(b), _ptr(x), C.byref(p),
+                                                     C.byref(st)))
+        return x, st.as_dict()
+
+    def mcsa_solve_dev(self, b_ptr, x_ptr, params: McsaParams | None = None, **kw):
+        """Device-pointer variant (e.g. torch tensors' data_ptr())."""
+        p = params if params is not None else mcsa_params(**kw)
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_solve_dev(self.h, C.c_void_p(b_ptr),
+                                                         C.c_void_p(x_ptr), C.byref(p),
+                                                         C.byref(st)))
+        return st.as_dict()
+
+    def spectral_radius(self, which=0, max_iters=2000, tol=1e-8, seed=7):
+        rho = C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_domain_spectral_radius(self.h, which, max_iters, tol,
+                                                                 seed, C.byref(rho)))
+        return rho.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_domain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def rank_seed(master: int, rank: int) -> int:
+    return int(load().mclsgpu_rank_seed(master, rank))

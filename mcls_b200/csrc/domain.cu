@@ -1,0 +1,174 @@
+// domain.cu -- device build of the Monte Carlo domain.
+//
+// Restates AlmostOptimalDomain::addMatrixToDomain
+// (src/MCLS_AlmostOptimalDomain_impl.hpp:257-366) as two passes over the
+// composite operator's rows: count the retained entries, then write the signed
+// iteration-matrix values h, the normalised CDF of |h| and the row weight
+// W = sum |h|.  FP64 arithmetic uses explicitly rounded operations so that
+// no multiply-add contraction changes the reference's rounding.  A third pass
+// packs the FP32 walk records: one fixed-stride record per row,
+//   slot 0:      { W (float bits), row length }
+//   slot 1..K:   { cdf_j (float bits), col_j | (h_j <= 0) << 31 }
+//   padding:     { 2.0f, 0 }  (never selected: every uniform is < 1)
+// so that one walk step reads exactly one contiguous record.
+#include <cfloat>
+#include <vector>
+
+#include "internal.h"
+
+namespace mclsgpu {
+int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int* d_rp,
+                              long long* total);
+
+namespace {
+
+inline int grid_for(long long work, int threads = 256) {
+    long long g = (work + threads - 1) / threads;
+    if (g < 1) g = 1;
+    return int(g > 148 * 16 ? 148 * 16 : g);
+}
+
+__device__ __forceinline__ double iteration_value(int row, int col, double m, double relax) {
+    // (col == row) ? 1 - w*m : -w*m, each operation rounded separately.
+    const double prod = __dmul_rn(relax, m);
+    return col == row ? __dsub_rn(1.0, prod) : -prod;
+}
+
+__global__ void k_domain_count(const int* rp, const int* ci, const double* v, int n,
+                               double relax, int* cnt, int* status, int* max_len) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int c = 0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            double h = iteration_value(i, ci[k], v[k], relax);
+            if (!(fabs(h) < DBL_EPSILON)) ++c;  // :312-317
+        }
+        cnt[i] = c;
+        if (c == 0) atomicOr(status, DEV_ERR_DEGENERATE);  // MCLS_CHECK(num_entries > 0)
+        atomicMax(max_len, c);
+    }
+}
+
+__global__ void k_domain_fill(const int* rp, const int* ci, const double* v, int n,
+                              double relax, const int* drp, int* dcol, double* dh,
+                              double* dcdf, double* dw, int* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int o = drp[i];
+        double c = 0.0;
+        const int o0 = o;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            double h = iteration_value(i, ci[k], v[k], relax);
+            if (fabs(h) < DBL_EPSILON) continue;
+            dcol[o] = ci[k];
+            dh[o] = h;
+            c = (o == o0) ? fabs(h) : __dadd_rn(fabs(h), c);  // :342-348
+            dcdf[o] = c;
+            ++o;
+        }
+        const double W = c;  // :353
+        dw[i] = W;
+        if (!(W > 0.0) || !isfinite(W)) {
+            atomicOr(status, DEV_ERR_DEGENERATE);
+            continue;
+        }
+        for (int k = o0; k < o; ++k) dcdf[k] = __ddiv_rn(dcdf[k], W);  // :357-362
+    }
+}
+
+__global__ void k_pack_records(const int* drp, const int* dcol, const double* dh,
+                               const double* dcdf, const double* dw, int n, int slots,
+                               uint2* rec) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint2* r = rec + size_t(i) * slots;
+        const int a = drp[i], len = drp[i + 1] - drp[i];
+        r[0] = make_uint2(__float_as_uint(__double2float_rn(dw[i])), unsigned(len));
+        for (int t = 0; t < slots - 1; ++t) {
+            if (t < len) {
+                unsigned cs = unsigned(dcol[a + t]) | (dh[a + t] > 0.0 ? 0u : 0x80000000u);
+                r[1 + t] = make_uint2(__float_as_uint(__double2float_rn(dcdf[a + t])), cs);
+            } else {
+                r[1 + t] = make_uint2(__float_as_uint(2.0f), 0u);
+            }
+        }
+    }
+}
+
+__global__ void k_to_float(const double* a, float* b, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        b[i] = __double2float_rn(a[i]);
+}
+
+}  // namespace
+
+// Build the FP64 domain arrays and FP32 records from the composite M.
+int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
+                        mclsgpu_domain* dom) {
+    cudaStream_t s = ctx->stream;
+    const int n = M.n;
+    int* cnt = nullptr;
+    int* maxlen = nullptr;
+    cudaError_t e;
+    if ((e = dmalloc(&cnt, n + 1)) != cudaSuccess || (e = dmalloc(&maxlen, 1)) != cudaSuccess) {
+        dfree(cnt);
+        return cuda_fail(ctx, e, "cudaMalloc");
+    }
+    cudaMemsetAsync(maxlen, 0, sizeof(int), s);
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    k_domain_count<<<grid_for(n), 256, 0, s>>>(M.rp, M.ci, M.v, n, relax, cnt, ctx->d_status,
+                                               maxlen);
+    DevCsr& D = dom->D;
+    D.release();
+    D.n = n;
+    int rc = MCLSGPU_OK;
+    if ((e = dmalloc(&D.rp, n + 1)) != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMalloc");
+    long long tot = 0;
+    if (!rc) rc = exclusive_scan_counts_dev(ctx, cnt, n, D.rp, &tot);
+    int hmax = 0;
+    if (!rc) {
+        cudaMemcpyAsync(&hmax, maxlen, sizeof(int), cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "domain count");
+    }
+    dfree(cnt);
+    dfree(maxlen);
+    if (rc) return rc;
+    if ((rc = check_device_status(ctx))) return rc;
+    D.nnz = int(tot);
+    dom->max_row = hmax;
+    if ((e = dmalloc(&D.ci, tot + 1)) != cudaSuccess || (e = dmalloc(&D.v, tot + 1)) != cudaSuccess ||
+        (e = dmalloc(&dom->cdf, tot + 1)) != cudaSuccess || (e = dmalloc(&dom->w, n + 1)) != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaMalloc");
+    k_domain_fill<<<grid_for(n), 256, 0, s>>>(M.rp, M.ci, M.v, n, relax, D.rp, D.ci, D.v,
+                                              dom->cdf, dom->w, ctx->d_status);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "domain fill");
+    if ((rc = check_device_status(ctx))) return rc;
+
+    // FP32 records: slot count = 1 + longest row, rounded up to a supported
+    // stride.
+    static const int kStrides[] = {4, 8, 12, 16, 24, 32};
+    int slots = 0;
+    for (int st : kStrides)
+        if (hmax + 1 <= st) {
+            slots = st;
+            break;
+        }
+    dom->slots = slots;  // 0: rows too long for packed records (FP64 walk only)
+    if (slots) {
+        if ((e = dmalloc(&dom->rec, size_t(n) * slots)) != cudaSuccess)
+            return cuda_fail(ctx, e, "cudaMalloc records");
+        k_pack_records<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n, slots,
+                                                   dom->rec);
+    }
+    // Transposed domain for the adjoint expected-value estimator.
+    if (dom->p.direction == MCLSGPU_ADJOINT && dom->p.estimator == MCLSGPU_EXPECTED_VALUE) {
+        if ((rc = csr_transpose(ctx, D, dom->DT))) return rc;
+        if ((e = dmalloc(&dom->dt_h32, dom->DT.nnz + 1)) != cudaSuccess)
+            return cuda_fail(ctx, e, "cudaMalloc");
+        k_to_float<<<grid_for(dom->DT.nnz), 256, 0, s>>>(dom->DT.v, dom->dt_h32, dom->DT.nnz);
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "domain records");
+    return MCLSGPU_OK;
+}
+
+}  // namespace mclsgpu

@@ -1,0 +1,207 @@
+// internal.h -- shared types of the mclsgpu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+
+#include "../../include/mclsgpu.h"
+
+namespace mclsgpu {
+
+// Device status word bits (set by kernels, read and cleared by the host).
+enum : int {
+    DEV_ERR_DEGENERATE = 1,   // empty / zero-weight domain row
+    DEV_ERR_NONFINITE = 2,    // non-finite weight, residual or tally
+    DEV_ERR_TIMEOUT = 4,      // a bounded wait gave up
+    DEV_ERR_BOUNDS = 8,       // an index failed a bounds check
+    DEV_ERR_CAPACITY = 16     // more histories than the buffers were sized for
+};
+
+struct Status {
+    int code = MCLSGPU_OK;
+    std::string msg;
+};
+
+}  // namespace mclsgpu
+
+struct mclsgpu_context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    int* d_status = nullptr;      // device error word
+    int* h_status = nullptr;      // pinned mirror
+    std::string err;
+};
+
+namespace mclsgpu {
+
+// Device CSR with int32 indices (n, nnz < 2^31).
+struct DevCsr {
+    int n = 0;
+    int nnz = 0;
+    int* rp = nullptr;
+    int* ci = nullptr;
+    double* v = nullptr;
+    void release();
+};
+
+}  // namespace mclsgpu
+
+struct mclsgpu_operator {
+    mclsgpu_context* ctx = nullptr;
+    mclsgpu::DevCsr A;
+    double* dinv = nullptr;       // reciprocal diagonal (built on demand)
+    uint64_t serial = 0;          // identity for "operator changed" checks
+};
+
+struct mclsgpu_precond {
+    mclsgpu_context* ctx = nullptr;
+    int kind = MCLSGPU_PREC_NONE;
+    int block_size = 1;
+    mclsgpu::DevCsr P;            // left preconditioner as CSR
+    double* diag = nullptr;       // POINT_JACOBI: the reciprocal diagonal
+    double rho = -1.0;            // LEARNED_SPAI: rho(H) estimate
+    int fallback = 0;             // LEARNED_SPAI replaced by Jacobi
+};
+
+namespace mclsgpu {
+
+struct McsaState {
+    int iter;            // iterations completed
+    int done;            // 1 once the loop must stop
+    int check_freq;
+    int max_iters;
+    double crit;         // tolerance * |PL b|
+    double rnorm;        // last |rp|_2
+    int converged;
+    int pad;
+};
+
+}  // namespace mclsgpu
+
+struct mclsgpu_domain {
+    mclsgpu_context* ctx = nullptr;
+    mclsgpu_operator* op = nullptr;
+    mclsgpu_precond* left = nullptr;
+    mclsgpu_precond* right = nullptr;
+    mclsgpu_mc_params p{};
+    int n = 0;
+    // FP64 domain (AlmostOptimalDomain data): row r lists (col, h, cdf).
+    mclsgpu::DevCsr D;            // D.v holds h
+    double* cdf = nullptr;
+    double* w = nullptr;
+    // Transposed domain for the expected-value estimator: DT(j,s) = h_sj.
+    mclsgpu::DevCsr DT;
+    float* dt_h32 = nullptr;
+    // Packed FP32 walk records: row r at rec + r*slots, slot 0 = {W, len},
+    // slots 1..slots-1 = {cdf (float bits), col | sign<<31}.
+    uint2* rec = nullptr;
+    int slots = 0;
+    int max_row = 0;
+    // Random stream.
+    uint64_t seed = 1;
+    unsigned long long* d_epoch = nullptr;  // counter mode: MC solves so far
+    uint64_t* d_jump = nullptr;    // reference mode: 64x64 jump tables
+    unsigned long long* d_pos = nullptr;  // reference mode: draws consumed
+    // Source / tally work buffers.
+    int64_t nh_cap = 0;
+    double* src = nullptr;         // scaled source vector (n)
+    double* scdf = nullptr;        // source CDF (n)
+    int* guide = nullptr;          // guide table (n)
+    int* counts = nullptr;         // histories per state (n)
+    int* offs = nullptr;           // emission offsets (n)
+    int* start = nullptr;          // start state | sign<<31 per history
+    float* y32 = nullptr;          // FP32 tallies (n)
+    double* y64 = nullptr;         // FP64 tallies (n)
+    float* c32 = nullptr;          // forward: FP32 tally source (n)
+    double* c64 = nullptr;         // forward: FP64 tally source (n)
+    int* d_nh = nullptr;           // histories of the current solve
+    int* d_counter = nullptr;      // walk work-queue counter
+    double* d_scalars = nullptr;   // [0] |src|_1, [1] cdf total, [2] 1/nh ...
+    unsigned long long* d_steps = nullptr;  // walk steps (running total)
+    unsigned long long* d_tim = nullptr;    // FP32 walk timing (see walk.cu)
+    double* part = nullptr;        // reduction / scan partials
+    int* ipart = nullptr;
+    int part_cap = 0;
+    // MCSA buffers.
+    double* x = nullptr;
+    double* b = nullptr;
+    double* rp = nullptr;
+    double* tmp = nullptr;
+    double* tmp2 = nullptr;
+    mclsgpu::McsaState* d_state = nullptr;
+    mclsgpu::McsaState* h_state = nullptr;  // pinned
+    cudaGraphExec_t graph = nullptr;
+    int graph_key = -1;
+    int body_kernels = 0;          // kernel nodes in one MCSA iteration
+    unsigned long long* d_hist = nullptr;   // histories transported (total)
+    double* d_resid = nullptr;     // per-iteration |rp|_2 history
+    int resid_cap = 0;
+};
+
+namespace mclsgpu {
+
+// ---- helpers (context.cu) --------------------------------------------------
+int set_error(mclsgpu_context* ctx, int code, const char* fmt, ...);
+int cuda_fail(mclsgpu_context* ctx, cudaError_t e, const char* what);
+int check_device_status(mclsgpu_context* ctx);
+template <class T>
+inline cudaError_t dmalloc(T** p, size_t count) {
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T) + 16);
+}
+template <class T>
+inline void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// ---- sparse (sparse.cu) ----------------------------------------------------
+// Upload a host CSR (int64 indices) to a DevCsr (int32).  Validates.
+int upload_csr(mclsgpu_context* ctx, int64_t n, const int64_t* rp,
+               const int64_t* ci, const double* v, DevCsr& out);
+int csr_transpose(mclsgpu_context* ctx, const DevCsr& A, DevCsr& T);
+// C = A*B (accumulated over A's row entries in column order) then filtered
+// by `threshold` relative to the signed row max.
+int csr_multiply(mclsgpu_context* ctx, const DevCsr& A, const DevCsr& B,
+                 double threshold, DevCsr& C);
+int csr_copy(mclsgpu_context* ctx, const DevCsr& A, DevCsr& B);
+// Column scaling: T.v[k] *= s[T.ci[k]] (composite with a diagonal factor).
+void csr_scale_cols(mclsgpu_context* ctx, DevCsr& T, const double* s);
+int csr_filter(mclsgpu_context* ctx, const DevCsr& A, double threshold,
+               DevCsr& out);
+void spmv(cudaStream_t s, const DevCsr& A, const double* x, double* y);
+int reciprocal_diagonal(mclsgpu_context* ctx, const DevCsr& A, double* dinv);
+int block_jacobi(mclsgpu_context* ctx, const DevCsr& A, int bs, DevCsr& P);
+int point_jacobi_csr(mclsgpu_context* ctx, int n, const double* dinv,
+                     DevCsr& P);
+// Exclusive scan of set-up counts into rp[0..n]; *total = sum.
+int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int* d_rp,
+                              long long* total);
+// Domain arrays and FP32 records from the composite operator (domain.cu).
+int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
+                        mclsgpu_domain* dom);
+
+// ---- scans and reductions (scan.cu) ------------------------------------------
+int scan_partials_needed(int n);
+// Deterministic FP64 sum of |v[i]*scale| (scale applied when has_scale).
+void abs_sum(cudaStream_t s, const double* v, int n, double scale,
+             int has_scale, double* part, double* out);
+// Source CDF: c[0] = v[0]*sc, c[i] = c[i-1] + |v[i]*sc|, then c /= c[n-1];
+// writes total to *total.  sequential != 0 reproduces the reference's
+// left-to-right order in one thread.
+void source_cdf(cudaStream_t s, const double* v, int n, double scale,
+                int has_scale, int sequential, double* part, double* cdf,
+                double* total);
+// Exclusive suffix sum: out[i] = sum_{j>i} in[j]; *total = sum.
+void suffix_scan_int(cudaStream_t s, const int* in, int n, int* part,
+                     int* out, int* total);
+// Inclusive max-scan in place (guide table).
+void max_scan_int(cudaStream_t s, int* a, int n, int* part);
+// Sum of squares (deterministic).
+void sum_sq(cudaStream_t s, const double* v, int n, double* part,
+            double* out);
+
+}  // namespace mclsgpu

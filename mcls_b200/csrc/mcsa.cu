@@ -1,0 +1,586 @@
+// mcsa.cu -- Monte Carlo solve and the MCSA Richardson/correction loop.
+//
+// MC solve (MonteCarloSolverManager::solve + MCSolver::solve,
+// src/MCLS_MonteCarloSolverManager_impl.hpp:199-235, 346-380,
+// src/MCLS_MCSolver_impl.hpp:82-112): source from the (left preconditioned
+// unless internal, Neumann-relaxed) right-hand side, transport, normalise by
+// the number of histories, right-preconditioner recovery unless internal.
+//
+// Estimators.  Collision: x = y / Nh with y the collision tally.
+// Expected value (no counterpart in this reference snapshot): every step adds
+// w * h_{s,j} to x_j for all j of the current row; summed over a history
+// this equals H applied to the history's collision tally, so the kernel
+// computes x = b_src + (D^T y) / Nh with one gather over the transposed
+// domain instead of k scattered updates per step (forward: the tally source
+// is H b_src instead of b_src).
+//
+// MCSA (MCSASolverManager::solve, src/MCLS_MCSASolverManager_impl.hpp:
+// 278-432): each iteration runs Richardson smoothing (x += w rp, then
+// rp = PL(b - A PR x)), zeroes the correction, solves the residual problem by
+// MC (internal), adds the correction and recomputes the residual; the loop
+// stops when |rp|_2 <= tol * |PL b|_2 or the iteration limit is reached,
+// checked every "Iteration Check Frequency" iterations.  The whole loop is one
+// CUDA graph: a WHILE conditional node whose body is one iteration and whose
+// condition is set on the device by the convergence check, so a solve makes
+// no host round trip per iteration.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "internal.h"
+#include "rng.cuh"
+
+namespace mclsgpu {
+
+void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega);
+void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega);
+void launch_advance_walk_pos(mclsgpu_domain* dom);
+void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
+                 int* tr_ev, long long* tr_start);
+
+namespace {
+
+inline int grid_for(long long work, int threads = 256, int cap = 148 * 16) {
+    long long g = (work + threads - 1) / threads;
+    if (g < 1) g = 1;
+    return int(g > cap ? cap : g);
+}
+
+// rp = (b - A x) [* dinv]   (LinearProblem::updatePrecResidual, :410-442)
+__global__ void __launch_bounds__(256) k_residual(const int* rp, const int* ci, const double* v,
+                                                  int n, const double* x, const double* b,
+                                                  const double* dinv, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) s = fma(v[k], x[ci[k]], s);
+        double r = b[i] - s;
+        out[i] = dinv ? dinv[i] * r : r;
+    }
+}
+
+// x += w * r  (RichardsonIteration::doOneIteration, :134-147)
+__global__ void k_richardson(double* x, const double* r, int n, double w) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[i] = __dadd_rn(x[i], __dmul_rn(w, r[i]));
+}
+
+struct FinalizeArgs {
+    int n;
+    int mode;            // 0 adjoint collision, 1 adjoint EV, 2 forward
+    int ev;
+    int accumulate;      // 1: out += delta (MCSA), 0: out = delta
+    int fp32;
+    double per;          // forward histories per state
+    const double* sc;    // [2] = 1/nh
+    const double* src;   // MC source vector before scaling
+    double omega;
+    int has_omega;
+    const float* y32;
+    const double* y64;
+    const int* dtrp;
+    const int* dtci;
+    const float* dth32;
+    const double* dth64;
+    double* out;
+    const int* d_nh;
+    unsigned long long* d_hist;
+};
+
+__global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
+    const double inv = a.sc[2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double d;
+        const double srci = a.has_omega ? a.src[i] * a.omega : a.src[i];
+        if (a.mode == 0) {
+            // AdjointTally::normalize: x *= 1/nh  (src/MCLS_AdjointTally_impl.hpp:68-72)
+            const double y = a.fp32 ? double(a.y32[i]) : a.y64[i];
+            d = __dmul_rn(y, inv);
+        } else if (a.mode == 1) {
+            double t = 0.0;
+            if (a.fp32) {
+                for (int k = a.dtrp[i]; k < a.dtrp[i + 1]; ++k)
+                    t = fma(double(a.dth32[k]), double(a.y32[a.dtci[k]]), t);
+            } else {
+                for (int k = a.dtrp[i]; k < a.dtrp[i + 1]; ++k)
+                    t = fma(a.dth64[k], a.y64[a.dtci[k]], t);
+            }
+            d = __dadd_rn(__dmul_rn(t, inv), srci);
+        } else {
+            // ForwardTally::finalize: sum / count  (src/MCLS_ForwardTally_impl.hpp:194-208)
+            const double y = a.fp32 ? double(a.y32[i]) : a.y64[i];
+            d = __ddiv_rn(y, a.per);
+            if (a.ev) d = __dadd_rn(d, srci);
+        }
+        a.out[i] = a.accumulate ? __dadd_rn(a.out[i], d) : d;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.d_hist) *a.d_hist += (unsigned long long)(*a.d_nh);
+}
+
+__global__ void k_epoch_inc(unsigned long long* e) { *e += 1ULL; }
+
+// Convergence check of one MCSA iteration (src/MCLS_MCSASolverManager_impl.hpp:380-394).
+__global__ void k_mcsa_check(McsaState* st, const double* sumsq, double* hist, int hist_cap,
+                             const int* status, cudaGraphConditionalHandle handle) {
+    McsaState s = *st;
+    s.iter += 1;
+    s.rnorm = sqrt(*sumsq);
+    if (hist && s.iter <= hist_cap) hist[s.iter - 1] = s.rnorm;
+    int keep = 1;
+    if (s.iter % s.check_freq == 0) keep = (s.rnorm > s.crit) && (s.iter < s.max_iters);
+    if (*status) keep = 0;
+    s.done = !keep;
+    s.converged = s.rnorm <= s.crit;
+    *st = s;
+    cudaGraphSetConditional(handle, keep ? 1u : 0u);
+}
+
+__global__ void k_mcsa_init(McsaState* st, const double* src_sumsq, double tol, int check_freq,
+                            int max_iters, const double* r_sumsq) {
+    McsaState s{};
+    double sn = sqrt(*src_sumsq);
+    s.pad = 0;
+    // Homogeneous case (:312-316)
+    double crit_norm = fabs(sn) < 10.0 * 2.220446049250313e-16 ? 1.0 : sn;
+    s.crit = tol * crit_norm;
+    s.check_freq = check_freq > 0 ? check_freq : 1;
+    s.max_iters = max_iters;
+    s.iter = 0;
+    s.done = 0;
+    s.rnorm = sqrt(*r_sumsq);
+    s.converged = 0;
+    *st = s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// rp = PL (b - A PR x)
+static void update_prec_residual(mclsgpu_domain* dom, const double* x, const double* b,
+                                 double* rp_out) {
+    cudaStream_t s = dom->ctx->stream;
+    const mclsgpu::DevCsr& A = dom->op->A;
+    const double* xin = x;
+    if (dom->right) {
+        spmv(s, dom->right->P, x, dom->tmp2);
+        xin = dom->tmp2;
+    }
+    mclsgpu_precond* L = dom->left;
+    if (!L) {
+        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, xin, b,
+                                                              nullptr, rp_out);
+    } else if (L->kind == MCLSGPU_PREC_POINT_JACOBI) {
+        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, xin, b,
+                                                              L->diag, rp_out);
+    } else {
+        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, xin, b,
+                                                              nullptr, dom->tmp);
+        spmv(s, L->P, dom->tmp, rp_out);
+    }
+}
+
+// One MC solve of the source vector `v` (device, already left preconditioned
+// when required) into out (accumulate: out += delta).
+static void enqueue_mc(mclsgpu_domain* dom, const double* v, double* out, int accumulate,
+                       long long max_trace, long long* tr_states, double* tr_w, int* tr_ev,
+                       long long* tr_start) {
+    const mclsgpu_mc_params& p = dom->p;
+    const double omega = p.neumann_relaxation;
+    const int has_omega = p.neumann_relaxation > 0.0;
+    if (p.direction == MCLSGPU_ADJOINT)
+        launch_adjoint_source(dom, v, omega, has_omega);
+    else
+        launch_forward_source(dom, v, omega, has_omega);
+    launch_walk(dom, max_trace, tr_states, tr_w, tr_ev, tr_start);
+    launch_advance_walk_pos(dom);
+    FinalizeArgs f{};
+    f.n = dom->n;
+    f.mode = p.direction == MCLSGPU_FORWARD ? 2 : (p.estimator == MCLSGPU_EXPECTED_VALUE ? 1 : 0);
+    f.ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
+    f.accumulate = accumulate;
+    f.fp32 = p.precision == MCLSGPU_FP32;
+    f.per = p.sample_ratio > 0.0 ? std::ceil(p.sample_ratio) : 1.0;
+    f.sc = dom->d_scalars;
+    f.src = v;
+    f.omega = omega;
+    f.has_omega = has_omega;
+    f.y32 = dom->y32;
+    f.y64 = dom->y64;
+    f.dtrp = dom->DT.rp;
+    f.dtci = dom->DT.ci;
+    f.dth32 = dom->dt_h32;
+    f.dth64 = dom->DT.v;
+    f.out = out;
+    f.d_nh = dom->d_nh;
+    f.d_hist = dom->d_hist;
+    k_finalize<<<grid_for(dom->n, 256, 148 * 8), 256, 0, dom->ctx->stream>>>(f);
+    k_epoch_inc<<<1, 1, 0, dom->ctx->stream>>>(dom->d_epoch);
+}
+
+static int read_stats(mclsgpu_domain* dom, mclsgpu_stats* st) {
+    if (!st) return MCLSGPU_OK;
+    unsigned long long steps = 0, hist = 0, tim[4] = {0, 0, 0, 0};
+    cudaMemcpyAsync(&steps, dom->d_steps, sizeof(steps), cudaMemcpyDeviceToHost, dom->ctx->stream);
+    cudaMemcpyAsync(&hist, dom->d_hist, sizeof(hist), cudaMemcpyDeviceToHost, dom->ctx->stream);
+    cudaMemcpyAsync(tim, dom->d_tim, sizeof(tim), cudaMemcpyDeviceToHost, dom->ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(dom->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "stats");
+    st->walk_steps = (int64_t)steps;
+    st->histories = (int64_t)hist;
+    st->walk_ms = double(tim[2]) * 1e-6;
+    st->walk_launches = (int64_t)tim[3];
+    return MCLSGPU_OK;
+}
+
+static void reset_counters(mclsgpu_domain* dom) {
+    cudaStream_t s = dom->ctx->stream;
+    cudaMemsetAsync(dom->d_steps, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(dom->d_hist, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(dom->d_tim + 2, 0, 2 * sizeof(unsigned long long), s);
+}
+
+// MC solve with device vectors.
+static int mc_solve_device(mclsgpu_domain* dom, const double* rhs_dev, double* x_dev, int internal,
+                           long long max_trace, long long* tr_states, double* tr_w, int* tr_ev,
+                           long long* tr_start, mclsgpu_stats* stats) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    reset_counters(dom);
+    const double* v = rhs_dev;
+    if (dom->left && !internal) {
+        spmv(s, dom->left->P, rhs_dev, dom->tmp);
+        v = dom->tmp;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    if (dom->right && !internal) {
+        // v is rhs_dev or tmp, so tmp2 is free for the unrecovered result.
+        enqueue_mc(dom, v, dom->tmp2, 0, max_trace, tr_states, tr_w, tr_ev, tr_start);
+        spmv(s, dom->right->P, dom->tmp2, x_dev);
+    } else {
+        enqueue_mc(dom, v, x_dev, 0, max_trace, tr_states, tr_w, tr_ev, tr_start);
+    }
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mc solve");
+    int rc = check_device_status(ctx);
+    if (rc) return rc;
+    if (stats) {
+        if ((rc = read_stats(dom, stats))) return rc;
+        stats->solve_ms = ms;
+        stats->iterations = 0;
+        stats->converged = 1;
+    }
+    return MCLSGPU_OK;
+}
+
+// Build the CUDA graph of the MCSA loop (WHILE node, one iteration per body).
+static int build_mcsa_graph(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    if (dom->graph) {
+        cudaGraphExecDestroy(dom->graph);
+        dom->graph = nullptr;
+    }
+    cudaGraph_t g;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphCreate");
+    cudaGraphConditionalHandle handle;
+    e = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(ctx, e, "cudaGraphConditionalHandleCreate");
+    }
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(ctx, e, "cudaGraphAddNode(conditional)");
+    }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(ctx, e, "cudaStreamBeginCaptureToGraph");
+    }
+    const int n = dom->n;
+    for (int l = 0; l < mp->smoother_steps; ++l) {
+        k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, n,
+                                                              mp->richardson_omega);
+        update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    }
+    enqueue_mc(dom, dom->rp, dom->x, 1, 0, nullptr, nullptr, nullptr, nullptr);
+    update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    k_mcsa_check<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid, dom->resid_cap,
+                                 ctx->d_status, handle);
+    cudaGraph_t captured = body;
+    e = cudaStreamEndCapture(s, &captured);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(ctx, e, "cudaStreamEndCapture");
+    }
+    size_t nn = 0;
+    cudaGraphGetNodes(body, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) cudaGraphGetNodes(body, nodes.data(), &nn);
+    dom->body_kernels = 0;
+    for (size_t k = 0; k < nn; ++k) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+            ++dom->body_kernels;
+    }
+    e = cudaGraphInstantiate(&dom->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        dom->graph = nullptr;
+        return cuda_fail(ctx, e, "cudaGraphInstantiate");
+    }
+    return MCLSGPU_OK;
+}
+
+static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
+                             const mclsgpu_mcsa_params* mp, mclsgpu_stats* stats) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    reset_counters(dom);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    if (mp->max_iters > dom->resid_cap) {
+        dfree(dom->d_resid);
+        cudaError_t e = dmalloc(&dom->d_resid, size_t(mp->max_iters));
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return cuda_fail(ctx, e, "cudaMalloc");
+        }
+        dom->resid_cap = mp->max_iters;
+        if (dom->graph) {
+            cudaGraphExecDestroy(dom->graph);
+            dom->graph = nullptr;
+        }
+    }
+    // Graph key: everything baked into the captured iteration.
+    const int key = mp->smoother_steps * 1000003 ^ int(mp->richardson_omega * 1e6);
+    if (!dom->graph || dom->graph_key != key) {
+        int rc = build_mcsa_graph(dom, mp);
+        if (rc) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
+        dom->graph_key = key;
+    }
+    cudaEventRecord(e0, s);
+    if (b_dev != dom->b)
+        cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (x_dev != dom->x)
+        cudaMemcpyAsync(dom->x, x_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    // Source norm |PL b|_2 (:299-318) and the initial preconditioned residual.
+    const double* pb = dom->b;
+    if (dom->left) {
+        spmv(s, dom->left->P, dom->b, dom->tmp);
+        pb = dom->tmp;
+    }
+    sum_sq(s, pb, n, dom->part, dom->d_scalars + 6);
+    update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    k_mcsa_init<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 6, mp->tolerance, mp->check_freq,
+                                mp->max_iters, dom->d_scalars + 5);
+    cudaError_t e = cudaGraphLaunch(dom->graph, s);
+    cudaEventRecord(e1, s);
+    if (e == cudaSuccess) {
+        // Right preconditioner recovery (:410-418).
+        if (dom->right) {
+            spmv(s, dom->right->P, dom->x, dom->tmp);
+            cudaMemcpyAsync(x_dev, dom->tmp, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        } else if (x_dev != dom->x) {
+            cudaMemcpyAsync(x_dev, dom->x, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        }
+        cudaMemcpyAsync(dom->h_state, dom->d_state, sizeof(McsaState), cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mcsa graph");
+    int rc = check_device_status(ctx);
+    if (rc) return rc;
+    double src_sumsq = 0.0;
+    cudaMemcpy(&src_sumsq, dom->d_scalars + 6, sizeof(double), cudaMemcpyDeviceToHost);
+    const McsaState st = *dom->h_state;
+    if (mp->verbose) {
+        std::vector<double> hist(st.iter < dom->resid_cap ? st.iter : dom->resid_cap);
+        if (!hist.empty())
+            cudaMemcpy(hist.data(), dom->d_resid, hist.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        const double sn = std::sqrt(src_sumsq) > 0.0 ? std::sqrt(src_sumsq) : 1.0;
+        std::printf("\n**************************************************\n");
+        std::printf("*       MCLS: Monte Carlo Linear Solvers         *\n");
+        std::printf("**************************************************\n\n");
+        std::printf("                     MCSA                         \n\n");
+        std::printf("%18s%18s\n", "Iteration", "|r|_2 / |b|_2");
+        const int pf = mp->print_freq > 0 ? mp->print_freq : 10;
+        for (int i = 0; i < (int)hist.size(); ++i)
+            if ((i + 1) % pf == 0 || i + 1 == st.iter)
+                std::printf("%18d%18.4e\n", i + 1, hist[i] / sn);
+        std::printf("\n**************************************************\n\n");
+    }
+    if (stats) {
+        if ((rc = read_stats(dom, stats))) return rc;
+        stats->iterations = st.iter;
+        stats->converged = st.converged;
+        stats->residual_norm = st.rnorm;
+        const double sn = std::sqrt(src_sumsq);
+        stats->achieved_tol = sn > 0.0 ? st.rnorm / sn : st.rnorm;  // achievedTol (:142-173)
+        stats->solve_ms = ms;
+        stats->fallback_taken = dom->left ? dom->left->fallback : 0;
+        // kernels of the captured iterations plus the set-up launches
+        // (source norm, initial residual and norm, state init)
+        stats->kernel_launches = int64_t(dom->body_kernels) * st.iter + 9;
+        stats->rho = dom->left ? dom->left->rho : -1.0;
+    }
+    return MCLSGPU_OK;
+}
+
+}  // namespace mclsgpu
+
+using namespace mclsgpu;
+
+static int check_mcsa_params(mclsgpu_domain* dom, const mclsgpu_mcsa_params* p,
+                             mclsgpu_mcsa_params* out) {
+    mclsgpu_mcsa_params d{};
+    d.size = sizeof(d);
+    d.max_iters = 1000;
+    d.tolerance = 1.0;
+    d.check_freq = 1;
+    d.smoother_steps = 1;
+    d.richardson_omega = 1.0;
+    d.print_freq = 10;
+    if (p) {
+        if (p->size < sizeof(mclsgpu_mcsa_params))
+            return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG, "mcsa params: size mismatch");
+        d = *p;
+    }
+    if (d.max_iters < 1 || d.check_freq < 1 || d.smoother_steps < 0 || !(d.tolerance >= 0.0))
+        return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG, "mcsa params out of range");
+    *out = d;
+    return MCLSGPU_OK;
+}
+
+extern "C" {
+
+int mclsgpu_mc_solve_dev(mclsgpu_domain* dom, const double* rhs_dev, double* x_dev, int internal,
+                         mclsgpu_stats* stats) {
+    if (!dom || !rhs_dev || !x_dev) return MCLSGPU_ERR_INVALID_ARG;
+    return mc_solve_device(dom, rhs_dev, x_dev, internal, 0, nullptr, nullptr, nullptr, nullptr,
+                           stats);
+}
+
+int mclsgpu_mc_solve(mclsgpu_domain* dom, const double* rhs, double* x, int internal,
+                     mclsgpu_stats* stats) {
+    if (!dom || !rhs || !x) return MCLSGPU_ERR_INVALID_ARG;
+    cudaStream_t s = dom->ctx->stream;
+    const size_t bytes = size_t(dom->n) * sizeof(double);
+    cudaMemcpyAsync(dom->b, rhs, bytes, cudaMemcpyHostToDevice, s);
+    int rc = mc_solve_device(dom, dom->b, dom->x, internal, 0, nullptr, nullptr, nullptr, nullptr,
+                             stats);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(x, dom->x, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(dom->ctx, e, "mc_solve copy-out");
+}
+
+int mclsgpu_mc_trace(mclsgpu_domain* dom, const double* rhs, double* x, int internal,
+                     int64_t max_trace, int64_t* states, double* final_weight, int32_t* events,
+                     int64_t* start_state, int64_t* num_histories) {
+    if (!dom || !rhs || !x || max_trace < 0) return MCLSGPU_ERR_INVALID_ARG;
+    if (dom->p.precision != MCLSGPU_FP64)
+        return set_error(dom->ctx, MCLSGPU_ERR_UNSUPPORTED, "trace needs the FP64 walk");
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int L = dom->p.history_length;
+    const size_t bytes = size_t(dom->n) * sizeof(double);
+    long long *d_states = nullptr, *d_start = nullptr;
+    double* d_w = nullptr;
+    int* d_ev = nullptr;
+    cudaError_t e;
+    if (max_trace > 0) {
+        if ((e = dmalloc(&d_states, size_t(max_trace) * (L + 1))) != cudaSuccess ||
+            (e = dmalloc(&d_start, size_t(max_trace))) != cudaSuccess ||
+            (e = dmalloc(&d_w, size_t(max_trace))) != cudaSuccess ||
+            (e = dmalloc(&d_ev, size_t(max_trace))) != cudaSuccess) {
+            dfree(d_states); dfree(d_start); dfree(d_w); dfree(d_ev);
+            return cuda_fail(ctx, e, "cudaMalloc trace");
+        }
+    }
+    cudaMemcpyAsync(dom->b, rhs, bytes, cudaMemcpyHostToDevice, s);
+    int rc = mc_solve_device(dom, dom->b, dom->x, internal, max_trace, d_states, d_w, d_ev, d_start,
+                             nullptr);
+    if (!rc) {
+        int nh = 0;
+        cudaMemcpyAsync(&nh, dom->d_nh, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(x, dom->x, bytes, cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "trace copy-out");
+        if (!rc) {
+            long long k = nh < max_trace ? nh : max_trace;
+            if (num_histories) *num_histories = nh;
+            if (k > 0) {
+                if (states)
+                    cudaMemcpy(states, d_states, size_t(k) * (L + 1) * sizeof(long long),
+                               cudaMemcpyDeviceToHost);
+                if (start_state)
+                    cudaMemcpy(start_state, d_start, size_t(k) * sizeof(long long),
+                               cudaMemcpyDeviceToHost);
+                if (final_weight)
+                    cudaMemcpy(final_weight, d_w, size_t(k) * sizeof(double), cudaMemcpyDeviceToHost);
+                if (events) cudaMemcpy(events, d_ev, size_t(k) * sizeof(int), cudaMemcpyDeviceToHost);
+            }
+        }
+    }
+    dfree(d_states); dfree(d_start); dfree(d_w); dfree(d_ev);
+    return rc;
+}
+
+int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
+                           const mclsgpu_mcsa_params* params, mclsgpu_stats* stats) {
+    if (!dom || !b_dev || !x_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_mcsa_params p;
+    int rc = check_mcsa_params(dom, params, &p);
+    if (rc) return rc;
+    return mcsa_solve_device(dom, b_dev, x_dev, &p, stats);
+}
+
+int mclsgpu_mcsa_solve(mclsgpu_domain* dom, const double* b, double* x,
+                       const mclsgpu_mcsa_params* params, mclsgpu_stats* stats) {
+    if (!dom || !b || !x) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_mcsa_params p;
+    int rc = check_mcsa_params(dom, params, &p);
+    if (rc) return rc;
+    cudaStream_t s = dom->ctx->stream;
+    const size_t bytes = size_t(dom->n) * sizeof(double);
+    cudaMemcpyAsync(dom->b, b, bytes, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dom->x, x, bytes, cudaMemcpyHostToDevice, s);
+    rc = mcsa_solve_device(dom, dom->b, dom->x, &p, stats);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(x, dom->x, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(dom->ctx, e, "mcsa copy-out");
+}
+
+}  // extern "C"

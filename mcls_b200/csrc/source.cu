@@ -1,0 +1,262 @@
+// source.cu -- device build of the Monte Carlo source.
+//
+// Adjoint (UniformAdjointSource, src/MCLS_UniformAdjointSource_impl.hpp:58-263):
+//   weight = |b|_1; random sampling draws nh = int(Nh * cdf.back() / |b|_1)
+//   starting states from the CDF of |b| (whose first element is the signed
+//   b[0], :185) with lower_bound; stratified sampling takes
+//   ceil(|b_i| * nh_local / sum|b|) histories per state.  Histories are
+//   emitted from the highest state down (the LIFO stack of :157-175); the
+//   emission order fixes which uniforms each history consumes in the
+//   reference stream.
+// Forward (UniformForwardSource, src/MCLS_UniformForwardSource_impl.hpp:60-148):
+//   ceil(Sample Ratio) histories per state in state order, weight 1.
+//
+// Sampling uses a guide table over the FP64 CDF: guide[t] is the first state
+// whose floor(cdf*G) reaches t, so the lower_bound of u lies in
+// [guide[t], guide[t+1]] with t = floor(u*G); a short binary search in that
+// window returns exactly std::lower_bound's answer.
+#include <cfloat>
+#include <climits>
+
+#include "internal.h"
+#include "rng.cuh"
+
+namespace mclsgpu {
+namespace {
+
+inline int grid_for(long long work, int threads = 256, int cap = 148 * 16) {
+    long long g = (work + threads - 1) / threads;
+    if (g < 1) g = 1;
+    return int(g > cap ? cap : g);
+}
+
+__device__ __forceinline__ double load_src(const double* v, int i, double omega, int has) {
+    return has ? v[i] * omega : v[i];
+}
+
+// nh = int(Nh_total * cdf.back() / norm1)  (:198); weight = norm1 (:67)
+__global__ void k_random_count(int nh_req, double* sc, int* d_nh, int cap, int* status) {
+    const double norm1 = sc[0], total = sc[1];
+    const double r = __ddiv_rn(__dmul_rn(double(nh_req), total), norm1);
+    int nh = (r >= 0.0 && r < 2147483647.0) ? int(r) : (r >= 2147483647.0 ? INT_MAX : 0);
+    if (!(norm1 > 0.0) || !isfinite(norm1)) {
+        nh = 0;
+        atomicOr(status, DEV_ERR_NONFINITE);
+    }
+    if (nh > cap) {
+        atomicOr(status, DEV_ERR_CAPACITY);
+        nh = cap;
+    }
+    *d_nh = nh;
+    sc[2] = nh > 0 ? 1.0 / double(nh) : 0.0;
+}
+
+__global__ void k_guide_marks(const double* cdf, int n, int* marks) {
+    // marks[t] = max j whose window starts at t = floor(cdf[j-1]*G)+1.
+    const double G = double(n);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        long long t0 = 0;
+        if (j > 0) {
+            double f = floor(cdf[j - 1] * G);
+            t0 = f < -1.0 ? 0 : (long long)f + 1;
+        }
+        if (t0 < 0) t0 = 0;
+        if (t0 <= n - 1) atomicMax(&marks[t0], j);
+    }
+}
+
+__device__ __forceinline__ int guided_lower_bound(const double* cdf, const int* guide, int n,
+                                                  double u) {
+    long long t = (long long)floor(u * double(n));
+    if (t < 0) t = 0;
+    if (t > n - 1) t = n - 1;
+    int lo = guide[t];
+    int hi = t + 1 < n ? guide[t + 1] : n - 1;
+    if (lo < 0) lo = 0;
+    if (hi < lo) hi = lo;
+    // first j in [lo, hi] with cdf[j] >= u (cdf[hi] >= u by construction)
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (cdf[mid] < u) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Random sampling: draw k in [0, nh) -> counts[lower_bound(cdf, u_k)]++.
+// Reference stream: each thread owns a contiguous run of draws and jumps once.
+__global__ void k_sample(const double* cdf, const int* guide, int n, const int* d_nh,
+                         int rng_mode, uint64_t seed, const unsigned long long* d_epoch,
+                         const uint64_t* jump, const unsigned long long* d_pos, int* counts) {
+    const int nh = *d_nh;
+    const uint64_t ekey = epoch_key(seed, *d_epoch);
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthreads = gridDim.x * blockDim.x;
+    if (rng_mode == MCLSGPU_RNG_COUNTER) {
+        for (int k = tid; k < nh; k += nthreads) {
+            uint64_t x = xs_step(counter_state(ekey, 1, uint64_t(k)));
+            int j = guided_lower_bound(cdf, guide, n, canonical64(x));
+            atomicAdd(&counts[j], 1);
+        }
+    } else {
+        const int per = (nh + nthreads - 1) / nthreads;
+        const long long k0 = (long long)tid * per;
+        if (k0 >= nh) return;
+        const long long k1 = k0 + per < nh ? k0 + per : nh;
+        uint64_t x = xs_jump(jump, seed, *d_pos + uint64_t(k0));
+        for (long long k = k0; k < k1; ++k) {
+            x = xs_step(x);
+            int j = guided_lower_bound(cdf, guide, n, canonical64(x));
+            atomicAdd(&counts[j], 1);
+        }
+    }
+}
+
+__global__ void k_advance_pos(unsigned long long* d_pos, const int* d_nh, int mult) {
+    *d_pos += (unsigned long long)(*d_nh) * (unsigned long long)mult;
+}
+
+// Stratified: nh_local = ceil(Nh * local_sum / weight) (:241);
+// counts_i = ceil(|b_i| * (nh_local / local_sum)) (:246-262).
+__global__ void k_strat_prep(int nh_req, double* sc) {
+    const double s = sc[0];
+    const double nh_local = ceil(__ddiv_rn(__dmul_rn(double(nh_req), s), s));
+    sc[3] = __ddiv_rn(double(int(nh_local)), s);
+}
+
+__global__ void k_strat_counts(const double* v, int n, double omega, int has, const double* sc,
+                               int* counts) {
+    const double num_over_sum = sc[3];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double c = ceil(__dmul_rn(fabs(load_src(v, i, omega, has)), num_over_sum));
+        counts[i] = c > 0.0 ? int(c) : 0;
+    }
+}
+
+__global__ void k_strat_total(int* d_nh, double* sc, int cap, int* status) {
+    int nh = *d_nh;
+    if (nh > cap) {
+        atomicOr(status, DEV_ERR_CAPACITY);
+        nh = cap;
+        *d_nh = nh;
+    }
+    sc[2] = nh > 0 ? 1.0 / double(nh) : 0.0;
+}
+
+// Emission order and step-0 collision tally: start[offs_i + t] = i | sign,
+// y_i = counts_i * w0_i (the tally every history makes at its first state).
+template <class TY>
+__global__ void k_expand(const double* v, int n, double omega, int has, const int* counts,
+                         const int* offs, const double* sc, int cap, int* start, TY* y,
+                         int* status) {
+    const double weight = sc[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = counts[i];
+        const double b = load_src(v, i, omega, has);
+        const unsigned sign = b > 0.0 ? 0u : 0x80000000u;  // weight_sign (:169)
+        if (c > 0) {
+            const int base = offs[i];
+            if (base + c > cap) {
+                atomicOr(status, DEV_ERR_CAPACITY);
+            } else {
+                for (int t = 0; t < c; ++t) start[base + t] = int(unsigned(i) | sign);
+            }
+            const double w0 = sign ? -weight : weight;
+            y[i] = TY(double(c) * w0);
+        } else {
+            y[i] = TY(0);
+        }
+    }
+}
+
+// Forward tally source: c = src (collision) or H src (expected value).
+template <class TC>
+__global__ void k_forward_c(const double* v, int n, double omega, int has, int ev, const int* rp,
+                            const int* ci, const double* h, TC* c) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s;
+        if (!ev) {
+            s = load_src(v, i, omega, has);
+        } else {
+            s = 0.0;
+            for (int k = rp[i]; k < rp[i + 1]; ++k)
+                s = fma(h[k], load_src(v, ci[k], omega, has), s);
+        }
+        c[i] = TC(s);
+    }
+}
+
+__global__ void k_forward_nh(int* d_nh, int nh, double* sc) {
+    *d_nh = nh;
+    sc[0] = 1.0;
+    sc[2] = 1.0 / double(nh);
+}
+
+}  // namespace
+
+// Build the adjoint source from v*omega (omega applied when has_omega).
+void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    const mclsgpu_mc_params& p = dom->p;
+    const bool parity = p.precision == MCLSGPU_FP64 && p.rng_mode == MCLSGPU_RNG_REFERENCE;
+    const int nh_req = p.sample_ratio > 0.0 ? int(double(n) * p.sample_ratio) : n;
+    const int cap = int(dom->nh_cap);
+    // weight = |b|_1
+    abs_sum(s, v, n, omega, has_omega, parity ? nullptr : dom->part, dom->d_scalars + 0);
+    cudaMemsetAsync(dom->counts, 0, size_t(n) * sizeof(int), s);
+    if (p.source_sampling == MCLSGPU_SOURCE_RANDOM) {
+        source_cdf(s, v, n, omega, has_omega, parity ? 1 : 0, dom->part, dom->scdf,
+                   dom->d_scalars + 1);
+        k_random_count<<<1, 1, 0, s>>>(nh_req, dom->d_scalars, dom->d_nh, cap, ctx->d_status);
+        cudaMemsetAsync(dom->guide, 0xFF, size_t(n) * sizeof(int), s);
+        k_guide_marks<<<grid_for(n), 256, 0, s>>>(dom->scdf, n, dom->guide);
+        max_scan_int(s, dom->guide, n, dom->ipart);
+        const int sample_grid = p.rng_mode == MCLSGPU_RNG_COUNTER ? ctx->num_sms * 8 : 64;
+        k_sample<<<sample_grid, 256, 0, s>>>(dom->scdf, dom->guide, n, dom->d_nh, p.rng_mode,
+                                             dom->seed, dom->d_epoch, dom->d_jump, dom->d_pos,
+                                             dom->counts);
+        if (p.rng_mode == MCLSGPU_RNG_REFERENCE) k_advance_pos<<<1, 1, 0, s>>>(dom->d_pos, dom->d_nh, 1);
+        suffix_scan_int(s, dom->counts, n, dom->ipart, dom->offs, nullptr);
+    } else {
+        k_strat_prep<<<1, 1, 0, s>>>(nh_req, dom->d_scalars);
+        k_strat_counts<<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, dom->d_scalars,
+                                                   dom->counts);
+        suffix_scan_int(s, dom->counts, n, dom->ipart, dom->offs, dom->d_nh);
+        k_strat_total<<<1, 1, 0, s>>>(dom->d_nh, dom->d_scalars, cap, ctx->d_status);
+    }
+    if (p.precision == MCLSGPU_FP32)
+        k_expand<float><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, dom->counts, dom->offs,
+                                                    dom->d_scalars, cap, dom->start, dom->y32,
+                                                    ctx->d_status);
+    else
+        k_expand<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, dom->counts,
+                                                     dom->offs, dom->d_scalars, cap, dom->start,
+                                                     dom->y64, ctx->d_status);
+}
+
+void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    const mclsgpu_mc_params& p = dom->p;
+    const int per = p.sample_ratio > 0.0 ? int(ceil(p.sample_ratio)) : 1;
+    const int ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
+    k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
+    if (p.precision == MCLSGPU_FP32) {
+        k_forward_c<float><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
+                                                       dom->D.ci, dom->D.v, dom->c32);
+        cudaMemsetAsync(dom->y32, 0, size_t(n) * sizeof(float), s);
+    } else {
+        k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
+                                                        dom->D.ci, dom->D.v, dom->c64);
+        cudaMemsetAsync(dom->y64, 0, size_t(n) * sizeof(double), s);
+    }
+}
+
+void launch_advance_walk_pos(mclsgpu_domain* dom) {
+    if (dom->p.rng_mode == MCLSGPU_RNG_REFERENCE)
+        k_advance_pos<<<1, 1, 0, dom->ctx->stream>>>(dom->d_pos, dom->d_nh, dom->p.history_length);
+}
+
+}  // namespace mclsgpu

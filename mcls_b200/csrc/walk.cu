@@ -1,0 +1,348 @@
+// walk.cu -- Neumann-Ulam random-walk kernels.
+//
+// One history restates DomainTransporter::transport
+// (src/MCLS_DomainTransporter_impl.hpp:70-119): tally at the pre-transition
+// state, then AlmostOptimalDomain::processTransition
+// (src/MCLS_AlmostOptimalDomain.hpp:254-284): u ~ U[0,1),
+// j = lower_bound(cdf_row, u), state <- col_j, w *= W_row * sign(h_j), and
+// termination once the history has taken "History Length" steps
+// (:135-136) or, with the legacy "Weight Cutoff", once |w| < cutoff * |w0|.
+//
+// walk32: the production kernel.  Persistent warps pull histories from a
+// work-queue counter and refill lanes as histories terminate.  A step reads
+// one packed FP32 record (slots * 8 bytes, 16-byte vector loads), selects the
+// first entry whose CDF value is >= u with predicated compares (the records'
+// padding entries hold 2.0 and are never selected), and adds the collision
+// tally with a fire-and-forget FP32 reduction.  The adjoint step-0 tally is
+// made by the source build (counts * w0), so walks tally from step 1.
+//
+// walk64: the parity kernel.  FP64 CSR domain, binary search with
+// std::lower_bound semantics, FP64 weights and tallies, optional trajectory
+// trace.  With the reference stream it reproduces the reference's
+// trajectories bit for bit.
+#include <climits>
+
+#include "internal.h"
+#include "rng.cuh"
+
+namespace mclsgpu {
+
+struct WalkArgs {
+    int n;
+    int L;
+    int per;                    // forward: histories per state
+    int rng_mode;
+    const int* d_nh;
+    int* d_counter;
+    const int* start;           // adjoint: state | sign<<31
+    const double* sc;           // [0] weight
+    float cutoff;               // relative weight cutoff (0 = off)
+    double cutoff64;
+    uint64_t seed;
+    const unsigned long long* d_epoch;
+    const uint64_t* jump;
+    const unsigned long long* d_pos;
+    // FP32 records
+    const uint2* rec;
+    // FP64 domain
+    const int* rp;
+    const int* col;
+    const double* h;
+    const double* cdf;
+    const double* W;
+    // tallies
+    float* y32;
+    double* y64;
+    const float* c32;
+    const double* c64;
+    unsigned long long* d_steps;
+    unsigned long long* d_tim;  // [0] first warp start, [1] last warp end (ns)
+    int* status;
+    // trace (FP64 only)
+    long long max_trace;
+    long long* tr_states;
+    double* tr_w;
+    int* tr_ev;
+    long long* tr_start;
+};
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint64_t history_state(const WalkArgs& a, uint64_t ekey, long long e) {
+    if (a.rng_mode == MCLSGPU_RNG_COUNTER) return counter_state(ekey, 2, uint64_t(e));
+    return xs_jump(a.jump, a.seed, *a.d_pos + uint64_t(e) * uint64_t(a.L));
+}
+
+template <int S, int DIR>
+__global__ void __launch_bounds__(256) walk32(WalkArgs a) {
+    static_assert(S % 2 == 0, "records are whole 16-byte vectors");
+    const int lane = threadIdx.x & 31;
+    const int nh = *a.d_nh;
+    const float wnorm = float(a.sc[0]);
+    const uint64_t ekey = epoch_key(a.seed, *a.d_epoch);
+    const uint4* __restrict__ rec = reinterpret_cast<const uint4*>(a.rec);
+    if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
+    int s = 0, s0 = 0, k = 0;
+    float w = 0.f, wcut = 0.f, acc = 0.f;
+    uint64_t x = 0;
+    bool alive = false, drained = false;
+    unsigned long long steps = 0;
+    while (true) {
+        const unsigned need = __ballot_sync(kFull, !alive);
+        if (need && !drained) {
+            const int leader = __ffs(need) - 1;
+            const int cnt = __popc(need);
+            int base = 0;
+            if (lane == leader) base = atomicAdd(a.d_counter, cnt);
+            base = __shfl_sync(kFull, base, leader);
+            if (base + cnt >= nh) drained = true;
+            if (!alive) {
+                const int e = base + __popc(need & ((1u << lane) - 1));
+                if (e < nh) {
+                    if (DIR == MCLSGPU_ADJOINT) {
+                        const int sv = a.start[e];
+                        s = sv & 0x7fffffff;
+                        w = sv < 0 ? -wnorm : wnorm;
+                    } else {
+                        s = e / a.per;
+                        w = 1.f;
+                        acc = 0.f;
+                    }
+                    s0 = s;
+                    wcut = a.cutoff * fabsf(w);
+                    x = history_state(a, ekey, e);
+                    k = 0;
+                    alive = true;
+                }
+            }
+        }
+        if (!__any_sync(kFull, alive)) break;
+        if (alive) {
+            // Tally at the pre-transition state.
+            if (DIR == MCLSGPU_ADJOINT) {
+                if (k > 0) atomicAdd(&a.y32[s], w);
+            } else {
+                acc = fmaf(w, __ldg(&a.c32[s]), acc);
+            }
+            // Transition: one packed record.
+            const uint4* r = rec + size_t(s) * (S / 2);
+            uint4 q[S / 2];
+#pragma unroll
+            for (int t = 0; t < S / 2; ++t) q[t] = __ldg(r + t);
+            x = xs_step(x);
+            const float u = canonical32(x);
+            unsigned sel = q[0].w;  // slot 1 (first entry)
+            bool found = __uint_as_float(q[0].z) >= u;
+#pragma unroll
+            for (int t = 1; t < S / 2; ++t) {
+                const bool c0 = !found && __uint_as_float(q[t].x) >= u;
+                sel = c0 ? q[t].y : sel;
+                found = found || c0;
+                const bool c1 = !found && __uint_as_float(q[t].z) >= u;
+                sel = c1 ? q[t].w : sel;
+                found = found || c1;
+            }
+            const float Wt = __uint_as_float(q[0].x);
+            w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
+            s = int(sel & 0x7fffffffu);
+            ++k;
+            ++steps;
+            if (k >= a.L || fabsf(w) < wcut) {
+                alive = false;
+                if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y32[s0], acc);
+            }
+        }
+    }
+    // Step count: one reduction per warp.
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) steps += __shfl_down_sync(kFull, steps, d);
+    if (lane == 0) {
+        if (steps) atomicAdd(a.d_steps, steps);
+        atomicMax(&a.d_tim[1], global_ns());
+    }
+}
+
+// Device-side duration of the last walk launch (first warp start to last warp
+// end), accumulated into d_tim[2] with the launch count in d_tim[3].
+__global__ void k_walk_time_acc(unsigned long long* t) {
+    if (t[1] > t[0]) t[2] += t[1] - t[0];
+    t[3] += 1;
+    t[0] = ~0ULL;
+    t[1] = 0;
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(128) walk64(WalkArgs a) {
+    const int nh = *a.d_nh;
+    const double weight = a.sc[0];
+    const int L = a.L;
+    const uint64_t ekey = epoch_key(a.seed, *a.d_epoch);
+    unsigned long long steps = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nh;
+         e += (long long)gridDim.x * blockDim.x) {
+        int s;
+        double w;
+        if (DIR == MCLSGPU_ADJOINT) {
+            const int sv = a.start[e];
+            s = sv & 0x7fffffff;
+            w = sv < 0 ? -weight : weight;
+        } else {
+            s = int(e / a.per);
+            w = 1.0;
+        }
+        const int s0 = s;
+        const double wcut = a.cutoff64 * fabs(w);
+        uint64_t x = history_state(a, ekey, e);
+        double acc = 0.0;
+        const bool tr = a.tr_states && e < a.max_trace;
+        if (tr) {
+            for (int t = 0; t <= L; ++t) a.tr_states[e * (L + 1) + t] = -1;
+            a.tr_states[e * (L + 1)] = s;
+        }
+        int k = 0;
+        while (true) {
+            if (DIR == MCLSGPU_ADJOINT) {
+                if (k > 0) atomicAdd(&a.y64[s], w);
+            } else {
+                acc = __dadd_rn(acc, __dmul_rn(w, a.c64[s]));
+            }
+            x = xs_step(x);
+            const double u = canonical64(x);
+            const int r0 = a.rp[s], len = a.rp[s + 1] - r0;
+            int lo = 0, hi = len;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (a.cdf[r0 + mid] < u) lo = mid + 1; else hi = mid;
+            }
+            if (lo >= len) {
+                atomicOr(a.status, DEV_ERR_BOUNDS);
+                lo = len - 1;
+            }
+            const double Ws = a.h[r0 + lo] > 0.0 ? a.W[s] : -a.W[s];
+            w = __dmul_rn(w, Ws);
+            s = a.col[r0 + lo];
+            ++k;
+            ++steps;
+            if (tr) a.tr_states[e * (L + 1) + k] = s;
+            if (k >= L || fabs(w) < wcut) break;
+        }
+        if (!isfinite(w)) atomicOr(a.status, DEV_ERR_NONFINITE);
+        if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y64[s0], acc);
+        if (e < a.max_trace) {
+            if (a.tr_w) a.tr_w[e] = w;
+            if (a.tr_ev) a.tr_ev[e] = 2;  // Event::CUTOFF
+            if (a.tr_start) a.tr_start[e] = s0;
+        }
+    }
+    atomicAdd(a.d_steps, steps);
+}
+
+template <int S, int DIR>
+int blocks_per_sm() {
+    static int cached = 0;
+    if (!cached) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR>, 256, 0);
+        cached = b > 0 ? b : 1;
+    }
+    return cached;
+}
+
+template <int S, int DIR>
+void launch32(const WalkArgs& a, int sms, cudaStream_t st) {
+    walk32<S, DIR><<<sms * blocks_per_sm<S, DIR>(), 256, 0, st>>>(a);
+}
+
+template <int DIR>
+void launch32_slots(int slots, const WalkArgs& a, int sms, cudaStream_t st) {
+    switch (slots) {
+        case 4: launch32<4, DIR>(a, sms, st); break;
+        case 8: launch32<8, DIR>(a, sms, st); break;
+        case 12: launch32<12, DIR>(a, sms, st); break;
+        case 16: launch32<16, DIR>(a, sms, st); break;
+        case 24: launch32<24, DIR>(a, sms, st); break;
+        default: launch32<32, DIR>(a, sms, st); break;
+    }
+}
+
+}  // namespace
+
+// Cache the occupancy of the walk kernel this domain will launch (set-up time,
+// outside any stream capture).
+void prepare_walk(mclsgpu_domain* dom) {
+    if (dom->p.precision != MCLSGPU_FP32) return;
+    const bool adj = dom->p.direction == MCLSGPU_ADJOINT;
+    switch (dom->slots) {
+        case 4: adj ? blocks_per_sm<4, 0>() : blocks_per_sm<4, 1>(); break;
+        case 8: adj ? blocks_per_sm<8, 0>() : blocks_per_sm<8, 1>(); break;
+        case 12: adj ? blocks_per_sm<12, 0>() : blocks_per_sm<12, 1>(); break;
+        case 16: adj ? blocks_per_sm<16, 0>() : blocks_per_sm<16, 1>(); break;
+        case 24: adj ? blocks_per_sm<24, 0>() : blocks_per_sm<24, 1>(); break;
+        default: adj ? blocks_per_sm<32, 0>() : blocks_per_sm<32, 1>(); break;
+    }
+}
+
+// Launch the walks of the current source.  Trace arrays only with FP64.
+void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
+                 int* tr_ev, long long* tr_start) {
+    mclsgpu_context* ctx = dom->ctx;
+    const mclsgpu_mc_params& p = dom->p;
+    WalkArgs a{};
+    a.n = dom->n;
+    a.L = p.history_length;
+    a.per = p.sample_ratio > 0.0 ? int(ceil(p.sample_ratio)) : 1;
+    a.rng_mode = p.rng_mode;
+    a.d_nh = dom->d_nh;
+    a.d_counter = dom->d_counter;
+    a.start = dom->start;
+    a.sc = dom->d_scalars;
+    a.cutoff = float(p.weight_cutoff > 0.0 ? p.weight_cutoff : 0.0);
+    a.cutoff64 = p.weight_cutoff > 0.0 ? p.weight_cutoff : 0.0;
+    a.seed = dom->seed;
+    a.d_epoch = dom->d_epoch;
+    a.jump = dom->d_jump;
+    a.d_pos = dom->d_pos;
+    a.rec = dom->rec;
+    a.rp = dom->D.rp;
+    a.col = dom->D.ci;
+    a.h = dom->D.v;
+    a.cdf = dom->cdf;
+    a.W = dom->w;
+    a.y32 = dom->y32;
+    a.y64 = dom->y64;
+    a.c32 = dom->c32;
+    a.c64 = dom->c64;
+    a.d_steps = dom->d_steps;
+    a.d_tim = dom->d_tim;
+    a.status = ctx->d_status;
+    a.max_trace = max_trace;
+    a.tr_states = tr_states;
+    a.tr_w = tr_w;
+    a.tr_ev = tr_ev;
+    a.tr_start = tr_start;
+    cudaStream_t st = ctx->stream;
+    if (p.precision == MCLSGPU_FP32) {
+        cudaMemsetAsync(dom->d_counter, 0, sizeof(int), st);
+        if (p.direction == MCLSGPU_ADJOINT)
+            launch32_slots<MCLSGPU_ADJOINT>(dom->slots, a, ctx->num_sms, st);
+        else
+            launch32_slots<MCLSGPU_FORWARD>(dom->slots, a, ctx->num_sms, st);
+        k_walk_time_acc<<<1, 1, 0, st>>>(dom->d_tim);
+    } else {
+        const int grid = ctx->num_sms * 8;
+        if (p.direction == MCLSGPU_ADJOINT)
+            walk64<MCLSGPU_ADJOINT><<<grid, 128, 0, st>>>(a);
+        else
+            walk64<MCLSGPU_FORWARD><<<grid, 128, 0, st>>>(a);
+    }
+}
+
+}  // namespace mclsgpu

@@ -1,0 +1,122 @@
+/*
+ * mcls_oracle.h -- C interface of the CPU oracle for the MCSA hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker: a plain C++
+ * restatement of the reference MCLS algorithm (adjoint/forward Neumann-Ulam
+ * transport inside MCSA's Richardson loop).  Only the tests, the smoke check
+ * and the CPU-baseline leg of bench.py may load it; the product library
+ * (libmclsgpu.so) never links or calls it.
+ *
+ * Every routine cites the reference file:line it restates (paths relative to
+ * the MCLS source tree).  Parity is pinned by (i) the reference's own
+ * known-answer tests restated in tests/test_oracle_*.py and (ii) golden
+ * vectors produced by the reference's own Xorshift / RNGTraits /
+ * SamplingTools code compiled from its sources into oracle/_ref.
+ */
+#ifndef MCLS_ORACLE_H
+#define MCLS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- RNG ------------------------------------------------------------- */
+/* Reference Xorshift<uint_fast64_t,13,7,17> draws mapped through libstdc++
+ * uniform_real_distribution<double>(0,1) (src/MCLS_Xorshift.hpp:100-108,
+ * src/MCLS_RNGTraits.hpp:147-160). */
+void orc_xorshift_uniforms(uint64_t seed, int64_t n, double* out);
+/* Seed of rank `rank` derived as in src/MCLS_PRNG_impl.hpp:56-75 with the
+ * std::random_device draw replaced by `master_seed`. */
+uint64_t orc_rank_seed(uint64_t master_seed, int rank);
+/* Counter-based generator (no reference counterpart). */
+void orc_counter_uniforms(uint64_t seed, uint64_t epoch, int kind, int64_t idx,
+                          int64_t n, double* out);
+/* src/MCLS_SamplingTools.hpp:67-80 */
+int orc_sample_discrete_cdf(const double* cdf, int size, double u);
+
+/* ---- sparse matrices (opaque CSR, FP64) ------------------------------ */
+typedef struct orc_csr orc_csr;
+orc_csr* orc_csr_create(int64_t n, const int64_t* rowptr, const int64_t* col,
+                        const double* val);
+void orc_csr_free(orc_csr*);
+int64_t orc_csr_n(const orc_csr*);
+int64_t orc_csr_nnz(const orc_csr*);
+void orc_csr_copy(const orc_csr*, int64_t* rowptr, int64_t* col, double* val);
+
+orc_csr* orc_transpose(const orc_csr* A);
+orc_csr* orc_multiply(const orc_csr* A, const orc_csr* B, double threshold);
+/* (PL A PR) or its transpose, per src/MCLS_LinearProblem_impl.hpp:143-221 */
+orc_csr* orc_composite(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
+                       int transpose, double threshold);
+orc_csr* orc_point_jacobi(const orc_csr* A);
+orc_csr* orc_block_jacobi(const orc_csr* A, int block_size);
+void orc_spmv(const orc_csr* A, const double* x, double* y);
+
+/* ---- Monte Carlo parameters ----------------------------------------- */
+typedef struct {
+    int direction;            /* 0 adjoint, 1 forward                          */
+    int estimator;            /* 0 collision, 1 expected value                 */
+    int history_length;       /* "History Length" (default 10)                 */
+    double weight_cutoff;     /* "Weight Cutoff" relative to |w0|; 0 = off    */
+    double sample_ratio;      /* "Sample Ratio"; <= 0 means key absent        */
+    int stratified;           /* "Source Sampling Type" == "Stratified"        */
+    double neumann_relaxation;/* "Neumann Relaxation"; <= 0 means key absent  */
+    double composite_threshold;
+    int rng_mode;             /* 0 reference Xorshift stream, 1 counter-based  */
+    uint64_t seed;            /* xorshift seed (mode 0) or key (mode 1)        */
+} orc_mc_params;
+
+/* Monte Carlo solver over one operator: owns the composite operator, the
+ * AlmostOptimalDomain restatement and the PRNG position. */
+typedef struct orc_mc orc_mc;
+orc_mc* orc_mc_create(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
+                      const orc_mc_params* p);
+void orc_mc_free(orc_mc*);
+/* Domain export: rowptr[n+1], col[], h[], cdf[], weights[n]. */
+int64_t orc_mc_domain_nnz(const orc_mc*);
+void orc_mc_domain_copy(const orc_mc*, int64_t* rowptr, int64_t* col,
+                        double* h, double* cdf, double* weights);
+/* One MC solve of (I-H) x = rhs_scaled.  `internal` follows
+ * MonteCarloSolverManager(internal_solver): when 0 the RHS is left
+ * preconditioned and the result right preconditioned.  Optional trace
+ * buffers (may be NULL) are indexed by emission order:
+ *   trace_states[e*(L+1)+k] state before step k (k<=steps), -1 after death;
+ *   final_weight[e], events[e] (2 = CUTOFF), start_state[e].
+ * Returns the number of histories (normalization), or -1 on error. */
+int64_t orc_mc_solve(orc_mc*, const double* rhs, double* x, int internal,
+                     int64_t max_trace, int64_t* trace_states,
+                     double* final_weight, int* events, int64_t* start_state);
+uint64_t orc_mc_stream_position(const orc_mc*);
+int64_t orc_mc_total_steps(const orc_mc*);
+
+/* ---- MCSA ------------------------------------------------------------ */
+typedef struct {
+    double tolerance;          /* "Convergence Tolerance" (default 1.0)     */
+    int max_iters;             /* "Maximum Iterations" (default 1000)       */
+    int check_freq;            /* "Iteration Check Frequency" (default 1)   */
+    int smoother_steps;        /* "Smoother Steps" (default 1)              */
+    double richardson_omega;   /* "Richardson Relaxation" (default 1.0)     */
+} orc_mcsa_params;
+
+/* MCSASolverManager::solve restatement.  x is updated in place.  Writes the
+ * iteration count, achieved relative residual and (optionally, up to
+ * max_hist entries) the per-iteration |rp|_2 history.  Returns 1 if
+ * converged, 0 if not, -1 on error. */
+int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
+                   const orc_mc_params* mp, const orc_mcsa_params* sp,
+                   const double* b, double* x, int* iters, double* achieved,
+                   int max_hist, double* res_hist, int64_t* total_steps);
+
+/* CPU baseline: independent histories on `threads` threads (one Xorshift per
+ * thread, as one MPI rank per core with subdomain transport), adjoint
+ * collision walks over the domain for `nh` histories of fixed length.
+ * Returns walk steps performed; elapsed seconds through *secs. */
+int64_t orc_bench_walks(const orc_mc*, const double* rhs, int64_t nh,
+                        int threads, double* x, double* secs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
