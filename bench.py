@@ -32,21 +32,29 @@ sys.path.insert(0, ROOT)
 METRIC = "MCSA time-to-1e-8 residual, learned vs Jacobi precond, one B200; walk-steps/sec"
 UNIT = "walk-steps/s"
 CONFIGS = {
-    "c2": dict(workload="3D 7-pt variable-coefficient diffusion 128^3, Jacobi MCSA, expected-value "
-                        "estimator, FP32 walks / FP64 residual, 2^22 histories per iteration",
-               n=128, sample_ratio=2.0, estimator=1, history_length=10),
-    "c1": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, collision estimator, FP64 walks, "
-                        "N histories per iteration",
-               n=100, sample_ratio=1.0, estimator=0, history_length=10),
+    "c2": dict(workload="3D 7-pt variable-coefficient diffusion 128^3, Jacobi MCSA, forward "
+                        "expected-value estimator, FP32 walks / FP64 tallies, residual and update, "
+                        "2^22 histories per iteration",
+               n=128, sample_ratio=2.0, estimator=1, history_length=10, direction=1),
+    "c1": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, adjoint collision estimator, "
+                        "FP64 walks, N histories per iteration",
+               n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0),
 }
-# Algorithmic bytes of one walk step for a k-entry row record: k * (4 B CDF +
-# 4 B column|sign) + 4 B row weight + 8 B FP32 tally read-modify-write.
+# Retained entries per H row (the Jacobi diagonal drops out).
 K_ENTRIES = {"c2": 6, "c1": 4}
 
 
 def step_bytes(cfg):
+    """Algorithmic bytes of one walk step on a k-entry row record.
+
+    Record: k * (4 B CDF + 4 B column|sign) + 4 B row weight.  Forward: plus
+    the 4 B FP32 tally source read.  Adjoint: plus an 8 B FP64 tally
+    read-modify-write (16 B).
+    """
     k = K_ENTRIES[cfg]
-    return 8 * k + 12
+    if CONFIGS[cfg]["direction"] == 1:
+        return 8 * k + 4 + 4
+    return 8 * k + 4 + 16
 
 
 def load_peaks():
@@ -239,6 +247,7 @@ def main():
     seed = 1234 + rank
     dom = capi.Domain(ctx, op, pc, precision=fp, rng_mode=capi.RNG_COUNTER, seed=seed,
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
+                      direction=cfgd["direction"],
                       history_length=cfgd["history_length"])
     mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
     bt = torch.tensor(b, device=f"cuda:{local}", dtype=torch.float64)

@@ -137,7 +137,6 @@ void release_domain(mclsgpu_domain* d) {
     dfree(d->counts);
     dfree(d->offs);
     dfree(d->start);
-    dfree(d->y32);
     dfree(d->y64);
     dfree(d->c32);
     dfree(d->c64);
@@ -452,7 +451,7 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
             (e = dmalloc(&dom->guide, n)) != cudaSuccess || (e = dmalloc(&dom->counts, n)) != cudaSuccess ||
             (e = dmalloc(&dom->offs, n)) != cudaSuccess ||
             (e = dmalloc(&dom->start, size_t(dom->nh_cap) + 1)) != cudaSuccess ||
-            (e = dmalloc(&dom->y32, n)) != cudaSuccess || (e = dmalloc(&dom->y64, n)) != cudaSuccess ||
+            (e = dmalloc(&dom->y64, n)) != cudaSuccess ||
             (e = dmalloc(&dom->c32, n)) != cudaSuccess || (e = dmalloc(&dom->c64, n)) != cudaSuccess ||
             (e = dmalloc(&dom->d_nh, 1)) != cudaSuccess || (e = dmalloc(&dom->d_counter, 1)) != cudaSuccess ||
             (e = dmalloc(&dom->d_scalars, 16)) != cudaSuccess ||

@@ -114,8 +114,7 @@ struct mclsgpu_domain {
     int* counts = nullptr;         // histories per state (n)
     int* offs = nullptr;           // emission offsets (n)
     int* start = nullptr;          // start state | sign<<31 per history
-    float* y32 = nullptr;          // FP32 tallies (n)
-    double* y64 = nullptr;         // FP64 tallies (n)
+    double* y64 = nullptr;         // tallies, reduced in FP64 (n)
     float* c32 = nullptr;          // forward: FP32 tally source (n)
     double* c64 = nullptr;         // forward: FP64 tally source (n)
     int* d_nh = nullptr;           // histories of the current solve

@@ -75,7 +75,6 @@ struct FinalizeArgs {
     const double* src;   // MC source vector before scaling
     double omega;
     int has_omega;
-    const float* y32;
     const double* y64;
     const int* dtrp;
     const int* dtci;
@@ -93,13 +92,12 @@ __global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
         const double srci = a.has_omega ? a.src[i] * a.omega : a.src[i];
         if (a.mode == 0) {
             // AdjointTally::normalize: x *= 1/nh  (src/MCLS_AdjointTally_impl.hpp:68-72)
-            const double y = a.fp32 ? double(a.y32[i]) : a.y64[i];
-            d = __dmul_rn(y, inv);
+            d = __dmul_rn(a.y64[i], inv);
         } else if (a.mode == 1) {
             double t = 0.0;
             if (a.fp32) {
                 for (int k = a.dtrp[i]; k < a.dtrp[i + 1]; ++k)
-                    t = fma(double(a.dth32[k]), double(a.y32[a.dtci[k]]), t);
+                    t = fma(double(a.dth32[k]), a.y64[a.dtci[k]], t);
             } else {
                 for (int k = a.dtrp[i]; k < a.dtrp[i + 1]; ++k)
                     t = fma(a.dth64[k], a.y64[a.dtci[k]], t);
@@ -107,8 +105,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
             d = __dadd_rn(__dmul_rn(t, inv), srci);
         } else {
             // ForwardTally::finalize: sum / count  (src/MCLS_ForwardTally_impl.hpp:194-208)
-            const double y = a.fp32 ? double(a.y32[i]) : a.y64[i];
-            d = __ddiv_rn(y, a.per);
+            d = __ddiv_rn(a.y64[i], a.per);
             if (a.ev) d = __dadd_rn(d, srci);
         }
         a.out[i] = a.accumulate ? __dadd_rn(a.out[i], d) : d;
@@ -203,7 +200,6 @@ static void enqueue_mc(mclsgpu_domain* dom, const double* v, double* out, int ac
     f.src = v;
     f.omega = omega;
     f.has_omega = has_omega;
-    f.y32 = dom->y32;
     f.y64 = dom->y64;
     f.dtrp = dom->DT.rp;
     f.dtci = dom->DT.ci;

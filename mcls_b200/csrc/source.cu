@@ -225,14 +225,9 @@ void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, i
         suffix_scan_int(s, dom->counts, n, dom->ipart, dom->offs, dom->d_nh);
         k_strat_total<<<1, 1, 0, s>>>(dom->d_nh, dom->d_scalars, cap, ctx->d_status);
     }
-    if (p.precision == MCLSGPU_FP32)
-        k_expand<float><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, dom->counts, dom->offs,
-                                                    dom->d_scalars, cap, dom->start, dom->y32,
-                                                    ctx->d_status);
-    else
-        k_expand<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, dom->counts,
-                                                     dom->offs, dom->d_scalars, cap, dom->start,
-                                                     dom->y64, ctx->d_status);
+    k_expand<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, dom->counts, dom->offs,
+                                                 dom->d_scalars, cap, dom->start, dom->y64,
+                                                 ctx->d_status);
 }
 
 void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega) {
@@ -246,7 +241,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     if (p.precision == MCLSGPU_FP32) {
         k_forward_c<float><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                        dom->D.ci, dom->D.v, dom->c32);
-        cudaMemsetAsync(dom->y32, 0, size_t(n) * sizeof(float), s);
+        cudaMemsetAsync(dom->y64, 0, size_t(n) * sizeof(double), s);
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);

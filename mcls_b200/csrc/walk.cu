@@ -12,9 +12,12 @@
 // work-queue counter and refill lanes as histories terminate.  A step reads
 // one packed FP32 record (slots * 8 bytes, 16-byte vector loads), selects the
 // first entry whose CDF value is >= u with predicated compares (the records'
-// padding entries hold 2.0 and are never selected), and adds the collision
-// tally with a fire-and-forget FP32 reduction.  The adjoint step-0 tally is
-// made by the source build (counts * w0), so walks tally from step 1.
+// padding entries hold 2.0 and are never selected) and carries the weight in
+// FP32.  Tallies reduce into FP64: the adjoint collision tally with a
+// fire-and-forget FP64 reduction per step, the forward history sum
+// Kahan-compensated in FP32 and reduced into FP64 once per history.  The
+// adjoint step-0 tally is made by the source build (counts * w0), so walks
+// tally from step 1.
 //
 // walk64: the parity kernel.  FP64 CSR domain, binary search with
 // std::lower_bound semantics, FP64 weights and tallies, optional trajectory
@@ -51,7 +54,6 @@ struct WalkArgs {
     const double* cdf;
     const double* W;
     // tallies
-    float* y32;
     double* y64;
     const float* c32;
     const double* c64;
@@ -91,7 +93,7 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
     const uint4* __restrict__ rec = reinterpret_cast<const uint4*>(a.rec);
     if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
     int s = 0, s0 = 0, k = 0;
-    float w = 0.f, wcut = 0.f, acc = 0.f;
+    float w = 0.f, wcut = 0.f, acc = 0.f, comp = 0.f;
     uint64_t x = 0;
     bool alive = false, drained = false;
     unsigned long long steps = 0;
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
                         s = e / a.per;
                         w = 1.f;
                         acc = 0.f;
+                        comp = 0.f;
                     }
                     s0 = s;
                     wcut = a.cutoff * fabsf(w);
@@ -128,9 +131,14 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
         if (alive) {
             // Tally at the pre-transition state.
             if (DIR == MCLSGPU_ADJOINT) {
-                if (k > 0) atomicAdd(&a.y32[s], w);
+                // FP32 weight, FP64 reduction (fire-and-forget RED.ADD.F64).
+                if (k > 0) atomicAdd(&a.y64[s], double(w));
             } else {
-                acc = fmaf(w, __ldg(&a.c32[s]), acc);
+                // Kahan-compensated FP32 history sum.
+                const float term = w * __ldg(&a.c32[s]) - comp;
+                const float t = acc + term;
+                comp = (t - acc) - term;
+                acc = t;
             }
             // Transition: one packed record.
             const uint4* r = rec + size_t(s) * (S / 2);
@@ -157,7 +165,7 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
             ++steps;
             if (k >= a.L || fabsf(w) < wcut) {
                 alive = false;
-                if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y32[s0], acc);
+                if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y64[s0], double(acc) - double(comp));
             }
         }
     }
@@ -316,7 +324,6 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
     a.h = dom->D.v;
     a.cdf = dom->cdf;
     a.W = dom->w;
-    a.y32 = dom->y32;
     a.y64 = dom->y64;
     a.c32 = dom->c32;
     a.c64 = dom->c64;
