@@ -199,7 +199,10 @@ void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, i
     cudaStream_t s = ctx->stream;
     const int n = dom->n;
     const mclsgpu_mc_params& p = dom->p;
-    const bool parity = p.precision == MCLSGPU_FP64 && p.rng_mode == MCLSGPU_RNG_REFERENCE;
+    // FP64 walks are the parity template: |b|_1 and the source CDF follow the
+    // reference's left-to-right summation order (one thread).  FP32 walks use
+    // the parallel tree order.
+    const bool parity = p.precision == MCLSGPU_FP64;
     const int nh_req = p.sample_ratio > 0.0 ? int(double(n) * p.sample_ratio) : n;
     const int cap = int(dom->nh_cap);
     // weight = |b|_1
