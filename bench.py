@@ -224,6 +224,9 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iters", type=int, default=20000)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="host-driven MCSA loop (for profilers that cannot see kernels "
+                         "inside conditional graph nodes)")
     args = ap.parse_args()
     world, rank, local, pg = dist_init(args)
     if args.impl == "reference":
@@ -249,7 +252,8 @@ def main():
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
                       direction=cfgd["direction"],
                       history_length=cfgd["history_length"])
-    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
+                          host_loop=1 if args.host_loop else 0)
     bt = torch.tensor(b, device=f"cuda:{local}", dtype=torch.float64)
     xt = torch.zeros_like(bt)
 

@@ -104,7 +104,9 @@ typedef struct {
     double richardson_omega;  /* "Richardson Relaxation" (1.0)      */
     int32_t print_freq;       /* "Iteration Print Frequency" (10)   */
     int32_t verbose;          /* print the reference's banner lines */
-    int32_t batch_iters;      /* iterations launched per host check (0 = auto) */
+    int32_t host_loop;        /* 1: host-driven loop (one launch sequence and
+                               * host check per iteration) instead of the
+                               * device-side graph loop; for profilers */
     int32_t reserved0;
 } mclsgpu_mcsa_params;
 

@@ -53,7 +53,7 @@ class McsaParams(C.Structure):
         ("richardson_omega", C.c_double),
         ("print_freq", C.c_int32),
         ("verbose", C.c_int32),
-        ("batch_iters", C.c_int32),
+        ("host_loop", C.c_int32),
         ("reserved0", C.c_int32),
     ]
 
@@ -280,7 +280,7 @@ def mc_params(direction=ADJOINT, estimator=COLLISION, history_length=10, weight_
 
 
 def mcsa_params(tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
-                richardson_omega=1.0, print_freq=10, verbose=0):
+                richardson_omega=1.0, print_freq=10, verbose=0, host_loop=0):
     p = McsaParams()
     p.size = C.sizeof(McsaParams)
     p.tolerance = tolerance
@@ -290,6 +290,7 @@ def mcsa_params(tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
     p.richardson_omega = richardson_omega
     p.print_freq = print_freq
     p.verbose = verbose
+    p.host_loop = host_loop
     return p
 
 

@@ -116,8 +116,8 @@ __global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
 __global__ void k_epoch_inc(unsigned long long* e) { *e += 1ULL; }
 
 // Convergence check of one MCSA iteration (src/MCLS_MCSASolverManager_impl.hpp:380-394).
-__global__ void k_mcsa_check(McsaState* st, const double* sumsq, double* hist, int hist_cap,
-                             const int* status, cudaGraphConditionalHandle handle) {
+__device__ __forceinline__ int mcsa_check(McsaState* st, const double* sumsq, double* hist,
+                                          int hist_cap, const int* status) {
     McsaState s = *st;
     s.iter += 1;
     s.rnorm = sqrt(*sumsq);
@@ -128,7 +128,18 @@ __global__ void k_mcsa_check(McsaState* st, const double* sumsq, double* hist, i
     s.done = !keep;
     s.converged = s.rnorm <= s.crit;
     *st = s;
+    return keep;
+}
+
+__global__ void k_mcsa_check(McsaState* st, const double* sumsq, double* hist, int hist_cap,
+                             const int* status, cudaGraphConditionalHandle handle) {
+    const int keep = mcsa_check(st, sumsq, hist, hist_cap, status);
     cudaGraphSetConditional(handle, keep ? 1u : 0u);
+}
+
+__global__ void k_mcsa_check_host(McsaState* st, const double* sumsq, double* hist, int hist_cap,
+                                  const int* status) {
+    mcsa_check(st, sumsq, hist, hist_cap, status);
 }
 
 __global__ void k_mcsa_init(McsaState* st, const double* src_sumsq, double tol, int check_freq,
@@ -276,6 +287,20 @@ static int mc_solve_device(mclsgpu_domain* dom, const double* rhs_dev, double* x
     return MCLSGPU_OK;
 }
 
+// One MCSA iteration without its convergence check.
+static void enqueue_iteration_body(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
+    cudaStream_t s = dom->ctx->stream;
+    const int n = dom->n;
+    for (int l = 0; l < mp->smoother_steps; ++l) {
+        k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, n,
+                                                              mp->richardson_omega);
+        update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    }
+    enqueue_mc(dom, dom->rp, dom->x, 1, 0, nullptr, nullptr, nullptr, nullptr);
+    update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+}
+
 // Build the CUDA graph of the MCSA loop (WHILE node, one iteration per body).
 static int build_mcsa_graph(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
     mclsgpu_context* ctx = dom->ctx;
@@ -310,15 +335,7 @@ static int build_mcsa_graph(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) 
         cudaGraphDestroy(g);
         return cuda_fail(ctx, e, "cudaStreamBeginCaptureToGraph");
     }
-    const int n = dom->n;
-    for (int l = 0; l < mp->smoother_steps; ++l) {
-        k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, n,
-                                                              mp->richardson_omega);
-        update_prec_residual(dom, dom->x, dom->b, dom->rp);
-    }
-    enqueue_mc(dom, dom->rp, dom->x, 1, 0, nullptr, nullptr, nullptr, nullptr);
-    update_prec_residual(dom, dom->x, dom->b, dom->rp);
-    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    enqueue_iteration_body(dom, mp);
     k_mcsa_check<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid, dom->resid_cap,
                                  ctx->d_status, handle);
     cudaGraph_t captured = body;
@@ -372,7 +389,7 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
     }
     // Graph key: everything baked into the captured iteration.
     const int key = mp->smoother_steps * 1000003 ^ int(mp->richardson_omega * 1e6);
-    if (!dom->graph || dom->graph_key != key) {
+    if (!mp->host_loop && (!dom->graph || dom->graph_key != key)) {
         int rc = build_mcsa_graph(dom, mp);
         if (rc) {
             cudaEventDestroy(e0);
@@ -397,7 +414,20 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
     sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
     k_mcsa_init<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 6, mp->tolerance, mp->check_freq,
                                 mp->max_iters, dom->d_scalars + 5);
-    cudaError_t e = cudaGraphLaunch(dom->graph, s);
+    cudaError_t e = cudaSuccess;
+    if (!mp->host_loop) {
+        e = cudaGraphLaunch(dom->graph, s);
+    } else {
+        // Host-driven loop: the same iteration, one state read-back each.
+        for (int it = 0; it < mp->max_iters && e == cudaSuccess; ++it) {
+            enqueue_iteration_body(dom, mp);
+            k_mcsa_check_host<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid,
+                                               dom->resid_cap, ctx->d_status);
+            cudaMemcpyAsync(dom->h_state, dom->d_state, sizeof(McsaState), cudaMemcpyDeviceToHost, s);
+            e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess && dom->h_state->done) break;
+        }
+    }
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) {
         // Right preconditioner recovery (:410-418).

@@ -199,10 +199,11 @@ void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, i
     cudaStream_t s = ctx->stream;
     const int n = dom->n;
     const mclsgpu_mc_params& p = dom->p;
-    // FP64 walks are the parity template: |b|_1 and the source CDF follow the
-    // reference's left-to-right summation order (one thread).  FP32 walks use
-    // the parallel tree order.
-    const bool parity = p.precision == MCLSGPU_FP64;
+    // The reproducible mode (FP64 walks on the reference stream) is the parity
+    // template: |b|_1 and the source CDF follow the reference's left-to-right
+    // summation order (one thread).  Every other mode uses the parallel tree
+    // order, which can differ in the last bits of |b|_1 and the CDF.
+    const bool parity = p.precision == MCLSGPU_FP64 && p.rng_mode == MCLSGPU_RNG_REFERENCE;
     const int nh_req = p.sample_ratio > 0.0 ? int(double(n) * p.sample_ratio) : n;
     const int cap = int(dom->nh_cap);
     // weight = |b|_1

@@ -101,8 +101,13 @@ def _trace_compare(ctx, A, b, prec, solves=3, **kw):
         assert nhg == nho
         assert np.array_equal(tg["start"], to["start"])
         assert np.array_equal(tg["states"], to["states"])
-        assert np.array_equal(tg["final_weight"], to["final_weight"])
         assert np.array_equal(tg["events"], to["events"])
+        if okw["rng_mode"] == capi.RNG_REFERENCE:
+            assert np.array_equal(tg["final_weight"], to["final_weight"])
+        else:
+            # Outside the reproducible mode |b|_1 (the starting weight) is a
+            # parallel tree sum: the weights agree to its rounding.
+            assert np.allclose(tg["final_weight"], to["final_weight"], rtol=1e-13, atol=0)
         assert tg["states"].shape[1] == L + 1
         scale = np.abs(xo).max()
         assert np.allclose(xg, xo, rtol=1e-12, atol=1e-12 * scale)
