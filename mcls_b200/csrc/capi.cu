@@ -153,6 +153,9 @@ void release_domain(mclsgpu_domain* d) {
     dfree(d->rp);
     dfree(d->tmp);
     dfree(d->tmp2);
+    dfree(d->x2);
+    dfree(d->rp2);
+    dfree(d->d_ticket);
     dfree(d->d_state);
     dfree(d->d_resid);
     if (d->h_state) cudaFreeHost(d->h_state);
@@ -462,6 +465,8 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
             (e = dmalloc(&dom->x, n)) != cudaSuccess || (e = dmalloc(&dom->b, n)) != cudaSuccess ||
             (e = dmalloc(&dom->rp, n)) != cudaSuccess || (e = dmalloc(&dom->tmp, n)) != cudaSuccess ||
             (e = dmalloc(&dom->tmp2, n)) != cudaSuccess || (e = dmalloc(&dom->d_state, 1)) != cudaSuccess ||
+            (e = dmalloc(&dom->x2, n)) != cudaSuccess || (e = dmalloc(&dom->rp2, n)) != cudaSuccess ||
+            (e = dmalloc(&dom->d_ticket, 1)) != cudaSuccess ||
             (e = cudaMallocHost(reinterpret_cast<void**>(&dom->h_state), sizeof(McsaState))) != cudaSuccess)
             rc = cuda_fail(ctx, e, "cudaMalloc domain buffers");
     }
@@ -471,6 +476,8 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
         cudaMemsetAsync(dom->d_epoch, 0, sizeof(unsigned long long), ctx->stream);
         cudaMemsetAsync(dom->d_steps, 0, sizeof(unsigned long long), ctx->stream);
         cudaMemsetAsync(dom->d_hist, 0, sizeof(unsigned long long), ctx->stream);
+        cudaMemsetAsync(dom->d_ticket, 0, sizeof(unsigned int), ctx->stream);
+        cudaMemsetAsync(dom->d_counter, 0, sizeof(int), ctx->stream);
         cudaMemsetAsync(dom->d_scalars, 0, 16 * sizeof(double), ctx->stream);
         const unsigned long long tim0[4] = {~0ULL, 0ULL, 0ULL, 0ULL};
         cudaMemcpyAsync(dom->d_tim, tim0, sizeof(tim0), cudaMemcpyHostToDevice, ctx->stream);

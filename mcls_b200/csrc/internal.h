@@ -131,6 +131,9 @@ struct mclsgpu_domain {
     double* rp = nullptr;
     double* tmp = nullptr;
     double* tmp2 = nullptr;
+    double* x2 = nullptr;          // fused iteration: x after smoothing
+    double* rp2 = nullptr;         // fused iteration: residual after smoothing
+    unsigned int* d_ticket = nullptr;  // last-block ticket of the fused residual
     mclsgpu::McsaState* d_state = nullptr;
     mclsgpu::McsaState* h_state = nullptr;  // pinned
     cudaGraphExec_t graph = nullptr;

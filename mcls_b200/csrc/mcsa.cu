@@ -33,10 +33,12 @@
 namespace mclsgpu {
 
 void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega);
-void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega);
+void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
+                           bool fused);
+void launch_forward_setup(mclsgpu_domain* dom);
 void launch_advance_walk_pos(mclsgpu_domain* dom);
 void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
-                 int* tr_ev, long long* tr_start);
+                 int* tr_ev, long long* tr_start, bool fused);
 
 namespace {
 
@@ -142,6 +144,128 @@ __global__ void k_mcsa_check_host(McsaState* st, const double* sumsq, double* hi
     mcsa_check(st, sumsq, hist, hist_cap, status);
 }
 
+// ---- fused iteration kernels (smoother_steps == 1, PL in {I, point Jacobi}) ----
+constexpr int kFusedThreads = 256;
+
+// Richardson smoothing fused with the residual: x2 = x + w rp (rounded as the
+// separate update would be) and rp2 = PL (b - A x2), reading x + w rp at the
+// neighbours on the fly.
+__global__ void __launch_bounds__(kFusedThreads) k_richardson_residual(
+    const int* rp, const int* ci, const double* v, int n, const double* b, const double* dinv,
+    const double* x, const double* r, double w, double* x2, double* r2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const int j = ci[k];
+            s = fma(v[k], __dadd_rn(x[j], __dmul_rn(w, r[j])), s);
+        }
+        const double res = b[i] - s;
+        r2[i] = dinv ? dinv[i] * res : res;
+        x2[i] = __dadd_rn(x[i], __dmul_rn(w, r[i]));
+    }
+}
+
+struct ResidArgs {
+    const int* rp;
+    const int* ci;
+    const double* v;
+    int n;
+    const double* b;
+    const double* dinv;       // null: no left preconditioner
+    const double* xin;        // x after smoothing
+    const double* rin;        // residual after smoothing (the MC source)
+    const double* y;          // tallies
+    const double* sc;         // [2] = 1/nh
+    double omega;
+    int has_omega;
+    double per;
+    int ev;
+    int mode;                 // 0 adjoint collision, 1 forward, 2 x already corrected
+    double* xout;
+    double* rout;
+    double* part;
+    unsigned int* ticket;
+    McsaState* st;
+    double* hist;
+    int hist_cap;
+    const int* status;
+    unsigned long long* d_epoch;
+    unsigned long long* d_tim;
+    int* d_counter;
+    unsigned long long* d_hist;
+    const int* d_nh;
+    cudaGraphConditionalHandle handle;
+    int use_cond;
+};
+
+// x + delta at state j: the MC correction of the estimator, rounded exactly
+// as the separate normalise-and-add kernel rounds it.
+__device__ __forceinline__ double corrected(const ResidArgs& a, int j, double inv) {
+    const double xj = a.xin[j];
+    if (a.mode == 0) return __dadd_rn(xj, __dmul_rn(a.y[j], inv));
+    if (a.mode == 1) {
+        double d = __ddiv_rn(a.y[j], a.per);
+        if (a.ev) d = __dadd_rn(d, a.has_omega ? a.rin[j] * a.omega : a.rin[j]);
+        return __dadd_rn(xj, d);
+    }
+    return xj;
+}
+
+// x = x2 + delta, rp = PL (b - A x), |rp|^2, then (last block) the MCSA
+// convergence check, the stream epoch, the walk timing, the work-queue reset
+// and the loop condition.
+__global__ void __launch_bounds__(kFusedThreads) k_update_residual(ResidArgs a) {
+    __shared__ double warp_sum[kFusedThreads / 32];
+    __shared__ bool last;
+    const double inv = a.sc[2];
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) s = fma(a.v[k], corrected(a, a.ci[k], inv), s);
+        const double res = a.b[i] - s;
+        const double r = a.dinv ? a.dinv[i] * res : res;
+        a.rout[i] = r;
+        a.xout[i] = corrected(a, i, inv);
+        acc = fma(r, r, acc);
+    }
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kFusedThreads / 32; ++w) t += warp_sum[w];
+        a.part[blockIdx.x] = t;
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double t = 0.0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) t += a.part[i];
+    for (int d = 16; d > 0; d >>= 1) t += __shfl_down_sync(0xffffffffu, t, d);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sumsq = 0.0;
+        for (int w = 0; w < kFusedThreads / 32; ++w) sumsq += warp_sum[w];
+        *a.ticket = 0u;
+        const int keep = mcsa_check(a.st, &sumsq, a.hist, a.hist_cap, a.status);
+        *a.d_epoch += 1ULL;
+        *a.d_hist += (unsigned long long)(*a.d_nh);
+        unsigned long long* tm = a.d_tim;
+        if (tm[1] > tm[0]) {
+            tm[2] += tm[1] - tm[0];
+            tm[3] += 1;
+        }
+        tm[0] = ~0ULL;
+        tm[1] = 0;
+        *a.d_counter = 0;
+        if (a.use_cond) cudaGraphSetConditional(a.handle, keep ? 1u : 0u);
+    }
+}
+
 __global__ void k_mcsa_init(McsaState* st, const double* src_sumsq, double tol, int check_freq,
                             int max_iters, const double* r_sumsq) {
     McsaState s{};
@@ -187,19 +311,24 @@ static void update_prec_residual(mclsgpu_domain* dom, const double* x, const dou
 }
 
 // One MC solve of the source vector `v` (device, already left preconditioned
-// when required) into out (accumulate: out += delta).
+// when required) into out (accumulate: out += delta).  `fused`: inside the
+// fused MCSA iteration the normalise-and-add of the collision and forward
+// estimators, the epoch increment and the walk bookkeeping are done by
+// k_update_residual; only the adjoint expected-value gather runs here.
 static void enqueue_mc(mclsgpu_domain* dom, const double* v, double* out, int accumulate,
                        long long max_trace, long long* tr_states, double* tr_w, int* tr_ev,
-                       long long* tr_start) {
+                       long long* tr_start, bool fused = false) {
     const mclsgpu_mc_params& p = dom->p;
     const double omega = p.neumann_relaxation;
     const int has_omega = p.neumann_relaxation > 0.0;
     if (p.direction == MCLSGPU_ADJOINT)
         launch_adjoint_source(dom, v, omega, has_omega);
     else
-        launch_forward_source(dom, v, omega, has_omega);
-    launch_walk(dom, max_trace, tr_states, tr_w, tr_ev, tr_start);
+        launch_forward_source(dom, v, omega, has_omega, fused);
+    launch_walk(dom, max_trace, tr_states, tr_w, tr_ev, tr_start, fused);
     launch_advance_walk_pos(dom);
+    if (fused && !(p.direction == MCLSGPU_ADJOINT && p.estimator == MCLSGPU_EXPECTED_VALUE))
+        return;
     FinalizeArgs f{};
     f.n = dom->n;
     f.mode = p.direction == MCLSGPU_FORWARD ? 2 : (p.estimator == MCLSGPU_EXPECTED_VALUE ? 1 : 0);
@@ -218,9 +347,9 @@ static void enqueue_mc(mclsgpu_domain* dom, const double* v, double* out, int ac
     f.dth64 = dom->DT.v;
     f.out = out;
     f.d_nh = dom->d_nh;
-    f.d_hist = dom->d_hist;
+    f.d_hist = fused ? nullptr : dom->d_hist;
     k_finalize<<<grid_for(dom->n, 256, 148 * 8), 256, 0, dom->ctx->stream>>>(f);
-    k_epoch_inc<<<1, 1, 0, dom->ctx->stream>>>(dom->d_epoch);
+    if (!fused) k_epoch_inc<<<1, 1, 0, dom->ctx->stream>>>(dom->d_epoch);
 }
 
 static int read_stats(mclsgpu_domain* dom, mclsgpu_stats* st) {
@@ -287,18 +416,84 @@ static int mc_solve_device(mclsgpu_domain* dom, const double* rhs_dev, double* x
     return MCLSGPU_OK;
 }
 
-// One MCSA iteration without its convergence check.
-static void enqueue_iteration_body(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
-    cudaStream_t s = dom->ctx->stream;
+// The fused iteration covers one smoothing step, no right preconditioner and
+// a left preconditioner that is the identity or point Jacobi.
+static bool fused_iteration(const mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
+    return mp->smoother_steps == 1 && !dom->right &&
+           (!dom->left || dom->left->kind == MCLSGPU_PREC_POINT_JACOBI);
+}
+
+static int fused_grid(const mclsgpu_domain* dom) {
+    return grid_for(dom->n, kFusedThreads, dom->ctx->num_sms * 8);
+}
+
+// One MCSA iteration including its convergence check.  The fused form is
+// three kernels around the walk: Richardson + residual, the source build
+// (forward: tally sources into the records), the walk, and correction +
+// residual + norm + check.
+static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp,
+                              cudaGraphConditionalHandle handle, int use_cond) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
     const int n = dom->n;
-    for (int l = 0; l < mp->smoother_steps; ++l) {
-        k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, n,
-                                                              mp->richardson_omega);
+    if (!fused_iteration(dom, mp)) {
+        for (int l = 0; l < mp->smoother_steps; ++l) {
+            k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, n,
+                                                                  mp->richardson_omega);
+            update_prec_residual(dom, dom->x, dom->b, dom->rp);
+        }
+        enqueue_mc(dom, dom->rp, dom->x, 1, 0, nullptr, nullptr, nullptr, nullptr);
         update_prec_residual(dom, dom->x, dom->b, dom->rp);
+        sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+        if (use_cond)
+            k_mcsa_check<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid,
+                                         dom->resid_cap, ctx->d_status, handle);
+        else
+            k_mcsa_check_host<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid,
+                                               dom->resid_cap, ctx->d_status);
+        return;
     }
-    enqueue_mc(dom, dom->rp, dom->x, 1, 0, nullptr, nullptr, nullptr, nullptr);
-    update_prec_residual(dom, dom->x, dom->b, dom->rp);
-    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    const mclsgpu::DevCsr& A = dom->op->A;
+    const double* dinv = dom->left ? dom->left->diag : nullptr;
+    const int grid = fused_grid(dom);
+    k_richardson_residual<<<grid, kFusedThreads, 0, s>>>(A.rp, A.ci, A.v, n, dom->b, dinv, dom->x,
+                                                         dom->rp, mp->richardson_omega, dom->x2,
+                                                         dom->rp2);
+    const mclsgpu_mc_params& p = dom->p;
+    const bool adj_ev = p.direction == MCLSGPU_ADJOINT && p.estimator == MCLSGPU_EXPECTED_VALUE;
+    enqueue_mc(dom, dom->rp2, dom->x2, 1, 0, nullptr, nullptr, nullptr, nullptr, true);
+    ResidArgs a{};
+    a.rp = A.rp;
+    a.ci = A.ci;
+    a.v = A.v;
+    a.n = n;
+    a.b = dom->b;
+    a.dinv = dinv;
+    a.xin = dom->x2;
+    a.rin = dom->rp2;
+    a.y = dom->y64;
+    a.sc = dom->d_scalars;
+    a.omega = p.neumann_relaxation;
+    a.has_omega = p.neumann_relaxation > 0.0;
+    a.per = p.sample_ratio > 0.0 ? std::ceil(p.sample_ratio) : 1.0;
+    a.ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
+    a.mode = p.direction == MCLSGPU_FORWARD ? 1 : (adj_ev ? 2 : 0);
+    a.xout = dom->x;
+    a.rout = dom->rp;
+    a.part = dom->part;
+    a.ticket = dom->d_ticket;
+    a.st = dom->d_state;
+    a.hist = dom->d_resid;
+    a.hist_cap = dom->resid_cap;
+    a.status = ctx->d_status;
+    a.d_epoch = dom->d_epoch;
+    a.d_tim = dom->d_tim;
+    a.d_counter = dom->d_counter;
+    a.d_hist = dom->d_hist;
+    a.d_nh = dom->d_nh;
+    a.handle = handle;
+    a.use_cond = use_cond;
+    k_update_residual<<<grid, kFusedThreads, 0, s>>>(a);
 }
 
 // Build the CUDA graph of the MCSA loop (WHILE node, one iteration per body).
@@ -335,9 +530,7 @@ static int build_mcsa_graph(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) 
         cudaGraphDestroy(g);
         return cuda_fail(ctx, e, "cudaStreamBeginCaptureToGraph");
     }
-    enqueue_iteration_body(dom, mp);
-    k_mcsa_check<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid, dom->resid_cap,
-                                 ctx->d_status, handle);
+    enqueue_iteration(dom, mp, handle, 1);
     cudaGraph_t captured = body;
     e = cudaStreamEndCapture(s, &captured);
     if (e != cudaSuccess) {
@@ -414,15 +607,14 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
     sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
     k_mcsa_init<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 6, mp->tolerance, mp->check_freq,
                                 mp->max_iters, dom->d_scalars + 5);
+    if (fused_iteration(dom, mp) && dom->p.direction == MCLSGPU_FORWARD) launch_forward_setup(dom);
     cudaError_t e = cudaSuccess;
     if (!mp->host_loop) {
         e = cudaGraphLaunch(dom->graph, s);
     } else {
         // Host-driven loop: the same iteration, one state read-back each.
         for (int it = 0; it < mp->max_iters && e == cudaSuccess; ++it) {
-            enqueue_iteration_body(dom, mp);
-            k_mcsa_check_host<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid,
-                                               dom->resid_cap, ctx->d_status);
+            enqueue_iteration(dom, mp, cudaGraphConditionalHandle(0), 0);
             cudaMemcpyAsync(dom->h_state, dom->d_state, sizeof(McsaState), cudaMemcpyDeviceToHost, s);
             e = cudaStreamSynchronize(s);
             if (e == cudaSuccess && dom->h_state->done) break;

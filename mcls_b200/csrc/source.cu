@@ -185,6 +185,25 @@ __global__ void k_forward_c(const double* v, int n, double omega, int has, int e
     }
 }
 
+// FP32 forward walk: the tally source of each state goes into its record's
+// header word (slot 0, second word) so that a step reads one record only;
+// the history-sum tallies are cleared in the same pass.
+__global__ void k_forward_rec(const double* v, int n, double omega, int has, int ev,
+                              const int* rp, const int* ci, const double* h, int slots,
+                              uint2* rec, double* y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double c;
+        if (!ev) {
+            c = load_src(v, i, omega, has);
+        } else {
+            c = 0.0;
+            for (int k = rp[i]; k < rp[i + 1]; ++k) c = fma(h[k], load_src(v, ci[k], omega, has), c);
+        }
+        rec[size_t(i) * slots].y = __float_as_uint(__double2float_rn(c));
+        y[i] = 0.0;
+    }
+}
+
 __global__ void k_forward_nh(int* d_nh, int nh, double* sc) {
     *d_nh = nh;
     sc[0] = 1.0;
@@ -234,18 +253,26 @@ void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, i
                                                  ctx->d_status);
 }
 
-void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega) {
+void launch_forward_setup(mclsgpu_domain* dom) {
+    const mclsgpu_mc_params& p = dom->p;
+    const int per = p.sample_ratio > 0.0 ? int(ceil(p.sample_ratio)) : 1;
+    k_forward_nh<<<1, 1, 0, dom->ctx->stream>>>(dom->d_nh, dom->n * per, dom->d_scalars);
+}
+
+// `fused`: the history count was set once by launch_forward_setup.
+void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
+                           bool fused) {
     mclsgpu_context* ctx = dom->ctx;
     cudaStream_t s = ctx->stream;
     const int n = dom->n;
     const mclsgpu_mc_params& p = dom->p;
     const int per = p.sample_ratio > 0.0 ? int(ceil(p.sample_ratio)) : 1;
     const int ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
-    k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
+    if (!fused) k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
     if (p.precision == MCLSGPU_FP32) {
-        k_forward_c<float><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
-                                                       dom->D.ci, dom->D.v, dom->c32);
-        cudaMemsetAsync(dom->y64, 0, size_t(n) * sizeof(double), s);
+        k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, omega, has_omega, ev,
+                                                               dom->D.rp, dom->D.ci, dom->D.v,
+                                                               dom->slots, dom->rec, dom->y64);
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);

@@ -72,6 +72,16 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// 256-bit read-only load of half a record, not allocated in L1 (records are
+// read once per step and reused across steps only through L2).
+__device__ __forceinline__ void ld_record256(const void* p, uint32_t* r) {
+    asm volatile(
+        "ld.global.nc.L1::no_allocate.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7])
+        : "l"(p));
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -129,36 +139,35 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
         }
         if (!__any_sync(kFull, alive)) break;
         if (alive) {
+            // One packed record: S/4 256-bit loads that bypass L1 (each step
+            // touches exactly the record's own sectors).
+            const char* r = reinterpret_cast<const char*>(rec) + size_t(s) * (S * 8);
+            uint32_t q[2 * S];
+#pragma unroll
+            for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
             // Tally at the pre-transition state.
             if (DIR == MCLSGPU_ADJOINT) {
                 // FP32 weight, FP64 reduction (fire-and-forget RED.ADD.F64).
                 if (k > 0) atomicAdd(&a.y64[s], double(w));
             } else {
-                // Kahan-compensated FP32 history sum.
-                const float term = w * __ldg(&a.c32[s]) - comp;
+                // Kahan-compensated FP32 history sum; the tally source of the
+                // state rides in the record header (slot 0, second word).
+                const float term = w * __uint_as_float(q[1]) - comp;
                 const float t = acc + term;
                 comp = (t - acc) - term;
                 acc = t;
             }
-            // Transition: one packed record.
-            const uint4* r = rec + size_t(s) * (S / 2);
-            uint4 q[S / 2];
-#pragma unroll
-            for (int t = 0; t < S / 2; ++t) q[t] = __ldg(r + t);
             x = xs_step(x);
             const float u = canonical32(x);
-            unsigned sel = q[0].w;  // slot 1 (first entry)
-            bool found = __uint_as_float(q[0].z) >= u;
+            unsigned sel = q[3];  // slot 1 (first entry)
+            bool found = __uint_as_float(q[2]) >= u;
 #pragma unroll
-            for (int t = 1; t < S / 2; ++t) {
-                const bool c0 = !found && __uint_as_float(q[t].x) >= u;
-                sel = c0 ? q[t].y : sel;
-                found = found || c0;
-                const bool c1 = !found && __uint_as_float(q[t].z) >= u;
-                sel = c1 ? q[t].w : sel;
-                found = found || c1;
+            for (int t = 2; t < S; ++t) {
+                const bool c = !found && __uint_as_float(q[2 * t]) >= u;
+                sel = c ? q[2 * t + 1] : sel;
+                found = found || c;
             }
-            const float Wt = __uint_as_float(q[0].x);
+            const float Wt = __uint_as_float(q[0]);
             w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
             s = int(sel & 0x7fffffffu);
             ++k;
@@ -299,8 +308,10 @@ void prepare_walk(mclsgpu_domain* dom) {
 }
 
 // Launch the walks of the current source.  Trace arrays only with FP64.
+// `fused`: the work-queue counter reset and the timing accumulation are done
+// by the fused residual kernel that follows the walk (MCSA loop).
 void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
-                 int* tr_ev, long long* tr_start) {
+                 int* tr_ev, long long* tr_start, bool fused) {
     mclsgpu_context* ctx = dom->ctx;
     const mclsgpu_mc_params& p = dom->p;
     WalkArgs a{};
@@ -337,12 +348,12 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
     a.tr_start = tr_start;
     cudaStream_t st = ctx->stream;
     if (p.precision == MCLSGPU_FP32) {
-        cudaMemsetAsync(dom->d_counter, 0, sizeof(int), st);
+        if (!fused) cudaMemsetAsync(dom->d_counter, 0, sizeof(int), st);
         if (p.direction == MCLSGPU_ADJOINT)
             launch32_slots<MCLSGPU_ADJOINT>(dom->slots, a, ctx->num_sms, st);
         else
             launch32_slots<MCLSGPU_FORWARD>(dom->slots, a, ctx->num_sms, st);
-        k_walk_time_acc<<<1, 1, 0, st>>>(dom->d_tim);
+        if (!fused) k_walk_time_acc<<<1, 1, 0, st>>>(dom->d_tim);
     } else {
         const int grid = ctx->num_sms * 8;
         if (p.direction == MCLSGPU_ADJOINT)
