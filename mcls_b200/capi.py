@@ -166,6 +166,10 @@ def _ptr(a):
 
 
 class Context:
+    """One device context.  Handles created on it are released before it is:
+    the C ABI requires every operator, preconditioner and domain of a context
+    to be destroyed before the context itself."""
+
     def __init__(self, device: int = 0):
         self.L = load()
         h = C.c_void_p()
@@ -173,13 +177,24 @@ class Context:
         if rc != OK:
             raise MclsError(rc, "context create failed")
         self.h = h
+        self._children = []  # weak references, released in reverse order
 
     def check(self, rc):
         if rc != OK:
             raise MclsError(rc, self.L.mclsgpu_last_error(self.h).decode())
 
+    def _adopt(self, child):
+        import weakref
+
+        self._children.append(weakref.ref(child))
+
     def close(self):
         if getattr(self, "h", None):
+            for ref in reversed(self._children):
+                child = ref()
+                if child is not None:
+                    child.close()
+            self._children = []
             self.L.mclsgpu_context_destroy(self.h)
             self.h = None
 
@@ -203,6 +218,7 @@ class Operator:
         h = C.c_void_p()
         ctx.check(ctx.L.mclsgpu_operator_upload(ctx.h, n, _ptr(rp), _ptr(ci), _ptr(v), C.byref(h)))
         self.h = h
+        ctx._adopt(self)
 
     def apply(self, x):
         x = np.ascontiguousarray(x, np.float64)
@@ -240,6 +256,7 @@ class Precond:
         ctx.check(ctx.L.mclsgpu_precond_build(ctx.h, op.h, C.byref(p), C.byref(h)))
         del keep
         self.h = h
+        ctx._adopt(self)
 
     def to_scipy(self, n):
         nnz = C.c_int64()
@@ -308,6 +325,7 @@ class Domain:
                                              right.h if right else None, C.byref(self.p),
                                              C.byref(h)))
         self.h = h
+        ctx._adopt(self)
 
     def export(self):
         L = self.ctx.L

@@ -156,14 +156,9 @@ __global__ void __launch_bounds__(kThreads) tile_rescan(Load ld, int n, Op op, T
     }
 }
 
-struct RawCdfStore {  // unnormalised CDF; the last element is the total
+struct RawCdfStore {  // unnormalised CDF
     double* cdf;
-    double* total;
-    int n;
-    __device__ __forceinline__ void operator()(int i, double v) const {
-        cdf[i] = v;
-        if (i == n - 1) *total = v;
-    }
+    __device__ __forceinline__ void operator()(int i, double v) const { cdf[i] = v; }
 };
 struct RevExclStore {  // inclusive over reversed index -> exclusive suffix
     int* out;
@@ -179,11 +174,14 @@ struct PlainStore {
     __device__ __forceinline__ void operator()(int i, int v) const { out[i] = v; }
 };
 
+// cdf[i] /= cdf.back()  (src/MCLS_UniformAdjointSource_impl.hpp:201-205).  The
+// total is the reduce-then-scan total, which uses the same association as the
+// |b|_1 reduction, so total == |b|_1 bit for bit whenever b[0] > 0 (as in the
+// reference's sequential sums); the last element is set to exactly 1.
 __global__ void normalize_cdf(double* cdf, int n, const double* total) {
-    // cdf[i] /= cdf.back()  (src/MCLS_UniformAdjointSource_impl.hpp:201-205)
     const double t = *total;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        cdf[i] = cdf[i] / t;
+        cdf[i] = i == n - 1 ? 1.0 : cdf[i] / t;
 }
 
 __global__ void seq_source_cdf(CdfLoad ld, int n, double* cdf, double* total) {
@@ -247,8 +245,8 @@ void source_cdf(cudaStream_t s, const double* v, int n, double scale, int has_sc
     int nb = tiles(n);
     tile_reduce<double><<<nb, kThreads, 0, s>>>(ld, n, AddOp(), 0.0, part);
     partial_scan<double><<<1, kThreads, 0, s>>>(part, nb, AddOp(), 0.0);
-    tile_rescan<double><<<nb, kThreads, 0, s>>>(ld, n, AddOp(), 0.0, part,
-                                                RawCdfStore{cdf, total, n});
+    copy_total<double><<<1, 1, 0, s>>>(part, nb, total);
+    tile_rescan<double><<<nb, kThreads, 0, s>>>(ld, n, AddOp(), 0.0, part, RawCdfStore{cdf});
     normalize_cdf<<<(n + 1023) / 1024 < 1184 ? (n + 1023) / 1024 : 1184, 1024, 0, s>>>(cdf, n, total);
 }
 

@@ -311,11 +311,13 @@ def test_device_vectors_entry_point(ctx):
     assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-6
 
 
-@pytest.mark.parametrize("direction,estimator", [(0, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("direction,estimator", [(0, 0), (0, 1), (1, 0), (1, 1)])
 def test_fused_iteration_matches_unfused(ctx, direction, estimator):
     # Point Jacobi runs the fused iteration (Richardson+residual, correction+
     # residual+norm+check); the same diagonal passed as a user CSR matrix runs
-    # the kernel-per-operation path.  Same bits, same iteration count.
+    # the kernel-per-operation path.  After a fixed number of iterations the
+    # iterates agree bit for bit (the two residual-norm reductions associate
+    # differently, so the stopping test is kept out of the comparison).
     A, b = P.diffusion3d_varcoef(10, seed=5)
     op = capi.Operator(ctx, A)
     pj = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
@@ -324,14 +326,15 @@ def test_fused_iteration_matches_unfused(ctx, direction, estimator):
               estimator=estimator, sample_ratio=2.0)
     d1 = capi.Domain(ctx, op, pj, **kw)
     d2 = capi.Domain(ctx, op, pu, **kw)
-    x1, s1 = d1.mcsa_solve(b, tolerance=1e-8, max_iters=3000)
-    x2, s2 = d2.mcsa_solve(b, tolerance=1e-8, max_iters=3000)
-    assert s1["converged"] == 1 and s1["iterations"] == s2["iterations"]
+    x1, s1 = d1.mcsa_solve(b, tolerance=0.0, max_iters=25)
+    x2, s2 = d2.mcsa_solve(b, tolerance=0.0, max_iters=25)
+    assert s1["iterations"] == s2["iterations"] == 25
     assert np.array_equal(x1, x2)
+    assert abs(s1["residual_norm"] - s2["residual_norm"]) <= 1e-12 * s2["residual_norm"]
     # host-driven loop: the same kernels, the same result
     d1.reseed(11)
-    x3, s3 = d1.mcsa_solve(b, tolerance=1e-8, max_iters=3000, host_loop=1)
-    assert s3["iterations"] == s1["iterations"] and np.array_equal(x1, x3)
+    x3, s3 = d1.mcsa_solve(b, tolerance=0.0, max_iters=25, host_loop=1)
+    assert s3["iterations"] == 25 and np.array_equal(x1, x3)
 
 
 def test_smoother_steps_and_relaxation(ctx):
