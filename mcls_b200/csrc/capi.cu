@@ -123,6 +123,7 @@ int copy_csr_out(mclsgpu_context* ctx, const DevCsr& A, int64_t* nnz_out, int64_
 
 void release_domain(mclsgpu_domain* d) {
     d->D.release();
+    d->DS.release();
     d->DT.release();
     dfree(d->cdf);
     dfree(d->w);
@@ -236,8 +237,10 @@ int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n, const int64_t* rowp
     op->ctx = ctx;
     op->serial = ++serial;
     int rc = upload_csr(ctx, n, rowptr, colind, values, op->A);
+    if (!rc) rc = csr_to_sell(ctx, op->A, op->S);
     if (rc) {
         op->A.release();
+        op->S.release();
         delete op;
         return rc;
     }
@@ -248,6 +251,7 @@ int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n, const int64_t* rowp
 int mclsgpu_operator_destroy(mclsgpu_operator* op) {
     if (!op) return MCLSGPU_OK;
     op->A.release();
+    op->S.release();
     dfree(op->dinv);
     delete op;
     return MCLSGPU_OK;

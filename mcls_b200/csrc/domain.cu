@@ -159,6 +159,10 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
         k_pack_records<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n, slots,
                                                    dom->rec);
     }
+    // SELL-32 copy for the forward tally source (c = H b per solve).
+    if (dom->p.direction == MCLSGPU_FORWARD) {
+        if ((rc = csr_to_sell(ctx, D, dom->DS))) return rc;
+    }
     // Transposed domain for the adjoint expected-value estimator.
     if (dom->p.direction == MCLSGPU_ADJOINT && dom->p.estimator == MCLSGPU_EXPECTED_VALUE) {
         if ((rc = csr_transpose(ctx, D, dom->DT))) return rc;

@@ -48,11 +48,26 @@ struct DevCsr {
     void release();
 };
 
+// Sliced ELL with slices of 32 rows (SELL-32): slice s holds rows 32s..32s+31
+// column-major, width w_s = the longest row of the slice, at off[s]; entry k
+// of row r sits at off[r/32] + 32k + r%32.  Padding entries repeat the row's
+// own index with value 0.  A warp that owns one slice reads each entry column
+// with one coalesced access.
+struct DevSell {
+    int n = 0;
+    int nslices = 0;
+    int* off = nullptr;      // nslices + 1 entry offsets
+    int* col = nullptr;
+    double* val = nullptr;
+    void release();
+};
+
 }  // namespace mclsgpu
 
 struct mclsgpu_operator {
     mclsgpu_context* ctx = nullptr;
     mclsgpu::DevCsr A;
+    mclsgpu::DevSell S;           // the same matrix as SELL-32 (residual kernels)
     double* dinv = nullptr;       // reciprocal diagonal (built on demand)
     uint64_t serial = 0;          // identity for "operator changed" checks
 };
@@ -93,6 +108,7 @@ struct mclsgpu_domain {
     mclsgpu::DevCsr D;            // D.v holds h
     double* cdf = nullptr;
     double* w = nullptr;
+    mclsgpu::DevSell DS;          // the domain as SELL-32 (forward tally source)
     // Transposed domain for the expected-value estimator: DT(j,s) = h_sj.
     mclsgpu::DevCsr DT;
     float* dt_h32 = nullptr;
@@ -179,6 +195,10 @@ int reciprocal_diagonal(mclsgpu_context* ctx, const DevCsr& A, double* dinv);
 int block_jacobi(mclsgpu_context* ctx, const DevCsr& A, int bs, DevCsr& P);
 int point_jacobi_csr(mclsgpu_context* ctx, int n, const double* dinv,
                      DevCsr& P);
+// SELL-32 copy of a CSR matrix (set-up).
+int csr_to_sell(mclsgpu_context* ctx, const DevCsr& A, DevSell& S);
+// y = A x over a SELL-32 matrix.
+void sell_spmv(cudaStream_t s, const DevSell& A, const double* x, double* y);
 // Exclusive scan of set-up counts into rp[0..n]; *total = sum.
 int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int* d_rp,
                               long long* total);

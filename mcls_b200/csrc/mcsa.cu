@@ -48,13 +48,25 @@ inline int grid_for(long long work, int threads = 256, int cap = 148 * 16) {
     return int(g > cap ? cap : g);
 }
 
+// Row r of a SELL-32 matrix: first entry index and width (entries at
+// o + 32k).  Padding entries have value 0 and add exactly nothing, so the
+// sums equal the CSR sums in column order.
+__device__ __forceinline__ void sell_row(const int* off, int r, int& o, int& w) {
+    const int a = off[r >> 5];
+    o = a + (r & 31);
+    w = (off[(r >> 5) + 1] - a) >> 5;
+}
+
 // rp = (b - A x) [* dinv]   (LinearProblem::updatePrecResidual, :410-442)
-__global__ void __launch_bounds__(256) k_residual(const int* rp, const int* ci, const double* v,
-                                                  int n, const double* x, const double* b,
-                                                  const double* dinv, double* out) {
+__global__ void __launch_bounds__(256) k_residual(const int* off, const int* col,
+                                                  const double* val, int n, const double* x,
+                                                  const double* b, const double* dinv,
+                                                  double* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int o, w;
+        sell_row(off, i, o, w);
         double s = 0.0;
-        for (int k = rp[i]; k < rp[i + 1]; ++k) s = fma(v[k], x[ci[k]], s);
+        for (int k = 0; k < w; ++k) s = fma(val[o + 32 * k], x[col[o + 32 * k]], s);
         double r = b[i] - s;
         out[i] = dinv ? dinv[i] * r : r;
     }
@@ -151,13 +163,15 @@ constexpr int kFusedThreads = 256;
 // separate update would be) and rp2 = PL (b - A x2), reading x + w rp at the
 // neighbours on the fly.
 __global__ void __launch_bounds__(kFusedThreads) k_richardson_residual(
-    const int* rp, const int* ci, const double* v, int n, const double* b, const double* dinv,
-    const double* x, const double* r, double w, double* x2, double* r2) {
+    const int* off, const int* col, const double* val, int n, const double* b,
+    const double* dinv, const double* x, const double* r, double w, double* x2, double* r2) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int o, wd;
+        sell_row(off, i, o, wd);
         double s = 0.0;
-        for (int k = rp[i]; k < rp[i + 1]; ++k) {
-            const int j = ci[k];
-            s = fma(v[k], __dadd_rn(x[j], __dmul_rn(w, r[j])), s);
+        for (int k = 0; k < wd; ++k) {
+            const int j = col[o + 32 * k];
+            s = fma(val[o + 32 * k], __dadd_rn(x[j], __dmul_rn(w, r[j])), s);
         }
         const double res = b[i] - s;
         r2[i] = dinv ? dinv[i] * res : res;
@@ -221,7 +235,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_update_residual(ResidArgs a) 
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         double s = 0.0;
-        for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) s = fma(a.v[k], corrected(a, a.ci[k], inv), s);
+        int o, w;
+        sell_row(a.rp, i, o, w);
+        for (int k = 0; k < w; ++k)
+            s = fma(a.v[o + 32 * k], corrected(a, a.ci[o + 32 * k], inv), s);
         const double res = a.b[i] - s;
         const double r = a.dinv ? a.dinv[i] * res : res;
         a.rout[i] = r;
@@ -290,7 +307,7 @@ __global__ void k_mcsa_init(McsaState* st, const double* src_sumsq, double tol, 
 static void update_prec_residual(mclsgpu_domain* dom, const double* x, const double* b,
                                  double* rp_out) {
     cudaStream_t s = dom->ctx->stream;
-    const mclsgpu::DevCsr& A = dom->op->A;
+    const mclsgpu::DevSell& A = dom->op->S;
     const double* xin = x;
     if (dom->right) {
         spmv(s, dom->right->P, x, dom->tmp2);
@@ -298,13 +315,13 @@ static void update_prec_residual(mclsgpu_domain* dom, const double* x, const dou
     }
     mclsgpu_precond* L = dom->left;
     if (!L) {
-        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, xin, b,
+        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, xin, b,
                                                               nullptr, rp_out);
     } else if (L->kind == MCLSGPU_PREC_POINT_JACOBI) {
-        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, xin, b,
+        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, xin, b,
                                                               L->diag, rp_out);
     } else {
-        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, xin, b,
+        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, xin, b,
                                                               nullptr, dom->tmp);
         spmv(s, L->P, dom->tmp, rp_out);
     }
@@ -453,19 +470,19 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
                                                dom->resid_cap, ctx->d_status);
         return;
     }
-    const mclsgpu::DevCsr& A = dom->op->A;
+    const mclsgpu::DevSell& A = dom->op->S;
     const double* dinv = dom->left ? dom->left->diag : nullptr;
     const int grid = fused_grid(dom);
-    k_richardson_residual<<<grid, kFusedThreads, 0, s>>>(A.rp, A.ci, A.v, n, dom->b, dinv, dom->x,
+    k_richardson_residual<<<grid, kFusedThreads, 0, s>>>(A.off, A.col, A.val, n, dom->b, dinv, dom->x,
                                                          dom->rp, mp->richardson_omega, dom->x2,
                                                          dom->rp2);
     const mclsgpu_mc_params& p = dom->p;
     const bool adj_ev = p.direction == MCLSGPU_ADJOINT && p.estimator == MCLSGPU_EXPECTED_VALUE;
     enqueue_mc(dom, dom->rp2, dom->x2, 1, 0, nullptr, nullptr, nullptr, nullptr, true);
     ResidArgs a{};
-    a.rp = A.rp;
-    a.ci = A.ci;
-    a.v = A.v;
+    a.rp = A.off;  // SELL-32 operator: rp = slice offsets, ci/v = entries
+    a.ci = A.col;
+    a.v = A.val;
     a.n = n;
     a.b = dom->b;
     a.dinv = dinv;

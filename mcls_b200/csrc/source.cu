@@ -188,16 +188,21 @@ __global__ void k_forward_c(const double* v, int n, double omega, int has, int e
 // FP32 forward walk: the tally source of each state goes into its record's
 // header word (slot 0, second word) so that a step reads one record only;
 // the history-sum tallies are cleared in the same pass.
-__global__ void k_forward_rec(const double* v, int n, double omega, int has, int ev,
-                              const int* rp, const int* ci, const double* h, int slots,
-                              uint2* rec, double* y) {
+__global__ void __launch_bounds__(256) k_forward_rec(const double* v, int n, double omega,
+                                                     int has, int ev, const int* off,
+                                                     const int* col, const double* h, int slots,
+                                                     uint2* rec, double* y) {
+    // H over SELL-32: a warp owns one slice, every entry column is one
+    // coalesced access.
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double c;
         if (!ev) {
             c = load_src(v, i, omega, has);
         } else {
             c = 0.0;
-            for (int k = rp[i]; k < rp[i + 1]; ++k) c = fma(h[k], load_src(v, ci[k], omega, has), c);
+            const int o = off[i >> 5] + (i & 31), w = (off[(i >> 5) + 1] - off[i >> 5]) >> 5;
+            for (int k = 0; k < w; ++k)
+                c = fma(h[o + 32 * k], load_src(v, col[o + 32 * k], omega, has), c);
         }
         rec[size_t(i) * slots].y = __float_as_uint(__double2float_rn(c));
         y[i] = 0.0;
@@ -271,8 +276,9 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     if (!fused) k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
     if (p.precision == MCLSGPU_FP32) {
         k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, omega, has_omega, ev,
-                                                               dom->D.rp, dom->D.ci, dom->D.v,
-                                                               dom->slots, dom->rec, dom->y64);
+                                                               dom->DS.off, dom->DS.col,
+                                                               dom->DS.val, dom->slots, dom->rec,
+                                                               dom->y64);
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);

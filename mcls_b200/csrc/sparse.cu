@@ -19,6 +19,13 @@ void DevCsr::release() {
     n = nnz = 0;
 }
 
+void DevSell::release() {
+    dfree(off);
+    dfree(col);
+    dfree(val);
+    n = nslices = 0;
+}
+
 namespace {
 
 inline int grid_for(long long work, int threads = 256, int cap = 148 * 16) {
@@ -526,6 +533,73 @@ int block_jacobi(mclsgpu_context* ctx, const DevCsr& A, int bs, DevCsr& P) {
     if (e != cudaSuccess) return cuda_fail(ctx, e, "block jacobi");
     if (hbad) return set_error(ctx, MCLSGPU_ERR_DEGENERATE, "singular Jacobi block");
     return MCLSGPU_OK;
+}
+
+namespace {
+
+__global__ void k_slice_width(const int* rp, int n, int nslices, int* width) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslices; s += gridDim.x * blockDim.x) {
+        int w = 0;
+        for (int r = 32 * s; r < 32 * s + 32 && r < n; ++r) w = max(w, rp[r + 1] - rp[r]);
+        width[s] = 32 * w;
+    }
+}
+
+__global__ void k_sell_fill(const int* rp, const int* ci, const double* v, int n, int nslices,
+                            const int* off, int* scol, double* sval) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < 32 * nslices;
+         r += gridDim.x * blockDim.x) {
+        const int s = r >> 5, lane = r & 31;
+        const int o = off[s], w = (off[s + 1] - o) >> 5;
+        const int a = r < n ? rp[r] : 0, len = r < n ? rp[r + 1] - rp[r] : 0;
+        for (int k = 0; k < w; ++k) {
+            const bool real = k < len;
+            scol[o + 32 * k + lane] = real ? ci[a + k] : (r < n ? r : 0);
+            sval[o + 32 * k + lane] = real ? v[a + k] : 0.0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sell_spmv(const int* off, const int* col,
+                                                   const double* val, int n, const double* x,
+                                                   double* y) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int o = off[r >> 5] + (r & 31), w = (off[(r >> 5) + 1] - off[r >> 5]) >> 5;
+        double s = 0.0;
+        for (int k = 0; k < w; ++k) s = fma(val[o + 32 * k], x[col[o + 32 * k]], s);
+        y[r] = s;
+    }
+}
+
+}  // namespace
+
+int csr_to_sell(mclsgpu_context* ctx, const DevCsr& A, DevSell& S) {
+    cudaStream_t s = ctx->stream;
+    S.release();
+    S.n = A.n;
+    S.nslices = (A.n + 31) / 32;
+    int* width = nullptr;
+    cudaError_t e = dmalloc(&width, S.nslices + 1);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    if ((e = dmalloc(&S.off, S.nslices + 1)) != cudaSuccess) {
+        dfree(width);
+        return cuda_fail(ctx, e, "cudaMalloc");
+    }
+    k_slice_width<<<grid_for(S.nslices), 256, 0, s>>>(A.rp, A.n, S.nslices, width);
+    long long tot = 0;
+    int rc = exclusive_scan_counts_dev(ctx, width, S.nslices, S.off, &tot);
+    dfree(width);
+    if (rc) return rc;
+    if ((e = dmalloc(&S.col, tot + 1)) != cudaSuccess || (e = dmalloc(&S.val, tot + 1)) != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaMalloc SELL");
+    k_sell_fill<<<grid_for(32LL * S.nslices), 256, 0, s>>>(A.rp, A.ci, A.v, A.n, S.nslices, S.off,
+                                                          S.col, S.val);
+    e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "SELL build");
+}
+
+void sell_spmv(cudaStream_t s, const DevSell& A, const double* x, double* y) {
+    k_sell_spmv<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, x, y);
 }
 
 }  // namespace mclsgpu

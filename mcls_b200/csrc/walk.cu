@@ -93,25 +93,41 @@ __device__ __forceinline__ uint64_t history_state(const WalkArgs& a, uint64_t ek
     return xs_jump(a.jump, a.seed, *a.d_pos + uint64_t(e) * uint64_t(a.L));
 }
 
+// Small records (up to 8 slots) run at full occupancy: 8 blocks of 256 threads
+// per SM, i.e. at most 32 registers per thread.  The per-launch constants
+// that are only needed when a lane takes a new history (history count,
+// stream key, starting weight) live in shared memory, not registers.
+template <int S>
+struct WalkOccupancy {
+    static constexpr int kMinBlocks = S <= 8 ? 8 : (S <= 24 ? 4 : 2);
+};
+
 template <int S, int DIR>
-__global__ void __launch_bounds__(256) walk32(WalkArgs a) {
-    static_assert(S % 2 == 0, "records are whole 16-byte vectors");
+__global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(WalkArgs a) {
+    static_assert(S % 4 == 0, "records are whole 32-byte halves");
+    __shared__ uint64_t s_ekey;
+    __shared__ int s_nh;
+    __shared__ float s_wnorm;
     const int lane = threadIdx.x & 31;
-    const int nh = *a.d_nh;
-    const float wnorm = float(a.sc[0]);
-    const uint64_t ekey = epoch_key(a.seed, *a.d_epoch);
+    if (threadIdx.x == 0) {
+        s_ekey = epoch_key(a.seed, *a.d_epoch);
+        s_nh = *a.d_nh;
+        s_wnorm = float(a.sc[0]);
+    }
+    __syncthreads();
     const uint4* __restrict__ rec = reinterpret_cast<const uint4*>(a.rec);
     if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
     int s = 0, s0 = 0, k = 0;
     float w = 0.f, wcut = 0.f, acc = 0.f, comp = 0.f;
     uint64_t x = 0;
     bool alive = false, drained = false;
-    unsigned long long steps = 0;
+    unsigned steps = 0;
     while (true) {
         const unsigned need = __ballot_sync(kFull, !alive);
         if (need && !drained) {
             const int leader = __ffs(need) - 1;
             const int cnt = __popc(need);
+            const int nh = s_nh;
             int base = 0;
             if (lane == leader) base = atomicAdd(a.d_counter, cnt);
             base = __shfl_sync(kFull, base, leader);
@@ -122,7 +138,7 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
                     if (DIR == MCLSGPU_ADJOINT) {
                         const int sv = a.start[e];
                         s = sv & 0x7fffffff;
-                        w = sv < 0 ? -wnorm : wnorm;
+                        w = sv < 0 ? -s_wnorm : s_wnorm;
                     } else {
                         s = e / a.per;
                         w = 1.f;
@@ -131,7 +147,7 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
                     }
                     s0 = s;
                     wcut = a.cutoff * fabsf(w);
-                    x = history_state(a, ekey, e);
+                    x = history_state(a, s_ekey, e);
                     k = 0;
                     alive = true;
                 }
@@ -182,7 +198,7 @@ __global__ void __launch_bounds__(256) walk32(WalkArgs a) {
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) steps += __shfl_down_sync(kFull, steps, d);
     if (lane == 0) {
-        if (steps) atomicAdd(a.d_steps, steps);
+        if (steps) atomicAdd(a.d_steps, (unsigned long long)steps);
         atomicMax(&a.d_tim[1], global_ns());
     }
 }
