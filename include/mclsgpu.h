@@ -90,9 +90,14 @@ typedef struct {
     double neumann_relaxation;
     double composite_threshold;
     int32_t rng_mode;
-    int32_t reserved0;
+    int32_t record_format;    /* FP32 walk records: 0 = automatic, 1 = packed
+                               * (column, CDF) pairs, 2 = stencil (CDF slots for
+                               * a fixed set of column offsets) */
     uint64_t seed;
 } mclsgpu_mc_params;
+
+/* Record formats (mclsgpu_mc_params.record_format). */
+enum { MCLSGPU_RECORD_AUTO = 0, MCLSGPU_RECORD_PACKED = 1, MCLSGPU_RECORD_STENCIL = 2 };
 
 /* MCSA parameters (src/MCLS_MCSASolverManager_impl.hpp:290-343). */
 typedef struct {

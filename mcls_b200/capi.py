@@ -22,6 +22,7 @@ COLLISION, EXPECTED_VALUE = 0, 1
 SOURCE_RANDOM, SOURCE_STRATIFIED = 0, 1
 FP64, FP32 = 0, 1
 RNG_REFERENCE, RNG_COUNTER = 0, 1
+RECORD_AUTO, RECORD_PACKED, RECORD_STENCIL = 0, 1, 2
 PREC_NONE, PREC_POINT_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED_SPAI, PREC_USER_CSR = range(5)
 
 
@@ -38,7 +39,7 @@ class McParams(C.Structure):
         ("neumann_relaxation", C.c_double),
         ("composite_threshold", C.c_double),
         ("rng_mode", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("record_format", C.c_int32),
         ("seed", C.c_uint64),
     ]
 
@@ -279,9 +280,11 @@ class Precond:
 
 def mc_params(direction=ADJOINT, estimator=COLLISION, history_length=10, weight_cutoff=0.0,
               sample_ratio=-1.0, source_sampling=SOURCE_RANDOM, precision=FP32,
-              neumann_relaxation=-1.0, composite_threshold=0.0, rng_mode=RNG_COUNTER, seed=1):
+              neumann_relaxation=-1.0, composite_threshold=0.0, rng_mode=RNG_COUNTER, seed=1,
+              record_format=0):
     p = McParams()
     p.size = C.sizeof(McParams)
+    p.record_format = record_format
     p.direction = direction
     p.estimator = estimator
     p.history_length = history_length

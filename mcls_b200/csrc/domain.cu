@@ -11,7 +11,9 @@
 //   slot 1..K:   { cdf_j (float bits), col_j | (h_j <= 0) << 31 }
 //   padding:     { 2.0f, 0 }  (never selected: every uniform is < 1)
 // so that one walk step reads exactly one contiguous record.
+#include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <vector>
 
 #include "internal.h"
@@ -92,12 +94,79 @@ __global__ void k_pack_records(const int* drp, const int* dcol, const double* dh
     }
 }
 
+// Distinct column offsets (col - row) into a 16-slot table; an offset takes
+// the first free slot it meets scanning from slot 0, so each offset owns one
+// slot.  More than 16 distinct offsets sets *overflow.
+__global__ void k_collect_offsets(const int* rp, const int* ci, int n, int* tab, int* overflow) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const int d = ci[k] - i;
+            bool placed = false;
+            for (int t = 0; t < 16 && !placed; ++t) {
+                int cur = tab[t];
+                if (cur == INT_MIN) cur = atomicCAS(&tab[t], INT_MIN, d);
+                if (cur == INT_MIN || cur == d) placed = true;
+            }
+            if (!placed) *overflow = 1;
+        }
+    }
+}
+
+// Stencil record of row i: word 0 = W, word 1 = tally source (forward),
+// word 2 + j = CDF value at offset off[j] with the sign of h in its sign bit,
+// or NaN when the row has no entry at that offset (never selected).
+__global__ void k_pack_stencil(const int* drp, const int* dcol, const double* dh,
+                               const double* dcdf, const double* dw, int n, int K,
+                               const int* off, int words, uint32_t* rec) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t* r = rec + size_t(i) * words;
+        r[0] = __float_as_uint(__double2float_rn(dw[i]));
+        r[1] = 0u;
+        for (int j = 2; j < words; ++j) r[j] = 0x7fc00000u;
+        for (int k = drp[i]; k < drp[i + 1]; ++k) {
+            const int d = dcol[k] - i;
+            int j = 0;
+            while (j < K && off[j] != d) ++j;
+            if (j == K) continue;  // cannot happen: every offset is in the table
+            const float c = __double2float_rn(dcdf[k]);
+            r[2 + j] = __float_as_uint(dh[k] > 0.0 ? c : -c);
+        }
+    }
+}
+
 __global__ void k_to_float(const double* a, float* b, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         b[i] = __double2float_rn(a[i]);
 }
 
 }  // namespace
+
+// Sorted distinct column offsets of D (at most 16; *K = 0 when there are more).
+int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int* offsets, int* K) {
+    cudaStream_t s = ctx->stream;
+    int* tab = nullptr;
+    cudaError_t e = dmalloc(&tab, 17);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    std::vector<int> init(17, INT_MIN);
+    init[16] = 0;
+    cudaMemcpyAsync(tab, init.data(), 17 * sizeof(int), cudaMemcpyHostToDevice, s);
+    k_collect_offsets<<<grid_for(D.n), 256, 0, s>>>(D.rp, D.ci, D.n, tab, tab + 16);
+    std::vector<int> h(17);
+    cudaMemcpyAsync(h.data(), tab, 17 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    dfree(tab);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "collect offsets");
+    *K = 0;
+    for (int t = 0; t < 16; ++t) offsets[t] = 0;
+    if (h[16]) return MCLSGPU_OK;
+    std::vector<int> v;
+    for (int t = 0; t < 16; ++t)
+        if (h[t] != INT_MIN) v.push_back(h[t]);
+    std::sort(v.begin(), v.end());
+    for (size_t t = 0; t < v.size(); ++t) offsets[t] = v[t];
+    *K = int(v.size());
+    return MCLSGPU_OK;
+}
 
 // Build the FP64 domain arrays and FP32 records from the composite M.
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
@@ -143,8 +212,8 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     if (e != cudaSuccess) return cuda_fail(ctx, e, "domain fill");
     if ((rc = check_device_status(ctx))) return rc;
 
-    // FP32 records: slot count = 1 + longest row, rounded up to a supported
-    // stride.
+    // FP32 records, packed format: slot count = 1 + longest row, rounded up to
+    // a supported stride.
     static const int kStrides[] = {4, 8, 12, 16, 24, 32};
     int slots = 0;
     for (int st : kStrides)
@@ -152,12 +221,43 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
             slots = st;
             break;
         }
+    // Stencil format: every row's columns are row + d for d in a global set
+    // of K offsets.  A record is {W, tally source, K signed CDF slots} with NaN
+    // for offsets the row lacks: 2 + K words instead of 2 + 2 * row length.
+    dom->stencil_k = 0;
+    const int fmt = dom->p.record_format;
+    if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED) {
+        int K = 0;
+        if ((rc = collect_offsets(ctx, D, dom->stencil_off, &K))) return rc;
+        const int words = K > 0 && K <= 6 ? 8 : (K > 0 && K <= 14 ? 16 : 0);
+        const int packed_words = slots ? 2 * slots : 1 << 30;
+        if (words && (fmt == MCLSGPU_RECORD_STENCIL || words < packed_words)) {
+            dom->stencil_k = K;
+            slots = words / 2;
+        } else if (fmt == MCLSGPU_RECORD_STENCIL) {
+            return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
+                             "stencil records need at most 14 distinct column offsets (found %d)",
+                             K);
+        }
+    }
     dom->slots = slots;  // 0: rows too long for packed records (FP64 walk only)
     if (slots) {
         if ((e = dmalloc(&dom->rec, size_t(n) * slots)) != cudaSuccess)
             return cuda_fail(ctx, e, "cudaMalloc records");
-        k_pack_records<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n, slots,
-                                                   dom->rec);
+        if (dom->stencil_k) {
+            int* doff = nullptr;
+            if ((e = dmalloc(&doff, 16)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+            cudaMemcpyAsync(doff, dom->stencil_off, 16 * sizeof(int), cudaMemcpyHostToDevice, s);
+            k_pack_stencil<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n,
+                                                       dom->stencil_k, doff, 2 * slots,
+                                                       reinterpret_cast<uint32_t*>(dom->rec));
+            e = cudaStreamSynchronize(s);
+            dfree(doff);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "stencil records");
+        } else {
+            k_pack_records<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n,
+                                                       slots, dom->rec);
+        }
     }
     // SELL-32 copy for the forward tally source (c = H b per solve).
     if (dom->p.direction == MCLSGPU_FORWARD) {

@@ -117,6 +117,9 @@ struct mclsgpu_domain {
     uint2* rec = nullptr;
     int slots = 0;
     int max_row = 0;
+    // Stencil records (stencil_k > 0): row r's slot j is column r + stencil_off[j].
+    int stencil_k = 0;
+    int stencil_off[16] = {0};
     // Random stream.
     uint64_t seed = 1;
     unsigned long long* d_epoch = nullptr;  // counter mode: MC solves so far

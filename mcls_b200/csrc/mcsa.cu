@@ -193,6 +193,8 @@ struct ResidArgs {
     double omega;
     int has_omega;
     double per;
+    double inv_per;
+    int per_pow2;
     int ev;
     int mode;                 // 0 adjoint collision, 1 forward, 2 x already corrected
     double* xout;
@@ -218,7 +220,9 @@ __device__ __forceinline__ double corrected(const ResidArgs& a, int j, double in
     const double xj = a.xin[j];
     if (a.mode == 0) return __dadd_rn(xj, __dmul_rn(a.y[j], inv));
     if (a.mode == 1) {
-        double d = __ddiv_rn(a.y[j], a.per);
+        // sum / count (ForwardTally::finalize); for a power-of-two count the
+        // product with its reciprocal is the same number and much cheaper.
+        double d = a.per_pow2 ? a.y[j] * a.inv_per : __ddiv_rn(a.y[j], a.per);
         if (a.ev) d = __dadd_rn(d, a.has_omega ? a.rin[j] * a.omega : a.rin[j]);
         return __dadd_rn(xj, d);
     }
@@ -493,6 +497,11 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
     a.omega = p.neumann_relaxation;
     a.has_omega = p.neumann_relaxation > 0.0;
     a.per = p.sample_ratio > 0.0 ? std::ceil(p.sample_ratio) : 1.0;
+    {
+        int ex = 0;
+        a.per_pow2 = std::frexp(a.per, &ex) == 0.5;  // per = 2^(ex-1)
+        a.inv_per = 1.0 / a.per;
+    }
     a.ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
     a.mode = p.direction == MCLSGPU_FORWARD ? 1 : (adj_ev ? 2 : 0);
     a.xout = dom->x;

@@ -60,6 +60,7 @@ struct WalkArgs {
     unsigned long long* d_steps;
     unsigned long long* d_tim;  // [0] first warp start, [1] last warp end (ns)
     int* status;
+    int stoff[16];              // stencil records: column offset of each slot
     // trace (FP64 only)
     long long max_trace;
     long long* tr_states;
@@ -102,7 +103,7 @@ struct WalkOccupancy {
     static constexpr int kMinBlocks = S <= 8 ? 8 : (S <= 24 ? 4 : 2);
 };
 
-template <int S, int DIR>
+template <int S, int DIR, bool ST>
 __global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(WalkArgs a) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
@@ -175,17 +176,35 @@ __global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(Walk
             }
             x = xs_step(x);
             const float u = canonical32(x);
-            unsigned sel = q[3];  // slot 1 (first entry)
-            bool found = __uint_as_float(q[2]) >= u;
-#pragma unroll
-            for (int t = 2; t < S; ++t) {
-                const bool c = !found && __uint_as_float(q[2 * t]) >= u;
-                sel = c ? q[2 * t + 1] : sel;
-                found = found || c;
-            }
             const float Wt = __uint_as_float(q[0]);
-            w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
-            s = int(sel & 0x7fffffffu);
+            if constexpr (!ST) {
+                unsigned sel = q[3];  // slot 1 (first entry)
+                bool found = __uint_as_float(q[2]) >= u;
+#pragma unroll
+                for (int t = 2; t < S; ++t) {
+                    const bool c = !found && __uint_as_float(q[2 * t]) >= u;
+                    sel = c ? q[2 * t + 1] : sel;
+                    found = found || c;
+                }
+                w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
+                s = int(sel & 0x7fffffffu);
+            } else {
+                // Stencil slots: first |cdf_j| >= u (NaN slots never match);
+                // the next state is s + offset_j, the sign of h_j is the sign
+                // bit of the slot.
+                int dsel = 0;
+                unsigned neg = 0u;
+                bool found = false;
+#pragma unroll
+                for (int j = 0; j < 2 * S - 2; ++j) {
+                    const bool c = !found && fabsf(__uint_as_float(q[2 + j])) >= u;
+                    dsel = c ? a.stoff[j] : dsel;
+                    neg = c ? (q[2 + j] & 0x80000000u) : neg;
+                    found = found || c;
+                }
+                w = neg ? -(w * Wt) : w * Wt;
+                s += dsel;
+            }
             ++k;
             ++steps;
             if (k >= a.L || fabsf(w) < wcut) {
@@ -278,31 +297,57 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
     atomicAdd(a.d_steps, steps);
 }
 
-template <int S, int DIR>
+template <int S, int DIR, bool ST>
 int blocks_per_sm() {
     static int cached = 0;
     if (!cached) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR, ST>, 256, 0);
         cached = b > 0 ? b : 1;
     }
     return cached;
 }
 
-template <int S, int DIR>
-void launch32(const WalkArgs& a, int sms, cudaStream_t st) {
-    walk32<S, DIR><<<sms * blocks_per_sm<S, DIR>(), 256, 0, st>>>(a);
+// Dispatch on the record stride; `launch` false only caches the occupancy.
+template <int DIR, bool ST>
+void launch32_slots(int slots, const WalkArgs& a, int sms, cudaStream_t st, bool launch) {
+#define MCLSGPU_WALK_CASE(SL)                                                        \
+    case SL:                                                                         \
+        if (launch)                                                                  \
+            walk32<SL, DIR, ST><<<sms * blocks_per_sm<SL, DIR, ST>(), 256, 0, st>>>(a); \
+        else                                                                         \
+            blocks_per_sm<SL, DIR, ST>();                                            \
+        break;
+    if (ST) {
+        switch (slots) {
+            MCLSGPU_WALK_CASE(4)
+            default:
+                MCLSGPU_WALK_CASE(8)
+        }
+    } else {
+        switch (slots) {
+            MCLSGPU_WALK_CASE(4)
+            MCLSGPU_WALK_CASE(8)
+            MCLSGPU_WALK_CASE(12)
+            MCLSGPU_WALK_CASE(16)
+            MCLSGPU_WALK_CASE(24)
+            default:
+                MCLSGPU_WALK_CASE(32)
+        }
+    }
+#undef MCLSGPU_WALK_CASE
 }
 
-template <int DIR>
-void launch32_slots(int slots, const WalkArgs& a, int sms, cudaStream_t st) {
-    switch (slots) {
-        case 4: launch32<4, DIR>(a, sms, st); break;
-        case 8: launch32<8, DIR>(a, sms, st); break;
-        case 12: launch32<12, DIR>(a, sms, st); break;
-        case 16: launch32<16, DIR>(a, sms, st); break;
-        case 24: launch32<24, DIR>(a, sms, st); break;
-        default: launch32<32, DIR>(a, sms, st); break;
+void dispatch_walk32(const mclsgpu_domain* dom, const WalkArgs& a, bool launch) {
+    const int sms = dom->ctx->num_sms;
+    cudaStream_t st = dom->ctx->stream;
+    const bool adj = dom->p.direction == MCLSGPU_ADJOINT;
+    if (dom->stencil_k) {
+        if (adj) launch32_slots<MCLSGPU_ADJOINT, true>(dom->slots, a, sms, st, launch);
+        else launch32_slots<MCLSGPU_FORWARD, true>(dom->slots, a, sms, st, launch);
+    } else {
+        if (adj) launch32_slots<MCLSGPU_ADJOINT, false>(dom->slots, a, sms, st, launch);
+        else launch32_slots<MCLSGPU_FORWARD, false>(dom->slots, a, sms, st, launch);
     }
 }
 
@@ -312,15 +357,8 @@ void launch32_slots(int slots, const WalkArgs& a, int sms, cudaStream_t st) {
 // outside any stream capture).
 void prepare_walk(mclsgpu_domain* dom) {
     if (dom->p.precision != MCLSGPU_FP32) return;
-    const bool adj = dom->p.direction == MCLSGPU_ADJOINT;
-    switch (dom->slots) {
-        case 4: adj ? blocks_per_sm<4, 0>() : blocks_per_sm<4, 1>(); break;
-        case 8: adj ? blocks_per_sm<8, 0>() : blocks_per_sm<8, 1>(); break;
-        case 12: adj ? blocks_per_sm<12, 0>() : blocks_per_sm<12, 1>(); break;
-        case 16: adj ? blocks_per_sm<16, 0>() : blocks_per_sm<16, 1>(); break;
-        case 24: adj ? blocks_per_sm<24, 0>() : blocks_per_sm<24, 1>(); break;
-        default: adj ? blocks_per_sm<32, 0>() : blocks_per_sm<32, 1>(); break;
-    }
+    WalkArgs a{};
+    dispatch_walk32(dom, a, false);
 }
 
 // Launch the walks of the current source.  Trace arrays only with FP64.
@@ -362,13 +400,11 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
     a.tr_w = tr_w;
     a.tr_ev = tr_ev;
     a.tr_start = tr_start;
+    for (int j = 0; j < 16; ++j) a.stoff[j] = dom->stencil_off[j];
     cudaStream_t st = ctx->stream;
     if (p.precision == MCLSGPU_FP32) {
         if (!fused) cudaMemsetAsync(dom->d_counter, 0, sizeof(int), st);
-        if (p.direction == MCLSGPU_ADJOINT)
-            launch32_slots<MCLSGPU_ADJOINT>(dom->slots, a, ctx->num_sms, st);
-        else
-            launch32_slots<MCLSGPU_FORWARD>(dom->slots, a, ctx->num_sms, st);
+        dispatch_walk32(dom, a, true);
         if (!fused) k_walk_time_acc<<<1, 1, 0, st>>>(dom->d_tim);
     } else {
         const int grid = ctx->num_sms * 8;
