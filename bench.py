@@ -40,21 +40,17 @@ CONFIGS = {
                         "FP64 walks, N histories per iteration",
                n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0),
 }
-# Retained entries per H row (the Jacobi diagonal drops out).
-K_ENTRIES = {"c2": 6, "c1": 4}
+def step_bytes(cfg, info):
+    """Bytes one FP32 walk step must move: its state's record, plus (adjoint)
+    an 8 B FP64 tally read-modify-write.
 
-
-def step_bytes(cfg):
-    """Algorithmic bytes of one walk step on a k-entry row record.
-
-    Record: k * (4 B CDF + 4 B column|sign) + 4 B row weight.  Forward: plus
-    the 4 B FP32 tally source read.  Adjoint: plus an 8 B FP64 tally
-    read-modify-write (16 B).
+    Packed records hold k (CDF, column|sign) pairs and a {W, tally source}
+    header; stencil records hold the header and one signed CDF slot per
+    stencil offset (3D 7-point Jacobi: 2 + 6 words = 32 B).  The forward tally
+    source rides in the record header, so the forward step is the record.
     """
-    k = K_ENTRIES[cfg]
-    if CONFIGS[cfg]["direction"] == 1:
-        return 8 * k + 4 + 4
-    return 8 * k + 4 + 16
+    rec = info["record_bytes"]
+    return rec if CONFIGS[cfg]["direction"] == 1 else rec + 16
 
 
 def load_peaks():
@@ -303,7 +299,9 @@ def main():
     walk_ms = sum(s["walk_ms"] for s in stats)
     walk_launches = sum(s["walk_launches"] for s in stats)
     per_launch_ms = walk_ms / max(walk_launches, 1)
-    bytes_per_launch = step_bytes(args.config) * steps_total / max(walk_launches, 1)
+    info = dom.info()
+    bstep = step_bytes(args.config, info)
+    bytes_per_launch = bstep * steps_total / max(walk_launches, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -324,7 +322,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": None,
                      "kernel": "walk32", "peak_kind": peak_kind,
-                     "bytes_per_step": step_bytes(args.config),
+                     "bytes_per_step": bstep,
+                     "record_format": "stencil" if info["record_format"] == 2 else "packed",
                      "walk_ms_per_launch": per_launch_ms,
                      "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
         "wall_s": wall,

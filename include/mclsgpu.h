@@ -208,6 +208,20 @@ int mclsgpu_domain_destroy(mclsgpu_domain* dom);
 int mclsgpu_domain_export(mclsgpu_domain* dom, int64_t* nnz_out,
                           int64_t* rowptr, int64_t* col, double* h,
                           double* cdf, double* weights);
+/* Layout of a built domain (no counterpart in the reference: the device
+ * record format replaces AlmostOptimalDomain's per-row arrays). */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_domain_info) */
+    int32_t record_format;    /* MCLSGPU_RECORD_PACKED or _STENCIL (FP32 walks) */
+    int64_t rows;
+    int64_t entries;          /* retained H entries */
+    int32_t record_bytes;     /* bytes of one FP32 walk record (0: FP64 walk only) */
+    int32_t max_row_entries;
+    int32_t stencil_offsets;  /* distinct column offsets (stencil records) */
+    int32_t operator_dia;     /* operator stored by diagonal offsets */
+} mclsgpu_domain_info;
+int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info);
+
 /* Replace the stream seed/position (restart the reproducible stream). */
 int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed);
 /* Per-rank Xorshift seed as PRNG<RNG>(rank) derives it

@@ -95,6 +95,19 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "size"}
 
 
+class DomainInfo(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("record_format", C.c_int32),
+        ("rows", C.c_int64),
+        ("entries", C.c_int64),
+        ("record_bytes", C.c_int32),
+        ("max_row_entries", C.c_int32),
+        ("stencil_offsets", C.c_int32),
+        ("operator_dia", C.c_int32),
+    ]
+
+
 #: Every entry point declared in include/mclsgpu.h.
 EXPORTS = [
     "mclsgpu_abi_version", "mclsgpu_build_info", "mclsgpu_context_create",
@@ -105,6 +118,7 @@ EXPORTS = [
     "mclsgpu_domain_destroy", "mclsgpu_domain_export", "mclsgpu_domain_reseed",
     "mclsgpu_rank_seed", "mclsgpu_mc_solve", "mclsgpu_mc_solve_dev", "mclsgpu_mc_trace",
     "mclsgpu_mcsa_solve", "mclsgpu_mcsa_solve_dev", "mclsgpu_domain_spectral_radius",
+    "mclsgpu_domain_query",
 ]
 
 _LIB = None
@@ -149,6 +163,7 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_domain_destroy.argtypes = [P]
     L.mclsgpu_domain_export.argtypes = [P, C.POINTER(i64), P, P, P, P, P]
     L.mclsgpu_domain_reseed.argtypes = [P, C.c_uint64]
+    L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
     L.mclsgpu_rank_seed.argtypes = [C.c_uint64, C.c_int]
     L.mclsgpu_rank_seed.restype = C.c_uint64
     L.mclsgpu_mc_solve.argtypes = [P, P, P, C.c_int, C.POINTER(Stats)]
@@ -343,6 +358,12 @@ class Domain:
         self.ctx.check(L.mclsgpu_domain_export(self.h, C.byref(nnz), _ptr(rp), _ptr(col), _ptr(h),
                                                _ptr(cdf), _ptr(w)))
         return dict(rowptr=rp, col=col[:k], h=h[:k], cdf=cdf[:k], weights=w)
+
+    def info(self):
+        d = DomainInfo()
+        d.size = C.sizeof(DomainInfo)
+        self.ctx.check(self.ctx.L.mclsgpu_domain_query(self.h, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in d._fields_ if k != "size"}
 
     def reseed(self, seed):
         self.ctx.check(self.ctx.L.mclsgpu_domain_reseed(self.h, seed))

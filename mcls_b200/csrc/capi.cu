@@ -238,9 +238,18 @@ int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n, const int64_t* rowp
     op->serial = ++serial;
     int rc = upload_csr(ctx, n, rowptr, colind, values, op->A);
     if (!rc) rc = csr_to_sell(ctx, op->A, op->S);
+    // Stencil operators also get diagonal-offset storage (no column indices)
+    // when it holds at most 25% more values than the CSR arrays.
+    int K = 0;
+    if (!rc) rc = collect_offsets(ctx, op->A, op->dia_off, &K);
+    if (!rc && K > 0 && double(K) * op->A.n <= 1.25 * op->A.nnz + op->A.n) {
+        rc = csr_to_dia(ctx, op->A, K, op->dia_off, &op->dia_val);
+        if (!rc) op->dia_k = K;
+    }
     if (rc) {
         op->A.release();
         op->S.release();
+        dfree(op->dia_val);
         delete op;
         return rc;
     }
@@ -252,6 +261,7 @@ int mclsgpu_operator_destroy(mclsgpu_operator* op) {
     if (!op) return MCLSGPU_OK;
     op->A.release();
     op->S.release();
+    dfree(op->dia_val);
     dfree(op->dinv);
     delete op;
     return MCLSGPU_OK;
@@ -528,6 +538,18 @@ int mclsgpu_domain_export(mclsgpu_domain* dom, int64_t* nnz_out, int64_t* rowptr
     if (weights) cudaMemcpyAsync(weights, dom->w, size_t(dom->n) * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(dom->ctx, e, "domain export");
+}
+
+int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info) {
+    if (!dom || !info || info->size < sizeof(mclsgpu_domain_info)) return MCLSGPU_ERR_INVALID_ARG;
+    info->record_format = dom->stencil_k ? MCLSGPU_RECORD_STENCIL : MCLSGPU_RECORD_PACKED;
+    info->rows = dom->n;
+    info->entries = dom->D.nnz;
+    info->record_bytes = dom->p.precision == MCLSGPU_FP32 ? dom->slots * 8 : 0;
+    info->max_row_entries = dom->max_row;
+    info->stencil_offsets = dom->stencil_k;
+    info->operator_dia = dom->op->dia_k;
+    return MCLSGPU_OK;
 }
 
 int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed) {

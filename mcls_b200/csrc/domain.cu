@@ -260,7 +260,7 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
         }
     }
     // SELL-32 copy for the forward tally source (c = H b per solve).
-    if (dom->p.direction == MCLSGPU_FORWARD) {
+    if (dom->p.direction == MCLSGPU_FORWARD && !dom->stencil_k) {
         if ((rc = csr_to_sell(ctx, D, dom->DS))) return rc;
     }
     // Transposed domain for the adjoint expected-value estimator.

@@ -68,6 +68,11 @@ struct mclsgpu_operator {
     mclsgpu_context* ctx = nullptr;
     mclsgpu::DevCsr A;
     mclsgpu::DevSell S;           // the same matrix as SELL-32 (residual kernels)
+    // Stencil operators (every column is row + dia_off[j], at most 16 offsets):
+    // values by diagonal, dia_val[j * n + r] = A(r, r + dia_off[j]) or 0.
+    int dia_k = 0;
+    int dia_off[16] = {0};
+    double* dia_val = nullptr;
     double* dinv = nullptr;       // reciprocal diagonal (built on demand)
     uint64_t serial = 0;          // identity for "operator changed" checks
 };
@@ -200,6 +205,11 @@ int point_jacobi_csr(mclsgpu_context* ctx, int n, const double* dinv,
                      DevCsr& P);
 // SELL-32 copy of a CSR matrix (set-up).
 int csr_to_sell(mclsgpu_context* ctx, const DevCsr& A, DevSell& S);
+// Sorted distinct column offsets (col - row) of A, at most 16 (*K = 0 if more).
+int collect_offsets(mclsgpu_context* ctx, const DevCsr& A, int* offsets, int* K);
+// Diagonal-offset values of a stencil matrix (K offsets): val[j*n + r].
+int csr_to_dia(mclsgpu_context* ctx, const DevCsr& A, int K, const int* offsets,
+               double** val);
 // y = A x over a SELL-32 matrix.
 void sell_spmv(cudaStream_t s, const DevSell& A, const double* x, double* y);
 // Exclusive scan of set-up counts into rp[0..n]; *total = sum.

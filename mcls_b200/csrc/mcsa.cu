@@ -48,25 +48,48 @@ inline int grid_for(long long work, int threads = 256, int cap = 148 * 16) {
     return int(g > cap ? cap : g);
 }
 
-// Row r of a SELL-32 matrix: first entry index and width (entries at
-// o + 32k).  Padding entries have value 0 and add exactly nothing, so the
-// sums equal the CSR sums in column order.
-__device__ __forceinline__ void sell_row(const int* off, int r, int& o, int& w) {
-    const int a = off[r >> 5];
-    o = a + (r & 31);
-    w = (off[(r >> 5) + 1] - a) >> 5;
-}
+// Row dot products A(r,:) . f(col) over the two operator layouts.  Both visit
+// a row's entries in ascending column order with FMA accumulation, and their
+// padding entries contribute a product with 0 (which adds exactly nothing),
+// so both return the CSR sum bit for bit.
+struct SellView {  // SELL-32
+    const int* off;
+    const int* col;
+    const double* val;
+    int n;
+    template <class F>
+    __device__ __forceinline__ double dot(int r, F f) const {
+        const int a = off[r >> 5];
+        const int o = a + (r & 31), w = (off[(r >> 5) + 1] - a) >> 5;
+        double s = 0.0;
+        for (int k = 0; k < w; ++k) s = fma(val[o + 32 * k], f(col[o + 32 * k]), s);
+        return s;
+    }
+};
+
+struct DiaView {  // stencil operator stored by diagonal offset (no indices)
+    const double* val;
+    int n;
+    int k;
+    int off[16];
+    template <class F>
+    __device__ __forceinline__ double dot(int r, F f) const {
+        double s = 0.0;
+#pragma unroll 4
+        for (int j = 0; j < k; ++j) {
+            const int c = r + off[j];
+            if (unsigned(c) < unsigned(n)) s = fma(val[size_t(j) * n + r], f(c), s);
+        }
+        return s;
+    }
+};
 
 // rp = (b - A x) [* dinv]   (LinearProblem::updatePrecResidual, :410-442)
-__global__ void __launch_bounds__(256) k_residual(const int* off, const int* col,
-                                                  const double* val, int n, const double* x,
-                                                  const double* b, const double* dinv,
-                                                  double* out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int o, w;
-        sell_row(off, i, o, w);
-        double s = 0.0;
-        for (int k = 0; k < w; ++k) s = fma(val[o + 32 * k], x[col[o + 32 * k]], s);
+template <class Op>
+__global__ void __launch_bounds__(256) k_residual(Op A, const double* x, const double* b,
+                                                  const double* dinv, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        const double s = A.dot(i, [&](int j) { return x[j]; });
         double r = b[i] - s;
         out[i] = dinv ? dinv[i] * r : r;
     }
@@ -162,17 +185,12 @@ constexpr int kFusedThreads = 256;
 // Richardson smoothing fused with the residual: x2 = x + w rp (rounded as the
 // separate update would be) and rp2 = PL (b - A x2), reading x + w rp at the
 // neighbours on the fly.
+template <class Op>
 __global__ void __launch_bounds__(kFusedThreads) k_richardson_residual(
-    const int* off, const int* col, const double* val, int n, const double* b,
-    const double* dinv, const double* x, const double* r, double w, double* x2, double* r2) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int o, wd;
-        sell_row(off, i, o, wd);
-        double s = 0.0;
-        for (int k = 0; k < wd; ++k) {
-            const int j = col[o + 32 * k];
-            s = fma(val[o + 32 * k], __dadd_rn(x[j], __dmul_rn(w, r[j])), s);
-        }
+    Op A, const double* b, const double* dinv, const double* x, const double* r, double w,
+    double* x2, double* r2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        const double s = A.dot(i, [&](int j) { return __dadd_rn(x[j], __dmul_rn(w, r[j])); });
         const double res = b[i] - s;
         r2[i] = dinv ? dinv[i] * res : res;
         x2[i] = __dadd_rn(x[i], __dmul_rn(w, r[i]));
@@ -180,9 +198,6 @@ __global__ void __launch_bounds__(kFusedThreads) k_richardson_residual(
 }
 
 struct ResidArgs {
-    const int* rp;
-    const int* ci;
-    const double* v;
     int n;
     const double* b;
     const double* dinv;       // null: no left preconditioner
@@ -229,24 +244,27 @@ __device__ __forceinline__ double corrected(const ResidArgs& a, int j, double in
     return xj;
 }
 
-// x = x2 + delta, rp = PL (b - A x), |rp|^2, then (last block) the MCSA
-// convergence check, the stream epoch, the walk timing, the work-queue reset
-// and the loop condition.
-__global__ void __launch_bounds__(kFusedThreads) k_update_residual(ResidArgs a) {
+// x = x2 + delta (the MC correction applied state by state).
+__global__ void __launch_bounds__(kFusedThreads) k_apply_correction(ResidArgs a) {
+    const double inv = a.sc[2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+        a.xout[i] = corrected(a, i, inv);
+}
+
+// rp = PL (b - A x), |rp|^2, then (last block) the MCSA convergence check,
+// the stream epoch, the walk timing, the work-queue reset and the loop
+// condition.
+template <class Op>
+__global__ void __launch_bounds__(kFusedThreads) k_residual_norm(Op A, ResidArgs a) {
     __shared__ double warp_sum[kFusedThreads / 32];
     __shared__ bool last;
-    const double inv = a.sc[2];
+    const double* x = a.xout;
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        double s = 0.0;
-        int o, w;
-        sell_row(a.rp, i, o, w);
-        for (int k = 0; k < w; ++k)
-            s = fma(a.v[o + 32 * k], corrected(a, a.ci[o + 32 * k], inv), s);
+        const double s = A.dot(i, [&](int j) { return x[j]; });
         const double res = a.b[i] - s;
         const double r = a.dinv ? a.dinv[i] * res : res;
         a.rout[i] = r;
-        a.xout[i] = corrected(a, i, inv);
         acc = fma(r, r, acc);
     }
     for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
@@ -307,11 +325,35 @@ __global__ void k_mcsa_init(McsaState* st, const double* src_sumsq, double tol, 
 }  // namespace
 
 // ---------------------------------------------------------------------------
+static SellView sell_view(const mclsgpu_operator* op) {
+    return SellView{op->S.off, op->S.col, op->S.val, op->S.n};
+}
+
+static DiaView dia_view(const mclsgpu_operator* op) {
+    DiaView v{};
+    v.val = op->dia_val;
+    v.n = op->A.n;
+    v.k = op->dia_k;
+    for (int j = 0; j < 16; ++j) v.off[j] = op->dia_off[j];
+    return v;
+}
+
+// Launch `kern<Op>` on the operator's fastest layout: diagonal-offset values
+// for stencil operators, SELL-32 otherwise.
+#define MCLSGPU_LAUNCH_OP(op, grid, threads, stream, kern, ...)                        \
+    do {                                                                               \
+        if ((op)->dia_k)                                                               \
+            kern<DiaView><<<grid, threads, 0, stream>>>(dia_view(op), __VA_ARGS__);    \
+        else                                                                           \
+            kern<SellView><<<grid, threads, 0, stream>>>(sell_view(op), __VA_ARGS__);  \
+    } while (0)
+
 // rp = PL (b - A PR x)
 static void update_prec_residual(mclsgpu_domain* dom, const double* x, const double* b,
                                  double* rp_out) {
     cudaStream_t s = dom->ctx->stream;
-    const mclsgpu::DevSell& A = dom->op->S;
+    const mclsgpu_operator* op = dom->op;
+    const int grid = grid_for(op->A.n, 256, 148 * 8);
     const double* xin = x;
     if (dom->right) {
         spmv(s, dom->right->P, x, dom->tmp2);
@@ -319,14 +361,11 @@ static void update_prec_residual(mclsgpu_domain* dom, const double* x, const dou
     }
     mclsgpu_precond* L = dom->left;
     if (!L) {
-        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, xin, b,
-                                                              nullptr, rp_out);
+        MCLSGPU_LAUNCH_OP(op, grid, 256, s, k_residual, xin, b, nullptr, rp_out);
     } else if (L->kind == MCLSGPU_PREC_POINT_JACOBI) {
-        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, xin, b,
-                                                              L->diag, rp_out);
+        MCLSGPU_LAUNCH_OP(op, grid, 256, s, k_residual, xin, b, L->diag, rp_out);
     } else {
-        k_residual<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, xin, b,
-                                                              nullptr, dom->tmp);
+        MCLSGPU_LAUNCH_OP(op, grid, 256, s, k_residual, xin, b, nullptr, dom->tmp);
         spmv(s, L->P, dom->tmp, rp_out);
     }
 }
@@ -474,19 +513,15 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
                                                dom->resid_cap, ctx->d_status);
         return;
     }
-    const mclsgpu::DevSell& A = dom->op->S;
+    const mclsgpu_operator* op = dom->op;
     const double* dinv = dom->left ? dom->left->diag : nullptr;
     const int grid = fused_grid(dom);
-    k_richardson_residual<<<grid, kFusedThreads, 0, s>>>(A.off, A.col, A.val, n, dom->b, dinv, dom->x,
-                                                         dom->rp, mp->richardson_omega, dom->x2,
-                                                         dom->rp2);
+    MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_richardson_residual, dom->b, dinv, dom->x,
+                      dom->rp, mp->richardson_omega, dom->x2, dom->rp2);
     const mclsgpu_mc_params& p = dom->p;
     const bool adj_ev = p.direction == MCLSGPU_ADJOINT && p.estimator == MCLSGPU_EXPECTED_VALUE;
     enqueue_mc(dom, dom->rp2, dom->x2, 1, 0, nullptr, nullptr, nullptr, nullptr, true);
     ResidArgs a{};
-    a.rp = A.off;  // SELL-32 operator: rp = slice offsets, ci/v = entries
-    a.ci = A.col;
-    a.v = A.val;
     a.n = n;
     a.b = dom->b;
     a.dinv = dinv;
@@ -519,7 +554,8 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
     a.d_nh = dom->d_nh;
     a.handle = handle;
     a.use_cond = use_cond;
-    k_update_residual<<<grid, kFusedThreads, 0, s>>>(a);
+    k_apply_correction<<<grid, kFusedThreads, 0, s>>>(a);
+    MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_residual_norm, a);
 }
 
 // Build the CUDA graph of the MCSA loop (WHILE node, one iteration per body).

@@ -209,6 +209,40 @@ __global__ void __launch_bounds__(256) k_forward_rec(const double* v, int n, dou
     }
 }
 
+struct StencilOffsets {
+    int off[16];
+};
+
+// Stencil records: the tally source H b is rebuilt from the record itself,
+// |h_j| = W * (cdf_j - cdf_prev), so the pass reads 32 bytes per row instead
+// of the FP64 domain.
+__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, double omega,
+                                                             int has, int ev, int K,
+                                                             StencilOffsets so, int words,
+                                                             uint32_t* rec, double* y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t* r = rec + size_t(i) * words;
+        double c;
+        if (!ev) {
+            c = load_src(v, i, omega, has);
+        } else {
+            const float W = __uint_as_float(r[0]);
+            float prev = 0.f;
+            c = 0.0;
+            for (int j = 0; j < K; ++j) {
+                const float q = __uint_as_float(r[2 + j]);
+                if (isnan(q)) continue;
+                const float a = fabsf(q);
+                const float h = W * (a - prev);
+                prev = a;
+                c = fma(double(q < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
+            }
+        }
+        r[1] = __float_as_uint(__double2float_rn(c));
+        y[i] = 0.0;
+    }
+}
+
 __global__ void k_forward_nh(int* d_nh, int nh, double* sc) {
     *d_nh = nh;
     sc[0] = 1.0;
@@ -275,10 +309,18 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     const int ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
     if (!fused) k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
     if (p.precision == MCLSGPU_FP32) {
-        k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, omega, has_omega, ev,
-                                                               dom->DS.off, dom->DS.col,
-                                                               dom->DS.val, dom->slots, dom->rec,
-                                                               dom->y64);
+        if (dom->stencil_k) {
+            StencilOffsets so{};
+            for (int j = 0; j < 16; ++j) so.off[j] = dom->stencil_off[j];
+            k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
+                v, n, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots,
+                reinterpret_cast<uint32_t*>(dom->rec), dom->y64);
+        } else {
+            k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, omega, has_omega, ev,
+                                                                   dom->DS.off, dom->DS.col,
+                                                                   dom->DS.val, dom->slots,
+                                                                   dom->rec, dom->y64);
+        }
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);

@@ -598,6 +598,37 @@ int csr_to_sell(mclsgpu_context* ctx, const DevCsr& A, DevSell& S) {
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "SELL build");
 }
 
+namespace {
+
+struct DiaOffsets {
+    int off[16];
+};
+
+__global__ void k_fill_dia(const int* rp, const int* ci, const double* v, int n, int K,
+                           DiaOffsets o, double* val) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        for (int j = 0; j < K; ++j) val[size_t(j) * n + r] = 0.0;
+        for (int k = rp[r]; k < rp[r + 1]; ++k) {
+            const int d = ci[k] - r;
+            for (int j = 0; j < K; ++j)
+                if (o.off[j] == d) val[size_t(j) * n + r] = v[k];
+        }
+    }
+}
+
+}  // namespace
+
+int csr_to_dia(mclsgpu_context* ctx, const DevCsr& A, int K, const int* offsets, double** val) {
+    *val = nullptr;
+    cudaError_t e = dmalloc(val, size_t(K) * A.n);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc DIA");
+    DiaOffsets o{};
+    for (int j = 0; j < K && j < 16; ++j) o.off[j] = offsets[j];
+    k_fill_dia<<<grid_for(A.n), 256, 0, ctx->stream>>>(A.rp, A.ci, A.v, A.n, K, o, *val);
+    e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "DIA build");
+}
+
 void sell_spmv(cudaStream_t s, const DevSell& A, const double* x, double* y) {
     k_sell_spmv<<<grid_for(A.n, 256, 148 * 8), 256, 0, s>>>(A.off, A.col, A.val, A.n, x, y);
 }
