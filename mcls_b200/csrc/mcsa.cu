@@ -67,22 +67,30 @@ struct SellView {  // SELL-32
     }
 };
 
-struct DiaView {  // stencil operator stored by diagonal offset (no indices)
+// Stencil operator stored by diagonal offset (no indices).  KK > 0 fixes the
+// number of offsets at compile time so the row loop unrolls and every load of
+// the row is issued before the first product.
+template <int KK>
+struct DiaViewT {
     const double* val;
     int n;
     int k;
     int off[16];
     template <class F>
     __device__ __forceinline__ double dot(int r, F f) const {
+        constexpr int kmax = KK > 0 ? KK : 16;
+        const int kk = KK > 0 ? KK : k;
         double s = 0.0;
-#pragma unroll 4
-        for (int j = 0; j < k; ++j) {
+#pragma unroll
+        for (int j = 0; j < kmax; ++j) {
+            if (j >= kk) break;
             const int c = r + off[j];
             if (unsigned(c) < unsigned(n)) s = fma(val[size_t(j) * n + r], f(c), s);
         }
         return s;
     }
 };
+using DiaView = DiaViewT<0>;
 
 // rp = (b - A x) [* dinv]   (LinearProblem::updatePrecResidual, :410-442)
 template <class Op>
@@ -329,8 +337,9 @@ static SellView sell_view(const mclsgpu_operator* op) {
     return SellView{op->S.off, op->S.col, op->S.val, op->S.n};
 }
 
-static DiaView dia_view(const mclsgpu_operator* op) {
-    DiaView v{};
+template <int KK>
+static DiaViewT<KK> dia_view(const mclsgpu_operator* op) {
+    DiaViewT<KK> v{};
     v.val = op->dia_val;
     v.n = op->A.n;
     v.k = op->dia_k;
@@ -339,13 +348,26 @@ static DiaView dia_view(const mclsgpu_operator* op) {
 }
 
 // Launch `kern<Op>` on the operator's fastest layout: diagonal-offset values
-// for stencil operators, SELL-32 otherwise.
-#define MCLSGPU_LAUNCH_OP(op, grid, threads, stream, kern, ...)                        \
-    do {                                                                               \
-        if ((op)->dia_k)                                                               \
-            kern<DiaView><<<grid, threads, 0, stream>>>(dia_view(op), __VA_ARGS__);    \
-        else                                                                           \
-            kern<SellView><<<grid, threads, 0, stream>>>(sell_view(op), __VA_ARGS__);  \
+// for stencil operators (unrolled for the 5-, 7- and 9-point stencils),
+// SELL-32 otherwise.
+#define MCLSGPU_LAUNCH_OP(op, grid, threads, stream, kern, ...)                              \
+    do {                                                                                     \
+        switch ((op)->dia_k) {                                                               \
+            case 0:                                                                          \
+                kern<SellView><<<grid, threads, 0, stream>>>(sell_view(op), __VA_ARGS__);    \
+                break;                                                                       \
+            case 5:                                                                          \
+                kern<DiaViewT<5>><<<grid, threads, 0, stream>>>(dia_view<5>(op), __VA_ARGS__); \
+                break;                                                                       \
+            case 7:                                                                          \
+                kern<DiaViewT<7>><<<grid, threads, 0, stream>>>(dia_view<7>(op), __VA_ARGS__); \
+                break;                                                                       \
+            case 9:                                                                          \
+                kern<DiaViewT<9>><<<grid, threads, 0, stream>>>(dia_view<9>(op), __VA_ARGS__); \
+                break;                                                                       \
+            default:                                                                         \
+                kern<DiaView><<<grid, threads, 0, stream>>>(dia_view<0>(op), __VA_ARGS__);   \
+        }                                                                                    \
     } while (0)
 
 // rp = PL (b - A PR x)

@@ -225,6 +225,31 @@ __global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, in
         double c;
         if (!ev) {
             c = load_src(v, i, omega, has);
+            r[1] = __float_as_uint(__double2float_rn(c));
+        } else if (words == 8) {
+            // One 256-bit load and one 256-bit store of the whole record.
+            uint32_t q[8];
+            asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]),
+                           "=r"(q[5]), "=r"(q[6]), "=r"(q[7])
+                         : "l"(r));
+            const float W = __uint_as_float(q[0]);
+            float prev = 0.f;
+            c = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const float qv = __uint_as_float(q[2 + j]);
+                if (j >= K || isnan(qv)) continue;
+                const float a = fabsf(qv);
+                const float h = W * (a - prev);
+                prev = a;
+                c = fma(double(qv < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
+            }
+            q[1] = __float_as_uint(__double2float_rn(c));
+            asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
+                         "r"(q[1]), "r"(q[2]), "r"(q[3]), "r"(q[4]), "r"(q[5]), "r"(q[6]),
+                         "r"(q[7])
+                         : "memory");
         } else {
             const float W = __uint_as_float(r[0]);
             float prev = 0.f;
@@ -237,8 +262,8 @@ __global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, in
                 prev = a;
                 c = fma(double(q < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
             }
+            r[1] = __float_as_uint(__double2float_rn(c));
         }
-        r[1] = __float_as_uint(__double2float_rn(c));
         y[i] = 0.0;
     }
 }

@@ -103,7 +103,83 @@ struct WalkOccupancy {
     static constexpr int kMinBlocks = S <= 8 ? 8 : (S <= 24 ? 4 : 2);
 };
 
+// One transition of a history at state s (DomainTransporter::transport's
+// loop body): tally at the pre-transition state, read the state's record,
+// draw u, select the first entry whose CDF value is >= u, update the state
+// and the weight.
 template <int S, int DIR, bool ST>
+__device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, int& s, float& w,
+                                          uint64_t& x, float& acc, float& comp, int k) {
+    // One record: S/4 256-bit loads that bypass L1 (each step touches exactly
+    // the record's own sectors).
+    const char* r = rec + size_t(s) * (S * 8);
+    uint32_t q[2 * S];
+#pragma unroll
+    for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
+    if (DIR == MCLSGPU_ADJOINT) {
+        // FP32 weight, FP64 reduction (fire-and-forget RED.ADD.F64).
+        if (k > 0) atomicAdd(&a.y64[s], double(w));
+    } else {
+        // Kahan-compensated FP32 history sum; the tally source of the state
+        // rides in the record header (slot 0, second word).
+        const float term = w * __uint_as_float(q[1]) - comp;
+        const float t = acc + term;
+        comp = (t - acc) - term;
+        acc = t;
+    }
+    x = xs_step(x);
+    const float u = canonical32(x);
+    const float Wt = __uint_as_float(q[0]);
+    if constexpr (!ST) {
+        unsigned sel = q[3];  // slot 1 (first entry)
+        bool found = __uint_as_float(q[2]) >= u;
+#pragma unroll
+        for (int t = 2; t < S; ++t) {
+            const bool c = !found && __uint_as_float(q[2 * t]) >= u;
+            sel = c ? q[2 * t + 1] : sel;
+            found = found || c;
+        }
+        w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
+        s = int(sel & 0x7fffffffu);
+    } else {
+        // Stencil slots: first |cdf_j| >= u (NaN slots never match); the next
+        // state is s + offset_j, the sign of h_j is the sign bit of the slot.
+        int dsel = 0;
+        unsigned neg = 0u;
+        bool found = false;
+#pragma unroll
+        for (int j = 0; j < 2 * S - 2; ++j) {
+            const bool c = !found && fabsf(__uint_as_float(q[2 + j])) >= u;
+            dsel = c ? a.stoff[j] : dsel;
+            neg = c ? (q[2 + j] & 0x80000000u) : neg;
+            found = found || c;
+        }
+        w = neg ? -(w * Wt) : w * Wt;
+        s += dsel;
+    }
+}
+
+// Starting state, weight and stream of history e.
+template <int DIR>
+__device__ __forceinline__ void walk_start(const WalkArgs& a, int e, uint64_t ekey, float wnorm,
+                                           int& s, float& w, uint64_t& x) {
+    if (DIR == MCLSGPU_ADJOINT) {
+        const int sv = a.start[e];
+        s = sv & 0x7fffffff;
+        w = sv < 0 ? -wnorm : wnorm;
+    } else {
+        s = e / a.per;
+        w = 1.f;
+    }
+    x = history_state(a, ekey, e);
+}
+
+// FIXED: every history takes exactly History Length steps (no weight
+// cutoff), so the lanes of a warp start and finish their histories together:
+// the warp takes 32 histories at a time and runs them without per-step
+// termination checks.  Otherwise lanes refill one by one from the queue as
+// their histories terminate.
+template <int S, int DIR, bool ST, bool FIXED>
 __global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(WalkArgs a) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
@@ -116,100 +192,69 @@ __global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(Walk
         s_wnorm = float(a.sc[0]);
     }
     __syncthreads();
-    const uint4* __restrict__ rec = reinterpret_cast<const uint4*>(a.rec);
+    const char* rec = reinterpret_cast<const char*>(a.rec);
     if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
-    int s = 0, s0 = 0, k = 0;
-    float w = 0.f, wcut = 0.f, acc = 0.f, comp = 0.f;
-    uint64_t x = 0;
-    bool alive = false, drained = false;
     unsigned steps = 0;
-    while (true) {
-        const unsigned need = __ballot_sync(kFull, !alive);
-        if (need && !drained) {
-            const int leader = __ffs(need) - 1;
-            const int cnt = __popc(need);
-            const int nh = s_nh;
+    if constexpr (FIXED) {
+        const int L = a.L;
+        while (true) {
             int base = 0;
-            if (lane == leader) base = atomicAdd(a.d_counter, cnt);
-            base = __shfl_sync(kFull, base, leader);
-            if (base + cnt >= nh) drained = true;
-            if (!alive) {
-                const int e = base + __popc(need & ((1u << lane) - 1));
-                if (e < nh) {
-                    if (DIR == MCLSGPU_ADJOINT) {
-                        const int sv = a.start[e];
-                        s = sv & 0x7fffffff;
-                        w = sv < 0 ? -s_wnorm : s_wnorm;
-                    } else {
-                        s = e / a.per;
-                        w = 1.f;
-                        acc = 0.f;
-                        comp = 0.f;
-                    }
-                    s0 = s;
-                    wcut = a.cutoff * fabsf(w);
-                    x = history_state(a, s_ekey, e);
-                    k = 0;
-                    alive = true;
-                }
+            if (lane == 0) base = atomicAdd(a.d_counter, 32);
+            base = __shfl_sync(kFull, base, 0);
+            const int nh = s_nh;
+            if (base >= nh) break;
+            const int e = base + lane;
+            const bool alive = e < nh;
+            int s = 0;
+            float w = 0.f, acc = 0.f, comp = 0.f;
+            uint64_t x = 0;
+            if (alive) walk_start<DIR>(a, e, s_ekey, s_wnorm, s, w, x);
+            const int s0 = s;
+            for (int k = 0; k < L; ++k)
+                if (alive) walk_step<S, DIR, ST>(a, rec, s, w, x, acc, comp, k);
+            if (alive) {
+                steps += L;
+                if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y64[s0], double(acc) - double(comp));
             }
         }
-        if (!__any_sync(kFull, alive)) break;
-        if (alive) {
-            // One packed record: S/4 256-bit loads that bypass L1 (each step
-            // touches exactly the record's own sectors).
-            const char* r = reinterpret_cast<const char*>(rec) + size_t(s) * (S * 8);
-            uint32_t q[2 * S];
-#pragma unroll
-            for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
-            // Tally at the pre-transition state.
-            if (DIR == MCLSGPU_ADJOINT) {
-                // FP32 weight, FP64 reduction (fire-and-forget RED.ADD.F64).
-                if (k > 0) atomicAdd(&a.y64[s], double(w));
-            } else {
-                // Kahan-compensated FP32 history sum; the tally source of the
-                // state rides in the record header (slot 0, second word).
-                const float term = w * __uint_as_float(q[1]) - comp;
-                const float t = acc + term;
-                comp = (t - acc) - term;
-                acc = t;
-            }
-            x = xs_step(x);
-            const float u = canonical32(x);
-            const float Wt = __uint_as_float(q[0]);
-            if constexpr (!ST) {
-                unsigned sel = q[3];  // slot 1 (first entry)
-                bool found = __uint_as_float(q[2]) >= u;
-#pragma unroll
-                for (int t = 2; t < S; ++t) {
-                    const bool c = !found && __uint_as_float(q[2 * t]) >= u;
-                    sel = c ? q[2 * t + 1] : sel;
-                    found = found || c;
+    } else {
+        int s = 0, s0 = 0, k = 0;
+        float w = 0.f, wcut = 0.f, acc = 0.f, comp = 0.f;
+        uint64_t x = 0;
+        bool alive = false, drained = false;
+        while (true) {
+            const unsigned need = __ballot_sync(kFull, !alive);
+            if (need && !drained) {
+                const int leader = __ffs(need) - 1;
+                const int cnt = __popc(need);
+                const int nh = s_nh;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(a.d_counter, cnt);
+                base = __shfl_sync(kFull, base, leader);
+                if (base + cnt >= nh) drained = true;
+                if (!alive) {
+                    const int e = base + __popc(need & ((1u << lane) - 1));
+                    if (e < nh) {
+                        walk_start<DIR>(a, e, s_ekey, s_wnorm, s, w, x);
+                        acc = 0.f;
+                        comp = 0.f;
+                        s0 = s;
+                        wcut = a.cutoff * fabsf(w);
+                        k = 0;
+                        alive = true;
+                    }
                 }
-                w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
-                s = int(sel & 0x7fffffffu);
-            } else {
-                // Stencil slots: first |cdf_j| >= u (NaN slots never match);
-                // the next state is s + offset_j, the sign of h_j is the sign
-                // bit of the slot.
-                int dsel = 0;
-                unsigned neg = 0u;
-                bool found = false;
-#pragma unroll
-                for (int j = 0; j < 2 * S - 2; ++j) {
-                    const bool c = !found && fabsf(__uint_as_float(q[2 + j])) >= u;
-                    dsel = c ? a.stoff[j] : dsel;
-                    neg = c ? (q[2 + j] & 0x80000000u) : neg;
-                    found = found || c;
-                }
-                w = neg ? -(w * Wt) : w * Wt;
-                s += dsel;
             }
-            ++k;
-            ++steps;
-            if (k >= a.L || fabsf(w) < wcut) {
-                alive = false;
-                if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y64[s0], double(acc) - double(comp));
+            if (!__any_sync(kFull, alive)) break;
+            if (alive) {
+                walk_step<S, DIR, ST>(a, rec, s, w, x, acc, comp, k);
+                ++k;
+                ++steps;
+                if (k >= a.L || fabsf(w) < wcut) {
+                    alive = false;
+                    if (DIR == MCLSGPU_FORWARD)
+                        atomicAdd(&a.y64[s0], double(acc) - double(comp));
+                }
             }
         }
     }
@@ -297,26 +342,26 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
     atomicAdd(a.d_steps, steps);
 }
 
-template <int S, int DIR, bool ST>
+template <int S, int DIR, bool ST, bool FX>
 int blocks_per_sm() {
     static int cached = 0;
     if (!cached) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR, ST>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR, ST, FX>, 256, 0);
         cached = b > 0 ? b : 1;
     }
     return cached;
 }
 
 // Dispatch on the record stride; `launch` false only caches the occupancy.
-template <int DIR, bool ST>
+template <int DIR, bool ST, bool FX>
 void launch32_slots(int slots, const WalkArgs& a, int sms, cudaStream_t st, bool launch) {
-#define MCLSGPU_WALK_CASE(SL)                                                        \
-    case SL:                                                                         \
-        if (launch)                                                                  \
-            walk32<SL, DIR, ST><<<sms * blocks_per_sm<SL, DIR, ST>(), 256, 0, st>>>(a); \
-        else                                                                         \
-            blocks_per_sm<SL, DIR, ST>();                                            \
+#define MCLSGPU_WALK_CASE(SL)                                                                  \
+    case SL:                                                                                   \
+        if (launch)                                                                            \
+            walk32<SL, DIR, ST, FX><<<sms * blocks_per_sm<SL, DIR, ST, FX>(), 256, 0, st>>>(a); \
+        else                                                                                   \
+            blocks_per_sm<SL, DIR, ST, FX>();                                                  \
         break;
     if (ST) {
         switch (slots) {
@@ -342,13 +387,18 @@ void dispatch_walk32(const mclsgpu_domain* dom, const WalkArgs& a, bool launch) 
     const int sms = dom->ctx->num_sms;
     cudaStream_t st = dom->ctx->stream;
     const bool adj = dom->p.direction == MCLSGPU_ADJOINT;
+    const bool fixed = !(dom->p.weight_cutoff > 0.0);
+#define MCLSGPU_WALK_DIR(DIRV, STV)                                                    \
+    (fixed ? launch32_slots<DIRV, STV, true>(dom->slots, a, sms, st, launch)           \
+           : launch32_slots<DIRV, STV, false>(dom->slots, a, sms, st, launch))
     if (dom->stencil_k) {
-        if (adj) launch32_slots<MCLSGPU_ADJOINT, true>(dom->slots, a, sms, st, launch);
-        else launch32_slots<MCLSGPU_FORWARD, true>(dom->slots, a, sms, st, launch);
+        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, true);
+        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, true);
     } else {
-        if (adj) launch32_slots<MCLSGPU_ADJOINT, false>(dom->slots, a, sms, st, launch);
-        else launch32_slots<MCLSGPU_FORWARD, false>(dom->slots, a, sms, st, launch);
+        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, false);
+        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, false);
     }
+#undef MCLSGPU_WALK_DIR
 }
 
 }  // namespace

@@ -77,3 +77,25 @@ def test_stencil_records_rejected_for_irregular_rows(ctx):
                       sample_ratio=4.0)
     x, st = dom.mc_solve(rng.uniform(0, 1, n))
     assert np.all(np.isfinite(x))
+
+
+@pytest.mark.parametrize("direction", [capi.ADJOINT, capi.FORWARD])
+def test_fp32_weight_cutoff_walks(ctx, direction):
+    # Variable-length histories take the lane-refill loop: fewer steps than
+    # the History Length cap, and an unbiased estimate of the same quantity.
+    A = P.poisson2d(20)
+    b = np.linspace(0.5, 1.5, A.shape[0])
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    kw = dict(precision=capi.FP32, direction=direction, sample_ratio=8.0, history_length=60)
+    d_cut = capi.Domain(ctx, op, pc, weight_cutoff=0.2, **kw)
+    x, st = d_cut.mc_solve(b)
+    nh = st["histories"]
+    assert 0 < st["walk_steps"] < 60 * nh
+    assert np.all(np.isfinite(x))
+    d_full = capi.Domain(ctx, op, pc, **kw)
+    xf, sf = d_full.mc_solve(b)
+    assert sf["walk_steps"] == 60 * sf["histories"]
+    # Jacobi-Poisson interior weights stay 1, so the cutoff only trims walks
+    # that lose weight at the boundary: the two estimates agree to MC noise.
+    assert np.linalg.norm(x - xf) / np.linalg.norm(xf) < 0.2
