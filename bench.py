@@ -220,6 +220,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iters", type=int, default=20000)
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--host-loop", action="store_true",
                     help="host-driven MCSA loop (for profilers that cannot see kernels "
                          "inside conditional graph nodes)")
@@ -252,6 +253,14 @@ def main():
                           host_loop=1 if args.host_loop else 0)
     bt = torch.tensor(b, device=f"cuda:{local}", dtype=torch.float64)
     xt = torch.zeros_like(bt)
+    tuned = None
+    if fp == capi.FP32 and not args.no_autotune:
+        # Launch-shape autotuning on the workload's own right-hand side
+        # (untimed set-up, like the domain build).
+        dt = torch.tensor((1.0 / A.diagonal()) * b, device=f"cuda:{local}", dtype=torch.float64)
+        torch.cuda.synchronize()
+        tuned = dom.autotune(dt.data_ptr(), reps=2)
+        del dt
 
     def device_step():
         dom.reseed(seed)
@@ -311,6 +320,7 @@ def main():
         "config": {"workload": cfgd["workload"], "n": n, "nnz": int(A.nnz),
                    "histories_per_iteration": int(s0["histories"] // max(s0["iterations"], 1)),
                    "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+                   "walk_launch": tuned,
                    "l2": "inputs larger than L2 (no flush)",
                    "time_to_1e-8_s": dev_ms_max / args.steps / 1e3,
                    "iterations": s0["iterations"], "achieved_tol": s0["achieved_tol"],

@@ -222,6 +222,19 @@ typedef struct {
 } mclsgpu_domain_info;
 int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info);
 
+/* FP32 walk launch shape: histories carried per lane (1 or 2; 2 applies to
+ * fixed-length histories on records of at most 64 bytes) and threads per
+ * block (128 or 256).  No counterpart in the reference. */
+int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane,
+                              int block_size);
+/* Autotuner: times every launch shape on `reps` Monte Carlo solves of the
+ * device vector rhs_dev (n entries), keeps the fastest walk and reports it.
+ * The random stream position is restored afterwards.  No counterpart in the
+ * reference. */
+int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps,
+                            int* histories_per_lane, int* block_size,
+                            double* walk_ms);
+
 /* Replace the stream seed/position (restart the reproducible stream). */
 int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed);
 /* Per-rank Xorshift seed as PRNG<RNG>(rank) derives it

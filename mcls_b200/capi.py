@@ -118,7 +118,7 @@ EXPORTS = [
     "mclsgpu_domain_destroy", "mclsgpu_domain_export", "mclsgpu_domain_reseed",
     "mclsgpu_rank_seed", "mclsgpu_mc_solve", "mclsgpu_mc_solve_dev", "mclsgpu_mc_trace",
     "mclsgpu_mcsa_solve", "mclsgpu_mcsa_solve_dev", "mclsgpu_domain_spectral_radius",
-    "mclsgpu_domain_query",
+    "mclsgpu_domain_query", "mclsgpu_domain_set_launch", "mclsgpu_domain_autotune",
 ]
 
 _LIB = None
@@ -164,6 +164,9 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_domain_export.argtypes = [P, C.POINTER(i64), P, P, P, P, P]
     L.mclsgpu_domain_reseed.argtypes = [P, C.c_uint64]
     L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
+    L.mclsgpu_domain_set_launch.argtypes = [P, C.c_int, C.c_int]
+    L.mclsgpu_domain_autotune.argtypes = [P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(d)]
     L.mclsgpu_rank_seed.argtypes = [C.c_uint64, C.c_int]
     L.mclsgpu_rank_seed.restype = C.c_uint64
     L.mclsgpu_mc_solve.argtypes = [P, P, P, C.c_int, C.POINTER(Stats)]
@@ -364,6 +367,18 @@ class Domain:
         d.size = C.sizeof(DomainInfo)
         self.ctx.check(self.ctx.L.mclsgpu_domain_query(self.h, C.byref(d)))
         return {k: getattr(d, k) for k, _ in d._fields_ if k != "size"}
+
+    def set_launch(self, histories_per_lane, block_size):
+        self.ctx.check(self.ctx.L.mclsgpu_domain_set_launch(self.h, histories_per_lane,
+                                                            block_size))
+
+    def autotune(self, rhs_dev_ptr, reps=3):
+        """Pick the fastest FP32 walk launch shape on a device right-hand side."""
+        hpl, blk, ms = C.c_int(), C.c_int(), C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_domain_autotune(self.h, C.c_void_p(rhs_dev_ptr), reps,
+                                                          C.byref(hpl), C.byref(blk),
+                                                          C.byref(ms)))
+        return {"histories_per_lane": hpl.value, "block_size": blk.value, "walk_ms": ms.value}
 
     def reseed(self, seed):
         self.ctx.check(self.ctx.L.mclsgpu_domain_reseed(self.h, seed))

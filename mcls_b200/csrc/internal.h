@@ -122,6 +122,9 @@ struct mclsgpu_domain {
     uint2* rec = nullptr;
     int slots = 0;
     int max_row = 0;
+    // FP32 walk launch shape (autotuned): histories per lane and block size.
+    int walk_ilp = 1;
+    int walk_block = 256;
     // Stencil records (stencil_k > 0): row r's slot j is column r + stencil_off[j].
     int stencil_k = 0;
     int stencil_off[16] = {0};

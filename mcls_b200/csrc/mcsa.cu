@@ -37,6 +37,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
                            bool fused);
 void launch_forward_setup(mclsgpu_domain* dom);
 void launch_advance_walk_pos(mclsgpu_domain* dom);
+void prepare_walk(mclsgpu_domain* dom);
 void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
                  int* tr_ev, long long* tr_start, bool fused);
 
@@ -866,6 +867,62 @@ int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_d
     int rc = check_mcsa_params(dom, params, &p);
     if (rc) return rc;
     return mcsa_solve_device(dom, b_dev, x_dev, &p, stats);
+}
+
+int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane, int block_size) {
+    if (!dom || (histories_per_lane != 1 && histories_per_lane != 2) ||
+        (block_size != 128 && block_size != 256))
+        return MCLSGPU_ERR_INVALID_ARG;
+    dom->walk_ilp = histories_per_lane;
+    dom->walk_block = block_size;
+    prepare_walk(dom);
+    dom->graph_key = -1;  // the launch shape is baked into the captured loop
+    return MCLSGPU_OK;
+}
+
+int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps,
+                            int* histories_per_lane, int* block_size, double* walk_ms) {
+    if (!dom || !rhs_dev || reps < 1) return MCLSGPU_ERR_INVALID_ARG;
+    if (dom->p.precision != MCLSGPU_FP32)
+        return set_error(dom->ctx, MCLSGPU_ERR_UNSUPPORTED, "autotune applies to FP32 walks");
+    cudaStream_t s = dom->ctx->stream;
+    unsigned long long saved[2] = {0, 0};
+    cudaMemcpyAsync(&saved[0], dom->d_epoch, sizeof(saved[0]), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&saved[1], dom->d_pos, sizeof(saved[1]), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "autotune");
+    const int shapes[4][2] = {{1, 256}, {2, 256}, {1, 128}, {2, 128}};
+    double best = 1e300;
+    int bh = 1, bb = 256;
+    for (const auto& sh : shapes) {
+        int rc = mclsgpu_domain_set_launch(dom, sh[0], sh[1]);
+        if (rc) return rc;
+        mclsgpu_stats st{};
+        st.size = sizeof(st);
+        rc = mc_solve_device(dom, rhs_dev, dom->tmp2, 1, 0, nullptr, nullptr, nullptr, nullptr,
+                             &st);  // warm-up
+        double tot = 0.0;
+        for (int r = 0; r < reps && !rc; ++r) {
+            rc = mc_solve_device(dom, rhs_dev, dom->tmp2, 1, 0, nullptr, nullptr, nullptr,
+                                 nullptr, &st);
+            tot += st.walk_ms;
+        }
+        if (rc) return rc;
+        if (tot / reps < best) {
+            best = tot / reps;
+            bh = sh[0];
+            bb = sh[1];
+        }
+    }
+    int rc = mclsgpu_domain_set_launch(dom, bh, bb);
+    cudaMemcpyAsync(dom->d_epoch, &saved[0], sizeof(saved[0]), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dom->d_pos, &saved[1], sizeof(saved[1]), cudaMemcpyHostToDevice, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "autotune");
+    if (histories_per_lane) *histories_per_lane = bh;
+    if (block_size) *block_size = bb;
+    if (walk_ms) *walk_ms = best;
+    return rc;
 }
 
 int mclsgpu_mcsa_solve(mclsgpu_domain* dom, const double* b, double* x,

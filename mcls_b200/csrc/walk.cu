@@ -179,8 +179,9 @@ __device__ __forceinline__ void walk_start(const WalkArgs& a, int e, uint64_t ek
 // the warp takes 32 histories at a time and runs them without per-step
 // termination checks.  Otherwise lanes refill one by one from the queue as
 // their histories terminate.
-template <int S, int DIR, bool ST, bool FIXED>
-__global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(WalkArgs a) {
+template <int S, int DIR, bool ST, bool FIXED, int ILP = 1>
+__global__ void __launch_bounds__(256, ILP == 1 ? WalkOccupancy<S>::kMinBlocks : 5)
+    walk32(WalkArgs a) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
     __shared__ int s_nh;
@@ -196,25 +197,41 @@ __global__ void __launch_bounds__(256, WalkOccupancy<S>::kMinBlocks) walk32(Walk
     if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
     unsigned steps = 0;
     if constexpr (FIXED) {
+        // ILP histories per lane, interleaved step by step so that each lane
+        // has ILP independent record loads in flight.
         const int L = a.L;
         while (true) {
             int base = 0;
-            if (lane == 0) base = atomicAdd(a.d_counter, 32);
+            if (lane == 0) base = atomicAdd(a.d_counter, 32 * ILP);
             base = __shfl_sync(kFull, base, 0);
             const int nh = s_nh;
             if (base >= nh) break;
-            const int e = base + lane;
-            const bool alive = e < nh;
-            int s = 0;
-            float w = 0.f, acc = 0.f, comp = 0.f;
-            uint64_t x = 0;
-            if (alive) walk_start<DIR>(a, e, s_ekey, s_wnorm, s, w, x);
-            const int s0 = s;
-            for (int k = 0; k < L; ++k)
-                if (alive) walk_step<S, DIR, ST>(a, rec, s, w, x, acc, comp, k);
-            if (alive) {
-                steps += L;
-                if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y64[s0], double(acc) - double(comp));
+            int s[ILP], s0[ILP];
+            float w[ILP], acc[ILP], comp[ILP];
+            uint64_t x[ILP];
+            bool alive[ILP];
+#pragma unroll
+            for (int m = 0; m < ILP; ++m) {
+                const int e = base + lane + 32 * m;
+                alive[m] = e < nh;
+                s[m] = 0;
+                w[m] = acc[m] = comp[m] = 0.f;
+                x[m] = 0;
+                if (alive[m]) walk_start<DIR>(a, e, s_ekey, s_wnorm, s[m], w[m], x[m]);
+                s0[m] = s[m];
+            }
+            for (int k = 0; k < L; ++k) {
+#pragma unroll
+                for (int m = 0; m < ILP; ++m)
+                    if (alive[m]) walk_step<S, DIR, ST>(a, rec, s[m], w[m], x[m], acc[m], comp[m], k);
+            }
+#pragma unroll
+            for (int m = 0; m < ILP; ++m) {
+                if (alive[m]) {
+                    steps += L;
+                    if (DIR == MCLSGPU_FORWARD)
+                        atomicAdd(&a.y64[s0[m]], double(acc[m]) - double(comp[m]));
+                }
             }
         }
     } else {
@@ -342,28 +359,32 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
     atomicAdd(a.d_steps, steps);
 }
 
-template <int S, int DIR, bool ST, bool FX>
-int blocks_per_sm() {
-    static int cached = 0;
-    if (!cached) {
+template <int S, int DIR, bool ST, bool FX, int ILP>
+int blocks_per_sm(int block) {
+    static int cached[5] = {0, 0, 0, 0, 0};  // block sizes 128..1024 by log2
+    const int slot = block <= 128 ? 0 : block <= 256 ? 1 : block <= 512 ? 2 : 3;
+    if (!cached[slot]) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR, ST, FX>, 256, 0);
-        cached = b > 0 ? b : 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32<S, DIR, ST, FX, ILP>, block, 0);
+        cached[slot] = b > 0 ? b : 1;
     }
-    return cached;
+    return cached[slot];
 }
 
 // Dispatch on the record stride; `launch` false only caches the occupancy.
-template <int DIR, bool ST, bool FX>
-void launch32_slots(int slots, const WalkArgs& a, int sms, cudaStream_t st, bool launch) {
-#define MCLSGPU_WALK_CASE(SL)                                                                  \
-    case SL:                                                                                   \
-        if (launch)                                                                            \
-            walk32<SL, DIR, ST, FX><<<sms * blocks_per_sm<SL, DIR, ST, FX>(), 256, 0, st>>>(a); \
-        else                                                                                   \
-            blocks_per_sm<SL, DIR, ST, FX>();                                                  \
+// Persistent grid: as many blocks as fit on every SM at once.
+template <int DIR, bool ST, bool FX, int ILP>
+void launch32_slots(int slots, const WalkArgs& a, int sms, int block, cudaStream_t st,
+                    bool launch) {
+#define MCLSGPU_WALK_CASE(SL)                                                             \
+    case SL:                                                                              \
+        if (launch)                                                                       \
+            walk32<SL, DIR, ST, FX, ILP>                                                  \
+                <<<sms * blocks_per_sm<SL, DIR, ST, FX, ILP>(block), block, 0, st>>>(a);  \
+        else                                                                              \
+            blocks_per_sm<SL, DIR, ST, FX, ILP>(block);                                   \
         break;
-    if (ST) {
+    if (ST || ILP > 1) {
         switch (slots) {
             MCLSGPU_WALK_CASE(4)
             default:
@@ -388,9 +409,14 @@ void dispatch_walk32(const mclsgpu_domain* dom, const WalkArgs& a, bool launch) 
     cudaStream_t st = dom->ctx->stream;
     const bool adj = dom->p.direction == MCLSGPU_ADJOINT;
     const bool fixed = !(dom->p.weight_cutoff > 0.0);
-#define MCLSGPU_WALK_DIR(DIRV, STV)                                                    \
-    (fixed ? launch32_slots<DIRV, STV, true>(dom->slots, a, sms, st, launch)           \
-           : launch32_slots<DIRV, STV, false>(dom->slots, a, sms, st, launch))
+    // Two histories per lane only for fixed-length histories on records of
+    // at most 8 slots (the register budget of 5 blocks per SM).
+    const bool ilp2 = fixed && dom->walk_ilp == 2 && dom->slots <= 8;
+    const int block = dom->walk_block;
+#define MCLSGPU_WALK_DIR(DIRV, STV)                                                           \
+    (ilp2 ? launch32_slots<DIRV, STV, true, 2>(dom->slots, a, sms, block, st, launch)         \
+          : fixed ? launch32_slots<DIRV, STV, true, 1>(dom->slots, a, sms, block, st, launch) \
+                  : launch32_slots<DIRV, STV, false, 1>(dom->slots, a, sms, block, st, launch))
     if (dom->stencil_k) {
         if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, true);
         else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, true);
