@@ -648,6 +648,10 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
     const int n = dom->n;
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
     reset_counters(dom);
+    // The fused iteration expects a zero work-queue counter and ticket on
+    // entry (it resets both itself at the end of every iteration).
+    cudaMemsetAsync(dom->d_counter, 0, sizeof(int), s);
+    cudaMemsetAsync(dom->d_ticket, 0, sizeof(unsigned int), s);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
