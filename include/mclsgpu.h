@@ -176,6 +176,18 @@ int64_t mclsgpu_operator_nnz(const mclsgpu_operator* op);
 /* y = A x with host vectors (MatrixTraits::apply,
  * tpetra/src/MCLS_TpetraCrsMatrixAdapter.hpp:366-371). */
 int mclsgpu_operator_apply(mclsgpu_operator* op, const double* x, double* y);
+/* y = A x with host vectors, allocating no device memory.  No counterpart in
+ * the reference: it exists for callers that cannot let a library call
+ * cudaMalloc/cudaFree (a thread under a real-time budget, since those calls
+ * can synchronise the device; an application whose pool owns all device
+ * memory).  x and y are staged through one static device array built into
+ * the library (16 MiB, held on every GPU that loads it until exit), so the
+ * operator may have at most 1,048,576 rows; larger ones get
+ * MCLSGPU_ERR_INVALID_ARG.  All calls on a device share that array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture begins. */
+int mclsgpu_operator_apply_static(mclsgpu_operator* op, const double* x, double* y);
 
 /* ---- preconditioner ------------------------------------------------------ */
 /* Replaces Preconditioner<Matrix>::buildPreconditioner / getLeftPreconditioner

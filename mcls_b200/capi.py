@@ -119,6 +119,7 @@ EXPORTS = [
     "mclsgpu_rank_seed", "mclsgpu_mc_solve", "mclsgpu_mc_solve_dev", "mclsgpu_mc_trace",
     "mclsgpu_mcsa_solve", "mclsgpu_mcsa_solve_dev", "mclsgpu_domain_spectral_radius",
     "mclsgpu_domain_query", "mclsgpu_domain_set_launch", "mclsgpu_domain_autotune",
+    "mclsgpu_operator_apply_static",
 ]
 
 _LIB = None
@@ -156,6 +157,7 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_operator_nnz.argtypes = [P]
     L.mclsgpu_operator_nnz.restype = i64
     L.mclsgpu_operator_apply.argtypes = [P, P, P]
+    L.mclsgpu_operator_apply_static.argtypes = [P, P, P]
     L.mclsgpu_precond_build.argtypes = [P, P, C.POINTER(PrecondParams), PP]
     L.mclsgpu_precond_destroy.argtypes = [P]
     L.mclsgpu_precond_export.argtypes = [P, C.POINTER(i64), P, P, P]
@@ -243,6 +245,14 @@ class Operator:
         x = np.ascontiguousarray(x, np.float64)
         y = np.empty_like(x)
         self.ctx.check(self.ctx.L.mclsgpu_operator_apply(self.h, _ptr(x), _ptr(y)))
+        return y
+
+    def apply_static(self, x):
+        """y = A x staged through the library's static device array: no
+        device allocation, at most 1,048,576 rows, calls must not overlap."""
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        self.ctx.check(self.ctx.L.mclsgpu_operator_apply_static(self.h, _ptr(x), _ptr(y)))
         return y
 
     def close(self):
