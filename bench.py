@@ -32,14 +32,19 @@ sys.path.insert(0, ROOT)
 METRIC = "MCSA time-to-1e-8 residual, learned vs Jacobi precond, one B200; walk-steps/sec"
 UNIT = "walk-steps/s"
 CONFIGS = {
-    "c2": dict(workload="3D 7-pt variable-coefficient diffusion 128^3, Jacobi MCSA, forward "
+    "diffusion128": dict(workload="3D 7-pt variable-coefficient diffusion 128^3, Jacobi MCSA, forward "
                         "expected-value estimator, FP32 walks / FP64 tallies, residual and update, "
                         "2^22 histories per iteration",
                n=128, sample_ratio=2.0, estimator=1, history_length=10, direction=1),
-    "c1": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, adjoint collision estimator, "
+    "poisson100": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, adjoint collision estimator, "
                         "FP64 walks, N histories per iteration",
                n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0),
 }
+# DRAM bytes (read + write) of one walk launch on each workload, from the ncu
+# capture summarised in profiles/walk32_stencil_diffusion128.md.
+WALK_DRAM_BYTES_PER_LAUNCH = {"diffusion128": 91.72e6}
+
+
 def step_bytes(cfg, info):
     """Bytes one FP32 walk step must move: its state's record, plus (adjoint)
     an 8 B FP64 tally read-modify-write.
@@ -115,7 +120,7 @@ def make_system(cfg):
     from mcls_b200 import problems as P
 
     c = CONFIGS[cfg]
-    if cfg == "c2":
+    if cfg == "diffusion128":
         A, b = P.diffusion3d_varcoef(c["n"], seed=0)
     else:
         A = P.poisson2d(c["n"])
@@ -217,10 +222,12 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mcls_b200", choices=["mcls_b200", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="diffusion128", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iters", type=int, default=20000)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--walk-shape", default=None,
+                    help="fixed walk launch shape 'histories_per_lane,block' (skips autotuning)")
     ap.add_argument("--host-loop", action="store_true",
                     help="host-driven MCSA loop (for profilers that cannot see kernels "
                          "inside conditional graph nodes)")
@@ -240,7 +247,7 @@ def main():
     torch.cuda.set_device(local)
     A, b = make_system(args.config)
     n = A.shape[0]
-    fp = capi.FP32 if args.config == "c2" else capi.FP64
+    fp = capi.FP32 if args.config == "diffusion128" else capi.FP64
     ctx = capi.Context(local)
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
@@ -254,7 +261,11 @@ def main():
     bt = torch.tensor(b, device=f"cuda:{local}", dtype=torch.float64)
     xt = torch.zeros_like(bt)
     tuned = None
-    if fp == capi.FP32 and not args.no_autotune:
+    if args.walk_shape:
+        hpl, blk = (int(v) for v in args.walk_shape.split(","))
+        dom.set_launch(hpl, blk)
+        tuned = {"histories_per_lane": hpl, "block_size": blk, "walk_ms": None}
+    elif fp == capi.FP32 and not args.no_autotune:
         # Launch-shape autotuning on the workload's own right-hand side
         # (untimed set-up, like the domain build).
         dt = torch.tensor((1.0 / A.diagonal()) * b, device=f"cuda:{local}", dtype=torch.float64)
@@ -330,7 +341,8 @@ def main():
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "frac": achieved / peak if achieved else None,
+                     "traffic": WALK_DRAM_BYTES_PER_LAUNCH.get(args.config),
                      "kernel": "walk32", "peak_kind": peak_kind,
                      "bytes_per_step": bstep,
                      "record_format": "stencil" if info["record_format"] == 2 else "packed",

@@ -1,0 +1,48 @@
+// MCLS_SolverFactory.hpp -- name -> solver manager
+// (src/MCLS_SolverFactory.hpp:61-95, src/MCLS_SolverFactory_impl.hpp:57-140).
+//
+// "Adjoint MC", "Forward MC", "Adjoint MCSA" and "Forward MCSA" create the
+// GPU managers.  "Adjoint Anderson", "Forward Anderson" and "Fixed Point"
+// are names the reference knows but this library does not provide; they
+// throw Assertion naming the solver, as unknown names do.
+#ifndef MCLS_SOLVERFACTORY_HPP
+#define MCLS_SOLVERFACTORY_HPP
+
+#include <map>
+#include <string>
+
+#include "MCLS_MCSASolverManager.hpp"
+#include "MCLS_MonteCarloSolverManager.hpp"
+
+namespace MCLS {
+
+template <class Vector, class Matrix>
+class SolverFactory {
+  public:
+    typedef SolverManager<Vector, Matrix> Solver;
+
+    SolverFactory() = default;
+
+    Teuchos::RCP<Solver> create(const std::string& solver_name,
+                                const Teuchos::RCP<Teuchos::ParameterList>& solver_parameters) {
+        if (!Teuchos::nonnull(solver_parameters)) throw Assertion("SolverFactory: null parameters");
+        if (solver_name == "Adjoint MC")
+            return Teuchos::rcp(
+                new MonteCarloSolverManager<Vector, Matrix, AdjointTag>(solver_parameters));
+        if (solver_name == "Forward MC")
+            return Teuchos::rcp(
+                new MonteCarloSolverManager<Vector, Matrix, ForwardTag>(solver_parameters));
+        if (solver_name == "Adjoint MCSA")
+            return Teuchos::rcp(new MCSASolverManager<Vector, Matrix, AdjointTag>(solver_parameters));
+        if (solver_name == "Forward MCSA")
+            return Teuchos::rcp(new MCSASolverManager<Vector, Matrix, ForwardTag>(solver_parameters));
+        if (solver_name == "Adjoint Anderson" || solver_name == "Forward Anderson" ||
+            solver_name == "Fixed Point")
+            throw Assertion("Solver type \"" + solver_name + "\" is not provided by the GPU path");
+        throw Assertion("Solver type not supported!");
+    }
+};
+
+}  // namespace MCLS
+
+#endif  // MCLS_SOLVERFACTORY_HPP

@@ -1,0 +1,251 @@
+// Facade test: the MCLS manager API (SolverFactory, MCSASolverManager,
+// MonteCarloSolverManager, LinearProblem, MultiSetLinearProblem,
+// preconditioners, ParameterList keys) over libmclsgpu.
+//
+//   facade_test cpu   checks that need no device: valid parameter lists,
+//                     factory names, ParameterList typing, and that a solve
+//                     without a device throws MCLS::Assertion.
+//   facade_test gpu   the solves, after the reference's manager tests
+//                     (tpetra/test/tstTpetraMCSASolverManager.cpp:72-355,
+//                     tpetra/test/tstTpetraMonteCarloSolverManager.cpp:73-197).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "MCLS_GpuPreconditioners.hpp"
+#include "MCLS_SolverFactory.hpp"
+
+typedef MCLS::HostVector Vec;
+typedef MCLS::HostCrsMatrix Mat;
+typedef MCLS::VectorTraits<Vec> VT;
+
+static int g_failures = 0;
+#define EXPECT(cond)                                                          \
+    do {                                                                      \
+        if (!(cond)) {                                                        \
+            std::printf("FAILED %s:%d: %s\n", __FILE__, __LINE__, #cond);    \
+            ++g_failures;                                                     \
+        }                                                                     \
+    } while (0)
+
+// Tridiagonal (-0.14, 1, -0.14) with the explicit zeros of the reference test.
+static Teuchos::RCP<Mat> tridiag(int n) {
+    auto A = Teuchos::rcp(new Mat);
+    A->n = n;
+    A->rowptr.assign(1, 0);
+    for (int i = 0; i < n; ++i) {
+        int c0 = i == 0 ? 0 : (i == n - 1 ? n - 3 : i - 1);
+        for (int c = c0; c < c0 + 3; ++c) {
+            double v = c == i ? 1.0 : (std::abs(c - i) == 1 ? -0.14 : 0.0);
+            A->colind.push_back(c);
+            A->values.push_back(v);
+        }
+        A->rowptr.push_back(std::int64_t(A->colind.size()));
+    }
+    return A;
+}
+
+// Dense Gaussian elimination for the exact solution of a small system.
+static Vec direct(const Mat& A, const Vec& b) {
+    const int n = int(A.n);
+    std::vector<double> M(size_t(n) * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (auto p = A.rowptr[i]; p < A.rowptr[i + 1]; ++p) M[size_t(i) * n + A.colind[p]] += A.values[p];
+    Vec x = b;
+    for (int k = 0; k < n; ++k)
+        for (int i = k + 1; i < n; ++i) {
+            double f = M[size_t(i) * n + k] / M[size_t(k) * n + k];
+            for (int j = k; j < n; ++j) M[size_t(i) * n + j] -= f * M[size_t(k) * n + j];
+            x[i] -= f * x[k];
+        }
+    for (int i = n - 1; i >= 0; --i) {
+        for (int j = i + 1; j < n; ++j) x[i] -= M[size_t(i) * n + j] * x[j];
+        x[i] /= M[size_t(i) * n + i];
+    }
+    return x;
+}
+
+static double rel_err(const Vec& a, const Vec& b) {
+    double d = 0, n = 0;
+    for (size_t i = 0; i < a.size(); ++i) {
+        d += (a[i] - b[i]) * (a[i] - b[i]);
+        n += b[i] * b[i];
+    }
+    return std::sqrt(d / n);
+}
+
+static Teuchos::RCP<Teuchos::ParameterList> mcsa_params() {
+    auto pl = Teuchos::rcp(new Teuchos::ParameterList());
+    pl->set<double>("Convergence Tolerance", 1.0e-8);
+    pl->set<int>("Maximum Iterations", 20);
+    pl->set<int>("MC Check Frequency", 50);
+    pl->set<double>("Sample Ratio", 1.0);
+    pl->set<std::string>("Transport Type", "Global");
+    pl->set<bool>("Print Iterations", false);
+    return pl;
+}
+
+static void cpu_checks() {
+    MCLS::SolverFactory<Vec, Mat> factory;
+    auto pl = mcsa_params();
+    for (const char* name : {"Adjoint MC", "Forward MC", "Adjoint MCSA", "Forward MCSA"}) {
+        auto s = factory.create(name, pl);
+        EXPECT(Teuchos::nonnull(s));
+        auto v = s->getValidParameters();
+        EXPECT(v->isParameter("Sample Ratio") && v->isParameter("History Length"));
+        EXPECT(v->isParameter("Neumann Relaxation") && v->isParameter("MC Check Frequency"));
+        EXPECT(s->getCurrentParameters() == pl);
+    }
+    auto mcsa = factory.create("Adjoint MCSA", pl);
+    auto v = mcsa->getValidParameters();
+    EXPECT(v->get<double>("Convergence Tolerance") == 1.0);
+    EXPECT(v->get<int>("Maximum Iterations") == 1000);
+    EXPECT(v->get<std::string>("Fixed Point Type") == "Richardson");
+    for (const char* name : {"Adjoint Anderson", "Forward Anderson", "Fixed Point", "Bogus"}) {
+        bool threw = false;
+        try {
+            factory.create(name, pl);
+        } catch (const MCLS::Assertion&) {
+            threw = true;
+        }
+        EXPECT(threw);
+    }
+    bool threw = false;
+    try {
+        auto bad = mcsa_params();
+        bad->set<std::string>("Fixed Point Type", "MINRES");
+        MCLS::MCSASolverManager<Vec, Mat> m(bad);
+    } catch (const MCLS::Assertion&) {
+        threw = true;
+    }
+    EXPECT(threw);
+    // Teuchos-strict typing.
+    threw = false;
+    try {
+        pl->get<int>("Sample Ratio");
+    } catch (const Teuchos::Exceptions::InvalidParameterType&) {
+        threw = true;
+    }
+    EXPECT(threw);
+    EXPECT(pl->get<int>("Smoother Steps", 1) == 1 && pl->isParameter("Smoother Steps"));
+
+    // A solve with no device reports it through MCLS::Assertion.
+    auto A = tridiag(10);
+    auto x = Teuchos::rcp(new Vec(10, 0.0));
+    auto b = Teuchos::rcp(new Vec(10, -1.0));
+    auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+    mcsa->setProblem(lp);
+    std::string msg;
+    try {
+        mcsa->solve();
+    } catch (const MCLS::Assertion& e) {
+        msg = e.what();
+    }
+    EXPECT(msg.find("no usable CUDA device") != std::string::npos);
+}
+
+static void gpu_checks() {
+    const int n = 10;
+    auto A = tridiag(n);
+    auto comm = Teuchos::DefaultComm<int>::getComm();
+    for (int forward = 0; forward < 2; ++forward) {
+        auto x = Teuchos::rcp(new Vec(n, 0.0));
+        auto b = Teuchos::rcp(new Vec(n, -1.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+        auto ms = Teuchos::rcp(new MCLS::MultiSetLinearProblem<Vec, Mat>(comm, 1, 0, lp));
+        auto pl = mcsa_params();
+        if (forward) pl->set<double>("Sample Ratio", 10.0);
+        Teuchos::RCP<MCLS::SolverManager<Vec, Mat>> sm;
+        if (forward)
+            sm = Teuchos::rcp(new MCLS::MCSASolverManager<Vec, Mat, MCLS::ForwardTag>(ms, pl));
+        else
+            sm = Teuchos::rcp(new MCLS::MCSASolverManager<Vec, Mat, MCLS::AdjointTag>(ms, pl));
+        const double rhs[4] = {-1.0, 2.0, -2.0, 1.0};
+        for (double r : rhs) {  // four successive solves on one manager
+            std::fill(b->begin(), b->end(), r);
+            std::fill(x->begin(), x->end(), 0.0);
+            lp->setLHS(x);
+            bool conv = sm->solve();
+            EXPECT(conv && sm->getConvergedStatus());
+            EXPECT(sm->getNumIters() < 20);
+            EXPECT(sm->achievedTol() > 0.0 && sm->achievedTol() <= 1e-8);
+            for (double xi : *x) EXPECT(r < 0 ? xi < 0.0 : xi > 0.0);
+            EXPECT(rel_err(*x, direct(*A, *b)) < 1e-7);
+        }
+    }
+
+    // Left point-Jacobi built on the device and handed to the problem.
+    {
+        auto x = Teuchos::rcp(new Vec(n, 0.0));
+        auto b = Teuchos::rcp(new Vec(n, 2.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+        MCLS::PointJacobiPreconditioner<Vec, Mat> prec;
+        prec.setOperator(A);
+        prec.buildPreconditioner();
+        auto PL = prec.getLeftPreconditioner();
+        EXPECT(Teuchos::nonnull(PL) && PL->n == n && PL->values.size() == size_t(n));
+        EXPECT(std::fabs(PL->values[3] - 1.0) < 1e-15);
+        lp->setLeftPrec(PL);
+        MCLS::SolverFactory<Vec, Mat> factory;
+        auto pl = mcsa_params();
+        auto sm = factory.create("Adjoint MCSA", pl);
+        sm->setProblem(lp);
+        EXPECT(sm->solve());
+        EXPECT(rel_err(*x, direct(*A, *b)) < 1e-7);
+    }
+
+    // Block Jacobi (blocks of 2) on a matrix with a non-unit diagonal.
+    {
+        auto B = tridiag(n);
+        for (int i = 0; i < n; ++i)
+            for (auto p = B->rowptr[i]; p < B->rowptr[i + 1]; ++p)
+                if (B->colind[p] == i) B->values[p] = 2.0 + 0.1 * i;
+        auto params = Teuchos::parameterList();
+        params->set<int>("Jacobi Block Size", 2);
+        MCLS::BlockJacobiPreconditioner<Vec, Mat> prec(params);
+        prec.setOperator(B);
+        prec.buildPreconditioner();
+        auto x = Teuchos::rcp(new Vec(n, 0.0));
+        auto b = Teuchos::rcp(new Vec(n, 1.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(B, x, b));
+        lp->setLeftPrec(prec.getLeftPreconditioner());
+        MCLS::MCSASolverManager<Vec, Mat> sm(mcsa_params());
+        sm.setProblem(lp);
+        EXPECT(sm.solve());
+        EXPECT(rel_err(*x, direct(*B, *b)) < 1e-7);
+    }
+
+    // Direct Monte Carlo: signs follow the source, sample ratio 10
+    // (tpetra/test/tstTpetraMonteCarloSolverManager.cpp:73-197).
+    for (const char* name : {"Adjoint MC", "Forward MC"}) {
+        auto x = Teuchos::rcp(new Vec(n, 0.0));
+        auto b = Teuchos::rcp(new Vec(n, -1.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+        auto pl = Teuchos::parameterList();
+        pl->set<double>("Sample Ratio", 10.0);
+        MCLS::SolverFactory<Vec, Mat> factory;
+        auto sm = factory.create(name, pl);
+        sm->setProblem(lp);
+        EXPECT(sm->solve() && sm->getConvergedStatus() && sm->getNumIters() == 0);
+        for (double xi : *x) EXPECT(xi < 0.0);
+        EXPECT(sm->achievedTol() < 0.5);
+        std::fill(b->begin(), b->end(), 2.0);
+        sm->solve();
+        for (double xi : *x) EXPECT(xi > 0.0);
+    }
+}
+
+int main(int argc, char** argv) {
+    const bool gpu = argc > 1 && std::strcmp(argv[1], "gpu") == 0;
+    try {
+        if (gpu) gpu_checks();
+        else cpu_checks();
+    } catch (const std::exception& e) {
+        std::printf("FAILED: exception %s\n", e.what());
+        return 2;
+    }
+    std::printf("%s: %d failure(s)\n", gpu ? "gpu" : "cpu", g_failures);
+    return g_failures ? 1 : 0;
+}
