@@ -203,6 +203,46 @@ int mclsgpu_precond_destroy(mclsgpu_precond* pc);
 int mclsgpu_precond_export(mclsgpu_precond* pc, int64_t* nnz_out,
                            int64_t* rowptr, int64_t* colind, double* values);
 
+/* ---- learned SPAI network ------------------------------------------------- */
+/* No counterpart in the reference (its preconditioner slot for ParaSails is
+ * the nearest relative).  A per-row MLP (16 stencil features -> 64 -> 64 ->
+ * 16, ReLU, BF16 tensor-core products with FP32 accumulation) emits row i of
+ * a sparse approximate inverse M on A's pattern for operators stored by
+ * diagonal offsets with `slots` (3..9) offsets.  It is trained on the GPU to
+ * minimise (1/R) sum_v |v - M A v|^2 / |v|^2 over vectors v (MCSA residual
+ * snapshots and random vectors) and used through mclsgpu_precond_build with
+ * kind MCLSGPU_PREC_LEARNED_SPAI, where point Jacobi replaces it when its
+ * rho(I - M A) reaches both rho_fallback and the Jacobi rho. */
+typedef struct mclsgpu_spai mclsgpu_spai;
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_spai_adam) */
+    double lr;                /* step size */
+    double beta1, beta2, eps; /* Adam moments and denominator guard */
+    double grad_clip;         /* per-component gradient clip; <= 0 = off */
+} mclsgpu_spai_adam;
+/* Number of FP32 parameters (W1[64][16], b1, W2[64][64], b2, W3[16][64], b3). */
+int mclsgpu_spai_num_params(void);
+/* He-uniform hidden layers from `seed`, zero output layer (= point Jacobi). */
+int mclsgpu_spai_create(mclsgpu_context* ctx, int slots, uint64_t seed, mclsgpu_spai** out);
+int mclsgpu_spai_destroy(mclsgpu_spai* net);
+int mclsgpu_spai_get_params(mclsgpu_spai* net, float* host);
+/* Replaces the parameters and clears the optimiser state. */
+int mclsgpu_spai_set_params(mclsgpu_spai* net, const float* host);
+/* Inference on every row of op: raw outputs out[n][16] and/or the values of
+ * M on A's CSR pattern (either may be NULL, not both). */
+int mclsgpu_spai_infer(mclsgpu_spai* net, mclsgpu_operator* op, float* out, double* mvals);
+/* Loss and parameter gradient (host, may be NULL) for nvec device vectors
+ * stored one after another (v_dev[k*n + i]). */
+int mclsgpu_spai_gradient(mclsgpu_spai* net, mclsgpu_operator* op, const double* v_dev,
+                          int nvec, double* loss, float* grad);
+/* One Adam step on that gradient; *loss receives the loss before the step. */
+int mclsgpu_spai_train_step(mclsgpu_spai* net, mclsgpu_operator* op, const double* v_dev,
+                            int nvec, const mclsgpu_spai_adam* opt, double* loss);
+/* Power-iteration estimates of rho(I - M A) for the network's M and for
+ * point Jacobi (either output may be NULL). */
+int mclsgpu_spai_rho(mclsgpu_spai* net, mclsgpu_operator* op, int iters, double* rho_learned,
+                     double* rho_jacobi);
+
 /* ---- Monte Carlo domain --------------------------------------------------- */
 /* Replaces MonteCarloSolverManager::buildMonteCarloDomain + the
  * AlmostOptimalDomain constructor (src/MCLS_MonteCarloSolverManager_impl.hpp:
@@ -287,6 +327,10 @@ int mclsgpu_mcsa_solve(mclsgpu_domain* dom, const double* b, double* x,
 int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev,
                            double* x_dev, const mclsgpu_mcsa_params* params,
                            mclsgpu_stats* stats);
+/* The preconditioned residual PL (b - A x) at the end of the last MCSA
+ * solve, copied to the device vector rp_dev (LinearProblem::getPrecResidual,
+ * src/MCLS_LinearProblem.hpp:121-122). */
+int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev);
 
 /* ---- spectral radius ------------------------------------------------------- */
 /* Replaces AlmostOptimalDomain::computeConvergenceCriteria

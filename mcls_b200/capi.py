@@ -95,6 +95,17 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "size"}
 
 
+class SpaiAdam(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("lr", C.c_double),
+        ("beta1", C.c_double),
+        ("beta2", C.c_double),
+        ("eps", C.c_double),
+        ("grad_clip", C.c_double),
+    ]
+
+
 class DomainInfo(C.Structure):
     _fields_ = [
         ("size", C.c_uint32),
@@ -119,7 +130,10 @@ EXPORTS = [
     "mclsgpu_rank_seed", "mclsgpu_mc_solve", "mclsgpu_mc_solve_dev", "mclsgpu_mc_trace",
     "mclsgpu_mcsa_solve", "mclsgpu_mcsa_solve_dev", "mclsgpu_domain_spectral_radius",
     "mclsgpu_domain_query", "mclsgpu_domain_set_launch", "mclsgpu_domain_autotune",
-    "mclsgpu_operator_apply_static",
+    "mclsgpu_operator_apply_static", "mclsgpu_spai_num_params", "mclsgpu_spai_create",
+    "mclsgpu_spai_destroy", "mclsgpu_spai_get_params", "mclsgpu_spai_set_params",
+    "mclsgpu_spai_infer", "mclsgpu_spai_gradient", "mclsgpu_spai_train_step", "mclsgpu_spai_rho",
+    "mclsgpu_domain_residual",
 ]
 
 _LIB = None
@@ -178,6 +192,16 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_mcsa_solve_dev.argtypes = [P, P, P, C.POINTER(McsaParams), C.POINTER(Stats)]
     L.mclsgpu_domain_spectral_radius.argtypes = [P, C.c_int, C.c_int, d, C.c_uint64,
                                                  C.POINTER(d)]
+    L.mclsgpu_domain_residual.argtypes = [P, P]
+    L.mclsgpu_spai_num_params.restype = C.c_int
+    L.mclsgpu_spai_create.argtypes = [P, C.c_int, C.c_uint64, PP]
+    L.mclsgpu_spai_destroy.argtypes = [P]
+    L.mclsgpu_spai_get_params.argtypes = [P, P]
+    L.mclsgpu_spai_set_params.argtypes = [P, P]
+    L.mclsgpu_spai_infer.argtypes = [P, P, P, P]
+    L.mclsgpu_spai_gradient.argtypes = [P, P, P, C.c_int, C.POINTER(d), P]
+    L.mclsgpu_spai_train_step.argtypes = [P, P, P, C.c_int, C.POINTER(SpaiAdam), C.POINTER(d)]
+    L.mclsgpu_spai_rho.argtypes = [P, P, C.c_int, C.POINTER(d), C.POINTER(d)]
     _LIB = L
     return L
 
@@ -280,7 +304,7 @@ class Precond:
             p.user_n = n
             p.user_rowptr, p.user_colind, p.user_values = _ptr(rp), _ptr(ci), _ptr(v)
         if net is not None:
-            p.spai_net = net
+            p.spai_net = net.h if isinstance(net, SpaiNet) else net
         h = C.c_void_p()
         ctx.check(ctx.L.mclsgpu_precond_build(ctx.h, op.h, C.byref(p), C.byref(h)))
         del keep
@@ -438,6 +462,10 @@ class Domain:
                                                          C.byref(st)))
         return st.as_dict()
 
+    def residual(self, rp_dev_ptr):
+        """Copy the last MCSA solve's preconditioned residual to a device vector."""
+        self.ctx.check(self.ctx.L.mclsgpu_domain_residual(self.h, C.c_void_p(rp_dev_ptr)))
+
     def spectral_radius(self, which=0, max_iters=2000, tol=1e-8, seed=7):
         rho = C.c_double()
         self.ctx.check(self.ctx.L.mclsgpu_domain_spectral_radius(self.h, which, max_iters, tol,
@@ -447,6 +475,70 @@ class Domain:
     def close(self):
         if getattr(self, "h", None):
             self.ctx.L.mclsgpu_domain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class SpaiNet:
+    """The learned-SPAI network (16 -> 64 -> 64 -> 16) on a context."""
+
+    def __init__(self, ctx: Context, slots: int, seed: int = 0):
+        self.ctx = ctx
+        self.slots = slots
+        self.nparams = int(ctx.L.mclsgpu_spai_num_params())
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_spai_create(ctx.h, slots, seed, C.byref(h)))
+        self.h = h
+        ctx._adopt(self)
+
+    @property
+    def params(self):
+        p = np.empty(self.nparams, np.float32)
+        self.ctx.check(self.ctx.L.mclsgpu_spai_get_params(self.h, _ptr(p)))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparams
+        self.ctx.check(self.ctx.L.mclsgpu_spai_set_params(self.h, _ptr(p)))
+
+    def infer(self, op: Operator, nnz: int):
+        """(raw outputs [n, 16], M values on A's pattern)."""
+        out = np.empty((op.n, 16), np.float32)
+        m = np.empty(nnz, np.float64)
+        self.ctx.check(self.ctx.L.mclsgpu_spai_infer(self.h, op.h, _ptr(out), _ptr(m)))
+        return out, m
+
+    def gradient(self, op: Operator, v_dev_ptr, nvec):
+        """(loss, FP32 parameter gradient) for nvec device vectors."""
+        loss = C.c_double()
+        g = np.empty(self.nparams, np.float32)
+        self.ctx.check(self.ctx.L.mclsgpu_spai_gradient(self.h, op.h, C.c_void_p(v_dev_ptr), nvec,
+                                                        C.byref(loss), _ptr(g)))
+        return loss.value, g
+
+    def train_step(self, op: Operator, v_dev_ptr, nvec, lr=1e-3, beta1=0.9, beta2=0.999,
+                   eps=1e-8, grad_clip=0.0):
+        a = SpaiAdam()
+        a.size = C.sizeof(SpaiAdam)
+        a.lr, a.beta1, a.beta2, a.eps, a.grad_clip = lr, beta1, beta2, eps, grad_clip
+        loss = C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_spai_train_step(self.h, op.h, C.c_void_p(v_dev_ptr),
+                                                          nvec, C.byref(a), C.byref(loss)))
+        return loss.value
+
+    def rho(self, op: Operator, iters=200):
+        """(rho(I - M A) learned, rho(I - D^-1 A) point Jacobi)."""
+        rl, rj = C.c_double(), C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_spai_rho(self.h, op.h, iters, C.byref(rl), C.byref(rj)))
+        return rl.value, rj.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_spai_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -163,13 +163,15 @@ __global__ void k_epoch_inc(unsigned long long* e) { *e += 1ULL; }
 
 // Convergence check of one MCSA iteration (src/MCLS_MCSASolverManager_impl.hpp:380-394).
 __device__ __forceinline__ int mcsa_check(McsaState* st, const double* sumsq, double* hist,
-                                          int hist_cap, const int* status) {
+                                          int hist_cap, int* status) {
     McsaState s = *st;
     s.iter += 1;
     s.rnorm = sqrt(*sumsq);
     if (hist && s.iter <= hist_cap) hist[s.iter - 1] = s.rnorm;
     int keep = 1;
     if (s.iter % s.check_freq == 0) keep = (s.rnorm > s.crit) && (s.iter < s.max_iters);
+    // A non-finite residual norm ends the loop as a divergence.
+    if (!isfinite(s.rnorm)) atomicOr(status, DEV_ERR_NONFINITE);
     if (*status) keep = 0;
     s.done = !keep;
     s.converged = s.rnorm <= s.crit;
@@ -178,13 +180,13 @@ __device__ __forceinline__ int mcsa_check(McsaState* st, const double* sumsq, do
 }
 
 __global__ void k_mcsa_check(McsaState* st, const double* sumsq, double* hist, int hist_cap,
-                             const int* status, cudaGraphConditionalHandle handle) {
+                             int* status, cudaGraphConditionalHandle handle) {
     const int keep = mcsa_check(st, sumsq, hist, hist_cap, status);
     cudaGraphSetConditional(handle, keep ? 1u : 0u);
 }
 
 __global__ void k_mcsa_check_host(McsaState* st, const double* sumsq, double* hist, int hist_cap,
-                                  const int* status) {
+                                  int* status) {
     mcsa_check(st, sumsq, hist, hist_cap, status);
 }
 
@@ -228,7 +230,7 @@ struct ResidArgs {
     McsaState* st;
     double* hist;
     int hist_cap;
-    const int* status;
+    int* status;
     unsigned long long* d_epoch;
     unsigned long long* d_tim;
     int* d_counter;
@@ -871,6 +873,15 @@ int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_d
     int rc = check_mcsa_params(dom, params, &p);
     if (rc) return rc;
     return mcsa_solve_device(dom, b_dev, x_dev, &p, stats);
+}
+
+int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev) {
+    if (!dom || !rp_dev || !dom->rp) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = dom->ctx;
+    cudaError_t e = cudaMemcpyAsync(rp_dev, dom->rp, size_t(dom->n) * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "domain residual");
 }
 
 int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane, int block_size) {

@@ -44,7 +44,9 @@ __global__ void k_random_count(int nh_req, double* sc, int* d_nh, int cap, int* 
         atomicOr(status, DEV_ERR_NONFINITE);
     }
     if (nh > cap) {
-        atomicOr(status, DEV_ERR_CAPACITY);
+        // total <= norm1 in exact arithmetic, so nh <= nh_req <= cap; more
+        // means the source sums lost all precision (a diverging iteration).
+        atomicOr(status, DEV_ERR_NONFINITE);
         nh = cap;
     }
     *d_nh = nh;
