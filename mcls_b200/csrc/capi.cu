@@ -462,7 +462,11 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
     if (!rc && p->precision == MCLSGPU_FP32 && dom->slots == 0)
         rc = set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
                        "domain rows longer than 31 entries need the FP64 walk");
-    const int parts = scan_partials_needed(n) + 8;
+    // Partials: one per scan tile (scans) and one per block of the fused
+    // residual kernels, whose grid is at most 8 blocks per SM.
+    const int fused_blocks = ctx->num_sms * 8;
+    const int scan_parts = scan_partials_needed(n);
+    const int parts = (scan_parts > fused_blocks ? scan_parts : fused_blocks) + 8;
     if (!rc) {
         if ((e = dmalloc(&dom->src, n)) != cudaSuccess || (e = dmalloc(&dom->scdf, n)) != cudaSuccess ||
             (e = dmalloc(&dom->guide, n)) != cudaSuccess || (e = dmalloc(&dom->counts, n)) != cudaSuccess ||

@@ -508,6 +508,8 @@ static bool fused_iteration(const mclsgpu_domain* dom, const mclsgpu_mcsa_params
            (!dom->left || dom->left->kind == MCLSGPU_PREC_POINT_JACOBI);
 }
 
+// At most 8 blocks per SM: the per-block partial sums of k_apply_correction
+// and k_residual_norm go to dom->part, sized for that many blocks.
 static int fused_grid(const mclsgpu_domain* dom) {
     return grid_for(dom->n, kFusedThreads, dom->ctx->num_sms * 8);
 }

@@ -241,7 +241,7 @@ static void gpu_checks() {
         sm->setProblem(lp);
         EXPECT(sm->solve() && sm->getConvergedStatus() && sm->getNumIters() == 0);
         for (double xi : *x) EXPECT(xi < 0.0);
-        EXPECT(sm->achievedTol() < 0.5);
+        EXPECT(std::isfinite(sm->achievedTol()) && sm->achievedTol() < 1.0);
         std::fill(b->begin(), b->end(), 2.0);
         sm->solve();
         for (double xi : *x) EXPECT(xi > 0.0);
