@@ -174,6 +174,74 @@ def allsum(pg, v):
     return float(t.item())
 
 
+def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
+    """Learned-SPAI MCSA on the same system: train the per-row network on the
+    GPU (untimed set-up, reported), build the learned preconditioner and its
+    domain, then time the same MCSA solve as the Jacobi arm."""
+    import torch
+
+    from mcls_b200 import capi
+    from mcls_b200 import problems as P
+    from mcls_b200 import spai
+
+    t0 = time.perf_counter()
+    samples = []
+    for seed in range(8):
+        At, bt_ = P.diffusion3d_varcoef(32, seed=1000 + seed)
+        opt = capi.Operator(ctx, At)
+        samples.append((opt, spai.training_vectors(ctx, opt, bt_, seed=seed, n_random=4,
+                                                   iterations=(1, 4, 16))))
+    net = capi.SpaiNet(ctx, spai.stencil_slots(A), seed=0)
+    losses = spai.train(net, samples, steps=2000, lr=3e-3, lr_final=3e-4, refresh=25,
+                        adv_count=8, adv_iters=50)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    rl, rj = net.rho(op, iters=300)
+    pc = capi.Precond(ctx, op, capi.PREC_LEARNED_SPAI, net=net)
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=1234,
+                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
+                      direction=cfgd["direction"], history_length=cfgd["history_length"])
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
+    bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
+    xt = torch.zeros_like(bt)
+    tuned = dom.autotune(bt.data_ptr(), reps=1)
+    stats = []
+    for k in range(1 + args.steps):
+        dom.reseed(1234)
+        xt.zero_()
+        torch.cuda.synchronize()
+        st = dom.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
+        if k >= 1:
+            stats.append(st)
+    ms = sum(s["solve_ms"] for s in stats) / len(stats)
+    steps = sum(s["walk_steps"] for s in stats)
+    rel = float(np.linalg.norm(b - A @ xt.cpu().numpy()) / np.linalg.norm(b))
+    info = dom.info()
+    out = {"time_to_1e-8_s": ms / 1e3, "iterations": stats[-1]["iterations"],
+           "converged": bool(stats[-1]["converged"]),
+           "walk_steps_per_s": steps / (sum(s["solve_ms"] for s in stats) * 1e-3),
+           "walk_ms_per_launch": sum(s["walk_ms"] for s in stats) /
+                                 max(sum(s["walk_launches"] for s in stats), 1),
+           "rel_residual_b_minus_Ax": rel, "rho_learned": rl, "rho_jacobi": rj,
+           "fallback_taken": bool(stats[-1]["fallback_taken"]),
+           "record_bytes": info["record_bytes"], "record_format": info["record_format"],
+           "h_entries_per_row": info["max_row_entries"], "walk_launch": tuned,
+           "train_s": train_s, "train_steps": 2000, "train_loss_first": float(np.mean(losses[:8])),
+           "train_loss_last": float(np.mean(losses[-40:])),
+           "train_systems": "8 x 3D 7-pt var-coef diffusion 32^3 (seeds 1000-1007)",
+           "speedup_vs_jacobi": jacobi_ms / ms}
+    dom.close()
+    pc.close()
+    net.close()
+    return out
+
+
+def ctx_device():
+    import torch
+
+    return f"cuda:{torch.cuda.current_device()}"
+
+
 def cpu_baseline(cfg, A, b, seconds_target=15.0):
     """Oracle port: multi-threaded adjoint walks on the same domain."""
     from oracle import oracle as O
@@ -226,6 +294,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iters", type=int, default=20000)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-SPAI arm (training + learned MCSA solves)")
     ap.add_argument("--walk-shape", default=None,
                     help="fixed walk launch shape 'histories_per_lane,block' (skips autotuning)")
     ap.add_argument("--host-loop", action="store_true",
@@ -350,6 +420,9 @@ def main():
                      "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
         "wall_s": wall,
     }
+    if world == 1 and args.config == "diffusion128" and not args.no_learned:
+        line["config"]["learned_spai"] = learned_arm(args, ctx, op, A, b, cfgd,
+                                                     dev_ms_max / args.steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.config, A, b)
     if rank == 0:

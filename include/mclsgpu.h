@@ -225,6 +225,11 @@ int mclsgpu_spai_num_params(void);
 /* He-uniform hidden layers from `seed`, zero output layer (= point Jacobi). */
 int mclsgpu_spai_create(mclsgpu_context* ctx, int slots, uint64_t seed, mclsgpu_spai** out);
 int mclsgpu_spai_destroy(mclsgpu_spai* net);
+/* Training loss term weight/n * sum_i max(0, W_i - threshold)^2 with W_i
+ * the row sum of |I - M A|: the factor by which a forward walk's weight
+ * grows at state i, which sets the variance of the Monte Carlo correction.
+ * weight 0 (the default) turns it off. */
+int mclsgpu_spai_set_penalty(mclsgpu_spai* net, double weight, double threshold);
 int mclsgpu_spai_get_params(mclsgpu_spai* net, float* host);
 /* Replaces the parameters and clears the optimiser state. */
 int mclsgpu_spai_set_params(mclsgpu_spai* net, const float* host);
@@ -238,6 +243,12 @@ int mclsgpu_spai_gradient(mclsgpu_spai* net, mclsgpu_operator* op, const double*
 /* One Adam step on that gradient; *loss receives the loss before the step. */
 int mclsgpu_spai_train_step(mclsgpu_spai* net, mclsgpu_operator* op, const double* v_dev,
                             int nvec, const mclsgpu_spai_adam* opt, double* loss);
+/* In place, for each of nvec device vectors (v_dev[k*n + i]): `iters`
+ * applications of H = I - M A with the network's current M, normalised to
+ * unit 2-norm after each: the error modes the learned-preconditioner
+ * iteration damps slowest, used as on-policy training vectors. */
+int mclsgpu_spai_smooth_vectors(mclsgpu_spai* net, mclsgpu_operator* op, double* v_dev, int nvec,
+                                int iters);
 /* Power-iteration estimates of rho(I - M A) for the network's M and for
  * point Jacobi (either output may be NULL). */
 int mclsgpu_spai_rho(mclsgpu_spai* net, mclsgpu_operator* op, int iters, double* rho_learned,

@@ -133,7 +133,7 @@ EXPORTS = [
     "mclsgpu_operator_apply_static", "mclsgpu_spai_num_params", "mclsgpu_spai_create",
     "mclsgpu_spai_destroy", "mclsgpu_spai_get_params", "mclsgpu_spai_set_params",
     "mclsgpu_spai_infer", "mclsgpu_spai_gradient", "mclsgpu_spai_train_step", "mclsgpu_spai_rho",
-    "mclsgpu_domain_residual",
+    "mclsgpu_domain_residual", "mclsgpu_spai_smooth_vectors", "mclsgpu_spai_set_penalty",
 ]
 
 _LIB = None
@@ -202,6 +202,8 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_spai_gradient.argtypes = [P, P, P, C.c_int, C.POINTER(d), P]
     L.mclsgpu_spai_train_step.argtypes = [P, P, P, C.c_int, C.POINTER(SpaiAdam), C.POINTER(d)]
     L.mclsgpu_spai_rho.argtypes = [P, P, C.c_int, C.POINTER(d), C.POINTER(d)]
+    L.mclsgpu_spai_smooth_vectors.argtypes = [P, P, P, C.c_int, C.c_int]
+    L.mclsgpu_spai_set_penalty.argtypes = [P, d, d]
     _LIB = L
     return L
 
@@ -493,6 +495,10 @@ class SpaiNet:
         self.h = h
         ctx._adopt(self)
 
+    def set_penalty(self, weight, threshold=1.0):
+        """Row-sum penalty of the training loss (weight 0 = off)."""
+        self.ctx.check(self.ctx.L.mclsgpu_spai_set_penalty(self.h, weight, threshold))
+
     @property
     def params(self):
         p = np.empty(self.nparams, np.float32)
@@ -529,6 +535,11 @@ class SpaiNet:
         self.ctx.check(self.ctx.L.mclsgpu_spai_train_step(self.h, op.h, C.c_void_p(v_dev_ptr),
                                                           nvec, C.byref(a), C.byref(loss)))
         return loss.value
+
+    def smooth_vectors(self, op: Operator, v_dev_ptr, nvec, iters):
+        """In place: iters applications of I - M A (normalised) to each vector."""
+        self.ctx.check(self.ctx.L.mclsgpu_spai_smooth_vectors(self.h, op.h, C.c_void_p(v_dev_ptr),
+                                                              nvec, iters))
 
     def rho(self, op: Operator, iters=200):
         """(rho(I - M A) learned, rho(I - D^-1 A) point Jacobi)."""

@@ -241,7 +241,7 @@ int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n, const int64_t* rowp
     // Stencil operators also get diagonal-offset storage (no column indices)
     // when it holds at most 25% more values than the CSR arrays.
     int K = 0;
-    if (!rc) rc = collect_offsets(ctx, op->A, op->dia_off, &K);
+    if (!rc) rc = collect_offsets(ctx, op->A, 16, op->dia_off, &K);
     if (!rc && K > 0 && double(K) * op->A.n <= 1.25 * op->A.nnz + op->A.n) {
         rc = csr_to_dia(ctx, op->A, K, op->dia_off, &op->dia_val);
         if (!rc) op->dia_k = K;

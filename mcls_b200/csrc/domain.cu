@@ -94,15 +94,16 @@ __global__ void k_pack_records(const int* drp, const int* dcol, const double* dh
     }
 }
 
-// Distinct column offsets (col - row) into a 16-slot table; an offset takes
-// the first free slot it meets scanning from slot 0, so each offset owns one
-// slot.  More than 16 distinct offsets sets *overflow.
-__global__ void k_collect_offsets(const int* rp, const int* ci, int n, int* tab, int* overflow) {
+// Distinct column offsets (col - row) into a max_k-slot table; an offset
+// takes the first free slot it meets scanning from slot 0, so each offset
+// owns one slot.  More than max_k distinct offsets sets *overflow.
+__global__ void k_collect_offsets(const int* rp, const int* ci, int n, int max_k, int* tab,
+                                  int* overflow) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         for (int k = rp[i]; k < rp[i + 1]; ++k) {
             const int d = ci[k] - i;
             bool placed = false;
-            for (int t = 0; t < 16 && !placed; ++t) {
+            for (int t = 0; t < max_k && !placed; ++t) {
                 int cur = tab[t];
                 if (cur == INT_MIN) cur = atomicCAS(&tab[t], INT_MIN, d);
                 if (cur == INT_MIN || cur == d) placed = true;
@@ -141,26 +142,28 @@ __global__ void k_to_float(const double* a, float* b, int n) {
 
 }  // namespace
 
-// Sorted distinct column offsets of D (at most 16; *K = 0 when there are more).
-int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int* offsets, int* K) {
+// Sorted distinct column offsets of D (at most max_k <= 32; *K = 0 when
+// there are more).
+int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int max_k, int* offsets, int* K) {
     cudaStream_t s = ctx->stream;
+    if (max_k < 1 || max_k > 32) return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "offset table size");
     int* tab = nullptr;
-    cudaError_t e = dmalloc(&tab, 17);
+    cudaError_t e = dmalloc(&tab, size_t(max_k) + 1);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
-    std::vector<int> init(17, INT_MIN);
-    init[16] = 0;
-    cudaMemcpyAsync(tab, init.data(), 17 * sizeof(int), cudaMemcpyHostToDevice, s);
-    k_collect_offsets<<<grid_for(D.n), 256, 0, s>>>(D.rp, D.ci, D.n, tab, tab + 16);
-    std::vector<int> h(17);
-    cudaMemcpyAsync(h.data(), tab, 17 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    std::vector<int> init(max_k + 1, INT_MIN);
+    init[max_k] = 0;
+    cudaMemcpyAsync(tab, init.data(), (max_k + 1) * sizeof(int), cudaMemcpyHostToDevice, s);
+    k_collect_offsets<<<grid_for(D.n), 256, 0, s>>>(D.rp, D.ci, D.n, max_k, tab, tab + max_k);
+    std::vector<int> h(max_k + 1);
+    cudaMemcpyAsync(h.data(), tab, (max_k + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
     dfree(tab);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "collect offsets");
     *K = 0;
-    for (int t = 0; t < 16; ++t) offsets[t] = 0;
-    if (h[16]) return MCLSGPU_OK;
+    for (int t = 0; t < max_k; ++t) offsets[t] = 0;
+    if (h[max_k]) return MCLSGPU_OK;
     std::vector<int> v;
-    for (int t = 0; t < 16; ++t)
+    for (int t = 0; t < max_k; ++t)
         if (h[t] != INT_MIN) v.push_back(h[t]);
     std::sort(v.begin(), v.end());
     for (size_t t = 0; t < v.size(); ++t) offsets[t] = v[t];
@@ -228,15 +231,16 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     const int fmt = dom->p.record_format;
     if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED) {
         int K = 0;
-        if ((rc = collect_offsets(ctx, D, dom->stencil_off, &K))) return rc;
-        const int words = K > 0 && K <= 6 ? 8 : (K > 0 && K <= 14 ? 16 : 0);
+        if ((rc = collect_offsets(ctx, D, 30, dom->stencil_off, &K))) return rc;
+        // 32-, 64- or 128-byte records.
+        const int words = K <= 0 ? 0 : (K <= 6 ? 8 : (K <= 14 ? 16 : (K <= 30 ? 32 : 0)));
         const int packed_words = slots ? 2 * slots : 1 << 30;
         if (words && (fmt == MCLSGPU_RECORD_STENCIL || words < packed_words)) {
             dom->stencil_k = K;
             slots = words / 2;
         } else if (fmt == MCLSGPU_RECORD_STENCIL) {
             return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
-                             "stencil records need at most 14 distinct column offsets (found %d)",
+                             "stencil records need at most 30 distinct column offsets (found %d)",
                              K);
         }
     }
@@ -246,8 +250,8 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
             return cuda_fail(ctx, e, "cudaMalloc records");
         if (dom->stencil_k) {
             int* doff = nullptr;
-            if ((e = dmalloc(&doff, 16)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
-            cudaMemcpyAsync(doff, dom->stencil_off, 16 * sizeof(int), cudaMemcpyHostToDevice, s);
+            if ((e = dmalloc(&doff, 32)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+            cudaMemcpyAsync(doff, dom->stencil_off, 32 * sizeof(int), cudaMemcpyHostToDevice, s);
             k_pack_stencil<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n,
                                                        dom->stencil_k, doff, 2 * slots,
                                                        reinterpret_cast<uint32_t*>(dom->rec));

@@ -127,7 +127,7 @@ struct mclsgpu_domain {
     int walk_block = 256;
     // Stencil records (stencil_k > 0): row r's slot j is column r + stencil_off[j].
     int stencil_k = 0;
-    int stencil_off[16] = {0};
+    int stencil_off[32] = {0};
     // Random stream.
     uint64_t seed = 1;
     unsigned long long* d_epoch = nullptr;  // counter mode: MC solves so far
@@ -208,8 +208,9 @@ int point_jacobi_csr(mclsgpu_context* ctx, int n, const double* dinv,
                      DevCsr& P);
 // SELL-32 copy of a CSR matrix (set-up).
 int csr_to_sell(mclsgpu_context* ctx, const DevCsr& A, DevSell& S);
-// Sorted distinct column offsets (col - row) of A, at most 16 (*K = 0 if more).
-int collect_offsets(mclsgpu_context* ctx, const DevCsr& A, int* offsets, int* K);
+// Sorted distinct column offsets (col - row) of A, at most max_k <= 32
+// (*K = 0 if more).
+int collect_offsets(mclsgpu_context* ctx, const DevCsr& A, int max_k, int* offsets, int* K);
 // Diagonal-offset values of a stencil matrix (K offsets): val[j*n + r].
 int csr_to_dia(mclsgpu_context* ctx, const DevCsr& A, int K, const int* offsets,
                double** val);

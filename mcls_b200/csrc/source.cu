@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256) k_forward_rec(const double* v, int n, dou
 }
 
 struct StencilOffsets {
-    int off[16];
+    int off[32];
 };
 
 // Stencil records: the tally source H b is rebuilt from the record itself,
@@ -338,7 +338,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     if (p.precision == MCLSGPU_FP32) {
         if (dom->stencil_k) {
             StencilOffsets so{};
-            for (int j = 0; j < 16; ++j) so.off[j] = dom->stencil_off[j];
+            for (int j = 0; j < 32; ++j) so.off[j] = dom->stencil_off[j];
             k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
                 v, n, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots,
                 reinterpret_cast<uint32_t*>(dom->rec), dom->y64);

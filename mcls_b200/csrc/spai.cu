@@ -28,6 +28,7 @@
 // The backward kernel propagates G through the network on the tensor cores.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -190,6 +191,11 @@ struct SlotTable {
     int off[kMaxSlots];
     int K;
     int centre;
+    // Two-step offsets o_s + o_t of H = I - M A: distinct values in
+    // ascending order, pair[s][t] their index, pcentre the index of 0.
+    unsigned char pair[kMaxSlots][kMaxSlots];
+    int npair;
+    int pcentre;
 };
 
 // Features of row i from the diagonal-offset storage of A (FP64).
@@ -639,16 +645,64 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
     }
 }
 
-// e_v = v - M (A v) per row; loss and the output gradient G.
+// e_v = v - M (A v) per row; loss and the output gradient G.  With
+// pen_w > 0 the loss adds pen_w/n * sum_i max(0, W_i - pen_c)^2, W_i the
+// row sum of |H| for H = I - M A (the factor by which a forward walk's
+// weight grows at state i), computed from row i of M and the rows of A at
+// its neighbours.
 __global__ void k_spai_loss_grad(int n, int nvec, const int* rp, const int* ci, const double* mval,
                                  const double* dia, SlotTable slots, const double* V,
-                                 const double* Z, const double* wv, float* G, double* loss) {
+                                 const double* Z, const double* wv, double pen_w, double pen_c,
+                                 float* G, double* loss) {
     double part = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double inv = 1.0 / dia[size_t(slots.centre) * n + i];
         double g[kO];
 #pragma unroll
         for (int k = 0; k < kO; ++k) g[k] = 0.0;
+        if (pen_w > 0.0) {
+            double m[kMaxSlots];
+            bool has[kMaxSlots];
+            for (int s = 0; s < kMaxSlots; ++s) {
+                m[s] = 0.0;
+                has[s] = false;
+            }
+            for (int p = rp[i]; p < rp[i + 1]; ++p) {
+                const int d = ci[p] - i;
+                for (int s = 0; s < slots.K; ++s)
+                    if (slots.off[s] == d) {
+                        m[s] = mval[p];
+                        has[s] = true;
+                    }
+            }
+            double h[kMaxSlots * kMaxSlots];
+            for (int q = 0; q < slots.npair; ++q) h[q] = 0.0;
+            h[slots.pcentre] = 1.0;
+            for (int s = 0; s < slots.K; ++s) {
+                const int k = i + slots.off[s];
+                if (!has[s] || k < 0 || k >= n) continue;
+                for (int t = 0; t < slots.K; ++t)
+                    h[slots.pair[s][t]] -= m[s] * dia[size_t(t) * n + k];
+            }
+            double W = 0.0;
+            for (int q = 0; q < slots.npair; ++q) W += fabs(h[q]);
+            const double pen = W - pen_c;
+            if (pen > 0.0) {
+                part += pen_w * pen * pen / double(n);
+                const double coef = 2.0 * pen_w * pen / double(n) * inv;
+                for (int s = 0; s < slots.K; ++s) {
+                    const int k = i + slots.off[s];
+                    if (!has[s] || k < 0 || k >= n) continue;
+                    double dW = 0.0;
+                    for (int t = 0; t < slots.K; ++t) {
+                        const double hv = h[slots.pair[s][t]];
+                        const double sg = hv > 0.0 ? 1.0 : (hv < 0.0 ? -1.0 : 0.0);
+                        dW -= sg * dia[size_t(t) * n + k];
+                    }
+                    g[s] += coef * dW;
+                }
+            }
+        }
         for (int v = 0; v < nvec; ++v) {
             const double* z = Z + size_t(v) * n;
             double mz = 0.0;
@@ -719,6 +773,8 @@ struct mclsgpu_spai {
     float* m = nullptr;       // Adam moments
     float* v = nullptr;
     long long step = 0;
+    double pen_w = 0.0;       // row-sum penalty weight (0 = off)
+    double pen_c = 1.0;       // row-sum threshold
 };
 
 namespace mclsgpu {
@@ -747,6 +803,19 @@ int slot_table(mclsgpu_context* ctx, const mclsgpu_operator* op, int want, SlotT
     for (int s = t.K; s < kMaxSlots; ++s) t.off[s] = 0x7fffffff;
     if (t.centre < 0)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "learned SPAI: operator has no diagonal");
+    std::vector<int> sums;
+    for (int a = 0; a < t.K; ++a)
+        for (int b = 0; b < t.K; ++b) sums.push_back(t.off[a] + t.off[b]);
+    std::sort(sums.begin(), sums.end());
+    sums.erase(std::unique(sums.begin(), sums.end()), sums.end());
+    t.npair = int(sums.size());
+    std::memset(t.pair, 0, sizeof(t.pair));
+    for (int a = 0; a < t.K; ++a)
+        for (int b = 0; b < t.K; ++b)
+            t.pair[a][b] = (unsigned char)(std::lower_bound(sums.begin(), sums.end(),
+                                                            t.off[a] + t.off[b]) -
+                                           sums.begin());
+    t.pcentre = int(std::lower_bound(sums.begin(), sums.end(), 0) - sums.begin());
     return MCLSGPU_OK;
 }
 
@@ -831,7 +900,8 @@ int gradient(mclsgpu_spai* net, mclsgpu_operator* op, const double* V, int nvec,
         }
         k_spai_weights<<<1, 1024, 0, s>>>(g.sq, nvec, g.wv);
         k_spai_loss_grad<<<grid_for(n), 256, 0, s>>>(n, nvec, op->A.rp, op->A.ci, g.mval,
-                                                     op->dia_val, t, V, g.Z, g.wv, g.G, g.loss);
+                                                     op->dia_val, t, V, g.Z, g.wv, net->pen_w,
+                                                     net->pen_c, g.G, g.loss);
         SpaiBwdArgs b{};
         b.params = net->params;
         b.dia = op->dia_val;
@@ -1020,6 +1090,13 @@ int mclsgpu_spai_destroy(mclsgpu_spai* net) {
     return MCLSGPU_OK;
 }
 
+int mclsgpu_spai_set_penalty(mclsgpu_spai* net, double weight, double threshold) {
+    if (!net || !(weight >= 0.0) || !(threshold > 0.0)) return MCLSGPU_ERR_INVALID_ARG;
+    net->pen_w = weight;
+    net->pen_c = threshold;
+    return MCLSGPU_OK;
+}
+
 int mclsgpu_spai_get_params(mclsgpu_spai* net, float* host) {
     if (!net || !host) return MCLSGPU_ERR_INVALID_ARG;
     cudaError_t e = cudaMemcpyAsync(host, net->params, sizeof(float) * kParams,
@@ -1096,6 +1173,45 @@ int mclsgpu_spai_train_step(mclsgpu_spai* net, mclsgpu_operator* op, const doubl
         float(opt->beta2), float(opt->eps), c1, c2, float(opt->grad_clip));
     cudaError_t e = cudaStreamSynchronize(net->ctx->stream);
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(net->ctx, e, "spai adam");
+}
+
+int mclsgpu_spai_smooth_vectors(mclsgpu_spai* net, mclsgpu_operator* op, double* v_dev, int nvec,
+                                int iters) {
+    if (!net || !op || !v_dev || nvec < 1 || iters < 0) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = net->ctx;
+    cudaStream_t s = ctx->stream;
+    SlotTable t;
+    int rc = slot_table(ctx, op, net->slots, t);
+    if (rc) return rc;
+    const int n = op->A.n;
+    DevCsr M;
+    double *w = nullptr, *u = nullptr, *part = nullptr, *sq = nullptr;
+    cudaError_t e;
+    if ((e = dmalloc(&w, n)) != cudaSuccess || (e = dmalloc(&u, n)) != cudaSuccess ||
+        (e = dmalloc(&part, size_t(scan_partials_needed(n)))) != cudaSuccess ||
+        (e = dmalloc(&sq, 1)) != cudaSuccess) {
+        dfree(w); dfree(u); dfree(part); dfree(sq);
+        return cuda_fail(ctx, e, "cudaMalloc");
+    }
+    rc = csr_copy(ctx, op->A, M);
+    if (!rc) rc = launch_forward(net, op, t, M.v, nullptr);
+    if (!rc) {
+        for (int k = 0; k < nvec; ++k) {
+            double* v = v_dev + size_t(k) * n;
+            for (int it = 0; it < iters; ++it) {
+                spmv(s, op->A, v, w);
+                spmv(s, M, w, u);
+                k_sub<<<grid_for(n), 256, 0, s>>>(n, v, u, v);
+                sum_sq(s, v, n, part, sq);
+                k_scale_by_norm<<<grid_for(n), 256, 0, s>>>(n, v, sq);
+            }
+        }
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "spai smooth vectors");
+    }
+    M.release();
+    dfree(w); dfree(u); dfree(part); dfree(sq);
+    return rc;
 }
 
 int mclsgpu_spai_rho(mclsgpu_spai* net, mclsgpu_operator* op, int iters, double* rho_learned,

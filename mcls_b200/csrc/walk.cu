@@ -60,7 +60,7 @@ struct WalkArgs {
     unsigned long long* d_steps;
     unsigned long long* d_tim;  // [0] first warp start, [1] last warp end (ns)
     int* status;
-    int stoff[16];              // stencil records: column offset of each slot
+    int stoff[32];              // stencil records: column offset of each slot
     // trace (FP64 only)
     long long max_trace;
     long long* tr_states;
@@ -384,11 +384,18 @@ void launch32_slots(int slots, const WalkArgs& a, int sms, int block, cudaStream
         else                                                                              \
             blocks_per_sm<SL, DIR, ST, FX, ILP>(block);                                   \
         break;
-    if (ST || ILP > 1) {
+    if (ILP > 1) {
         switch (slots) {
             MCLSGPU_WALK_CASE(4)
             default:
                 MCLSGPU_WALK_CASE(8)
+        }
+    } else if (ST) {
+        switch (slots) {
+            MCLSGPU_WALK_CASE(4)
+            MCLSGPU_WALK_CASE(8)
+            default:
+                MCLSGPU_WALK_CASE(16)
         }
     } else {
         switch (slots) {
@@ -476,7 +483,7 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
     a.tr_w = tr_w;
     a.tr_ev = tr_ev;
     a.tr_start = tr_start;
-    for (int j = 0; j < 16; ++j) a.stoff[j] = dom->stencil_off[j];
+    for (int j = 0; j < 32; ++j) a.stoff[j] = dom->stencil_off[j];
     cudaStream_t st = ctx->stream;
     if (p.precision == MCLSGPU_FP32) {
         if (!fused) cudaMemsetAsync(dom->d_counter, 0, sizeof(int), st);

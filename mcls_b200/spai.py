@@ -59,12 +59,39 @@ def training_vectors(ctx, op, b, n_random=8, seed=0, device=0, iterations=(1, 2,
     return torch.cat([res, rnd], 0).contiguous()
 
 
-def train(net, samples, steps, lr=2e-3, lr_final=2e-4, grad_clip=0.0, log_every=0):
-    """Adam over the (operator, vectors) samples in round robin; cosine-decayed
-    step size.  Returns the per-step losses."""
+def onpolicy_vectors(net, op, count, iters, generator, device=0):
+    """`count` random vectors smoothed by `iters` steps of the current
+    I - M A: the modes the learned-preconditioner iteration (and so MCSA
+    with it) leaves behind, i.e. its residual history from random starts."""
+    import torch
+
+    V = torch.randn((count, op.n), dtype=torch.float64, device=f"cuda:{device}",
+                    generator=generator)
+    net.smooth_vectors(op, V.data_ptr(), count, iters)
+    return V
+
+
+def train(net, samples, steps, lr=2e-3, lr_final=2e-4, grad_clip=0.0, log_every=0,
+          refresh=0, adv_count=4, adv_iters=30, seed=0, device=0):
+    """Adam over the (operator, vectors) samples in round robin with a
+    cosine-decayed step size.  With refresh > 0, every `refresh` steps each
+    sample also gets `adv_count` on-policy vectors (onpolicy_vectors) from
+    the network as it stands, stacked over its fixed vectors.  Returns the
+    per-step losses."""
+    import torch
+
+    gen = torch.Generator(device=f"cuda:{device}")
+    gen.manual_seed(seed)
+    adv = [None] * len(samples)
     losses = []
     for k in range(steps):
-        op, V = samples[k % len(samples)]
+        j = k % len(samples)
+        op, V = samples[j]
+        if refresh > 0:
+            if adv[j] is None or k % refresh < len(samples):
+                adv[j] = torch.cat([onpolicy_vectors(net, op, adv_count, adv_iters, gen, device),
+                                    V], 0).contiguous()
+            V = adv[j]
         t = k / max(steps - 1, 1)
         step_lr = lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * t))
         loss = net.train_step(op, V.data_ptr(), V.shape[0], lr=step_lr, grad_clip=grad_clip)

@@ -110,8 +110,9 @@ def mvalues(A, out):
     return ((d == 0).astype(np.float64) + o) / dia[c][rows]
 
 
-def loss_grad(A, mvals, V):
-    """Loss and dL/dout [n, 16] for vectors V [R, n] (FP64)."""
+def loss_grad(A, mvals, V, pen_w=0.0, pen_c=1.0):
+    """Loss and dL/dout [n, 16] for vectors V [R, n] (FP64).  pen_w > 0 adds
+    pen_w/n * sum_i max(0, W_i - pen_c)^2, W_i = sum_j |(I - M A)_ij|."""
     A = sp.csr_matrix(A)
     n = A.shape[0]
     offs, dia = stencil(A)
@@ -129,6 +130,19 @@ def loss_grad(A, mvals, V):
         loss += w * float(e @ e)
         contrib = -2.0 * w * e[rows] * z[A.indices] / dia[c][rows]
         np.add.at(G, (rows, s), contrib)
+    if pen_w > 0.0:
+        H = (sp.identity(n) - M @ A).tocsr()
+        H.sum_duplicates()
+        W = np.asarray(abs(H).sum(1)).ravel()
+        pen = np.maximum(W - pen_c, 0.0)
+        loss += pen_w * float(pen @ pen) / n
+        # dW_i/dM_ik = -sum_j sign(H_ij) A_kj over the entries (i, k) of M.
+        S = H.copy()
+        S.data = np.sign(S.data)
+        dW = -(S @ A.T).tocsr()  # dW[i, k]
+        coef = 2.0 * pen_w * pen / n
+        dWik = np.asarray(dW[rows, A.indices]).ravel()
+        np.add.at(G, (rows, s), coef[rows] * dWik / dia[c][rows])
     return loss, G
 
 
@@ -153,12 +167,12 @@ def backward(params, acts, G, rounded=True):
     return g
 
 
-def loss_and_gradient(params, A, V, rounded=True):
+def loss_and_gradient(params, A, V, rounded=True, pen_w=0.0, pen_c=1.0):
     """Loss and parameter gradient of the whole chain on (A, V)."""
     X = features(A)
     out, acts = forward(params, X, rounded)
     m = mvalues(A, out)
-    loss, G = loss_grad(A, m, V)
+    loss, G = loss_grad(A, m, V, pen_w, pen_c)
     return loss, backward(params, acts, G, rounded)
 
 

@@ -53,17 +53,18 @@ def test_zero_output_layer_gives_point_jacobi(ctx):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,seed", [(30, 4), (40, 9)])
-def test_gradient_matches_oracle(ctx, n, seed):
+@pytest.mark.parametrize("n,seed,pen_w", [(30, 4, 0.0), (40, 9, 0.0), (30, 4, 5.0)])
+def test_gradient_matches_oracle(ctx, n, seed, pen_w):
     import torch
 
     A, _, _, _ = P.anisotropic2d_sample(n, seed=seed)
     p = so.init_params(5, zero_last=False)
     op, net = _op_and_net(ctx, A, p)
+    net.set_penalty(pen_w, 0.9)
     V = np.random.default_rng(seed).standard_normal((3, A.shape[0]))
     Vt = torch.tensor(V, device="cuda:0").contiguous()
     loss, g = net.gradient(op, Vt.data_ptr(), 3)
-    loss_o, g_o = so.loss_and_gradient(p, A, V, rounded=True)
+    loss_o, g_o = so.loss_and_gradient(p, A, V, rounded=True, pen_w=pen_w, pen_c=0.9)
     np.testing.assert_allclose(loss, loss_o, rtol=5e-3)
     for name, (lo, hi) in BLOCKS.items():
         err = np.linalg.norm(g[lo:hi] - g_o[lo:hi]) / np.linalg.norm(g_o[lo:hi])

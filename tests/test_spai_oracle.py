@@ -6,6 +6,7 @@ pinned by mathematics: the analytic gradient of the loss through the network
 output layer, and the BF16 rounding rule.
 """
 import numpy as np
+import pytest
 import scipy.sparse as sp
 
 from mcls_b200 import problems as P
@@ -52,12 +53,14 @@ def test_features_of_constant_coefficient_stencil():
     assert X[0, 0] == 0 and X[0, 2] == 0
 
 
-def test_analytic_gradient_matches_finite_differences():
+@pytest.mark.parametrize("pen_w", [0.0, 5.0])
+def test_analytic_gradient_matches_finite_differences(pen_w):
     A = _system(n=7, seed=5)
     rng = np.random.default_rng(0)
     V = rng.standard_normal((3, A.shape[0]))
     p = so.init_params(2, zero_last=False).astype(np.float64)
-    loss, g = so.loss_and_gradient(p, A, V, rounded=False)
+    kw = dict(rounded=False, pen_w=pen_w, pen_c=0.9)
+    loss, g = so.loss_and_gradient(p, A, V, **kw)
     assert loss > 0
     idx = np.concatenate([rng.choice(np.arange(so.W1, so.B1), 8, replace=False),
                           rng.choice(np.arange(so.B1, so.W2), 4, replace=False),
@@ -69,9 +72,9 @@ def test_analytic_gradient_matches_finite_differences():
     for k in idx:
         q = p.copy()
         q[k] += eps
-        lp, _ = so.loss_and_gradient(q, A, V, rounded=False)
+        lp, _ = so.loss_and_gradient(q, A, V, **kw)
         q[k] -= 2 * eps
-        lm, _ = so.loss_and_gradient(q, A, V, rounded=False)
+        lm, _ = so.loss_and_gradient(q, A, V, **kw)
         fd = (lp - lm) / (2 * eps)
         assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)) + 1e-5 * abs(g).max(), (k, fd, g[k])
 
@@ -86,3 +89,14 @@ def test_loss_of_jacobi_equals_jacobi_damping():
     Hj = np.eye(A.shape[0]) - np.diag(1.0 / A.diagonal()) @ A.toarray()
     ref = np.mean([np.sum((Hj @ v) ** 2) / np.sum(v * v) for v in V])
     np.testing.assert_allclose(loss, ref, rtol=1e-12)
+
+
+def test_row_sum_penalty_is_active_and_zero_below_threshold():
+    A = _system()
+    V = np.random.default_rng(2).standard_normal((2, A.shape[0]))
+    p = so.init_params(4, zero_last=False)
+    l0, _ = so.loss_and_gradient(p, A, V)
+    l1, _ = so.loss_and_gradient(p, A, V, pen_w=3.0, pen_c=0.5)
+    l2, _ = so.loss_and_gradient(p, A, V, pen_w=3.0, pen_c=100.0)
+    assert l1 > l0
+    assert l2 == l0

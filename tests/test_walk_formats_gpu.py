@@ -45,6 +45,37 @@ def test_stencil_and_packed_records_walk_identically(ctx, name, estimator):
         assert np.allclose(x1, x2, rtol=1e-5, atol=1e-6 * np.abs(x1).max())
 
 
+@pytest.mark.parametrize("direction", [capi.FORWARD, capi.ADJOINT])
+def test_wide_stencil_records_walk_like_packed(ctx, direction):
+    """A left preconditioner on A's 7-point pattern makes H = I - M A a
+    25-offset stencil: 128-byte stencil records (2 + 25 words, padded)
+    against 256-byte packed records."""
+    import scipy.sparse as sp
+
+    A, b = P.diffusion3d_varcoef(10, seed=4)
+    d = 1.0 / A.diagonal()
+    N = sp.diags(d) @ (sp.diags(A.diagonal()) - A)  # D^-1 (D - A), off-diagonal
+    M = (sp.diags(d) @ (sp.identity(A.shape[0]) + 0.3 * N)).tocsr()
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_USER_CSR, user=M)
+    out = {}
+    for fmt in (capi.RECORD_PACKED, capi.RECORD_STENCIL):
+        dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=5,
+                          record_format=fmt, direction=direction, estimator=capi.COLLISION,
+                          sample_ratio=2.0)
+        info = dom.info()
+        x, st = dom.mcsa_solve(b, tolerance=0.0, max_iters=15)
+        out[fmt] = (x, st, info)
+    (x1, s1, i1), (x2, s2, i2) = out[capi.RECORD_PACKED], out[capi.RECORD_STENCIL]
+    assert i2["record_format"] == capi.RECORD_STENCIL and i2["stencil_offsets"] == 25
+    assert i2["record_bytes"] == 128 and i1["record_bytes"] == 256
+    assert s1["walk_steps"] == s2["walk_steps"] > 0
+    if direction == capi.FORWARD:
+        assert np.array_equal(x1, x2)
+    else:  # adjoint tallies: FP64 atomics from many histories, any order
+        assert np.linalg.norm(x1 - x2) <= 1e-9 * np.linalg.norm(x1)
+
+
 def test_domain_query_reports_layouts(ctx):
     A, _ = P.diffusion3d_varcoef(8, seed=1)
     op = capi.Operator(ctx, A)
