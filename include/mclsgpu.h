@@ -343,6 +343,41 @@ int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev,
  * src/MCLS_LinearProblem.hpp:121-122). */
 int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev);
 
+/* ---- batched MCSA: many systems, many right-hand sides -------------------- */
+/* No single counterpart in the reference, which solves one system per
+ * manager (MCSASolverManager::solve, src/MCLS_MCSASolverManager_impl.hpp:
+ * 278-432).  m square systems (host int64 CSR each) with 1..16 right-hand
+ * sides each are solved in one MCSA loop: one block-diagonal point-Jacobi
+ * domain, one shared set of forward FP32 walks per iteration whose histories
+ * carry a tally per right-hand side, and a separate convergence test
+ * |rp|_2 <= tol |D^-1 b|_2 for every (system, right-hand side) pair.  The
+ * loop (six kernels per iteration) runs in a captured CUDA graph.  params
+ * must ask for forward FP32 walks without a weight cutoff. */
+typedef struct mclsgpu_batch mclsgpu_batch;
+int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
+                        const int64_t* const* rowptr, const int64_t* const* colind,
+                        const double* const* values, const int32_t* nrhs,
+                        const mclsgpu_mc_params* params, mclsgpu_batch** out);
+int mclsgpu_batch_destroy(mclsgpu_batch* b);
+/* Vector layout: [rows][width] row-major FP64; system s owns rows
+ * row_offsets[s] .. row_offsets[s+1]-1 and columns 0 .. nrhs[s]-1 (the other
+ * columns are ignored).  row_offsets has nsys+1 entries (may be NULL). */
+int mclsgpu_batch_layout(mclsgpu_batch* b, int64_t* row_offsets, int32_t* width);
+/* The batch's block-diagonal domain (for mclsgpu_domain_query/reseed). */
+int mclsgpu_batch_domain(mclsgpu_batch* b, mclsgpu_domain** dom);
+/* Walk threads per block (128 or 256); the autotuner times both on `reps`
+ * iterations of b_dev (x_dev is overwritten) and keeps the faster. */
+int mclsgpu_batch_set_launch(mclsgpu_batch* b, int block_size);
+int mclsgpu_batch_autotune(mclsgpu_batch* b, const double* b_dev, double* x_dev, int reps,
+                           int* block_size, double* walk_ms);
+/* x_dev holds the initial guesses and receives the solutions.  Optional host
+ * outputs, [nsys][width]: conv_iters = the iteration at which each pair first
+ * met the tolerance (-1: never, or an unused column), rel_resid = the final
+ * |rp|_2 / |D^-1 b|_2.  params->smoother_steps must be 1. */
+int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* x_dev,
+                                 const mclsgpu_mcsa_params* params, int32_t* conv_iters,
+                                 double* rel_resid, mclsgpu_stats* stats);
+
 /* ---- spectral radius ------------------------------------------------------- */
 /* Replaces AlmostOptimalDomain::computeConvergenceCriteria
  * (src/MCLS_AlmostOptimalDomain_impl.hpp:437-635): FP64 power iteration

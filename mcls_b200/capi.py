@@ -134,6 +134,9 @@ EXPORTS = [
     "mclsgpu_spai_destroy", "mclsgpu_spai_get_params", "mclsgpu_spai_set_params",
     "mclsgpu_spai_infer", "mclsgpu_spai_gradient", "mclsgpu_spai_train_step", "mclsgpu_spai_rho",
     "mclsgpu_domain_residual", "mclsgpu_spai_smooth_vectors", "mclsgpu_spai_set_penalty",
+    "mclsgpu_batch_build", "mclsgpu_batch_destroy", "mclsgpu_batch_layout",
+    "mclsgpu_batch_domain", "mclsgpu_batch_set_launch", "mclsgpu_batch_autotune",
+    "mclsgpu_batch_mcsa_solve_dev",
 ]
 
 _LIB = None
@@ -204,6 +207,14 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_spai_rho.argtypes = [P, P, C.c_int, C.POINTER(d), C.POINTER(d)]
     L.mclsgpu_spai_smooth_vectors.argtypes = [P, P, P, C.c_int, C.c_int]
     L.mclsgpu_spai_set_penalty.argtypes = [P, d, d]
+    L.mclsgpu_batch_build.argtypes = [P, C.c_int, P, P, P, P, P, C.POINTER(McParams), PP]
+    L.mclsgpu_batch_destroy.argtypes = [P]
+    L.mclsgpu_batch_layout.argtypes = [P, P, C.POINTER(C.c_int32)]
+    L.mclsgpu_batch_domain.argtypes = [P, PP]
+    L.mclsgpu_batch_set_launch.argtypes = [P, C.c_int]
+    L.mclsgpu_batch_autotune.argtypes = [P, P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(d)]
+    L.mclsgpu_batch_mcsa_solve_dev.argtypes = [P, P, P, C.POINTER(McsaParams), P, P,
+                                               C.POINTER(Stats)]
     _LIB = L
     return L
 
@@ -550,6 +561,90 @@ class SpaiNet:
     def close(self):
         if getattr(self, "h", None):
             self.ctx.L.mclsgpu_spai_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Many systems with 1..16 right-hand sides each in one MCSA loop
+    (forward FP32 walks shared by every right-hand side)."""
+
+    def __init__(self, ctx: Context, systems, nrhs, params: McParams | None = None, **kw):
+        self.ctx = ctx
+        p = params if params is not None else mc_params(**kw)
+        mats = [_csr64(A) for A in systems]
+        self.nsys = len(mats)
+        n = np.array([m[0] for m in mats], np.int64)
+        rp = (C.c_void_p * self.nsys)(*[m[1].ctypes.data for m in mats])
+        ci = (C.c_void_p * self.nsys)(*[m[2].ctypes.data for m in mats])
+        va = (C.c_void_p * self.nsys)(*[m[3].ctypes.data for m in mats])
+        self.nrhs = np.ascontiguousarray(nrhs, np.int32)
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_batch_build(ctx.h, self.nsys, _ptr(n), rp, ci, va,
+                                            _ptr(self.nrhs), C.byref(p), C.byref(h)))
+        del mats
+        self.h = h
+        off = np.empty(self.nsys + 1, np.int64)
+        w = C.c_int32()
+        ctx.check(ctx.L.mclsgpu_batch_layout(self.h, _ptr(off), C.byref(w)))
+        self.offsets, self.width = off, w.value
+        self.rows = int(off[-1])
+        ctx._adopt(self)
+
+    def pack(self, vectors):
+        """[rows, width] array from per-system [n_s, nrhs_s] blocks."""
+        out = np.zeros((self.rows, self.width))
+        for s, v in enumerate(vectors):
+            v = np.asarray(v, np.float64).reshape(self.offsets[s + 1] - self.offsets[s], -1)
+            out[self.offsets[s]:self.offsets[s + 1], : v.shape[1]] = v
+        return out
+
+    def unpack(self, X):
+        X = np.asarray(X)
+        return [X[self.offsets[s]:self.offsets[s + 1], : self.nrhs[s]] for s in range(self.nsys)]
+
+    def domain_info(self):
+        hd = C.c_void_p()
+        self.ctx.check(self.ctx.L.mclsgpu_batch_domain(self.h, C.byref(hd)))
+        d = DomainInfo()
+        d.size = C.sizeof(DomainInfo)
+        self.ctx.check(self.ctx.L.mclsgpu_domain_query(hd, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in d._fields_ if k != "size"}
+
+    def reseed(self, seed):
+        hd = C.c_void_p()
+        self.ctx.check(self.ctx.L.mclsgpu_batch_domain(self.h, C.byref(hd)))
+        self.ctx.check(self.ctx.L.mclsgpu_domain_reseed(hd, seed))
+
+    def set_launch(self, block_size):
+        self.ctx.check(self.ctx.L.mclsgpu_batch_set_launch(self.h, block_size))
+
+    def autotune(self, b_ptr, x_ptr, reps=3):
+        blk, ms = C.c_int(), C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_batch_autotune(self.h, C.c_void_p(b_ptr),
+                                                         C.c_void_p(x_ptr), reps, C.byref(blk),
+                                                         C.byref(ms)))
+        return {"block_size": blk.value, "walk_ms": ms.value}
+
+    def mcsa_solve_dev(self, b_ptr, x_ptr, params: McsaParams | None = None, **kw):
+        """Solve in place on device [rows, width] arrays; returns (stats,
+        per-pair convergence iterations [nsys, width], final relative
+        preconditioned residuals [nsys, width])."""
+        p = params if params is not None else mcsa_params(**kw)
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        it = np.empty((self.nsys, self.width), np.int32)
+        rr = np.empty((self.nsys, self.width), np.float64)
+        self.ctx.check(self.ctx.L.mclsgpu_batch_mcsa_solve_dev(self.h, C.c_void_p(b_ptr),
+                                                               C.c_void_p(x_ptr), C.byref(p),
+                                                               _ptr(it), _ptr(rr), C.byref(st)))
+        return st.as_dict(), it, rr
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

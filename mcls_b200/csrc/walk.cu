@@ -444,14 +444,120 @@ void prepare_walk(mclsgpu_domain* dom) {
     dispatch_walk32(dom, a, false);
 }
 
-// Launch the walks of the current source.  Trace arrays only with FP64.
-// `fused`: the work-queue counter reset and the timing accumulation are done
-// by the fused residual kernel that follows the walk (MCSA loop).
-void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
-                 int* tr_ev, long long* tr_start, bool fused) {
+namespace {
+
+// Forward walks shared by R right-hand sides (batched MCSA): the walk does
+// not depend on the source, so each history carries R Kahan-compensated FP32
+// sums of w * c_r(state) (cR is row-major [n][R], the tally source of every
+// right-hand side at a state) and adds them into Y[start][r] in FP64.
+// Fixed-length histories only.
+template <int S, bool ST, int R>
+__global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* __restrict__ cR,
+                                                       double* __restrict__ Y) {
+    static_assert(S % 4 == 0, "records are whole 32-byte halves");
+    __shared__ uint64_t s_ekey;
+    __shared__ int s_nh;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_ekey = epoch_key(a.seed, *a.d_epoch);
+        s_nh = *a.d_nh;
+    }
+    __syncthreads();
+    const char* rec = reinterpret_cast<const char*>(a.rec);
+    if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
+    unsigned steps = 0;
+    const int L = a.L;
+    while (true) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(a.d_counter, 32);
+        base = __shfl_sync(kFull, base, 0);
+        const int nh = s_nh;
+        if (base >= nh) break;
+        const int e = base + lane;
+        const bool alive = e < nh;
+        int s = 0;
+        float w = 0.f;
+        uint64_t x = 0;
+        if (alive) walk_start<MCLSGPU_FORWARD>(a, e, s_ekey, 1.f, s, w, x);
+        const int s0 = s;
+        float acc[R], comp[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = comp[r] = 0.f;
+        if (alive) {
+            for (int k = 0; k < L; ++k) {
+                float c[R];
+                const float* cs = cR + size_t(s) * R;
+                if constexpr (R % 4 == 0) {
+#pragma unroll
+                    for (int r = 0; r < R; r += 4) {
+                        const float4 q = __ldg(reinterpret_cast<const float4*>(cs + r));
+                        c[r] = q.x;
+                        c[r + 1] = q.y;
+                        c[r + 2] = q.z;
+                        c[r + 3] = q.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) c[r] = __ldg(cs + r);
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float term = w * c[r] - comp[r];
+                    const float t = acc[r] + term;
+                    comp[r] = (t - acc[r]) - term;
+                    acc[r] = t;
+                }
+                float da = 0.f, dc = 0.f;  // the record header's own tally is unused here
+                walk_step<S, MCLSGPU_FORWARD, ST>(a, rec, s, w, x, da, dc, k);
+            }
+            steps += L;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (acc[r] != 0.f || comp[r] != 0.f)
+                    atomicAdd(&Y[size_t(s0) * R + r], double(acc[r]) - double(comp[r]));
+        }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) steps += __shfl_down_sync(kFull, steps, d);
+    if (lane == 0) {
+        if (steps) atomicAdd(a.d_steps, (unsigned long long)steps);
+        atomicMax(&a.d_tim[1], global_ns());
+    }
+}
+
+template <int S, bool ST, int R>
+void launch_multi_sr(const WalkArgs& a, const float* cR, double* Y, int sms, int block,
+                     cudaStream_t st) {
+    static int cached[2] = {0, 0};
+    const int slot = block == 128 ? 0 : 1;
+    if (!cached[slot]) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32_multi<S, ST, R>, block, 0);
+        cached[slot] = b > 0 ? b : 1;
+    }
+    walk32_multi<S, ST, R><<<sms * cached[slot], block, 0, st>>>(a, cR, Y);
+}
+
+template <int S, bool ST>
+bool launch_multi_s(int R, const WalkArgs& a, const float* cR, double* Y, int sms, int block,
+                    cudaStream_t st) {
+    switch (R) {
+        case 1: launch_multi_sr<S, ST, 1>(a, cR, Y, sms, block, st); return true;
+        case 2: launch_multi_sr<S, ST, 2>(a, cR, Y, sms, block, st); return true;
+        case 4: launch_multi_sr<S, ST, 4>(a, cR, Y, sms, block, st); return true;
+        case 8: launch_multi_sr<S, ST, 8>(a, cR, Y, sms, block, st); return true;
+        case 16: launch_multi_sr<S, ST, 16>(a, cR, Y, sms, block, st); return true;
+        default: return false;
+    }
+}
+
+}  // namespace
+
+// Fill the walk arguments of a domain (shared by the single- and the
+// multi-right-hand-side walks).
+static void fill_walk_args(mclsgpu_domain* dom, WalkArgs& a) {
     mclsgpu_context* ctx = dom->ctx;
     const mclsgpu_mc_params& p = dom->p;
-    WalkArgs a{};
     a.n = dom->n;
     a.L = p.history_length;
     a.per = p.sample_ratio > 0.0 ? int(ceil(p.sample_ratio)) : 1;
@@ -460,13 +566,63 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
     a.d_counter = dom->d_counter;
     a.start = dom->start;
     a.sc = dom->d_scalars;
-    a.cutoff = float(p.weight_cutoff > 0.0 ? p.weight_cutoff : 0.0);
-    a.cutoff64 = p.weight_cutoff > 0.0 ? p.weight_cutoff : 0.0;
     a.seed = dom->seed;
     a.d_epoch = dom->d_epoch;
     a.jump = dom->d_jump;
     a.d_pos = dom->d_pos;
     a.rec = dom->rec;
+    a.d_steps = dom->d_steps;
+    a.d_tim = dom->d_tim;
+    a.status = ctx->d_status;
+    for (int j = 0; j < 32; ++j) a.stoff[j] = dom->stencil_off[j];
+}
+
+// Multi-right-hand-side forward walks over the domain's FP32 records (R in
+// {1, 2, 4, 8, 16}; records of at most 16 slots).  The work-queue counter must
+// be zero on entry; the caller resets it afterwards.
+int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y) {
+    mclsgpu_context* ctx = dom->ctx;
+    if (dom->p.precision != MCLSGPU_FP32 || dom->p.direction != MCLSGPU_FORWARD || !dom->slots)
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batched walks need FP32 forward records");
+    WalkArgs a{};
+    fill_walk_args(dom, a);
+    const int sms = ctx->num_sms;
+    const int block = dom->walk_block;
+    cudaStream_t st = ctx->stream;
+    bool ok = false;
+    if (dom->stencil_k) {
+        switch (dom->slots) {
+            case 4: ok = launch_multi_s<4, true>(R, a, cR, Y, sms, block, st); break;
+            case 8: ok = launch_multi_s<8, true>(R, a, cR, Y, sms, block, st); break;
+            default: ok = false;
+        }
+    } else {
+        switch (dom->slots) {
+            case 4: ok = launch_multi_s<4, false>(R, a, cR, Y, sms, block, st); break;
+            case 8: ok = launch_multi_s<8, false>(R, a, cR, Y, sms, block, st); break;
+            case 12: ok = launch_multi_s<12, false>(R, a, cR, Y, sms, block, st); break;
+            case 16: ok = launch_multi_s<16, false>(R, a, cR, Y, sms, block, st); break;
+            default: ok = false;
+        }
+    }
+    if (!ok)
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
+                         "batched walks: %d right-hand sides on %d-slot records not supported", R,
+                         dom->slots);
+    return MCLSGPU_OK;
+}
+
+// Launch the walks of the current source.  Trace arrays only with FP64.
+// `fused`: the work-queue counter reset and the timing accumulation are done
+// by the fused residual kernel that follows the walk (MCSA loop).
+void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states, double* tr_w,
+                 int* tr_ev, long long* tr_start, bool fused) {
+    mclsgpu_context* ctx = dom->ctx;
+    const mclsgpu_mc_params& p = dom->p;
+    WalkArgs a{};
+    fill_walk_args(dom, a);
+    a.cutoff = float(p.weight_cutoff > 0.0 ? p.weight_cutoff : 0.0);
+    a.cutoff64 = p.weight_cutoff > 0.0 ? p.weight_cutoff : 0.0;
     a.rp = dom->D.rp;
     a.col = dom->D.ci;
     a.h = dom->D.v;
@@ -475,15 +631,11 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
     a.y64 = dom->y64;
     a.c32 = dom->c32;
     a.c64 = dom->c64;
-    a.d_steps = dom->d_steps;
-    a.d_tim = dom->d_tim;
-    a.status = ctx->d_status;
     a.max_trace = max_trace;
     a.tr_states = tr_states;
     a.tr_w = tr_w;
     a.tr_ev = tr_ev;
     a.tr_start = tr_start;
-    for (int j = 0; j < 32; ++j) a.stoff[j] = dom->stencil_off[j];
     cudaStream_t st = ctx->stream;
     if (p.precision == MCLSGPU_FP32) {
         if (!fused) cudaMemsetAsync(dom->d_counter, 0, sizeof(int), st);
