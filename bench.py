@@ -36,6 +36,12 @@ CONFIGS = {
                         "expected-value estimator, FP32 walks / FP64 tallies, residual and update, "
                         "2^22 histories per iteration",
                n=128, sample_ratio=2.0, estimator=1, history_length=10, direction=1),
+    "batched": dict(workload="batched: 1024 systems (2D/3D Poisson and var-coef diffusion, N "
+                             "log-uniform in [1e3, nmax] on square/cube grids), 1-16 right-hand "
+                             "sides uniform(0,1) each, point-Jacobi forward expected-value MCSA, "
+                             "FP32 walks shared by all right-hand sides, FP64 residuals, one "
+                             "graph-captured loop, per-(system, rhs) convergence to 1e-8",
+                    n=0, sample_ratio=1.0, estimator=1, history_length=10, direction=1),
     "poisson100": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, adjoint collision estimator, "
                         "FP64 walks, N histories per iteration",
                n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0),
@@ -236,6 +242,112 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     return out
 
 
+def run_batched(args, world, rank, local, pg):
+    """Batched workload: every step solves all (system, rhs) pairs to 1e-8."""
+    import torch
+
+    from mcls_b200 import capi
+    from mcls_b200 import problems as P
+
+    cfgd = CONFIGS["batched"]
+    torch.cuda.set_device(local)
+    systems, nrhs, rhs, kinds = P.batch_sample(args.batch_systems, 1e3, args.batch_nmax,
+                                               seed=rank)
+    ctx = capi.Context(local)
+    seed = 1234 + rank
+    bt = capi.Batch(ctx, systems, nrhs, direction=capi.FORWARD, estimator=cfgd["estimator"],
+                    precision=capi.FP32, sample_ratio=cfgd["sample_ratio"],
+                    history_length=cfgd["history_length"], seed=seed)
+    Bh = bt.pack(rhs)
+    B = torch.tensor(Bh, device=f"cuda:{local}").contiguous()
+    X = torch.zeros_like(B)
+    tuned = bt.autotune(B.data_ptr(), X.data_ptr(), reps=3)
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
+                          host_loop=1 if args.host_loop else 0)
+
+    def step():
+        bt.reseed(seed)
+        X.zero_()
+        torch.cuda.synchronize()
+        return bt.mcsa_solve_dev(B.data_ptr(), X.data_ptr(), params=mp)
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    barrier(pg)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = time.perf_counter()
+    res = [step() for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(pg)
+    clk = clocks.stop()
+    stats = [r[0] for r in res]
+    dev_ms = sum(s["solve_ms"] for s in stats)
+    dev_ms_max = allmax(pg, dev_ms)
+    steps_all = allsum(pg, sum(s["walk_steps"] for s in stats))
+    value = steps_all / (dev_ms_max * 1e-3)
+    # End to end: host right-hand sides in, host solutions out, every step.
+    pinned_b = torch.tensor(Bh).pin_memory()
+    pinned_x = torch.empty_like(pinned_b).pin_memory()
+    e2e_ms = 0.0
+    e2e_steps = 0
+    barrier(pg)
+    for _ in range(args.steps):
+        bt.reseed(seed)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        B.copy_(pinned_b, non_blocking=True)
+        X.zero_()
+        st, _, _ = bt.mcsa_solve_dev(B.data_ptr(), X.data_ptr(), params=mp)
+        pinned_x.copy_(X, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_ms += (time.perf_counter() - t1) * 1e3
+        e2e_steps += st["walk_steps"]
+    e2e_ms = allmax(pg, e2e_ms)
+    e2e_value = allsum(pg, e2e_steps) / (e2e_ms * 1e-3)
+    s0, it, rr = res[-1]
+    pairs = int(sum(nrhs))
+    info = bt.domain_info()
+    peak, peak_kind = load_peaks()
+    walk_ms = sum(s["walk_ms"] for s in stats)
+    launches = sum(s["walk_launches"] for s in stats)
+    per_launch = walk_ms / max(launches, 1)
+    bstep = info["record_bytes"] + 4 * bt.width  # record + one FP32 tally-source row
+    walk_steps = sum(s["walk_steps"] for s in stats)
+    achieved = (bstep * walk_steps / max(launches, 1)) / (per_launch * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfgd["workload"].replace("nmax", f"{args.batch_nmax:g}"),
+                   "systems": args.batch_systems, "rows": bt.rows, "rhs_width": bt.width,
+                   "pairs": pairs, "kinds": {k: kinds.count(k) for k in sorted(set(kinds))},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single batch",
+                   "walk_launch": tuned, "l2": "inputs larger than L2 (no flush)",
+                   "time_to_1e-8_s": dev_ms_max / args.steps / 1e3,
+                   "iterations": s0["iterations"], "pairs_converged": int((it >= 0).sum()),
+                   "max_rel_residual": float(rr.max()),
+                   "median_pair_iterations":
+                       float(np.median(it[it >= 0])) if (it >= 0).any() else None},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(Bh.nbytes),
+                "d2h_bytes_per_step": int(Bh.nbytes)},
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "kernel": "walk32_multi", "peak_kind": peak_kind, "bytes_per_step": bstep,
+                     "walk_ms_per_launch": per_launch,
+                     "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
+        "wall_s": wall,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    bt.close()
+    ctx.close()
+
+
 def ctx_device():
     import torch
 
@@ -301,8 +413,16 @@ def main():
     ap.add_argument("--host-loop", action="store_true",
                     help="host-driven MCSA loop (for profilers that cannot see kernels "
                          "inside conditional graph nodes)")
+    ap.add_argument("--batch-systems", type=int, default=1024)
+    ap.add_argument("--batch-nmax", type=float, default=1e4,
+                    help="largest system of the batched workload (5e5 for the full size)")
     args = ap.parse_args()
     world, rank, local, pg = dist_init(args)
+    if args.impl == "mcls_b200" and args.config == "batched":
+        run_batched(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, world, rank, pg)
         if pg is not None:

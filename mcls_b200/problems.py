@@ -177,3 +177,69 @@ def anisotropic2d_sample(n: int, seed: int):
     A = anisotropic2d(n, ratio, theta)
     b = rng.uniform(0.0, 1.0, size=n * n)
     return A, b, ratio, theta
+
+
+def _diffusion2d(D: np.ndarray, sigma: np.ndarray, h: float):
+    """5-point finite-volume operator for per-cell D and sigma (shape n x n),
+    harmonic face coefficients, Dirichlet zero boundary (cell coefficient)."""
+    n = D.shape[0]
+    N = n * n
+    inv = 1.0 / (h * h)
+    diag = sigma.reshape(N).astype(np.float64).copy()
+    offs, vals = [], []
+    for axis, stride in ((1, 1), (0, n)):
+        a = np.take(D, range(0, n - 1), axis=axis)
+        b = np.take(D, range(1, n), axis=axis)
+        Df = 2.0 * a * b / (a + b)
+        up = np.zeros_like(D)
+        dn = np.zeros_like(D)
+        sl = [slice(None)] * 2
+        sl[axis] = slice(0, n - 1)
+        up[tuple(sl)] = Df
+        sl[axis] = slice(1, n)
+        dn[tuple(sl)] = Df
+        bnd = np.zeros_like(D)
+        lo = [slice(None)] * 2
+        hi = [slice(None)] * 2
+        lo[axis] = 0
+        hi[axis] = n - 1
+        bnd[tuple(lo)] += D[tuple(lo)]
+        bnd[tuple(hi)] += D[tuple(hi)]
+        diag += (up.reshape(N) + dn.reshape(N) + bnd.reshape(N)) * inv
+        offs += [stride, -stride]
+        vals += [-up.reshape(N)[: N - stride] * inv, -dn.reshape(N)[stride:] * inv]
+    A = sp.diags([diag] + vals, [0] + offs, shape=(N, N), format="csr")
+    return _csr(A)
+
+
+def batch_sample(count: int, nmin: float, nmax: float, seed: int = 0, rhs_max: int = 16):
+    """Batched workload: `count` systems, each 2D Poisson / 2D var-coef / 3D
+    Poisson / 3D var-coef with probability 1/4, N log-uniform in
+    [nmin, nmax] rounded to the nearest square or cube grid, 1..rhs_max
+    right-hand sides uniform(0, 1) each (coefficients log-uniform in
+    [0.1, 10] per cell, absorption 0.01 for the var-coef kinds)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    systems, nrhs, rhs, kinds = [], [], [], []
+    for _ in range(count):
+        kind = int(rng.integers(0, 4))
+        N = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        if kind < 2:
+            n = max(3, int(round(np.sqrt(N))))
+            if kind == 0:
+                A = poisson2d(n)
+            else:
+                D = np.exp(rng.uniform(np.log(0.1), np.log(10.0), size=(n, n)))
+                A = _diffusion2d(D, np.full((n, n), 0.01), 1.0 / (n + 1))
+        else:
+            n = max(3, int(round(N ** (1.0 / 3.0))))
+            if kind == 2:
+                A = _diffusion3d(np.ones((n, n, n)), np.zeros((n, n, n)), 1.0 / (n + 1))
+            else:
+                D = np.exp(rng.uniform(np.log(0.1), np.log(10.0), size=(n, n, n)))
+                A = _diffusion3d(D, np.full((n, n, n), 0.01), 1.0 / (n + 1))
+        r = int(rng.integers(1, rhs_max + 1))
+        systems.append(A)
+        nrhs.append(r)
+        rhs.append(rng.uniform(0.0, 1.0, size=(A.shape[0], r)))
+        kinds.append(("poisson2d", "varcoef2d", "poisson3d", "varcoef3d")[kind])
+    return systems, nrhs, rhs, kinds
