@@ -22,7 +22,8 @@
 
 namespace mclsgpu {
 
-int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y);
+int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y, const int* rsys,
+                      const int* sys_done);
 
 namespace {
 
@@ -66,6 +67,8 @@ struct BatchArgs {
     double* bnorm2;
     int* conv_iter;      // [nsys][R]
     const int* nrhs;
+    int* sys_done;       // per system: every right-hand side converged
+    int skip;            // skip the rows of finished systems
     BatchState* st;
     double omega;        // Richardson relaxation
     double nomega;       // Neumann relaxation (1 when absent)
@@ -77,31 +80,33 @@ struct BatchArgs {
     int* status;
 };
 
+// All per-row kernels below run one thread per (row, column) element: with
+// the [rows][R] row-major layout a warp then reads whole 8R-byte rows of X,
+// RP and B at every matrix entry, so every load and store is coalesced.
+template <int R>
+__device__ __forceinline__ void elem_rc(long long t, int& i, int& r) {
+    i = int(t / R);
+    r = int(t % R);
+}
+
 // x2 = x + w rp;  rp2 = D^-1 (b - S x2), with x2 at the neighbours formed on
 // the fly (RichardsonIteration::doOneIteration then updatePrecResidual,
 // src/MCLS_RichardsonIteration_impl.hpp:134-147).
 template <int R>
 __global__ void __launch_bounds__(kThreads) k_b_richardson_residual(BatchArgs a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        double acc[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) acc[r] = 0.0;
+    const long long total = (long long)a.n * R;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, r;
+        elem_rc<R>(t, i, r);
+        if (a.skip && a.sys_done[a.rsys[i]]) continue;
+        double acc = 0.0;
         for (int p = a.rp[i]; p < a.rp[i + 1]; ++p) {
-            const int j = a.ci[p];
-            const double v = a.v[p];
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                acc[r] = fma(v, __dadd_rn(a.X[size_t(j) * R + r],
-                                          __dmul_rn(a.omega, a.RP[size_t(j) * R + r])),
-                             acc[r]);
+            const size_t k = size_t(a.ci[p]) * R + r;
+            acc = fma(a.v[p], __dadd_rn(a.X[k], __dmul_rn(a.omega, a.RP[k])), acc);
         }
-        const double d = a.dinv[i];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const size_t k = size_t(i) * R + r;
-            a.X2[k] = __dadd_rn(a.X[k], __dmul_rn(a.omega, a.RP[k]));
-            a.RP2[k] = d * (a.B[k] - acc[r]);
-        }
+        a.X2[t] = __dadd_rn(a.X[t], __dmul_rn(a.omega, a.RP[t]));
+        a.RP2[t] = a.dinv[i] * (a.B[t] - acc);
     }
 }
 
@@ -109,24 +114,21 @@ __global__ void __launch_bounds__(kThreads) k_b_richardson_residual(BatchArgs a)
 // collision c = w rp2 (FP32).
 template <int R>
 __global__ void __launch_bounds__(kThreads) k_b_source(BatchArgs a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        float* c = a.cR + size_t(i) * R;
+    const long long total = (long long)a.n * R;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, r;
+        elem_rc<R>(t, i, r);
+        if (a.skip && a.sys_done[a.rsys[i]]) continue;  // walks skip these rows too
+        double v;
         if (a.ev) {
-            double acc[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) acc[r] = 0.0;
-            for (int p = a.hrp[i]; p < a.hrp[i + 1]; ++p) {
-                const int j = a.hci[p];
-                const double h = a.hv[p];
-#pragma unroll
-                for (int r = 0; r < R; ++r) acc[r] = fma(h, a.RP2[size_t(j) * R + r], acc[r]);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) c[r] = __double2float_rn(a.nomega * acc[r]);
+            v = 0.0;
+            for (int p = a.hrp[i]; p < a.hrp[i + 1]; ++p)
+                v = fma(a.hv[p], a.RP2[size_t(a.hci[p]) * R + r], v);
         } else {
-#pragma unroll
-            for (int r = 0; r < R; ++r) c[r] = __double2float_rn(a.nomega * a.RP2[size_t(i) * R + r]);
+            v = a.RP2[t];
         }
+        a.cR[t] = __double2float_rn(a.nomega * v);
     }
 }
 
@@ -135,65 +137,53 @@ __global__ void __launch_bounds__(kThreads) k_b_source(BatchArgs a) {
 // (ForwardTally::finalize, src/MCLS_ForwardTally_impl.hpp:180-209).
 template <int R>
 __global__ void __launch_bounds__(kThreads) k_b_correction(BatchArgs a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const size_t k = size_t(i) * R + r;
-            double d = a.Y[k] * a.inv_per;
-            if (a.ev) d += a.nomega * a.RP2[k];
-            a.X[k] = a.X2[k] + d;
-            a.Y[k] = 0.0;
-        }
+    const long long total = (long long)a.n * R;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (a.skip && a.sys_done[a.rsys[int(t / R)]]) continue;
+        double d = a.Y[t] * a.inv_per;
+        if (a.ev) d += a.nomega * a.RP2[t];
+        a.X[t] = a.X2[t] + d;
+        a.Y[t] = 0.0;
     }
 }
 
-// rp = D^-1 (b - S x) and the per-(system, rhs) sums of squares: a warp whose
-// rows all belong to one system reduces with shuffles, otherwise each lane
-// adds its own.
+// rp = D^-1 (b - S x) and the per-(system, rhs) sums of squares.  A warp
+// covers 32/R rows: when they all belong to one system the lanes of each
+// column reduce with shuffles and one lane per column adds the sum,
+// otherwise every lane adds its own square.
 template <int R>
 __global__ void __launch_bounds__(kThreads) k_b_residual_norm(BatchArgs a, const double* Xin) {
     const unsigned full = 0xffffffffu;
-    for (int base = blockIdx.x * blockDim.x; base < a.n; base += gridDim.x * blockDim.x) {
-        const int i = base + threadIdx.x;
-        const bool live = i < a.n;
-        double sq[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) sq[r] = 0.0;
-        int sys = -1;
+    const long long total = (long long)a.n * R;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < total;
+         base += (long long)gridDim.x * blockDim.x) {
+        const long long t = base + threadIdx.x;
+        const bool live = t < total;
+        double sq = 0.0;
+        int sys = -1, r = 0;
         if (live) {
-            double acc[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) acc[r] = 0.0;
-            for (int p = a.rp[i]; p < a.rp[i + 1]; ++p) {
-                const int j = a.ci[p];
-                const double v = a.v[p];
-#pragma unroll
-                for (int r = 0; r < R; ++r) acc[r] = fma(v, Xin[size_t(j) * R + r], acc[r]);
-            }
-            const double d = a.dinv[i];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const size_t k = size_t(i) * R + r;
-                const double rv = d * (a.B[k] - acc[r]);
-                a.RP[k] = rv;
-                sq[r] = rv * rv;
-            }
+            int i;
+            elem_rc<R>(t, i, r);
             sys = a.rsys[i];
+            if (!(a.skip && a.sys_done[sys])) {
+                double acc = 0.0;
+                for (int p = a.rp[i]; p < a.rp[i + 1]; ++p)
+                    acc = fma(a.v[p], Xin[size_t(a.ci[p]) * R + r], acc);
+                const double rv = a.dinv[i] * (a.B[t] - acc);
+                a.RP[t] = rv;
+                sq = rv * rv;
+            }
         }
         const int s0 = __shfl_sync(full, sys, 0);
         const bool uniform = __all_sync(full, sys == s0) && s0 >= 0;
         if (uniform) {
+            double v = sq;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                double v = sq[r];
-#pragma unroll
-                for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(full, v, d);
-                if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&a.norm2[size_t(s0) * R + r], v);
-            }
-        } else if (live) {
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (sq[r] != 0.0) atomicAdd(&a.norm2[size_t(sys) * R + r], sq[r]);
+            for (int d = 16; d >= R; d >>= 1) v += __shfl_xor_sync(full, v, d);
+            if ((threadIdx.x & 31) < R && v != 0.0) atomicAdd(&a.norm2[size_t(s0) * R + r], v);
+        } else if (live && sq != 0.0) {
+            atomicAdd(&a.norm2[size_t(sys) * R + r], sq);
         }
     }
 }
@@ -220,6 +210,12 @@ __global__ void k_b_check(BatchArgs a, int R, int use_cond, cudaGraphConditional
     }
     atomicAdd(&s_conv, conv);
     __syncthreads();
+    // Systems whose every right-hand side has converged stop iterating.
+    for (int s = threadIdx.x; s < a.nsys; s += blockDim.x) {
+        int all = 1;
+        for (int r = 0; r < a.nrhs[s]; ++r) all &= a.conv_iter[size_t(s) * R + r] >= 0;
+        a.sys_done[s] = all;
+    }
     if (threadIdx.x == 0) {
         st.iter = it;
         st.converged = s_conv;
@@ -237,25 +233,27 @@ __global__ void k_b_check(BatchArgs a, int R, int use_cond, cudaGraphConditional
     }
 }
 
-// Before the loop: sums of squares of D^-1 b per pair, convergence records.
+// Before the loop: sums of squares of D^-1 b per pair.
 template <int R>
 __global__ void k_b_init_norms(BatchArgs a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        const int s = a.rsys[i];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const double v = a.dinv[i] * a.B[size_t(i) * R + r];
-            if (v != 0.0) atomicAdd(&a.bnorm2[size_t(s) * R + r], v * v);
-        }
+    const long long total = (long long)a.n * R;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, r;
+        elem_rc<R>(t, i, r);
+        const double v = a.dinv[i] * a.B[t];
+        if (v != 0.0) atomicAdd(&a.bnorm2[size_t(a.rsys[i]) * R + r], v * v);
     }
 }
 
 __global__ void k_b_state_init(BatchState* st, int max_iters, int check_freq, double tol, int pairs,
-                               int* conv_iter, int count, double* norm2) {
+                               int* conv_iter, int count, double* norm2, int* sys_done,
+                               int nsys) {
     for (int q = threadIdx.x; q < count; q += blockDim.x) {
         conv_iter[q] = -1;
         norm2[q] = 0.0;
     }
+    for (int q = threadIdx.x; q < nsys; q += blockDim.x) sys_done[q] = 0;
     if (threadIdx.x == 0) {
         BatchState s{};
         s.max_iters = max_iters;
@@ -288,6 +286,7 @@ struct mclsgpu_batch {
     double* norm2 = nullptr;
     double* bnorm2 = nullptr;
     int* conv_iter = nullptr;
+    int* sys_done = nullptr;
     mclsgpu::BatchState* d_state = nullptr;
     mclsgpu::BatchState* h_state = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -316,6 +315,7 @@ void batch_release(mclsgpu_batch* b) {
     dfree(b->norm2);
     dfree(b->bnorm2);
     dfree(b->conv_iter);
+    dfree(b->sys_done);
     dfree(b->d_state);
     if (b->h_state) cudaFreeHost(b->h_state);
     delete b;
@@ -345,6 +345,8 @@ BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     a.bnorm2 = b->bnorm2;
     a.conv_iter = b->conv_iter;
     a.nrhs = b->d_nrhs;
+    a.sys_done = b->sys_done;
+    a.skip = 1;
     a.st = b->d_state;
     a.omega = mp ? mp->richardson_omega : 1.0;
     a.nomega = p.neumann_relaxation > 0.0 ? p.neumann_relaxation : 1.0;
@@ -371,14 +373,14 @@ int enqueue_batch_iteration(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp, int
                             cudaGraphConditionalHandle handle) {
     cudaStream_t s = b->ctx->stream;
     BatchArgs a = batch_args(b, mp);
-    const int grid = grid_for(b->n);
+    const int grid = grid_for((long long)b->n * b->R);
 #define K1(R) k_b_richardson_residual<R><<<grid, kThreads, 0, s>>>(a)
     MCLSGPU_BATCH_R(b->R, K1)
 #undef K1
 #define K2(R) k_b_source<R><<<grid, kThreads, 0, s>>>(a)
     MCLSGPU_BATCH_R(b->R, K2)
 #undef K2
-    int rc = launch_walk_multi(b->dom, b->R, b->cR, b->Y);
+    int rc = launch_walk_multi(b->dom, b->R, b->cR, b->Y, b->d_rsys, b->sys_done);
     if (rc) return rc;
 #define K3(R) k_b_correction<R><<<grid, kThreads, 0, s>>>(a)
     MCLSGPU_BATCH_R(b->R, K3)
@@ -541,7 +543,8 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
          (e = dmalloc(&b->B, NR)) != cudaSuccess || (e = dmalloc(&b->Y, NR)) != cudaSuccess ||
          (e = dmalloc(&b->cR, NR)) != cudaSuccess || (e = dmalloc(&b->norm2, PR)) != cudaSuccess ||
          (e = dmalloc(&b->bnorm2, PR)) != cudaSuccess ||
-         (e = dmalloc(&b->conv_iter, PR)) != cudaSuccess || (e = dmalloc(&b->d_state, 1)) != cudaSuccess ||
+         (e = dmalloc(&b->conv_iter, PR)) != cudaSuccess || (e = dmalloc(&b->sys_done, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->d_state, 1)) != cudaSuccess ||
          (e = cudaMallocHost(reinterpret_cast<void**>(&b->h_state), sizeof(BatchState))) != cudaSuccess))
         rc = cuda_fail(ctx, e, "cudaMalloc batch");
     if (!rc) {
@@ -656,9 +659,10 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
     cudaMemsetAsync(b->bnorm2, 0, sizeof(double) * PR, s);
     k_b_forward_nh<<<1, 1, 0, s>>>(b->dom->d_nh, b->n * b->per);
     k_b_state_init<<<1, 1024, 0, s>>>(b->d_state, params->max_iters, params->check_freq,
-                                       params->tolerance, pairs, b->conv_iter, int(PR), b->norm2);
+                                       params->tolerance, pairs, b->conv_iter, int(PR), b->norm2,
+                                       b->sys_done, b->nsys);
     BatchArgs a = batch_args(b, params);
-    const int grid = grid_for(b->n);
+    const int grid = grid_for((long long)b->n * b->R);
 #define KI(R)                                                 \
     k_b_init_norms<R><<<grid, kThreads, 0, s>>>(a);           \
     k_b_residual_norm<R><<<grid, kThreads, 0, s>>>(a, b->X)
@@ -696,6 +700,7 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         std::vector<double> nr(PR), bn(PR);
         std::vector<int> ci(PR);
         cudaMemsetAsync(b->norm2, 0, sizeof(double) * PR, s);
+        a.skip = 0;  // every system's final residual
 #define KF(R) k_b_residual_norm<R><<<grid, kThreads, 0, s>>>(a, b->X)
         MCLSGPU_BATCH_R(b->R, KF)
 #undef KF

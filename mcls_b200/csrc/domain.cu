@@ -100,6 +100,9 @@ __global__ void k_pack_records(const int* drp, const int* dcol, const double* dh
 __global__ void k_collect_offsets(const int* rp, const int* ci, int n, int max_k, int* tab,
                                   int* overflow) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        // Once the table has overflowed the answer is known: stop early
+        // instead of contending on the full table.
+        if (*reinterpret_cast<volatile int*>(overflow)) return;
         for (int k = rp[i]; k < rp[i + 1]; ++k) {
             const int d = ci[k] - i;
             bool placed = false;

@@ -451,9 +451,16 @@ namespace {
 // sums of w * c_r(state) (cR is row-major [n][R], the tally source of every
 // right-hand side at a state) and adds them into Y[start][r] in FP64.
 // Fixed-length histories only.
+// Histories that start in a row whose system is finished (done[rsys[row]])
+// are skipped; rsys / done may be null.
+struct MultiSkip {
+    const int* rsys;
+    const int* done;
+};
+
 template <int S, bool ST, int R>
 __global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* __restrict__ cR,
-                                                       double* __restrict__ Y) {
+                                                       double* __restrict__ Y, MultiSkip skip) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
     __shared__ int s_nh;
@@ -474,11 +481,12 @@ __global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* 
         const int nh = s_nh;
         if (base >= nh) break;
         const int e = base + lane;
-        const bool alive = e < nh;
+        bool alive = e < nh;
         int s = 0;
         float w = 0.f;
         uint64_t x = 0;
         if (alive) walk_start<MCLSGPU_FORWARD>(a, e, s_ekey, 1.f, s, w, x);
+        if (alive && skip.done && skip.done[skip.rsys[s]]) alive = false;
         const int s0 = s;
         float acc[R], comp[R];
 #pragma unroll
@@ -526,8 +534,8 @@ __global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* 
 }
 
 template <int S, bool ST, int R>
-void launch_multi_sr(const WalkArgs& a, const float* cR, double* Y, int sms, int block,
-                     cudaStream_t st) {
+void launch_multi_sr(const WalkArgs& a, const float* cR, double* Y, MultiSkip sk, int sms,
+                     int block, cudaStream_t st) {
     static int cached[2] = {0, 0};
     const int slot = block == 128 ? 0 : 1;
     if (!cached[slot]) {
@@ -535,18 +543,18 @@ void launch_multi_sr(const WalkArgs& a, const float* cR, double* Y, int sms, int
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32_multi<S, ST, R>, block, 0);
         cached[slot] = b > 0 ? b : 1;
     }
-    walk32_multi<S, ST, R><<<sms * cached[slot], block, 0, st>>>(a, cR, Y);
+    walk32_multi<S, ST, R><<<sms * cached[slot], block, 0, st>>>(a, cR, Y, sk);
 }
 
 template <int S, bool ST>
-bool launch_multi_s(int R, const WalkArgs& a, const float* cR, double* Y, int sms, int block,
-                    cudaStream_t st) {
+bool launch_multi_s(int R, const WalkArgs& a, const float* cR, double* Y, MultiSkip sk, int sms,
+                    int block, cudaStream_t st) {
     switch (R) {
-        case 1: launch_multi_sr<S, ST, 1>(a, cR, Y, sms, block, st); return true;
-        case 2: launch_multi_sr<S, ST, 2>(a, cR, Y, sms, block, st); return true;
-        case 4: launch_multi_sr<S, ST, 4>(a, cR, Y, sms, block, st); return true;
-        case 8: launch_multi_sr<S, ST, 8>(a, cR, Y, sms, block, st); return true;
-        case 16: launch_multi_sr<S, ST, 16>(a, cR, Y, sms, block, st); return true;
+        case 1: launch_multi_sr<S, ST, 1>(a, cR, Y, sk, sms, block, st); return true;
+        case 2: launch_multi_sr<S, ST, 2>(a, cR, Y, sk, sms, block, st); return true;
+        case 4: launch_multi_sr<S, ST, 4>(a, cR, Y, sk, sms, block, st); return true;
+        case 8: launch_multi_sr<S, ST, 8>(a, cR, Y, sk, sms, block, st); return true;
+        case 16: launch_multi_sr<S, ST, 16>(a, cR, Y, sk, sms, block, st); return true;
         default: return false;
     }
 }
@@ -580,7 +588,8 @@ static void fill_walk_args(mclsgpu_domain* dom, WalkArgs& a) {
 // Multi-right-hand-side forward walks over the domain's FP32 records (R in
 // {1, 2, 4, 8, 16}; records of at most 16 slots).  The work-queue counter must
 // be zero on entry; the caller resets it afterwards.
-int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y) {
+int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y, const int* rsys,
+                      const int* sys_done) {
     mclsgpu_context* ctx = dom->ctx;
     if (dom->p.precision != MCLSGPU_FP32 || dom->p.direction != MCLSGPU_FORWARD || !dom->slots)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batched walks need FP32 forward records");
@@ -589,19 +598,20 @@ int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y) {
     const int sms = ctx->num_sms;
     const int block = dom->walk_block;
     cudaStream_t st = ctx->stream;
+    const MultiSkip sk{rsys, sys_done};
     bool ok = false;
     if (dom->stencil_k) {
         switch (dom->slots) {
-            case 4: ok = launch_multi_s<4, true>(R, a, cR, Y, sms, block, st); break;
-            case 8: ok = launch_multi_s<8, true>(R, a, cR, Y, sms, block, st); break;
+            case 4: ok = launch_multi_s<4, true>(R, a, cR, Y, sk, sms, block, st); break;
+            case 8: ok = launch_multi_s<8, true>(R, a, cR, Y, sk, sms, block, st); break;
             default: ok = false;
         }
     } else {
         switch (dom->slots) {
-            case 4: ok = launch_multi_s<4, false>(R, a, cR, Y, sms, block, st); break;
-            case 8: ok = launch_multi_s<8, false>(R, a, cR, Y, sms, block, st); break;
-            case 12: ok = launch_multi_s<12, false>(R, a, cR, Y, sms, block, st); break;
-            case 16: ok = launch_multi_s<16, false>(R, a, cR, Y, sms, block, st); break;
+            case 4: ok = launch_multi_s<4, false>(R, a, cR, Y, sk, sms, block, st); break;
+            case 8: ok = launch_multi_s<8, false>(R, a, cR, Y, sk, sms, block, st); break;
+            case 12: ok = launch_multi_s<12, false>(R, a, cR, Y, sk, sms, block, st); break;
+            case 16: ok = launch_multi_s<16, false>(R, a, cR, Y, sk, sms, block, st); break;
             default: ok = false;
         }
     }
