@@ -135,49 +135,27 @@ def make_system(cfg):
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
+    from mcls_b200 import dist
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-    return world, rank, local, pg
+    return dist.init("nccl")
 
 
 def barrier(pg):
-    if pg is not None:
-        import torch
+    from mcls_b200 import dist
 
-        pg.barrier()
-        torch.cuda.synchronize()
+    dist.barrier(pg)
 
 
 def allmax(pg, v):
-    if pg is None:
-        return v
-    import torch
+    from mcls_b200 import dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    return dist.allmax(pg, v)
 
 
 def allsum(pg, v):
-    if pg is None:
-        return v
-    import torch
+    from mcls_b200 import dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t)
-    return float(t.item())
+    return dist.allsum(pg, v)
 
 
 def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):

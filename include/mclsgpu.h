@@ -338,6 +338,25 @@ int mclsgpu_mcsa_solve(mclsgpu_domain* dom, const double* b, double* x,
 int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev,
                            double* x_dev, const mclsgpu_mcsa_params* params,
                            mclsgpu_stats* stats);
+/* MCSA one iteration at a time, for drivers that combine the Monte Carlo
+ * corrections of several sets (one set per GPU): the loop of
+ * MCSASolverManager::solve with MultiSetLinearProblem::blockConstantVectorSum
+ * between the Monte Carlo solve and the update
+ * (src/MCLS_MCSASolverManager_impl.hpp:344-400,
+ *  src/MCLS_MultiSetLinearProblem_impl.hpp:102-120).
+ *   begin:      x = x0, rp = PL (b - A PR x); *rnorm = |rp|_2, *bnorm = |PL b|_2
+ *   correction: smoother_steps Richardson steps, then delta_dev = the Monte
+ *               Carlo estimate of the correction (this set's histories)
+ *   apply:      x += scale * delta_dev (scale = 1 / number of sets after the
+ *               caller summed delta over the sets), new rp; *rnorm = |rp|_2
+ *   finish:     x_dev = PR x; stats of the walks since begin
+ * Device vectors of length n. */
+int mclsgpu_mcsa_begin(mclsgpu_domain* dom, const double* b_dev, const double* x0_dev,
+                       const mclsgpu_mcsa_params* params, double* rnorm, double* bnorm);
+int mclsgpu_mcsa_correction(mclsgpu_domain* dom, double* delta_dev);
+int mclsgpu_mcsa_apply(mclsgpu_domain* dom, const double* delta_dev, double scale,
+                       double* rnorm);
+int mclsgpu_mcsa_finish(mclsgpu_domain* dom, double* x_dev, mclsgpu_stats* stats);
 /* The preconditioned residual PL (b - A x) at the end of the last MCSA
  * solve, copied to the device vector rp_dev (LinearProblem::getPrecResidual,
  * src/MCLS_LinearProblem.hpp:121-122). */

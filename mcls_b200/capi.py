@@ -136,7 +136,8 @@ EXPORTS = [
     "mclsgpu_domain_residual", "mclsgpu_spai_smooth_vectors", "mclsgpu_spai_set_penalty",
     "mclsgpu_batch_build", "mclsgpu_batch_destroy", "mclsgpu_batch_layout",
     "mclsgpu_batch_domain", "mclsgpu_batch_set_launch", "mclsgpu_batch_autotune",
-    "mclsgpu_batch_mcsa_solve_dev",
+    "mclsgpu_batch_mcsa_solve_dev", "mclsgpu_mcsa_begin", "mclsgpu_mcsa_correction",
+    "mclsgpu_mcsa_apply", "mclsgpu_mcsa_finish",
 ]
 
 _LIB = None
@@ -196,6 +197,10 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_domain_spectral_radius.argtypes = [P, C.c_int, C.c_int, d, C.c_uint64,
                                                  C.POINTER(d)]
     L.mclsgpu_domain_residual.argtypes = [P, P]
+    L.mclsgpu_mcsa_begin.argtypes = [P, P, P, C.POINTER(McsaParams), C.POINTER(d), C.POINTER(d)]
+    L.mclsgpu_mcsa_correction.argtypes = [P, P]
+    L.mclsgpu_mcsa_apply.argtypes = [P, P, d, C.POINTER(d)]
+    L.mclsgpu_mcsa_finish.argtypes = [P, P, C.POINTER(Stats)]
     L.mclsgpu_spai_num_params.restype = C.c_int
     L.mclsgpu_spai_create.argtypes = [P, C.c_int, C.c_uint64, PP]
     L.mclsgpu_spai_destroy.argtypes = [P]
@@ -473,6 +478,29 @@ class Domain:
         self.ctx.check(self.ctx.L.mclsgpu_mcsa_solve_dev(self.h, C.c_void_p(b_ptr),
                                                          C.c_void_p(x_ptr), C.byref(p),
                                                          C.byref(st)))
+        return st.as_dict()
+
+    def mcsa_begin(self, b_ptr, x0_ptr, params: McsaParams | None = None, **kw):
+        """Step-wise MCSA: initial residual; returns (|rp|_2, |PL b|_2)."""
+        p = params if params is not None else mcsa_params(**kw)
+        rn, bn = C.c_double(), C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_begin(self.h, C.c_void_p(b_ptr), C.c_void_p(x0_ptr),
+                                                     C.byref(p), C.byref(rn), C.byref(bn)))
+        return rn.value, bn.value
+
+    def mcsa_correction(self, delta_ptr):
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_correction(self.h, C.c_void_p(delta_ptr)))
+
+    def mcsa_apply(self, delta_ptr, scale=1.0):
+        rn = C.c_double()
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_apply(self.h, C.c_void_p(delta_ptr), scale,
+                                                     C.byref(rn)))
+        return rn.value
+
+    def mcsa_finish(self, x_ptr):
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_finish(self.h, C.c_void_p(x_ptr), C.byref(st)))
         return st.as_dict()
 
     def residual(self, rp_dev_ptr):

@@ -169,6 +169,9 @@ struct mclsgpu_domain {
     unsigned long long* d_hist = nullptr;   // histories transported (total)
     double* d_resid = nullptr;     // per-iteration |rp|_2 history
     int resid_cap = 0;
+    // Step-wise MCSA (mclsgpu_mcsa_begin .. _finish).
+    mclsgpu_mcsa_params step_p{};
+    int step_ready = 0;
 };
 
 namespace mclsgpu {

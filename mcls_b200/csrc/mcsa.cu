@@ -877,6 +877,101 @@ int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_d
     return mcsa_solve_device(dom, b_dev, x_dev, &p, stats);
 }
 
+int mclsgpu_mcsa_begin(mclsgpu_domain* dom, const double* b_dev, const double* x0_dev,
+                       const mclsgpu_mcsa_params* params, double* rnorm, double* bnorm) {
+    if (!dom || !b_dev || !x0_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_mcsa_params p;
+    int rc = check_mcsa_params(dom, params, &p);
+    if (rc) return rc;
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    reset_counters(dom);
+    if (b_dev != dom->b) cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (x0_dev != dom->x) cudaMemcpyAsync(dom->x, x0_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    // |PL b|_2 and the initial preconditioned residual
+    // (src/MCLS_MCSASolverManager_impl.hpp:299-346).
+    const double* pb = dom->b;
+    if (dom->left) {
+        spmv(s, dom->left->P, dom->b, dom->tmp);
+        pb = dom->tmp;
+    }
+    sum_sq(s, pb, n, dom->part, dom->d_scalars + 6);
+    update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    double h[2] = {0.0, 0.0};
+    cudaMemcpyAsync(h, dom->d_scalars + 5, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mcsa begin");
+    if ((rc = check_device_status(ctx))) return rc;
+    if (rnorm) *rnorm = std::sqrt(h[0]);
+    if (bnorm) *bnorm = std::sqrt(h[1]);
+    dom->step_p = p;
+    dom->step_ready = 1;
+    return MCLSGPU_OK;
+}
+
+int mclsgpu_mcsa_correction(mclsgpu_domain* dom, double* delta_dev) {
+    if (!dom || !delta_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = dom->ctx;
+    if (!dom->step_ready)
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_mcsa_begin first");
+    cudaStream_t s = ctx->stream;
+    const mclsgpu_mcsa_params& p = dom->step_p;
+    for (int l = 0; l < p.smoother_steps; ++l) {
+        k_richardson<<<grid_for(dom->n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, dom->n,
+                                                                    p.richardson_omega);
+        update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    }
+    // The residual problem's source is already left preconditioned.
+    enqueue_mc(dom, dom->rp, delta_dev, 0, 0, nullptr, nullptr, nullptr, nullptr);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mcsa correction");
+    return check_device_status(ctx);
+}
+
+int mclsgpu_mcsa_apply(mclsgpu_domain* dom, const double* delta_dev, double scale,
+                       double* rnorm) {
+    if (!dom || !delta_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = dom->ctx;
+    if (!dom->step_ready)
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_mcsa_begin first");
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, delta_dev, n, scale);
+    update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    double h = 0.0;
+    cudaMemcpyAsync(&h, dom->d_scalars + 5, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mcsa apply");
+    int rc = check_device_status(ctx);
+    if (rc) return rc;
+    if (!std::isfinite(h)) return set_error(ctx, MCLSGPU_ERR_DIVERGED, "non-finite residual");
+    if (rnorm) *rnorm = std::sqrt(h);
+    return MCLSGPU_OK;
+}
+
+int mclsgpu_mcsa_finish(mclsgpu_domain* dom, double* x_dev, mclsgpu_stats* stats) {
+    if (!dom || !x_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = dom->ctx;
+    if (!dom->step_ready)
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_mcsa_begin first");
+    cudaStream_t s = ctx->stream;
+    const size_t bytes = size_t(dom->n) * sizeof(double);
+    if (dom->right) {
+        spmv(s, dom->right->P, dom->x, dom->tmp);  // right-preconditioner recovery
+        cudaMemcpyAsync(x_dev, dom->tmp, bytes, cudaMemcpyDeviceToDevice, s);
+    } else if (x_dev != dom->x) {
+        cudaMemcpyAsync(x_dev, dom->x, bytes, cudaMemcpyDeviceToDevice, s);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mcsa finish");
+    dom->step_ready = 0;
+    return stats ? read_stats(dom, stats) : MCLSGPU_OK;
+}
+
 int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev) {
     if (!dom || !rp_dev || !dom->rp) return MCLSGPU_ERR_INVALID_ARG;
     mclsgpu_context* ctx = dom->ctx;

@@ -1,0 +1,77 @@
+"""Multi-set MCSA: one set (one domain, its own random streams) per process,
+the Monte Carlo corrections summed over the sets by an all-reduce and
+divided by the set count -- the loop of MCSASolverManager::solve with
+MultiSetLinearProblem::blockConstantVectorSum
+(src/MCLS_MCSASolverManager_impl.hpp:344-400,
+src/MCLS_MultiSetLinearProblem_impl.hpp:102-120).
+
+The driver is written against a small engine interface so that the same
+host logic runs on GPUs (DeviceEngine: the library's step-wise MCSA entry
+points, NCCL all-reduce) and, in the tests, on CPU processes over gloo.
+Every rank takes the same collective steps in the same order: one
+all-reduce of the correction and one of the residual norm per iteration.
+"""
+from __future__ import annotations
+
+from . import capi
+
+
+class DeviceEngine:
+    """One set on one GPU through mclsgpu_mcsa_begin/_correction/_apply/_finish."""
+
+    def __init__(self, domain: "capi.Domain", n: int, device: int = 0):
+        import torch
+
+        self.dom = domain
+        self.n = n
+        self.dev = f"cuda:{device}"
+        self.delta = torch.zeros(n, dtype=torch.float64, device=self.dev)
+
+    def begin(self, b, x0, params):
+        import torch
+
+        self.b = torch.as_tensor(b, dtype=torch.float64, device=self.dev).contiguous()
+        self.x = torch.as_tensor(x0, dtype=torch.float64, device=self.dev).clone().contiguous()
+        return self.dom.mcsa_begin(self.b.data_ptr(), self.x.data_ptr(), params=params)
+
+    def correction(self):
+        self.dom.mcsa_correction(self.delta.data_ptr())
+        return self.delta
+
+    def apply(self, delta, scale):
+        return self.dom.mcsa_apply(delta.data_ptr(), scale)
+
+    def finish(self):
+        stats = self.dom.mcsa_finish(self.x.data_ptr())
+        return self.x, stats
+
+
+def solve(engine, b, x0, group=None, tolerance=1e-8, max_iters=1000, check_freq=1,
+          smoother_steps=1, richardson_omega=1.0):
+    """Multi-set MCSA on every rank of `group` (torch.distributed module or
+    None for one set).  Returns (x, iterations, converged, |rp|/|PL b|, stats)."""
+    import torch
+
+    world = group.get_world_size() if group is not None else 1
+    params = capi.mcsa_params(tolerance=tolerance, max_iters=max_iters, check_freq=check_freq,
+                              smoother_steps=smoother_steps, richardson_omega=richardson_omega)
+    rnorm, bnorm = engine.begin(b, x0, params)
+    crit = tolerance * (bnorm if bnorm > 0.0 else 1.0)
+    it = 0
+    converged = rnorm <= crit
+    while not converged and it < max_iters:
+        it += 1
+        delta = engine.correction()
+        if world > 1:
+            group.all_reduce(delta)  # blockConstantVectorSum over the sets
+        rnorm = engine.apply(delta, 1.0 / world)
+        if world > 1:
+            # Identical x on every rank gives identical norms; the MAX keeps
+            # the stopping decision common to all ranks regardless.
+            t = torch.tensor([rnorm], dtype=torch.float64, device=delta.device)
+            group.all_reduce(t, op=group.ReduceOp.MAX)
+            rnorm = float(t.item())
+        if it % check_freq == 0:
+            converged = rnorm <= crit
+    x, stats = engine.finish()
+    return x, it, converged, rnorm / (bnorm if bnorm > 0.0 else 1.0), stats
