@@ -99,3 +99,62 @@ def train(net, samples, steps, lr=2e-3, lr_final=2e-4, grad_clip=0.0, log_every=
         if log_every and k % log_every == 0:
             print(f"spai step {k}: loss {loss:.6f} lr {step_lr:.2e}", flush=True)
     return losses
+
+
+def main(argv=None):
+    """Train a learned-SPAI network on seeded systems of one family and save
+    its parameters (numpy .npy, FP32, the flat order of mclsgpu_spai_*)."""
+    import argparse
+    import time
+
+    import torch
+
+    from . import problems as P
+
+    ap = argparse.ArgumentParser(prog="python -m mcls_b200.spai")
+    ap.add_argument("--family", choices=["diffusion3d", "anisotropic2d"], default="diffusion3d")
+    ap.add_argument("--grid", type=int, default=32, help="grid points per axis of each system")
+    ap.add_argument("--systems", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--seed", type=int, default=1000)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default=None, help="where to save the parameters (.npy)")
+    args = ap.parse_args(argv)
+    ctx = capi.Context(args.device)
+    samples, slots = [], None
+    t0 = time.perf_counter()
+    for k in range(args.systems):
+        if args.family == "diffusion3d":
+            A, b = P.diffusion3d_varcoef(args.grid, seed=args.seed + k)
+        else:
+            A, b, _, _ = P.anisotropic2d_sample(args.grid, seed=args.seed + k)
+        if slots is None:
+            slots = stencil_slots(A)
+        if stencil_slots(A) != slots:
+            continue
+        op = capi.Operator(ctx, A)
+        if args.family == "diffusion3d":
+            V = training_vectors(ctx, op, b, seed=k, n_random=4, iterations=(1, 4, 16),
+                                 device=args.device)
+        else:  # point-Jacobi MCSA may diverge on this family: random vectors only
+            g = torch.Generator(device=f"cuda:{args.device}")
+            g.manual_seed(k)
+            V = torch.randn((4, op.n), dtype=torch.float64, device=f"cuda:{args.device}",
+                            generator=g)
+        samples.append((op, V))
+    net = capi.SpaiNet(ctx, slots, seed=0)
+    losses = train(net, samples, steps=args.steps, lr=args.lr, lr_final=args.lr / 10,
+                   refresh=25 if args.steps >= 100 else 0, adv_count=8, adv_iters=50,
+                   device=args.device)
+    torch.cuda.synchronize()
+    print(f"{len(samples)} systems, {args.steps} steps, {time.perf_counter() - t0:.1f} s, "
+          f"loss {np.mean(losses[:8]):.4f} -> {np.mean(losses[-8:]):.4f}", flush=True)
+    if args.out:
+        np.save(args.out, net.params)
+    net.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
