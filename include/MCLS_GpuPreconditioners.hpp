@@ -10,6 +10,9 @@
 #ifndef MCLS_GPUPRECONDITIONERS_HPP
 #define MCLS_GPUPRECONDITIONERS_HPP
 
+#include <algorithm>
+#include <vector>
+
 #include "MCLS_GpuBackend.hpp"
 #include "MCLS_Preconditioner.hpp"
 
@@ -99,6 +102,81 @@ class BlockJacobiPreconditioner : public GpuPreconditionerBase<Vector, Matrix> {
         pp.block_size = int(gpu::numeric(*this->d_plist, "Jacobi Block Size", 1.0));
         this->buildWith(pp);
     }
+};
+
+// Learned sparse approximate inverse on A's pattern (mclsgpu_spai_*): M from
+// a trained per-row network; point Jacobi replaces it when its
+// power-iteration rho(I - M A) reaches both "Rho Fallback" and the Jacobi
+// rho, or when A has no fixed stencil.  The network is either a trained
+// handle given with setNetwork() (owned by the caller) or the flat FP32
+// parameters in "SPAI Weights" (std::vector<float>, mclsgpu_spai_num_params()
+// values, e.g. saved by `python -m mcls_b200.spai --out`).  No counterpart in
+// the reference.
+template <class Vector, class Matrix>
+class LearnedSpaiPreconditioner : public GpuPreconditionerBase<Vector, Matrix> {
+  public:
+    typedef MatrixTraits<Vector, Matrix> MT;
+
+    explicit LearnedSpaiPreconditioner(
+        const Teuchos::RCP<Teuchos::ParameterList>& params = Teuchos::null)
+        : GpuPreconditionerBase<Vector, Matrix>(params) {}
+    Teuchos::RCP<const Teuchos::ParameterList> getValidParameters() const override {
+        auto pl = Teuchos::parameterList();
+        pl->set<std::vector<float>>("SPAI Weights", std::vector<float>());
+        pl->set<double>("Rho Fallback", 0.95);
+        pl->set<int>("GPU Device", 0);
+        return pl;
+    }
+    void setNetwork(mclsgpu_spai* net) { d_net = net; }
+    void buildPreconditioner() override {
+        if (!Teuchos::nonnull(this->d_A)) throw Assertion("preconditioner: setOperator() first");
+        mclsgpu_spai* net = d_net;
+        mclsgpu_spai* own = nullptr;
+        std::shared_ptr<gpu::Context> ctx;
+        if (!net && this->d_plist->isParameter("SPAI Weights")) {
+            const auto& w = this->d_plist->template get<std::vector<float>>("SPAI Weights");
+            if (!w.empty()) {
+                if (int(w.size()) != mclsgpu_spai_num_params())
+                    throw Assertion("SPAI Weights: wrong parameter count");
+                ctx = gpu::Context::on(int(gpu::numeric(*this->d_plist, "GPU Device", 0.0)));
+                ctx->check(mclsgpu_spai_create(ctx->get(), stencilSlots(), 0, &own),
+                           "mclsgpu_spai_create");
+                int rc = mclsgpu_spai_set_params(own, w.data());
+                if (rc != MCLSGPU_OK) {
+                    mclsgpu_spai_destroy(own);
+                    ctx->check(rc, "mclsgpu_spai_set_params");
+                }
+                net = own;
+            }
+        }
+        mclsgpu_precond_params pp{};
+        pp.size = sizeof(pp);
+        pp.kind = MCLSGPU_PREC_LEARNED_SPAI;
+        pp.spai_net = net;
+        pp.rho_fallback = gpu::numeric(*this->d_plist, "Rho Fallback", 0.95);
+        try {
+            this->buildWith(pp);
+        } catch (...) {
+            if (own) mclsgpu_spai_destroy(own);
+            throw;
+        }
+        if (own) mclsgpu_spai_destroy(own);  // M is built; the network is no longer needed
+    }
+
+  private:
+    // Distinct column offsets of A: the network's stencil slots.
+    int stencilSlots() const {
+        std::vector<std::int64_t> rp, ci;
+        std::vector<double> v;
+        MT::getCsr(*this->d_A, rp, ci, v);
+        std::vector<std::int64_t> offs;
+        for (size_t i = 0; i + 1 < rp.size(); ++i)
+            for (std::int64_t p = rp[i]; p < rp[i + 1]; ++p) offs.push_back(ci[p] - std::int64_t(i));
+        std::sort(offs.begin(), offs.end());
+        return int(std::unique(offs.begin(), offs.end()) - offs.begin());
+    }
+
+    mclsgpu_spai* d_net = nullptr;
 };
 
 }  // namespace MCLS

@@ -227,6 +227,50 @@ static void gpu_checks() {
         EXPECT(rel_err(*x, direct(*B, *b)) < 1e-7);
     }
 
+    // Learned SPAI with a network whose output layer is zero: M is point
+    // Jacobi, the rho gate keeps the plain preconditioner, the solve converges.
+    {
+        g_section = "learned SPAI";
+        const int m = 8, N = m * m;
+        auto P2 = Teuchos::rcp(new Mat);
+        P2->n = N;
+        P2->rowptr.assign(1, 0);
+        for (int i = 0; i < N; ++i) {
+            const int x = i % m, y = i / m;
+            const int nb[5] = {y > 0 ? i - m : -1, x > 0 ? i - 1 : -1, i, x < m - 1 ? i + 1 : -1,
+                               y < m - 1 ? i + m : -1};
+            for (int c : nb)
+                if (c >= 0) {
+                    P2->colind.push_back(c);
+                    P2->values.push_back(c == i ? 4.0 : -1.0);
+                }
+            P2->rowptr.push_back(std::int64_t(P2->colind.size()));
+        }
+        std::vector<float> w(size_t(mclsgpu_spai_num_params()), 0.0f);
+        auto sp = Teuchos::parameterList();
+        sp->set<std::vector<float>>("SPAI Weights", w);
+        MCLS::LearnedSpaiPreconditioner<Vec, Mat> prec(sp);
+        prec.setOperator(P2);
+        prec.buildPreconditioner();
+        auto PL = prec.getLeftPreconditioner();
+        // Kept on A's pattern (rho below the gate) or replaced by point
+        // Jacobi: either way 1/4 on the diagonal and zero elsewhere.
+        EXPECT(Teuchos::nonnull(PL) && PL->n == N);
+        for (int i = 0; i < N; ++i)
+            for (auto p = PL->rowptr[i]; p < PL->rowptr[i + 1]; ++p)
+                EXPECT(std::fabs(PL->values[p] - (PL->colind[p] == i ? 0.25 : 0.0)) < 1e-15);
+        auto x = Teuchos::rcp(new Vec(N, 0.0));
+        auto b = Teuchos::rcp(new Vec(N, 1.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(P2, x, b));
+        lp->setLeftPrec(PL);
+        auto pl = mcsa_params();
+        pl->set<int>("Maximum Iterations", 2000);
+        MCLS::MCSASolverManager<Vec, Mat> sm(pl);
+        sm.setProblem(lp);
+        EXPECT(sm.solve());
+        EXPECT(rel_err(*x, direct(*P2, *b)) < 1e-7);
+    }
+
     // Direct Monte Carlo: signs follow the source, sample ratio 10
     // (tpetra/test/tstTpetraMonteCarloSolverManager.cpp:73-197).
     for (const char* name : {"Adjoint MC", "Forward MC"}) {
