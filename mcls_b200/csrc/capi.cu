@@ -333,6 +333,7 @@ int mclsgpu_precond_build(mclsgpu_context* ctx, mclsgpu_operator* op,
     if (rc) {
         pc->P.release();
         dfree(pc->diag);
+        dfree(pc->mdia);
         delete pc;
         return rc;
     }
@@ -344,6 +345,7 @@ int mclsgpu_precond_destroy(mclsgpu_precond* pc) {
     if (!pc) return MCLSGPU_OK;
     pc->P.release();
     dfree(pc->diag);
+    dfree(pc->mdia);
     delete pc;
     return MCLSGPU_OK;
 }

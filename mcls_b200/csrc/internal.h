@@ -83,6 +83,7 @@ struct mclsgpu_precond {
     int block_size = 1;
     mclsgpu::DevCsr P;            // left preconditioner as CSR
     double* diag = nullptr;       // POINT_JACOBI: the reciprocal diagonal
+    double* mdia = nullptr;       // LEARNED_SPAI kept: M by A's diagonal offsets
     double rho = -1.0;            // LEARNED_SPAI: rho(H) estimate
     int fallback = 0;             // LEARNED_SPAI replaced by Jacobi
 };

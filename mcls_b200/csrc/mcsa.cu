@@ -265,19 +265,12 @@ __global__ void __launch_bounds__(kFusedThreads) k_apply_correction(ResidArgs a)
 // rp = PL (b - A x), |rp|^2, then (last block) the MCSA convergence check,
 // the stream epoch, the walk timing, the work-queue reset and the loop
 // condition.
-template <class Op>
-__global__ void __launch_bounds__(kFusedThreads) k_residual_norm(Op A, ResidArgs a) {
+// Block sum of the threads' acc, then (last block to finish) the MCSA
+// convergence check, the stream epoch, the walk timing, the work-queue reset
+// and the loop condition.
+__device__ __forceinline__ void norm_and_check(const ResidArgs& a, double acc) {
     __shared__ double warp_sum[kFusedThreads / 32];
     __shared__ bool last;
-    const double* x = a.xout;
-    double acc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        const double s = A.dot(i, [&](int j) { return x[j]; });
-        const double res = a.b[i] - s;
-        const double r = a.dinv ? a.dinv[i] * res : res;
-        a.rout[i] = r;
-        acc = fma(r, r, acc);
-    }
     for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = acc;
     __syncthreads();
@@ -316,6 +309,40 @@ __global__ void __launch_bounds__(kFusedThreads) k_residual_norm(Op A, ResidArgs
     }
 }
 
+template <class Op>
+__global__ void __launch_bounds__(kFusedThreads) k_residual_norm(Op A, ResidArgs a) {
+    const double* x = a.xout;
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double s = A.dot(i, [&](int j) { return x[j]; });
+        const double res = a.b[i] - s;
+        const double r = a.dinv ? a.dinv[i] * res : res;
+        a.rout[i] = r;
+        acc = fma(r, r, acc);
+    }
+    norm_and_check(a, acc);
+}
+
+// A left preconditioner M stored on A's diagonals (learned SPAI): out = M v.
+template <class Op>
+__global__ void __launch_bounds__(kFusedThreads) k_dia_apply(Op M, const double* v, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M.n; i += gridDim.x * blockDim.x)
+        out[i] = M.dot(i, [&](int j) { return v[j]; });
+}
+
+// rp = M (b - A x) from the raw residual, its norm and the convergence check.
+template <class Op>
+__global__ void __launch_bounds__(kFusedThreads) k_precond_norm(Op M, ResidArgs a,
+                                                               const double* raw) {
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double r = M.dot(i, [&](int j) { return raw[j]; });
+        a.rout[i] = r;
+        acc = fma(r, r, acc);
+    }
+    norm_and_check(a, acc);
+}
+
 __global__ void k_mcsa_init(McsaState* st, const double* src_sumsq, double tol, int check_freq,
                             int max_iters, const double* r_sumsq) {
     McsaState s{};
@@ -349,6 +376,35 @@ static DiaViewT<KK> dia_view(const mclsgpu_operator* op) {
     for (int j = 0; j < 16; ++j) v.off[j] = op->dia_off[j];
     return v;
 }
+
+// The diagonal-offset view of another matrix on the operator's offsets.
+template <int KK>
+static DiaViewT<KK> dia_view_vals(const mclsgpu_operator* op, const double* vals) {
+    DiaViewT<KK> v = dia_view<KK>(op);
+    v.val = vals;
+    return v;
+}
+
+#define MCLSGPU_LAUNCH_M(op, vals, grid, threads, stream, kern, ...)                         \
+    do {                                                                                     \
+        switch ((op)->dia_k) {                                                               \
+            case 5:                                                                          \
+                kern<DiaViewT<5>><<<grid, threads, 0, stream>>>(dia_view_vals<5>(op, vals),  \
+                                                                __VA_ARGS__);                \
+                break;                                                                       \
+            case 7:                                                                          \
+                kern<DiaViewT<7>><<<grid, threads, 0, stream>>>(dia_view_vals<7>(op, vals),  \
+                                                                __VA_ARGS__);                \
+                break;                                                                       \
+            case 9:                                                                          \
+                kern<DiaViewT<9>><<<grid, threads, 0, stream>>>(dia_view_vals<9>(op, vals),  \
+                                                                __VA_ARGS__);                \
+                break;                                                                       \
+            default:                                                                         \
+                kern<DiaView><<<grid, threads, 0, stream>>>(dia_view_vals<0>(op, vals),      \
+                                                            __VA_ARGS__);                    \
+        }                                                                                    \
+    } while (0)
 
 // Launch `kern<Op>` on the operator's fastest layout: diagonal-offset values
 // for stencil operators (unrolled for the 5-, 7- and 9-point stencils),
@@ -505,7 +561,8 @@ static int mc_solve_device(mclsgpu_domain* dom, const double* rhs_dev, double* x
 // a left preconditioner that is the identity or point Jacobi.
 static bool fused_iteration(const mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
     return mp->smoother_steps == 1 && !dom->right &&
-           (!dom->left || dom->left->kind == MCLSGPU_PREC_POINT_JACOBI);
+           (!dom->left || dom->left->kind == MCLSGPU_PREC_POINT_JACOBI ||
+            (dom->left->mdia && dom->op->dia_k > 0));
 }
 
 // At most 8 blocks per SM: the per-block partial sums of k_apply_correction
@@ -542,9 +599,18 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
     }
     const mclsgpu_operator* op = dom->op;
     const double* dinv = dom->left ? dom->left->diag : nullptr;
+    // A left preconditioner on A's diagonals (learned SPAI): the raw residual
+    // goes to tmp and a second pass applies M.
+    const double* mdia = dom->left ? dom->left->mdia : nullptr;
     const int grid = fused_grid(dom);
-    MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_richardson_residual, dom->b, dinv, dom->x,
-                      dom->rp, mp->richardson_omega, dom->x2, dom->rp2);
+    if (mdia) {
+        MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_richardson_residual, dom->b, nullptr,
+                          dom->x, dom->rp, mp->richardson_omega, dom->x2, dom->tmp);
+        MCLSGPU_LAUNCH_M(op, mdia, grid, kFusedThreads, s, k_dia_apply, dom->tmp, dom->rp2);
+    } else {
+        MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_richardson_residual, dom->b, dinv, dom->x,
+                          dom->rp, mp->richardson_omega, dom->x2, dom->rp2);
+    }
     const mclsgpu_mc_params& p = dom->p;
     const bool adj_ev = p.direction == MCLSGPU_ADJOINT && p.estimator == MCLSGPU_EXPECTED_VALUE;
     enqueue_mc(dom, dom->rp2, dom->x2, 1, 0, nullptr, nullptr, nullptr, nullptr, true);
@@ -582,7 +648,13 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
     a.handle = handle;
     a.use_cond = use_cond;
     k_apply_correction<<<grid, kFusedThreads, 0, s>>>(a);
-    MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_residual_norm, a);
+    if (mdia) {
+        MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_residual, dom->x, dom->b, nullptr,
+                          dom->tmp);
+        MCLSGPU_LAUNCH_M(op, mdia, grid, kFusedThreads, s, k_precond_norm, a, dom->tmp);
+    } else {
+        MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_residual_norm, a);
+    }
 }
 
 // Build the CUDA graph of the MCSA loop (WHILE node, one iteration per body).

@@ -218,53 +218,55 @@ struct StencilOffsets {
 // Stencil records: the tally source H b is rebuilt from the record itself,
 // |h_j| = W * (cdf_j - cdf_prev), so the pass reads 32 bytes per row instead
 // of the FP64 domain.
+// Tally source of one stencil record of WORDS 32-bit words: c = sum_j h_j
+// v[i + off_j] with |h_j| = W (|cdf_j| - |cdf_prev|) and the sign of slot j.
+// The record is read with 256-bit loads and its first 32 bytes (W, c and the
+// first CDF slots) written back with one 256-bit store.
+template <int WORDS>
+__device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, const double* v,
+                                                   double omega, int has, int K,
+                                                   const StencilOffsets& so) {
+    uint32_t q[WORDS];
+#pragma unroll
+    for (int t = 0; t < WORDS / 8; ++t)
+        asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(q[8 * t]), "=r"(q[8 * t + 1]), "=r"(q[8 * t + 2]), "=r"(q[8 * t + 3]),
+                       "=r"(q[8 * t + 4]), "=r"(q[8 * t + 5]), "=r"(q[8 * t + 6]),
+                       "=r"(q[8 * t + 7])
+                     : "l"(r + 8 * t));
+    const float W = __uint_as_float(q[0]);
+    float prev = 0.f;
+    double c = 0.0;
+#pragma unroll
+    for (int j = 0; j < WORDS - 2; ++j) {
+        if (j >= K) break;
+        const float qv = __uint_as_float(q[2 + j]);
+        if (isnan(qv)) continue;
+        const float a = fabsf(qv);
+        const float h = W * (a - prev);
+        prev = a;
+        c = fma(double(qv < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
+    }
+    q[1] = __float_as_uint(__double2float_rn(c));
+    asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
+                 "r"(q[1]), "r"(q[2]), "r"(q[3]), "r"(q[4]), "r"(q[5]), "r"(q[6]), "r"(q[7])
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, double omega,
                                                              int has, int ev, int K,
                                                              StencilOffsets so, int words,
                                                              uint32_t* rec, double* y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* r = rec + size_t(i) * words;
-        double c;
         if (!ev) {
-            c = load_src(v, i, omega, has);
-            r[1] = __float_as_uint(__double2float_rn(c));
+            r[1] = __float_as_uint(__double2float_rn(load_src(v, i, omega, has)));
         } else if (words == 8) {
-            // One 256-bit load and one 256-bit store of the whole record.
-            uint32_t q[8];
-            asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                         : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]),
-                           "=r"(q[5]), "=r"(q[6]), "=r"(q[7])
-                         : "l"(r));
-            const float W = __uint_as_float(q[0]);
-            float prev = 0.f;
-            c = 0.0;
-#pragma unroll
-            for (int j = 0; j < 6; ++j) {
-                const float qv = __uint_as_float(q[2 + j]);
-                if (j >= K || isnan(qv)) continue;
-                const float a = fabsf(qv);
-                const float h = W * (a - prev);
-                prev = a;
-                c = fma(double(qv < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
-            }
-            q[1] = __float_as_uint(__double2float_rn(c));
-            asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
-                         "r"(q[1]), "r"(q[2]), "r"(q[3]), "r"(q[4]), "r"(q[5]), "r"(q[6]),
-                         "r"(q[7])
-                         : "memory");
+            rec_stencil_source<8>(r, i, v, omega, has, K, so);
+        } else if (words == 16) {
+            rec_stencil_source<16>(r, i, v, omega, has, K, so);
         } else {
-            const float W = __uint_as_float(r[0]);
-            float prev = 0.f;
-            c = 0.0;
-            for (int j = 0; j < K; ++j) {
-                const float q = __uint_as_float(r[2 + j]);
-                if (isnan(q)) continue;
-                const float a = fabsf(q);
-                const float h = W * (a - prev);
-                prev = a;
-                c = fma(double(q < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
-            }
-            r[1] = __float_as_uint(__double2float_rn(c));
+            rec_stencil_source<32>(r, i, v, omega, has, K, so);
         }
         y[i] = 0.0;
     }

@@ -1019,6 +1019,12 @@ int spai_build(mclsgpu_context* ctx, mclsgpu_operator* op, const mclsgpu_precond
     if (keep) {
         J.release();
         dfree(dinv);
+        // M on A's diagonals too, for the fused MCSA iteration.
+        rc = csr_to_dia(ctx, pc->P, op->dia_k, op->dia_off, &pc->mdia);
+        if (rc) {
+            pc->P.release();
+            return rc;
+        }
         pc->kind = MCLSGPU_PREC_LEARNED_SPAI;
         pc->rho = rho_l;
         pc->fallback = 0;
