@@ -36,6 +36,11 @@ CONFIGS = {
                         "expected-value estimator, FP32 walks / FP64 tallies, residual and update, "
                         "2^22 histories per iteration",
                n=128, sample_ratio=2.0, estimator=1, history_length=10, direction=1),
+    "blocks256": dict(workload="3D 7-pt diffusion-reaction 256^3, piecewise-constant D in "
+                               "[0.5,5] and sigma_a in [0.001,0.1] on 8^3 random blocks, Jacobi "
+                               "MCSA, forward expected-value estimator, FP32 walks / FP64 "
+                               "tallies, residual and update, 2^24 histories per iteration",
+                      n=256, sample_ratio=1.0, estimator=1, history_length=10, direction=1),
     "batched": dict(workload="batched: 1024 systems (2D/3D Poisson and var-coef diffusion, N "
                              "log-uniform in [1e3, nmax] on square/cube grids), 1-16 right-hand "
                              "sides uniform(0,1) each, point-Jacobi forward expected-value MCSA, "
@@ -128,6 +133,8 @@ def make_system(cfg):
     c = CONFIGS[cfg]
     if cfg == "diffusion128":
         A, b = P.diffusion3d_varcoef(c["n"], seed=0)
+    elif cfg == "blocks256":
+        A, b = P.diffusion3d_blocks(c["n"], 8, seed=0)
     else:
         A = P.poisson2d(c["n"])
         b = np.ones(A.shape[0])
@@ -171,7 +178,10 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     t0 = time.perf_counter()
     samples = []
     for seed in range(8):
-        At, bt_ = P.diffusion3d_varcoef(32, seed=1000 + seed)
+        if args.config == "blocks256":
+            At, bt_ = P.diffusion3d_blocks(32, 4, seed=1000 + seed)
+        else:
+            At, bt_ = P.diffusion3d_varcoef(32, seed=1000 + seed)
         opt = capi.Operator(ctx, At)
         samples.append((opt, spai.training_vectors(ctx, opt, bt_, seed=seed, n_random=4,
                                                    iterations=(1, 4, 16))))
@@ -212,7 +222,9 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
            "h_entries_per_row": info["max_row_entries"], "walk_launch": tuned,
            "train_s": train_s, "train_steps": 2000, "train_loss_first": float(np.mean(losses[:8])),
            "train_loss_last": float(np.mean(losses[-40:])),
-           "train_systems": "8 x 3D 7-pt var-coef diffusion 32^3 (seeds 1000-1007)",
+           "train_systems": ("8 x 3D 7-pt diffusion-reaction 32^3 on 4^3 random blocks "
+                             "(seeds 1000-1007)" if args.config == "blocks256" else
+                             "8 x 3D 7-pt var-coef diffusion 32^3 (seeds 1000-1007)"),
            "speedup_vs_jacobi": jacobi_ms / ms}
     dom.close()
     pc.close()
@@ -415,7 +427,7 @@ def main():
     torch.cuda.set_device(local)
     A, b = make_system(args.config)
     n = A.shape[0]
-    fp = capi.FP32 if args.config == "diffusion128" else capi.FP64
+    fp = capi.FP32 if args.config in ("diffusion128", "blocks256") else capi.FP64
     ctx = capi.Context(local)
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
@@ -518,7 +530,7 @@ def main():
                      "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
         "wall_s": wall,
     }
-    if world == 1 and args.config == "diffusion128" and not args.no_learned:
+    if world == 1 and args.config in ("diffusion128", "blocks256") and not args.no_learned:
         line["config"]["learned_spai"] = learned_arm(args, ctx, op, A, b, cfgd,
                                                      dev_ms_max / args.steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

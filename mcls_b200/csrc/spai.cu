@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <cstring>
 #include <random>
 #include <utility>
@@ -819,17 +820,30 @@ int slot_table(mclsgpu_context* ctx, const mclsgpu_operator* op, int want, SlotT
     return MCLSGPU_OK;
 }
 
-bool g_attr_set = false;
+// The kernels' dynamic shared memory exceeds the 48 KB default: opt in once
+// per device (the attribute belongs to the device's context).
+std::mutex g_attr_mutex;
+bool g_attr_set[64] = {false};
+
+int set_smem_attributes(mclsgpu_context* ctx) {
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    const int d = ctx->device;
+    if (d >= 0 && d < 64 && g_attr_set[d]) return MCLSGPU_OK;
+    cudaError_t e = cudaFuncSetAttribute(k_spai_forward,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spai_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kBwSmem);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "spai shared-memory opt-in");
+    if (d >= 0 && d < 64) g_attr_set[d] = true;
+    return MCLSGPU_OK;
+}
 
 int launch_forward(mclsgpu_spai* net, mclsgpu_operator* op, const SlotTable& t, double* mval,
                    float* out) {
     mclsgpu_context* ctx = net->ctx;
-    if (!g_attr_set) {
-        cudaFuncSetAttribute(k_spai_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
-        cudaFuncSetAttribute(k_spai_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kBwSmem);
-        g_attr_set = true;
-    }
+    int rc = set_smem_attributes(ctx);
+    if (rc) return rc;
     SpaiFwdArgs a{};
     a.params = net->params;
     a.dia = op->dia_val;
