@@ -186,8 +186,8 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
         samples.append((opt, spai.training_vectors(ctx, opt, bt_, seed=seed, n_random=4,
                                                    iterations=(1, 4, 16))))
     net = capi.SpaiNet(ctx, spai.stencil_slots(A), seed=0)
-    losses = spai.train(net, samples, steps=2000, lr=3e-3, lr_final=3e-4, refresh=25,
-                        adv_count=8, adv_iters=50)
+    losses = spai.train(net, samples, steps=args.spai_steps, lr=3e-3, lr_final=3e-4,
+                        refresh=25, adv_count=8, adv_iters=50)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     rl, rj = net.rho(op, iters=300)
@@ -195,7 +195,8 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=1234,
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
                       direction=cfgd["direction"], history_length=cfgd["history_length"])
-    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
+                          host_loop=1 if args.host_loop else 0)
     bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
     xt = torch.zeros_like(bt)
     tuned = dom.autotune(bt.data_ptr(), reps=1)
@@ -220,7 +221,7 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
            "fallback_taken": bool(stats[-1]["fallback_taken"]),
            "record_bytes": info["record_bytes"], "record_format": info["record_format"],
            "h_entries_per_row": info["max_row_entries"], "walk_launch": tuned,
-           "train_s": train_s, "train_steps": 2000, "train_loss_first": float(np.mean(losses[:8])),
+           "train_s": train_s, "train_steps": args.spai_steps, "train_loss_first": float(np.mean(losses[:8])),
            "train_loss_last": float(np.mean(losses[-40:])),
            "train_systems": ("8 x 3D 7-pt diffusion-reaction 32^3 on 4^3 random blocks "
                              "(seeds 1000-1007)" if args.config == "blocks256" else
@@ -403,6 +404,8 @@ def main():
     ap.add_argument("--host-loop", action="store_true",
                     help="host-driven MCSA loop (for profilers that cannot see kernels "
                          "inside conditional graph nodes)")
+    ap.add_argument("--spai-steps", type=int, default=2000,
+                    help="training steps of the learned-SPAI network")
     ap.add_argument("--batch-systems", type=int, default=1024)
     ap.add_argument("--batch-nmax", type=float, default=1e4,
                     help="largest system of the batched workload (5e5 for the full size)")
