@@ -39,9 +39,11 @@ __global__ void k_random_count(int nh_req, double* sc, int* d_nh, int cap, int* 
     const double norm1 = sc[0], total = sc[1];
     const double r = __ddiv_rn(__dmul_rn(double(nh_req), total), norm1);
     int nh = (r >= 0.0 && r < 2147483647.0) ? int(r) : (r >= 2147483647.0 ? INT_MAX : 0);
-    if (!(norm1 > 0.0) || !isfinite(norm1)) {
+    if (!isfinite(norm1) || !isfinite(total)) {
         nh = 0;
         atomicOr(status, DEV_ERR_NONFINITE);
+    } else if (!(norm1 > 0.0)) {
+        nh = 0;  // zero source (an exact iterate): no histories, zero correction
     }
     if (nh > cap) {
         // total <= norm1 in exact arithmetic, so nh <= nh_req <= cap; more
@@ -121,6 +123,10 @@ __global__ void k_advance_pos(unsigned long long* d_pos, const int* d_nh, int mu
 // counts_i = ceil(|b_i| * (nh_local / local_sum)) (:246-262).
 __global__ void k_strat_prep(int nh_req, double* sc) {
     const double s = sc[0];
+    if (!(s > 0.0)) {  // zero source: no histories (non-finite sums are flagged elsewhere)
+        sc[3] = 0.0;
+        return;
+    }
     const double nh_local = ceil(__ddiv_rn(__dmul_rn(double(nh_req), s), s));
     sc[3] = __ddiv_rn(double(int(nh_local)), s);
 }
