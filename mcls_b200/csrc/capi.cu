@@ -48,6 +48,7 @@ int check_device_status(mclsgpu_context* ctx) {
 }
 
 void prepare_walk(mclsgpu_domain* dom);
+void prepare_source(mclsgpu_domain* dom);
 int spai_build(mclsgpu_context* ctx, mclsgpu_operator* op, const mclsgpu_precond_params* p,
                mclsgpu_precond* pc);
 
@@ -514,6 +515,7 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
     }
     if (!rc) {
         prepare_walk(dom);
+        prepare_source(dom);
         e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "domain build");
     }

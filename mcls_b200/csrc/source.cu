@@ -18,6 +18,8 @@
 #include <cfloat>
 #include <climits>
 
+#include <mutex>
+
 #include "internal.h"
 #include "rng.cuh"
 
@@ -284,7 +286,205 @@ __global__ void k_forward_nh(int* d_nh, int nh, double* sc) {
     sc[2] = 1.0 / double(nh);
 }
 
+// ---- small systems: the whole adjoint source in one CTA ------------------
+// For a few thousand states the multi-kernel source build (reductions,
+// scans, guide table, sampling, expansion: about 19 launches) is all launch
+// latency.  One block of 1024 threads does the same steps in shared memory
+// and registers: |v|_1 and the CDF with the reference's signed first element
+// (both sums with one association, so that they agree when v[0] >= 0), the
+// history count, the normalised CDF, the counter-stream draws with
+// lower_bound (the guide table only narrows that search), the counts' suffix
+// scan (LIFO emission order) and the expansion into starting states.
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallSourceMax = 16384;
+
+// Inclusive block scan of one value per thread (all 1024 threads call it).
+__device__ __forceinline__ double block_scan_incl(double x, double* warp_tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        double t = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, t, d);
+            if (lane >= d) t += y;
+        }
+        warp_tot[lane] = t;
+    }
+    __syncthreads();
+    const double r = w > 0 ? x + warp_tot[w - 1] : x;
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ int block_scan_incl_int(int x, int* warp_tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = warp_tot[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, d);
+            if (lane >= d) t += y;
+        }
+        warp_tot[lane] = t;
+    }
+    __syncthreads();
+    const int r = w > 0 ? x + warp_tot[w - 1] : x;
+    __syncthreads();
+    return r;
+}
+
+// Shared memory: the CDF (n doubles) and the per-state counts (n ints).
+constexpr int kSmallSmem = kSmallSourceMax * (sizeof(double) + sizeof(int));
+
+__global__ void __launch_bounds__(kSmallThreads) k_small_adjoint_source(
+    const double* v, int n, double omega, int has, int nh_req, int cap, uint64_t seed,
+    const unsigned long long* d_epoch, int* start, double* y, double* sc, int* d_nh,
+    int* status) {
+    extern __shared__ __align__(16) unsigned char smem_src[];
+    double* cdf = reinterpret_cast<double*>(smem_src);
+    int* counts = reinterpret_cast<int*>(smem_src + sizeof(double) * kSmallSourceMax);
+    __shared__ double wtot[32];
+    __shared__ int wtoti[32];
+    __shared__ double s_carry[2];
+    __shared__ int s_carry_i;
+    __shared__ int s_nh;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_carry[0] = 0.0;
+        s_carry[1] = 0.0;
+        s_carry_i = 0;
+    }
+    __syncthreads();
+    // 1. Raw CDF (signed first element) and |v|_1 with the same association.
+    for (int base = 0; base < n; base += kSmallThreads) {
+        const int i = base + tid;
+        double a = 0.0, sgn = 0.0;
+        if (i < n) {
+            const double b = load_src(v, i, omega, has);
+            a = fabs(b);
+            sgn = i == 0 ? b : a;
+        }
+        const double cs = block_scan_incl(sgn, wtot) + s_carry[0];
+        const double ca = block_scan_incl(a, wtot) + s_carry[1];
+        if (i < n) cdf[i] = cs;
+        __syncthreads();
+        if (tid == kSmallThreads - 1) {
+            s_carry[0] = cs;
+            s_carry[1] = ca;
+        }
+        __syncthreads();
+    }
+    // 2. History count nh = int(Nh * cdf.back() / |v|_1) (:198), weights.
+    if (tid == 0) {
+        const double norm1 = s_carry[1], total = s_carry[0];
+        const double r = __ddiv_rn(__dmul_rn(double(nh_req), total), norm1);
+        int nh = (r >= 0.0 && r < 2147483647.0) ? int(r) : (r >= 2147483647.0 ? INT_MAX : 0);
+        if (!isfinite(norm1) || !isfinite(total)) {
+            nh = 0;
+            atomicOr(status, DEV_ERR_NONFINITE);
+        } else if (!(norm1 > 0.0)) {
+            nh = 0;
+        }
+        if (nh > cap) {
+            atomicOr(status, DEV_ERR_NONFINITE);
+            nh = cap;
+        }
+        sc[0] = norm1;
+        sc[1] = total;
+        sc[2] = nh > 0 ? 1.0 / double(nh) : 0.0;
+        *d_nh = nh;
+        s_nh = nh;
+    }
+    __syncthreads();
+    const int nh = s_nh;
+    // 3. Normalise (cdf[n-1] = 1 exactly) and clear the counts.
+    const double total = s_carry[0];
+    for (int i = tid; i < n; i += kSmallThreads) {
+        cdf[i] = i == n - 1 ? 1.0 : cdf[i] / total;
+        counts[i] = 0;
+    }
+    __syncthreads();
+    // 4. Draw the starting states (counter stream, kind 1).
+    const uint64_t ekey = epoch_key(seed, *d_epoch);
+    for (int k = tid; k < nh; k += kSmallThreads) {
+        const double u = canonical64(xs_step(counter_state(ekey, 1, uint64_t(k))));
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf[mid] < u) lo = mid + 1; else hi = mid;
+        }
+        atomicAdd(&counts[lo], 1);
+    }
+    __syncthreads();
+    // 5. Exclusive suffix sum of the counts (LIFO emission: highest state
+    //    first) and, chunk by chunk, the expansion into starting states and
+    //    step-0 tallies.
+    const double weight = sc[0];
+    for (int base = 0; base < n; base += kSmallThreads) {
+        const int k = base + tid;      // position in reversed order
+        const int i = n - 1 - k;       // state
+        const int c = k < n ? counts[i] : 0;
+        const int incl = block_scan_incl_int(c, wtoti) + s_carry_i;
+        if (k < n) {
+            const int o = incl - c;
+            const double b = load_src(v, i, omega, has);
+            const unsigned sign = b > 0.0 ? 0u : 0x80000000u;
+            if (c > 0) {
+                if (o + c > cap) {
+                    atomicOr(status, DEV_ERR_CAPACITY);
+                } else {
+                    for (int t = 0; t < c; ++t) start[o + t] = int(unsigned(i) | sign);
+                }
+                y[i] = double(c) * (sign ? -weight : weight);
+            } else {
+                y[i] = 0.0;
+            }
+        }
+        __syncthreads();
+        if (tid == kSmallThreads - 1) s_carry_i = incl;
+        __syncthreads();
+    }
+}
+
+// Dynamic shared memory opt-in for k_small_adjoint_source, once per device.
+std::mutex g_small_mutex;
+bool g_small_set[64] = {false};
+
+bool small_source_ready(mclsgpu_context* ctx) {
+    std::lock_guard<std::mutex> lock(g_small_mutex);
+    const int d = ctx->device;
+    if (d >= 0 && d < 64 && g_small_set[d]) return true;
+    if (cudaFuncSetAttribute(k_small_adjoint_source, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmallSmem) != cudaSuccess) {
+        cudaGetLastError();
+        return false;  // keep the multi-kernel path
+    }
+    if (d >= 0 && d < 64) g_small_set[d] = true;
+    return true;
+}
+
 }  // namespace
+
+// Set-up time (outside any stream capture): the small-system source kernel's
+// shared-memory opt-in.
+void prepare_source(mclsgpu_domain* dom) {
+    if (dom->n <= kSmallSourceMax && dom->p.direction == MCLSGPU_ADJOINT)
+        small_source_ready(dom->ctx);
+}
 
 // Build the adjoint source from v*omega (omega applied when has_omega).
 void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega) {
@@ -299,6 +499,14 @@ void launch_adjoint_source(mclsgpu_domain* dom, const double* v, double omega, i
     const bool parity = p.precision == MCLSGPU_FP64 && p.rng_mode == MCLSGPU_RNG_REFERENCE;
     const int nh_req = p.sample_ratio > 0.0 ? int(double(n) * p.sample_ratio) : n;
     const int cap = int(dom->nh_cap);
+    if (!parity && p.rng_mode == MCLSGPU_RNG_COUNTER &&
+        p.source_sampling == MCLSGPU_SOURCE_RANDOM && n <= kSmallSourceMax &&
+        small_source_ready(ctx)) {
+        k_small_adjoint_source<<<1, kSmallThreads, kSmallSmem, s>>>(
+            v, n, omega, has_omega, nh_req, cap, dom->seed, dom->d_epoch, dom->start, dom->y64,
+            dom->d_scalars, dom->d_nh, ctx->d_status);
+        return;
+    }
     // weight = |b|_1
     abs_sum(s, v, n, omega, has_omega, parity ? nullptr : dom->part, dom->d_scalars + 0);
     cudaMemsetAsync(dom->counts, 0, size_t(n) * sizeof(int), s);

@@ -356,7 +356,11 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
             if (a.tr_start) a.tr_start[e] = s0;
         }
     }
-    atomicAdd(a.d_steps, steps);
+    // Step count: one atomic per warp (one per thread serialises on the
+    // counter when most threads have no history).
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) steps += __shfl_down_sync(kFull, steps, d);
+    if ((threadIdx.x & 31) == 0 && steps) atomicAdd(a.d_steps, steps);
 }
 
 template <int S, int DIR, bool ST, bool FX, int ILP>
@@ -652,7 +656,11 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
         dispatch_walk32(dom, a, true);
         if (!fused) k_walk_time_acc<<<1, 1, 0, st>>>(dom->d_tim);
     } else {
-        const int grid = ctx->num_sms * 8;
+        // One thread per history up to 8 blocks per SM (the kernel strides
+        // beyond that); no more blocks than the history capacity needs.
+        long long g = (dom->nh_cap + 127) / 128;
+        if (g < 1) g = 1;
+        const int grid = int(g < ctx->num_sms * 8 ? g : ctx->num_sms * 8);
         if (p.direction == MCLSGPU_ADJOINT)
             walk64<MCLSGPU_ADJOINT><<<grid, 128, 0, st>>>(a);
         else
