@@ -367,6 +367,11 @@ def cpu_baseline(cfg, A, b, seconds_target=15.0):
 def run_reference(args, world, rank, pg):
     if rank != 0:
         return
+    if args.config == "batched":
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement solves one "
+                          "system per call; the batched workload has no single-system "
+                          "reference timing"}))
+        return
     A, b = make_system(args.config)
     vals = []
     base = None
