@@ -315,6 +315,16 @@ inline mclsgpu_mc_params mcParams(const Teuchos::ParameterList& pl, int directio
     return p;
 }
 
+// "Fixed Point Type" (src/MCLS_FixedPointIterationFactory_impl.hpp:56-107).
+inline int fixedPointType(const Teuchos::ParameterList& pl) {
+    const std::string fp = text(pl, "Fixed Point Type", "Richardson");
+    if (fp == "Richardson") return MCLSGPU_FIXED_POINT_RICHARDSON;
+    if (fp == "Steepest Descent") return MCLSGPU_FIXED_POINT_STEEPEST_DESCENT;
+    if (fp == "MINRES") return MCLSGPU_FIXED_POINT_MINRES;
+    if (fp == "RNSD") return MCLSGPU_FIXED_POINT_RNSD;
+    throw Assertion("Iteration type not supported!");
+}
+
 // MCSA keys (src/MCLS_MCSASolverManager_impl.hpp:290-343,
 // src/MCLS_RichardsonIteration_impl.hpp:56-99).
 inline mclsgpu_mcsa_params mcsaParams(const Teuchos::ParameterList& pl) {
@@ -329,10 +339,15 @@ inline mclsgpu_mcsa_params mcsaParams(const Teuchos::ParameterList& pl) {
     // The reference prints its banner and every print_freq-th residual on
     // rank 0; "Print Iterations" = false silences it.
     p.verbose = flag(pl, "Print Iterations", true) ? 1 : 0;
-    const std::string fp = text(pl, "Fixed Point Type", "Richardson");
-    if (fp != "Richardson")
-        throw Assertion("Fixed Point Type \"" + fp +
-                        "\": the GPU MCSA path provides the Richardson smoother only");
+    p.fixed_point_type = fixedPointType(pl);
+    return p;
+}
+
+// FixedPointSolverManager keys (src/MCLS_FixedPointSolverManager_impl.hpp:
+// 214-268): the MCSA keys without the smoother count.
+inline mclsgpu_mcsa_params fixedPointParams(const Teuchos::ParameterList& pl) {
+    mclsgpu_mcsa_params p = mcsaParams(pl);
+    p.smoother_steps = 1;
     return p;
 }
 

@@ -3,7 +3,8 @@
 // Same constructors and SolverManager methods as the reference manager
 // (src/MCLS_MCSASolverManager.hpp:85-135,
 // src/MCLS_MCSASolverManager_impl.hpp:56-432).  solve() runs the whole MCSA
-// loop on the device -- Richardson smoothing, preconditioned residual, the
+// loop on the device -- smoothing ("Fixed Point Type": Richardson, Steepest
+// Descent, MINRES or RNSD), preconditioned residual, the
 // Monte Carlo correction and the convergence test
 // |rp|_2 <= tol * |PL b|_2 -- and updates x in place.
 #ifndef MCLS_MCSASOLVERMANAGER_HPP

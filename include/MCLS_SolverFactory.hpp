@@ -1,8 +1,8 @@
 // MCLS_SolverFactory.hpp -- name -> solver manager
 // (src/MCLS_SolverFactory.hpp:61-95, src/MCLS_SolverFactory_impl.hpp:57-140).
 //
-// "Adjoint MC", "Forward MC", "Adjoint MCSA" and "Forward MCSA" create the
-// GPU managers.  "Adjoint Anderson", "Forward Anderson" and "Fixed Point"
+// "Adjoint MC", "Forward MC", "Adjoint MCSA", "Forward MCSA" and "Fixed
+// Point" create the GPU managers.  "Adjoint Anderson" and "Forward Anderson"
 // are names the reference knows but this library does not provide; they
 // throw Assertion naming the solver, as unknown names do.
 #ifndef MCLS_SOLVERFACTORY_HPP
@@ -11,6 +11,7 @@
 #include <map>
 #include <string>
 
+#include "MCLS_FixedPointSolverManager.hpp"
 #include "MCLS_MCSASolverManager.hpp"
 #include "MCLS_MonteCarloSolverManager.hpp"
 
@@ -36,8 +37,9 @@ class SolverFactory {
             return Teuchos::rcp(new MCSASolverManager<Vector, Matrix, AdjointTag>(solver_parameters));
         if (solver_name == "Forward MCSA")
             return Teuchos::rcp(new MCSASolverManager<Vector, Matrix, ForwardTag>(solver_parameters));
-        if (solver_name == "Adjoint Anderson" || solver_name == "Forward Anderson" ||
-            solver_name == "Fixed Point")
+        if (solver_name == "Fixed Point")
+            return Teuchos::rcp(new FixedPointSolverManager<Vector, Matrix>(solver_parameters));
+        if (solver_name == "Adjoint Anderson" || solver_name == "Forward Anderson")
             throw Assertion("Solver type \"" + solver_name + "\" is not provided by the GPU path");
         throw Assertion("Solver type not supported!");
     }

@@ -112,8 +112,18 @@ typedef struct {
     int32_t host_loop;        /* 1: host-driven loop (one launch sequence and
                                * host check per iteration) instead of the
                                * device-side graph loop; for profilers */
-    int32_t reserved0;
+    int32_t fixed_point_type; /* "Fixed Point Type": MCLSGPU_FIXED_POINT_*
+                               * (Richardson) -- the smoother's iteration */
 } mclsgpu_mcsa_params;
+
+/* Fixed-point iterations (FixedPointIterationFactory names,
+ * src/MCLS_FixedPointIterationFactory_impl.hpp:61-64). */
+enum {
+    MCLSGPU_FIXED_POINT_RICHARDSON = 0,       /* "Richardson"       */
+    MCLSGPU_FIXED_POINT_STEEPEST_DESCENT = 1, /* "Steepest Descent" */
+    MCLSGPU_FIXED_POINT_MINRES = 2,           /* "MINRES"           */
+    MCLSGPU_FIXED_POINT_RNSD = 3              /* "RNSD"             */
+};
 
 /* Preconditioner parameters. */
 typedef struct {
@@ -338,6 +348,36 @@ int mclsgpu_mcsa_solve(mclsgpu_domain* dom, const double* b, double* x,
 int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev,
                            double* x_dev, const mclsgpu_mcsa_params* params,
                            mclsgpu_stats* stats);
+/* ---- fixed-point solve ------------------------------------------------------ */
+/* Replaces FixedPointSolverManager::solve (src/MCLS_FixedPointSolverManager_
+ * impl.hpp:208-321): params->fixed_point_type iterations alone, no Monte
+ * Carlo, until |rp|_inf <= tolerance |PL b|_inf (checked every check_freq
+ * iterations) or max_iters.  The iterations are
+ *   Richardson        x += w rp; rp = PL (b - A PR x)
+ *                     (src/MCLS_RichardsonIteration_impl.hpp:134-147)
+ *   Steepest Descent  p = Op rp; a = <rp,rp>/<p,rp>; x += a rp; rp -= a p
+ *                     (src/MCLS_SteepestDescentIteration_impl.hpp:114-136)
+ *   MINRES            p = Op rp; a = <p,rp>/<p,p>;   x += a rp; rp -= a p
+ *                     (src/MCLS_MinimalResidualIteration_impl.hpp:114-136)
+ *   RNSD              v = Op^T rp; w = Op v; a = <v,v>/<w,w>; x += a v;
+ *                     rp -= a w  (src/MCLS_RNSDIteration_impl.hpp:118-142)
+ * with Op = PL A PR (LinearProblem::apply / applyTranspose,
+ * src/MCLS_LinearProblem_impl.hpp:251-315).  A zero denominator gives a = 0
+ * (the reference divides by it).  left and right may be NULL.  Host
+ * vectors (b, x: x holds the initial guess and receives PR x) or, in the
+ * _dev form, device vectors.  stats->iterations, converged, residual_norm
+ * (|rp|_inf) and achieved_tol (|rp|_inf / |PL b|_inf) are filled. */
+int mclsgpu_fixed_point_solve(mclsgpu_context* ctx, mclsgpu_operator* op,
+                              mclsgpu_precond* left, mclsgpu_precond* right,
+                              const double* b, double* x,
+                              const mclsgpu_mcsa_params* params,
+                              mclsgpu_stats* stats);
+int mclsgpu_fixed_point_solve_dev(mclsgpu_context* ctx, mclsgpu_operator* op,
+                                  mclsgpu_precond* left, mclsgpu_precond* right,
+                                  const double* b_dev, double* x_dev,
+                                  const mclsgpu_mcsa_params* params,
+                                  mclsgpu_stats* stats);
+
 /* MCSA one iteration at a time, for drivers that combine the Monte Carlo
  * corrections of several sets (one set per GPU): the loop of
  * MCSASolverManager::solve with MultiSetLinearProblem::blockConstantVectorSum
@@ -345,7 +385,7 @@ int mclsgpu_mcsa_solve_dev(mclsgpu_domain* dom, const double* b_dev,
  * (src/MCLS_MCSASolverManager_impl.hpp:344-400,
  *  src/MCLS_MultiSetLinearProblem_impl.hpp:102-120).
  *   begin:      x = x0, rp = PL (b - A PR x); *rnorm = |rp|_2, *bnorm = |PL b|_2
- *   correction: smoother_steps Richardson steps, then delta_dev = the Monte
+ *   correction: smoother_steps fixed-point steps, then delta_dev = the Monte
  *               Carlo estimate of the correction (this set's histories)
  *   apply:      x += scale * delta_dev (scale = 1 / number of sets after the
  *               caller summed delta over the sets), new rp; *rnorm = |rp|_2

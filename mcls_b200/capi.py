@@ -24,6 +24,11 @@ FP64, FP32 = 0, 1
 RNG_REFERENCE, RNG_COUNTER = 0, 1
 RECORD_AUTO, RECORD_PACKED, RECORD_STENCIL = 0, 1, 2
 PREC_NONE, PREC_POINT_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED_SPAI, PREC_USER_CSR = range(5)
+FIXED_POINT_RICHARDSON, FIXED_POINT_STEEPEST_DESCENT, FIXED_POINT_MINRES, FIXED_POINT_RNSD = range(4)
+#: "Fixed Point Type" names (FixedPointIterationFactory) to the C enum.
+FIXED_POINT_TYPES = {"Richardson": FIXED_POINT_RICHARDSON,
+                     "Steepest Descent": FIXED_POINT_STEEPEST_DESCENT,
+                     "MINRES": FIXED_POINT_MINRES, "RNSD": FIXED_POINT_RNSD}
 
 
 class McParams(C.Structure):
@@ -55,7 +60,7 @@ class McsaParams(C.Structure):
         ("print_freq", C.c_int32),
         ("verbose", C.c_int32),
         ("host_loop", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("fixed_point_type", C.c_int32),
     ]
 
 
@@ -137,7 +142,8 @@ EXPORTS = [
     "mclsgpu_batch_build", "mclsgpu_batch_destroy", "mclsgpu_batch_layout",
     "mclsgpu_batch_domain", "mclsgpu_batch_set_launch", "mclsgpu_batch_autotune",
     "mclsgpu_batch_mcsa_solve_dev", "mclsgpu_mcsa_begin", "mclsgpu_mcsa_correction",
-    "mclsgpu_mcsa_apply", "mclsgpu_mcsa_finish",
+    "mclsgpu_mcsa_apply", "mclsgpu_mcsa_finish", "mclsgpu_fixed_point_solve",
+    "mclsgpu_fixed_point_solve_dev",
 ]
 
 _LIB = None
@@ -201,6 +207,10 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_mcsa_correction.argtypes = [P, P]
     L.mclsgpu_mcsa_apply.argtypes = [P, P, d, C.POINTER(d)]
     L.mclsgpu_mcsa_finish.argtypes = [P, P, C.POINTER(Stats)]
+    L.mclsgpu_fixed_point_solve.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
+                                            C.POINTER(Stats)]
+    L.mclsgpu_fixed_point_solve_dev.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
+                                                C.POINTER(Stats)]
     L.mclsgpu_spai_num_params.restype = C.c_int
     L.mclsgpu_spai_create.argtypes = [P, C.c_int, C.c_uint64, PP]
     L.mclsgpu_spai_destroy.argtypes = [P]
@@ -370,7 +380,10 @@ def mc_params(direction=ADJOINT, estimator=COLLISION, history_length=10, weight_
 
 
 def mcsa_params(tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
-                richardson_omega=1.0, print_freq=10, verbose=0, host_loop=0):
+                richardson_omega=1.0, print_freq=10, verbose=0, host_loop=0,
+                fixed_point_type=FIXED_POINT_RICHARDSON):
+    if isinstance(fixed_point_type, str):
+        fixed_point_type = FIXED_POINT_TYPES[fixed_point_type]
     p = McsaParams()
     p.size = C.sizeof(McsaParams)
     p.tolerance = tolerance
@@ -381,7 +394,24 @@ def mcsa_params(tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
     p.print_freq = print_freq
     p.verbose = verbose
     p.host_loop = host_loop
+    p.fixed_point_type = fixed_point_type
     return p
+
+
+def fixed_point_solve(ctx: Context, op: Operator, b, x0=None, left: Precond | None = None,
+                      right: Precond | None = None, params: McsaParams | None = None, **kw):
+    """FixedPointSolverManager::solve on the GPU: (x, stats).  Keywords as
+    mcsa_params; the reference's default tolerance here is 1.0."""
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+    kw.setdefault("tolerance", 1.0)
+    p = params if params is not None else mcsa_params(**kw)
+    st = Stats()
+    st.size = C.sizeof(Stats)
+    ctx.check(ctx.L.mclsgpu_fixed_point_solve(ctx.h, op.h, left.h if left else None,
+                                              right.h if right else None, _ptr(b), _ptr(x),
+                                              C.byref(p), C.byref(st)))
+    return x, st.as_dict()
 
 
 class Domain:

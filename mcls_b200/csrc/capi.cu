@@ -261,6 +261,7 @@ int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n, const int64_t* rowp
 int mclsgpu_operator_destroy(mclsgpu_operator* op) {
     if (!op) return MCLSGPU_OK;
     op->A.release();
+    op->AT.release();
     op->S.release();
     dfree(op->dia_val);
     dfree(op->dinv);
@@ -345,6 +346,7 @@ int mclsgpu_precond_build(mclsgpu_context* ctx, mclsgpu_operator* op,
 int mclsgpu_precond_destroy(mclsgpu_precond* pc) {
     if (!pc) return MCLSGPU_OK;
     pc->P.release();
+    pc->PT.release();
     dfree(pc->diag);
     dfree(pc->mdia);
     delete pc;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <functional>
 #include <string>
 
 #include "../../include/mclsgpu.h"
@@ -74,6 +75,7 @@ struct mclsgpu_operator {
     int dia_off[16] = {0};
     double* dia_val = nullptr;
     double* dinv = nullptr;       // reciprocal diagonal (built on demand)
+    mclsgpu::DevCsr AT;           // A^T (built on demand: RNSD iterations)
     uint64_t serial = 0;          // identity for "operator changed" checks
 };
 
@@ -82,6 +84,7 @@ struct mclsgpu_precond {
     int kind = MCLSGPU_PREC_NONE;
     int block_size = 1;
     mclsgpu::DevCsr P;            // left preconditioner as CSR
+    mclsgpu::DevCsr PT;           // P^T (built on demand: RNSD iterations)
     double* diag = nullptr;       // POINT_JACOBI: the reciprocal diagonal
     double* mdia = nullptr;       // LEARNED_SPAI kept: M by A's diagonal offsets
     double rho = -1.0;            // LEARNED_SPAI: rho(H) estimate
@@ -226,6 +229,24 @@ int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int
 // Domain arrays and FP32 records from the composite operator (domain.cu).
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
                         mclsgpu_domain* dom);
+
+// ---- MCSA helpers (mcsa.cu) ----------------------------------------------------
+// rp_out = PL (b - A PR x)   (LinearProblem::updatePrecResidual)
+void prec_residual(mclsgpu_domain* dom, const double* x, const double* b, double* rp_out);
+// y = PL A PR x   (LinearProblem::apply); uses dom->tmp and dom->tmp2.
+void composite_apply(mclsgpu_domain* dom, const double* x, double* y);
+
+// ---- fixed-point iterations (fixedpoint.cu) ------------------------------------
+// Transposes the RNSD iteration needs (set-up: never inside a stream capture).
+int prepare_fixed_point(mclsgpu_domain* dom, int type);
+// One fixed-point step of `type` on dom->x and dom->rp (dom->x2, rp2, tmp and
+// tmp2 as scratch; dom->part, d_ticket and d_scalars[7] for the step length).
+void enqueue_fixed_point_step(mclsgpu_domain* dom, int type, double omega);
+// Instantiate a graph whose only node is a WHILE loop around the launches
+// `body` enqueues on ctx->stream (captured); body_kernels = its kernel nodes.
+int build_while_graph(mclsgpu_context* ctx,
+                      const std::function<void(cudaGraphConditionalHandle)>& body,
+                      cudaGraphExec_t* exec, int* body_kernels);
 
 // ---- scans and reductions (scan.cu) ------------------------------------------
 int scan_partials_needed(int n);

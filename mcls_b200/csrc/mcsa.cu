@@ -104,6 +104,16 @@ __global__ void __launch_bounds__(256) k_residual(Op A, const double* x, const d
     }
 }
 
+// out = [dinv *] A x   (the A and PL factors of LinearProblem::apply, :251-279)
+template <class Op>
+__global__ void __launch_bounds__(256) k_matvec(Op A, const double* x, const double* dinv,
+                                                double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        const double s = A.dot(i, [&](int j) { return x[j]; });
+        out[i] = dinv ? dinv[i] * s : s;
+    }
+}
+
 // x += w * r  (RichardsonIteration::doOneIteration, :134-147)
 __global__ void k_richardson(double* x, const double* r, int n, double w) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -451,6 +461,31 @@ static void update_prec_residual(mclsgpu_domain* dom, const double* x, const dou
     }
 }
 
+void prec_residual(mclsgpu_domain* dom, const double* x, const double* b, double* rp_out) {
+    update_prec_residual(dom, x, b, rp_out);
+}
+
+// y = PL A PR x  (LinearProblem::apply, src/MCLS_LinearProblem_impl.hpp:251-279)
+void composite_apply(mclsgpu_domain* dom, const double* x, double* y) {
+    cudaStream_t s = dom->ctx->stream;
+    const mclsgpu_operator* op = dom->op;
+    const int grid = grid_for(op->A.n, 256, 148 * 8);
+    const double* xin = x;
+    if (dom->right) {
+        spmv(s, dom->right->P, x, dom->tmp2);
+        xin = dom->tmp2;
+    }
+    mclsgpu_precond* L = dom->left;
+    if (!L) {
+        MCLSGPU_LAUNCH_OP(op, grid, 256, s, k_matvec, xin, nullptr, y);
+    } else if (L->kind == MCLSGPU_PREC_POINT_JACOBI) {
+        MCLSGPU_LAUNCH_OP(op, grid, 256, s, k_matvec, xin, L->diag, y);
+    } else {
+        MCLSGPU_LAUNCH_OP(op, grid, 256, s, k_matvec, xin, nullptr, dom->tmp);
+        spmv(s, L->P, dom->tmp, y);
+    }
+}
+
 // One MC solve of the source vector `v` (device, already left preconditioned
 // when required) into out (accumulate: out += delta).  `fused`: inside the
 // fused MCSA iteration the normalise-and-add of the collision and forward
@@ -560,7 +595,8 @@ static int mc_solve_device(mclsgpu_domain* dom, const double* rhs_dev, double* x
 // The fused iteration covers one smoothing step, no right preconditioner and
 // a left preconditioner that is the identity or point Jacobi.
 static bool fused_iteration(const mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
-    return mp->smoother_steps == 1 && !dom->right &&
+    return mp->smoother_steps == 1 && mp->fixed_point_type == MCLSGPU_FIXED_POINT_RICHARDSON &&
+           !dom->right &&
            (!dom->left || dom->left->kind == MCLSGPU_PREC_POINT_JACOBI ||
             (dom->left->mdia && dom->op->dia_k > 0));
 }
@@ -581,11 +617,8 @@ static void enqueue_iteration(mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp
     cudaStream_t s = ctx->stream;
     const int n = dom->n;
     if (!fused_iteration(dom, mp)) {
-        for (int l = 0; l < mp->smoother_steps; ++l) {
-            k_richardson<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, n,
-                                                                  mp->richardson_omega);
-            update_prec_residual(dom, dom->x, dom->b, dom->rp);
-        }
+        for (int l = 0; l < mp->smoother_steps; ++l)
+            enqueue_fixed_point_step(dom, mp->fixed_point_type, mp->richardson_omega);
         enqueue_mc(dom, dom->rp, dom->x, 1, 0, nullptr, nullptr, nullptr, nullptr);
         update_prec_residual(dom, dom->x, dom->b, dom->rp);
         sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
@@ -746,7 +779,13 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
         }
     }
     // Graph key: everything baked into the captured iteration.
-    const int key = mp->smoother_steps * 1000003 ^ int(mp->richardson_omega * 1e6);
+    const int key = (mp->smoother_steps * 1000003 ^ int(mp->richardson_omega * 1e6)) * 4 +
+                    mp->fixed_point_type;
+    if (int rc = prepare_fixed_point(dom, mp->fixed_point_type)) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+    }
     if (!mp->host_loop && (!dom->graph || dom->graph_key != key)) {
         int rc = build_mcsa_graph(dom, mp);
         if (rc) {
@@ -861,6 +900,9 @@ static int check_mcsa_params(mclsgpu_domain* dom, const mclsgpu_mcsa_params* p,
     }
     if (d.max_iters < 1 || d.check_freq < 1 || d.smoother_steps < 0 || !(d.tolerance >= 0.0))
         return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG, "mcsa params out of range");
+    if (d.fixed_point_type < MCLSGPU_FIXED_POINT_RICHARDSON ||
+        d.fixed_point_type > MCLSGPU_FIXED_POINT_RNSD)
+        return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG, "Iteration type not supported!");
     *out = d;
     return MCLSGPU_OK;
 }
@@ -958,7 +1000,9 @@ int mclsgpu_mcsa_begin(mclsgpu_domain* dom, const double* b_dev, const double* x
     mclsgpu_context* ctx = dom->ctx;
     cudaStream_t s = ctx->stream;
     const int n = dom->n;
+    if ((rc = prepare_fixed_point(dom, p.fixed_point_type))) return rc;
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    cudaMemsetAsync(dom->d_ticket, 0, sizeof(unsigned int), s);
     reset_counters(dom);
     if (b_dev != dom->b) cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
     if (x0_dev != dom->x) cudaMemcpyAsync(dom->x, x0_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -991,11 +1035,8 @@ int mclsgpu_mcsa_correction(mclsgpu_domain* dom, double* delta_dev) {
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_mcsa_begin first");
     cudaStream_t s = ctx->stream;
     const mclsgpu_mcsa_params& p = dom->step_p;
-    for (int l = 0; l < p.smoother_steps; ++l) {
-        k_richardson<<<grid_for(dom->n, 256, 148 * 8), 256, 0, s>>>(dom->x, dom->rp, dom->n,
-                                                                    p.richardson_omega);
-        update_prec_residual(dom, dom->x, dom->b, dom->rp);
-    }
+    for (int l = 0; l < p.smoother_steps; ++l)
+        enqueue_fixed_point_step(dom, p.fixed_point_type, p.richardson_omega);
     // The residual problem's source is already left preconditioned.
     enqueue_mc(dom, dom->rp, delta_dev, 0, 0, nullptr, nullptr, nullptr, nullptr);
     cudaError_t e = cudaStreamSynchronize(s);

@@ -51,6 +51,26 @@ def tridiag_test(n: int = 10, diag: float = 1.0, off: float = -0.14):
     return A
 
 
+def fixed_point_test(n: int = 10):
+    """System of tpetra/test/tstTpetraFixedPointSolverManager.cpp:89-116:
+    interior rows 0.14 / 1 / 0.14; the first row holds 0.14, 0.14, 1 at
+    columns 0, 1, 2 and the last row 0.14, 0.14, 1 at n-3, n-2, n-1."""
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        if i == 0:
+            cs, vs = [0, 1, 2], [0.14, 0.14, 1.0]
+        elif i == n - 1:
+            cs, vs = [n - 3, n - 2, n - 1], [0.14, 0.14, 1.0]
+        else:
+            cs, vs = [i - 1, i, i + 1], [0.14, 1.0, 0.14]
+        rows += [i] * 3
+        cols += cs
+        vals += vs
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    A.sort_indices()
+    return A
+
+
 def poisson2d(nx: int, ny: int | None = None):
     """5-point Laplacian, A_ii = 4/h^2, A_ij = -1/h^2, h = 1/(nx+1)."""
     ny = nx if ny is None else ny

@@ -672,6 +672,159 @@ int64_t orc_mc_solve(orc_mc* mc, const double* rhs, double* x, int internal,
     return nh_total;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The linear problem's operators (src/MCLS_LinearProblem_impl.hpp) over the
+// oracle's CSR matrices; transposes are formed when first needed.
+struct Problem {
+    const Csr& A;
+    const Csr* PL;
+    const Csr* PR;
+    const double* b;
+    int64_t n;
+    std::vector<double> tmp, tmp2;
+    Csr AT, PLT, PRT;
+    bool have_t = false;
+    Problem(const Csr& A_, const Csr* PL_, const Csr* PR_, const double* b_)
+        : A(A_), PL(PL_), PR(PR_), b(b_), n(A_.n), tmp(A_.n), tmp2(A_.n) {}
+    // LinearProblem::updatePrecResidual (:410-442): rp = PL (b - A PR x)
+    void prec_residual(const std::vector<double>& x, std::vector<double>& rp) {
+        if (PR) {
+            spmv(*PR, x.data(), tmp.data());
+            spmv(A, tmp.data(), rp.data());
+        } else {
+            spmv(A, x.data(), rp.data());
+        }
+        for (int64_t i = 0; i < n; ++i) rp[i] = -rp[i] + b[i];
+        if (PL) {
+            tmp = rp;
+            spmv(*PL, tmp.data(), rp.data());
+        }
+    }
+    // LinearProblem::apply (:251-279): y = PL A PR x
+    void apply(const std::vector<double>& x, std::vector<double>& y) {
+        const double* t = x.data();
+        if (PR) {
+            spmv(*PR, x.data(), tmp2.data());
+            t = tmp2.data();
+        }
+        if (PL) {
+            spmv(A, t, tmp.data());
+            spmv(*PL, tmp.data(), y.data());
+        } else {
+            spmv(A, t, y.data());
+        }
+    }
+    // LinearProblem::applyTranspose (:286-315): y = PR^T A^T PL^T x
+    void apply_transpose(const std::vector<double>& x, std::vector<double>& y) {
+        if (!have_t) {
+            AT = transpose(A);
+            if (PL) PLT = transpose(*PL);
+            if (PR) PRT = transpose(*PR);
+            have_t = true;
+        }
+        const double* t = x.data();
+        if (PL) {
+            spmv(PLT, x.data(), tmp.data());
+            t = tmp.data();
+        }
+        if (PR) {
+            spmv(AT, t, tmp2.data());
+            spmv(PRT, tmp2.data(), y.data());
+        } else {
+            spmv(AT, t, y.data());
+        }
+    }
+};
+
+double dot(const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) s = s + a[i] * b[i];
+    return s;
+}
+
+// One fixed-point iteration on (x, rp) with p, v as work vectors.  A zero
+// denominator gives a step of 0 (the reference divides by it).
+void fixed_point_step(Problem& P, int type, double omega, std::vector<double>& x,
+                      std::vector<double>& rp, std::vector<double>& p, std::vector<double>& v) {
+    const int64_t n = P.n;
+    auto step = [&](double num, double den, const std::vector<double>& s) {
+        const double a = den != 0.0 ? num / den : 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] = x[i] + a * s[i];
+            rp[i] = rp[i] + (-a) * p[i];
+        }
+    };
+    switch (type) {
+        case 1:  // SteepestDescentIteration::doOneIteration (src/MCLS_SteepestDescentIteration_impl.hpp:114-136)
+            P.apply(rp, p);
+            step(dot(rp, rp), dot(p, rp), rp);
+            break;
+        case 2:  // MinimalResidualIteration::doOneIteration (src/MCLS_MinimalResidualIteration_impl.hpp:114-136)
+            P.apply(rp, p);
+            step(dot(p, rp), dot(p, p), rp);
+            break;
+        case 3:  // RNSDIteration::doOneIteration (src/MCLS_RNSDIteration_impl.hpp:118-142)
+            P.apply_transpose(rp, v);
+            P.apply(v, p);
+            step(dot(v, v), dot(p, p), v);
+            break;
+        default:  // RichardsonIteration::doOneIteration (src/MCLS_RichardsonIteration_impl.hpp:134-147)
+            for (int64_t i = 0; i < n; ++i) x[i] = x[i] + omega * rp[i];
+            P.prec_residual(x, rp);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_fixed_point_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
+                          const orc_mcsa_params* sp, const double* b, double* x, int* iters,
+                          double* achieved, int max_hist, double* res_hist) {
+    // FixedPointSolverManager::solve (src/MCLS_FixedPointSolverManager_impl.hpp:208-321)
+    const int64_t n = A->m.n;
+    Problem P(A->m, PL ? &PL->m : nullptr, PR ? &PR->m : nullptr, b);
+    auto norm_inf = [](const std::vector<double>& v) {
+        double m = 0.0;
+        for (double e : v) m = std::max(m, std::abs(e));
+        return m;
+    };
+    std::vector<double> xv(x, x + n), rp(n), p(n), v(n), bv(b, b + n);
+    double source_norm;
+    if (PL) {
+        std::vector<double> t(n);
+        spmv(PL->m, b, t.data());
+        source_norm = norm_inf(t);
+    } else {
+        source_norm = norm_inf(bv);
+    }
+    const double raw_source = source_norm;
+    if (std::abs(source_norm) < 10.0 * std::numeric_limits<double>::epsilon()) source_norm = 1.0;
+    const double criteria = sp->tolerance * source_norm;
+    P.prec_residual(xv, rp);
+    double rnorm = norm_inf(rp);
+    int it = 0;
+    bool go = true;
+    while (go) {
+        ++it;
+        fixed_point_step(P, sp->fixed_point_type, sp->richardson_omega, xv, rp, p, v);
+        rnorm = norm_inf(rp);
+        if (res_hist && it <= max_hist) res_hist[it - 1] = rnorm;
+        if (it % sp->check_freq == 0) go = (rnorm > criteria) && (it < sp->max_iters);
+    }
+    if (PR) {
+        spmv(PR->m, xv.data(), p.data());
+        xv = p;
+    }
+    std::copy(xv.begin(), xv.end(), x);
+    if (iters) *iters = it;
+    if (achieved) *achieved = raw_source > 0.0 ? rnorm / raw_source : rnorm;
+    return rnorm <= criteria ? 1 : 0;
+}
+
 int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
                    const orc_mc_params* mp, const orc_mcsa_params* sp,
                    const double* b, double* x, int* iters, double* achieved,
@@ -686,21 +839,10 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
         for (double e : v) s += e * e;
         return std::sqrt(s);
     };
-    std::vector<double> xv(x, x + n), rp(n), tmp(n), delta(n);
+    std::vector<double> xv(x, x + n), rp(n), tmp(n), delta(n), pw(n), vw(n);
+    Problem P(Am, PL ? &PL->m : nullptr, PR ? &PR->m : nullptr, b);
     // LinearProblem::updatePrecResidual (src/MCLS_LinearProblem_impl.hpp:410-442)
-    auto update_prec_residual = [&]() {
-        if (PR) {
-            spmv(PR->m, xv.data(), tmp.data());
-            spmv(Am, tmp.data(), rp.data());
-        } else {
-            spmv(Am, xv.data(), rp.data());
-        }
-        for (int64_t i = 0; i < n; ++i) rp[i] = -rp[i] + b[i];
-        if (PL) {
-            tmp = rp;
-            spmv(PL->m, tmp.data(), rp.data());
-        }
-    };
+    auto update_prec_residual = [&]() { P.prec_residual(xv, rp); };
     std::vector<double> bv(b, b + n);
     double source_norm;
     if (PL) {
@@ -719,11 +861,8 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
     bool go = true;
     while (go) {
         ++it;
-        for (int l = 0; l < sp->smoother_steps; ++l) {
-            // RichardsonIteration::doOneIteration (src/MCLS_RichardsonIteration_impl.hpp:134-147)
-            for (int64_t i = 0; i < n; ++i) xv[i] = xv[i] + sp->richardson_omega * rp[i];
-            update_prec_residual();
-        }
+        for (int l = 0; l < sp->smoother_steps; ++l)
+            fixed_point_step(P, sp->fixed_point_type, sp->richardson_omega, xv, rp, pw, vw);
         std::fill(delta.begin(), delta.end(), 0.0);
         if (orc_mc_solve(mc, rp.data(), delta.data(), 1, 0, nullptr, nullptr, nullptr, nullptr) < 0) {
             orc_mc_free(mc);

@@ -98,6 +98,8 @@ typedef struct {
     int check_freq;            /* "Iteration Check Frequency" (default 1)   */
     int smoother_steps;        /* "Smoother Steps" (default 1)              */
     double richardson_omega;   /* "Richardson Relaxation" (default 1.0)     */
+    int fixed_point_type;      /* "Fixed Point Type": 0 Richardson, 1 Steepest
+                                * Descent, 2 MINRES, 3 RNSD (default 0)     */
 } orc_mcsa_params;
 
 /* MCSASolverManager::solve restatement.  x is updated in place.  Writes the
@@ -108,6 +110,14 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
                    const orc_mc_params* mp, const orc_mcsa_params* sp,
                    const double* b, double* x, int* iters, double* achieved,
                    int max_hist, double* res_hist, int64_t* total_steps);
+
+/* FixedPointSolverManager::solve restatement: sp->fixed_point_type
+ * iterations alone until |rp|_inf <= tolerance |PL b|_inf (or max_iters).
+ * x is updated in place (x = PR x at the end).  res_hist gets |rp|_inf per
+ * iteration (up to max_hist).  Returns 1 if converged, 0 if not. */
+int orc_fixed_point_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
+                          const orc_mcsa_params* sp, const double* b, double* x,
+                          int* iters, double* achieved, int max_hist, double* res_hist);
 
 /* CPU baseline: independent histories on `threads` threads (one Xorshift per
  * thread, as one MPI rank per core with subdomain transport), adjoint

@@ -46,6 +46,7 @@ class MCSAParams(C.Structure):
         ("check_freq", C.c_int),
         ("smoother_steps", C.c_int),
         ("richardson_omega", C.c_double),
+        ("fixed_point_type", C.c_int),
     ]
 
 
@@ -104,6 +105,10 @@ def lib():
                                      f64p, f64p, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                      C.c_int, P, C.POINTER(C.c_int64)]
         L.orc_mcsa_solve.restype = C.c_int
+        L.orc_fixed_point_solve.argtypes = [P, P, P, C.POINTER(MCSAParams), f64p, f64p,
+                                            C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
+                                            P]
+        L.orc_fixed_point_solve.restype = C.c_int
         L.orc_bench_walks.argtypes = [P, f64p, C.c_int64, C.c_int, P, C.POINTER(C.c_double)]
         L.orc_bench_walks.restype = C.c_int64
         _LIB = L
@@ -290,9 +295,10 @@ class MC:
 
 def mcsa_solve(A: Csr, b, x0=None, PL=None, PR=None, mc: MCParams | None = None,
                tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
-               richardson_omega=1.0, **mckw):
+               richardson_omega=1.0, fixed_point_type=0, **mckw):
     mp = mc if mc is not None else mc_params(**mckw)
-    spp = MCSAParams(tolerance, max_iters, check_freq, smoother_steps, richardson_omega)
+    spp = MCSAParams(tolerance, max_iters, check_freq, smoother_steps, richardson_omega,
+                     fixed_point_type)
     b = np.ascontiguousarray(b, np.float64)
     x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
     iters = C.c_int(0)
@@ -306,3 +312,18 @@ def mcsa_solve(A: Csr, b, x0=None, PL=None, PR=None, mc: MCParams | None = None,
         raise RuntimeError("oracle MCSA failed")
     return dict(x=x, converged=bool(rc), iters=iters.value, achieved=ach.value,
                 residuals=hist[: iters.value], steps=steps.value)
+
+
+def fixed_point_solve(A: Csr, b, x0=None, PL=None, PR=None, tolerance=1.0, max_iters=1000,
+                      check_freq=1, richardson_omega=1.0, fixed_point_type=0):
+    """FixedPointSolverManager::solve restatement (no Monte Carlo)."""
+    spp = MCSAParams(tolerance, max_iters, check_freq, 1, richardson_omega, fixed_point_type)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+    iters = C.c_int(0)
+    ach = C.c_double(0.0)
+    hist = np.zeros(max_iters, np.float64)
+    rc = lib().orc_fixed_point_solve(A.h, _h(PL), _h(PR), C.byref(spp), b, x, C.byref(iters),
+                                     C.byref(ach), max_iters, hist.ctypes.data)
+    return dict(x=x, converged=bool(rc), iters=iters.value, achieved=ach.value,
+                residuals=hist[: iters.value])

@@ -7,7 +7,8 @@
 //                     without a device throws MCLS::Assertion.
 //   facade_test gpu   the solves, after the reference's manager tests
 //                     (tpetra/test/tstTpetraMCSASolverManager.cpp:72-355,
-//                     tpetra/test/tstTpetraMonteCarloSolverManager.cpp:73-197).
+//                     tpetra/test/tstTpetraMonteCarloSolverManager.cpp:73-197,
+//                     tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -104,7 +105,11 @@ static void cpu_checks() {
     EXPECT(v->get<double>("Convergence Tolerance") == 1.0);
     EXPECT(v->get<int>("Maximum Iterations") == 1000);
     EXPECT(v->get<std::string>("Fixed Point Type") == "Richardson");
-    for (const char* name : {"Adjoint Anderson", "Forward Anderson", "Fixed Point", "Bogus"}) {
+    auto fp = factory.create("Fixed Point", pl);
+    EXPECT(Teuchos::nonnull(fp));
+    EXPECT(fp->getValidParameters()->get<std::string>("Fixed Point Type") == "Richardson");
+    EXPECT(fp->getValidParameters()->get<double>("Richardson Relaxation") == 1.0);
+    for (const char* name : {"Adjoint Anderson", "Forward Anderson", "Bogus"}) {
         bool threw = false;
         try {
             factory.create(name, pl);
@@ -113,13 +118,19 @@ static void cpu_checks() {
         }
         EXPECT(threw);
     }
+    for (const char* type : {"Richardson", "Steepest Descent", "MINRES", "RNSD"}) {
+        auto ok = mcsa_params();
+        ok->set<std::string>("Fixed Point Type", type);
+        MCLS::MCSASolverManager<Vec, Mat> m(ok);
+        MCLS::FixedPointSolverManager<Vec, Mat> f(ok);
+    }
     bool threw = false;
     try {
         auto bad = mcsa_params();
-        bad->set<std::string>("Fixed Point Type", "MINRES");
+        bad->set<std::string>("Fixed Point Type", "Jacobi");
         MCLS::MCSASolverManager<Vec, Mat> m(bad);
-    } catch (const MCLS::Assertion&) {
-        threw = true;
+    } catch (const MCLS::Assertion& e) {
+        threw = std::string(e.what()).find("Iteration type not supported!") != std::string::npos;
     }
     EXPECT(threw);
     // Teuchos-strict typing.
@@ -269,6 +280,72 @@ static void gpu_checks() {
         sm.setProblem(lp);
         EXPECT(sm.solve());
         EXPECT(rel_err(*x, direct(*P2, *b)) < 1e-7);
+    }
+
+    // Fixed point, Richardson: exactly 15 iterations, the solution's sign
+    // follows the source, also with PL = PR = I
+    // (tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345).
+    {
+        auto F = Teuchos::rcp(new Mat);
+        F->n = n;
+        F->rowptr.assign(1, 0);
+        for (int i = 0; i < n; ++i) {
+            const int c0 = i == 0 ? 0 : (i == n - 1 ? n - 3 : i - 1);
+            const double v[3] = {0.14, i == 0 || i == n - 1 ? 0.14 : 1.0,
+                                 i == 0 || i == n - 1 ? 1.0 : 0.14};
+            for (int k = 0; k < 3; ++k) {
+                F->colind.push_back(c0 + k);
+                F->values.push_back(v[k]);
+            }
+            F->rowptr.push_back(std::int64_t(F->colind.size()));
+        }
+        auto I = Teuchos::rcp(new Mat);
+        I->n = n;
+        I->rowptr.assign(1, 0);
+        for (int i = 0; i < n; ++i) {
+            I->colind.push_back(i);
+            I->values.push_back(1.0);
+            I->rowptr.push_back(i + 1);
+        }
+        for (int prec = 0; prec < 2; ++prec) {
+            auto x = Teuchos::rcp(new Vec(n, 0.0));
+            auto b = Teuchos::rcp(new Vec(n, -1.0));
+            auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(F, x, b));
+            if (prec) {
+                lp->setLeftPrec(I);
+                lp->setRightPrec(I);
+            }
+            auto pl = Teuchos::parameterList();
+            pl->set<int>("Iteration Print Frequency", 1);
+            pl->set<double>("Convergence Tolerance", 1.0e-8);
+            pl->set<int>("Maximum Iterations", 100);
+            pl->set<double>("Richardson Relaxation", 1.0);
+            pl->set<bool>("Print Iterations", false);
+            MCLS::FixedPointSolverManager<Vec, Mat> sm(lp, pl);
+            for (double r : {-1.0, 2.0, 2.0, -2.0}) {
+                g_section = std::string("fixed point, b = ") + std::to_string(r);
+                std::fill(b->begin(), b->end(), r);
+                std::fill(x->begin(), x->end(), 0.0);
+                lp->setLHS(x);
+                sm.setProblem(lp);
+                EXPECT(sm.solve() && sm.getConvergedStatus());
+                EXPECT(sm.getNumIters() == 15);
+                EXPECT(sm.achievedTol() > 0.0);
+                for (double xi : *x) EXPECT(r < 0 ? xi < 0.0 : xi > 0.0);
+            }
+        }
+        // MCSA with a MINRES smoother through the factory.
+        g_section = "MCSA with MINRES smoother";
+        auto x = Teuchos::rcp(new Vec(n, 0.0));
+        auto b = Teuchos::rcp(new Vec(n, -1.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+        auto pl = mcsa_params();
+        pl->set<std::string>("Fixed Point Type", "MINRES");
+        MCLS::SolverFactory<Vec, Mat> factory;
+        auto sm = factory.create("Adjoint MCSA", pl);
+        sm->setProblem(lp);
+        EXPECT(sm->solve() && sm->getNumIters() < 20);
+        EXPECT(rel_err(*x, direct(*A, *b)) < 1e-7);
     }
 
     // Direct Monte Carlo: signs follow the source, sample ratio 10

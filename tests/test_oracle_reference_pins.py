@@ -8,7 +8,9 @@
   tpetra/test/tstTpetraDomainTransporter.cpp:97-172 (Cutoff),
   tpetra/test/tstTpetraAdjointTally.cpp:83-167 (normalize),
   tpetra/test/tstTpetraUniformAdjointSource.cpp:75-161 (counts, weight),
-  tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations).
+  tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations),
+  tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345 (Richardson: 15
+  iterations, solution sign).
 """
 import json
 import os
@@ -150,6 +152,38 @@ def test_mcsa_forward_tridiagonal(b):
     r = O.mcsa_solve(A, np.full(10, b), tolerance=1e-8, max_iters=20, seed=3, direction=1)
     assert r["converged"] and r["iters"] < 20
     assert np.all(np.sign(r["x"]) == np.sign(b))
+
+
+@pytest.mark.parametrize("b", [-1.0, 2.0, -2.0])
+@pytest.mark.parametrize("prec", [False, True])
+def test_fixed_point_richardson_known_answer(b, prec):
+    # tstTpetraFixedPointSolverManager one_by_one and one_by_one_prec
+    # (PL = PR = I): Richardson, tolerance 1e-8, exactly 15 iterations.
+    A = O.Csr.from_scipy(P.fixed_point_test(10))
+    I = O.Csr.from_scipy(sp.identity(10, format="csr")) if prec else None
+    r = O.fixed_point_solve(A, np.full(10, b), PL=I, PR=I, tolerance=1e-8, max_iters=100)
+    assert r["converged"] and r["iters"] == 15 and r["achieved"] > 0
+    assert np.all(np.sign(r["x"]) == np.sign(b))
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3])
+def test_fixed_point_iterations_minimise_their_residuals(kind):
+    # Steepest descent and MINRES take the step that makes the new residual
+    # orthogonal to r (SD) or to A r (MINRES); RNSD to A A^T r.  One step
+    # from x = 0 on a nonsymmetric system checks each against its
+    # Petrov-Galerkin condition.
+    rng = np.random.default_rng(kind)
+    n = 12
+    M = sp.random(n, n, density=0.3, random_state=3) + sp.identity(n) * 4.0
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    b = rng.standard_normal(n)
+    r = O.fixed_point_solve(O.Csr.from_scipy(M), b, tolerance=0.0, max_iters=1,
+                            fixed_point_type=kind)
+    r1 = b - M @ r["x"]
+    Md = M.toarray()
+    w = {1: b, 2: Md @ b, 3: Md @ (Md.T @ b)}[kind]
+    assert abs(w @ r1) <= 1e-12 * np.linalg.norm(w) * np.linalg.norm(b)
 
 
 def test_monte_carlo_solve_sign():
