@@ -351,6 +351,34 @@ inline mclsgpu_mcsa_params fixedPointParams(const Teuchos::ParameterList& pl) {
     return p;
 }
 
+// AndersonSolverManager keys (src/MCLS_AndersonSolverManager_impl.hpp:
+// 232-247) and NOX's "Anderson Parameters" sublist.
+inline mclsgpu_anderson_params andersonParams(const Teuchos::ParameterList& pl) {
+    mclsgpu_anderson_params p{};
+    p.size = sizeof(p);
+    p.tolerance = numeric(pl, "Convergence Tolerance", 1.0e-8);
+    p.max_iters = int(numeric(pl, "Maximum Iterations", 1000.0));
+    p.smoother_steps = int(numeric(pl, "Smoother Steps", 1.0));
+    p.storage_depth = 2;
+    p.mixing = 1.0;
+    p.start_iteration = 1;
+    p.adjust_condition = 0;
+    p.drop_tolerance = 1.0e-12;
+    if (pl.isSublist("Anderson Parameters")) {
+        const Teuchos::ParameterList& a = pl.sublist("Anderson Parameters");
+        p.storage_depth = int(numeric(a, "Storage Depth", 2.0));
+        p.mixing = numeric(a, "Mixing Parameter", 1.0);
+        p.start_iteration = int(numeric(a, "Acceleration Start Iteration", 1.0));
+        p.adjust_condition = flag(a, "Adjust Matrix for Condition Number", false) ? 1 : 0;
+        p.drop_tolerance = numeric(a, "Condition Number Drop Tolerance", 1.0e-12);
+    }
+    if (p.storage_depth < 0 || p.storage_depth > 16)
+        throw Assertion("Anderson Parameters: Storage Depth must be in 0..16");
+    if (p.start_iteration < 1)
+        throw Assertion("Anderson Parameters: Acceleration Start Iteration must be >= 1");
+    return p;
+}
+
 inline bool sameParams(const mclsgpu_mc_params& a, const mclsgpu_mc_params& b) {
     return a.direction == b.direction && a.estimator == b.estimator &&
            a.history_length == b.history_length && a.weight_cutoff == b.weight_cutoff &&

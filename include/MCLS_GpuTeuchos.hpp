@@ -128,6 +128,16 @@ class ParameterList {
         return get<std::string>(key, std::string(def));
     }
 
+    // Nested list `key`, created empty when absent (Teuchos::ParameterList::sublist).
+    ParameterList& sublist(const std::string& key) {
+        if (!isParameter(key)) set<ParameterList>(key, ParameterList(key));
+        return get<ParameterList>(key);
+    }
+    const ParameterList& sublist(const std::string& key) const {
+        return get<ParameterList>(key);
+    }
+    bool isSublist(const std::string& key) const { return isType<ParameterList>(key); }
+
     bool isParameter(const std::string& key) const { return entries_.count(key) != 0; }
     template <class T>
     bool isType(const std::string& key) const {

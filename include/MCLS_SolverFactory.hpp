@@ -1,16 +1,16 @@
 // MCLS_SolverFactory.hpp -- name -> solver manager
 // (src/MCLS_SolverFactory.hpp:61-95, src/MCLS_SolverFactory_impl.hpp:57-140).
 //
-// "Adjoint MC", "Forward MC", "Adjoint MCSA", "Forward MCSA" and "Fixed
-// Point" create the GPU managers.  "Adjoint Anderson" and "Forward Anderson"
-// are names the reference knows but this library does not provide; they
-// throw Assertion naming the solver, as unknown names do.
+// Every name the reference knows creates the GPU manager: "Adjoint MC",
+// "Forward MC", "Adjoint MCSA", "Forward MCSA", "Adjoint Anderson",
+// "Forward Anderson" and "Fixed Point".  Unknown names throw Assertion.
 #ifndef MCLS_SOLVERFACTORY_HPP
 #define MCLS_SOLVERFACTORY_HPP
 
 #include <map>
 #include <string>
 
+#include "MCLS_AndersonSolverManager.hpp"
 #include "MCLS_FixedPointSolverManager.hpp"
 #include "MCLS_MCSASolverManager.hpp"
 #include "MCLS_MonteCarloSolverManager.hpp"
@@ -39,8 +39,12 @@ class SolverFactory {
             return Teuchos::rcp(new MCSASolverManager<Vector, Matrix, ForwardTag>(solver_parameters));
         if (solver_name == "Fixed Point")
             return Teuchos::rcp(new FixedPointSolverManager<Vector, Matrix>(solver_parameters));
-        if (solver_name == "Adjoint Anderson" || solver_name == "Forward Anderson")
-            throw Assertion("Solver type \"" + solver_name + "\" is not provided by the GPU path");
+        if (solver_name == "Adjoint Anderson")
+            return Teuchos::rcp(
+                new AndersonSolverManager<Vector, Matrix, AdjointTag>(solver_parameters));
+        if (solver_name == "Forward Anderson")
+            return Teuchos::rcp(
+                new AndersonSolverManager<Vector, Matrix, ForwardTag>(solver_parameters));
         throw Assertion("Solver type not supported!");
     }
 };

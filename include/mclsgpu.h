@@ -378,6 +378,46 @@ int mclsgpu_fixed_point_solve_dev(mclsgpu_context* ctx, mclsgpu_operator* op,
                                   const mclsgpu_mcsa_params* params,
                                   mclsgpu_stats* stats);
 
+/* ---- Anderson-accelerated MCSA --------------------------------------------- */
+/* Replaces AndersonSolverManager::solve (src/MCLS_AndersonSolverManager_
+ * impl.hpp:186-284): NOX's "Anderson Accelerated Fixed-Point" solver on the
+ * MCSAModelEvaluator map (src/MCLS_MCSAModelEvaluator_impl.hpp:306-350)
+ *   F(x) = f + delta - x,  f = x smoothed by smoother_steps steps f += r,
+ *   r = PL (b - A f), delta = the Monte Carlo estimate of (I-H)^-1 r,
+ * accelerated as Walker & Ni (SIAM J. Numer. Anal. 49, 2011) state it:
+ *   x_{k+1} = x_k + beta F_k - (dX + beta dF) gamma,
+ *   gamma = argmin |F_k - dF gamma|_2 over the last storage_depth
+ *   differences, solved through a QR factorisation of dF that is updated in
+ *   place (modified Gram-Schmidt to add a column, Givens rotations to drop
+ *   the oldest; with adjust_condition, older columns are also dropped while
+ *   the reciprocal 1-norm condition number of R is below drop_tolerance).
+ * Stops when |PL (b - A x)|_2 < tolerance |b|_2 (MCSAStatusTest,
+ * src/MCLS_MCSAStatusTest_impl.hpp:65-110; checked on x0 too) or after
+ * max_iters steps.  NOX is not part of the reference tree; its parameter
+ * names are kept.  The whole loop runs on the device (a captured graph
+ * with a WHILE node).  The domain must have no right preconditioner (the
+ * model evaluator applies the left one only).  x is updated in place;
+ * stats->iterations = steps taken, achieved_tol = |rp|_2 / |b|_2. */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_anderson_params) */
+    int32_t max_iters;        /* "Maximum Iterations" (1000)                 */
+    double tolerance;         /* "Convergence Tolerance" (1e-8)              */
+    int32_t smoother_steps;   /* "Smoother Steps" (1)                        */
+    int32_t storage_depth;    /* "Anderson Parameters" sublist: "Storage
+                               * Depth" (2), 0..16                           */
+    double mixing;            /* "Mixing Parameter" (1.0)                    */
+    int32_t start_iteration;  /* "Acceleration Start Iteration" (1), >= 1    */
+    int32_t adjust_condition; /* "Adjust Matrix for Condition Number" (0)    */
+    double drop_tolerance;    /* "Condition Number Drop Tolerance" (1e-12)   */
+    int32_t host_loop;        /* 1: host-driven loop instead of the graph   */
+    int32_t reserved0;
+} mclsgpu_anderson_params;
+
+int mclsgpu_anderson_solve(mclsgpu_domain* dom, const double* b, double* x,
+                           const mclsgpu_anderson_params* params, mclsgpu_stats* stats);
+int mclsgpu_anderson_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
+                               const mclsgpu_anderson_params* params, mclsgpu_stats* stats);
+
 /* MCSA one iteration at a time, for drivers that combine the Monte Carlo
  * corrections of several sets (one set per GPU): the loop of
  * MCSASolverManager::solve with MultiSetLinearProblem::blockConstantVectorSum

@@ -64,6 +64,22 @@ class McsaParams(C.Structure):
     ]
 
 
+class AndersonParams(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("max_iters", C.c_int32),
+        ("tolerance", C.c_double),
+        ("smoother_steps", C.c_int32),
+        ("storage_depth", C.c_int32),
+        ("mixing", C.c_double),
+        ("start_iteration", C.c_int32),
+        ("adjust_condition", C.c_int32),
+        ("drop_tolerance", C.c_double),
+        ("host_loop", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
 class PrecondParams(C.Structure):
     _fields_ = [
         ("size", C.c_uint32),
@@ -143,7 +159,7 @@ EXPORTS = [
     "mclsgpu_batch_domain", "mclsgpu_batch_set_launch", "mclsgpu_batch_autotune",
     "mclsgpu_batch_mcsa_solve_dev", "mclsgpu_mcsa_begin", "mclsgpu_mcsa_correction",
     "mclsgpu_mcsa_apply", "mclsgpu_mcsa_finish", "mclsgpu_fixed_point_solve",
-    "mclsgpu_fixed_point_solve_dev",
+    "mclsgpu_fixed_point_solve_dev", "mclsgpu_anderson_solve", "mclsgpu_anderson_solve_dev",
 ]
 
 _LIB = None
@@ -207,6 +223,9 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_mcsa_correction.argtypes = [P, P]
     L.mclsgpu_mcsa_apply.argtypes = [P, P, d, C.POINTER(d)]
     L.mclsgpu_mcsa_finish.argtypes = [P, P, C.POINTER(Stats)]
+    L.mclsgpu_anderson_solve.argtypes = [P, P, P, C.POINTER(AndersonParams), C.POINTER(Stats)]
+    L.mclsgpu_anderson_solve_dev.argtypes = [P, P, P, C.POINTER(AndersonParams),
+                                             C.POINTER(Stats)]
     L.mclsgpu_fixed_point_solve.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
                                             C.POINTER(Stats)]
     L.mclsgpu_fixed_point_solve_dev.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
@@ -398,6 +417,23 @@ def mcsa_params(tolerance=1e-8, max_iters=1000, check_freq=1, smoother_steps=1,
     return p
 
 
+def anderson_params(tolerance=1e-8, max_iters=1000, smoother_steps=1, storage_depth=2,
+                    mixing=1.0, start_iteration=1, adjust_condition=0, drop_tolerance=1e-12,
+                    host_loop=0):
+    p = AndersonParams()
+    p.size = C.sizeof(AndersonParams)
+    p.tolerance = tolerance
+    p.max_iters = max_iters
+    p.smoother_steps = smoother_steps
+    p.storage_depth = storage_depth
+    p.mixing = mixing
+    p.start_iteration = start_iteration
+    p.adjust_condition = adjust_condition
+    p.drop_tolerance = drop_tolerance
+    p.host_loop = host_loop
+    return p
+
+
 def fixed_point_solve(ctx: Context, op: Operator, b, x0=None, left: Precond | None = None,
                       right: Precond | None = None, params: McsaParams | None = None, **kw):
     """FixedPointSolverManager::solve on the GPU: (x, stats).  Keywords as
@@ -508,6 +544,26 @@ class Domain:
         self.ctx.check(self.ctx.L.mclsgpu_mcsa_solve_dev(self.h, C.c_void_p(b_ptr),
                                                          C.c_void_p(x_ptr), C.byref(p),
                                                          C.byref(st)))
+        return st.as_dict()
+
+    def anderson_solve(self, b, x0=None, params: AndersonParams | None = None, **kw):
+        """Anderson-accelerated MCSA (AndersonSolverManager::solve)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+        p = params if params is not None else anderson_params(**kw)
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_solve(self.h, _ptr(b), _ptr(x), C.byref(p),
+                                                         C.byref(st)))
+        return x, st.as_dict()
+
+    def anderson_solve_dev(self, b_ptr, x_ptr, params: AndersonParams | None = None, **kw):
+        p = params if params is not None else anderson_params(**kw)
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_solve_dev(self.h, C.c_void_p(b_ptr),
+                                                             C.c_void_p(x_ptr), C.byref(p),
+                                                             C.byref(st)))
         return st.as_dict()
 
     def mcsa_begin(self, b_ptr, x0_ptr, params: McsaParams | None = None, **kw):

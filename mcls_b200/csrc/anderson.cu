@@ -1,0 +1,684 @@
+// anderson.cu -- Anderson-accelerated MCSA on the device.
+//
+// AndersonSolverManager (src/MCLS_AndersonSolverManager_impl.hpp:65-284)
+// hands the MCSAModelEvaluator fixed-point map
+// (src/MCLS_MCSAModelEvaluator_impl.hpp:306-350) to NOX's Anderson solver.
+// NOX is not part of the reference tree; the acceleration follows Walker &
+// Ni, "Anderson acceleration for fixed-point iterations", SIAM J. Numer.
+// Anal. 49 (2011): x_{k+1} = x_k + beta F_k - (dX + beta dF) gamma with
+// gamma the least-squares fit of F_k by the stored differences dF, solved
+// through a QR factorisation of dF that is updated as columns are added
+// (modified Gram-Schmidt) and dropped (Givens rotations).
+//
+// One step on the device, all inside a captured graph with a WHILE node:
+//   smoothing + residual (one fused pass), the Monte Carlo correction,
+//   F pass         F = f + delta - x, |F|^2; the last block plans the step
+//                  (drop the oldest column when the store is full)
+//   MGS passes     the rotations of the drop on Q, the new column
+//                  v = F - F_old and dX = x - x_old, then one pass per
+//                  stored column: v -= r q_{j-1}, r = <q_j, v> (or |v|^2)
+//   control        R's new diagonal; optional drops for the condition number
+//   RHS pass       q_new = v / |v|, post-add rotations, <F, q_j>; the last
+//                  block back-solves R gamma = Q^T F
+//   update pass    x = x + beta F - sum (gamma_j dX_j + beta (R gamma)_j q_j)
+//   residual       rp = PL (b - A x), |rp|_2 and the status test.
+// Q and dX hold storage_depth vectors each; dX is a ring indexed from the
+// device state, so the captured graph never changes.
+#include <cmath>
+#include <vector>
+
+#include "internal.h"
+
+namespace mclsgpu {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxDepth = 16;
+constexpr int kMaxRot = kMaxDepth * kMaxDepth;
+
+struct AaState {
+    int k;            // steps taken (NOX's iteration count)
+    int nstore;       // stored columns
+    int add;          // this step adds a column
+    int newcol;       // its index
+    int ok;           // the new column was kept (nonzero norm)
+    int nrot;         // Givens rotations waiting for the next Q pass
+    int dx_head;      // ring slot of the oldest dX column
+    int done;
+    int converged;
+    int max_iters;
+    int m;            // storage depth
+    int start;        // acceleration start iteration
+    int adjust;       // drop columns for the condition number
+    int pad;
+    double beta;
+    double droptol;
+    double crit;      // tolerance * |b|_2
+    double bnorm;
+    double rnorm;     // |PL (b - A x)|_2 at the current iterate
+    double fnorm2;    // |F|^2 of this step
+    double vnorm2;    // |v|^2 after Gram-Schmidt
+    double inv_rnn;   // 1 / R(new, new)
+    double R[kMaxDepth][kMaxDepth];
+    double rc[kMaxRot], rs[kMaxRot];
+    int ri[kMaxRot];
+    double gamma[kMaxDepth];
+    double rgamma[kMaxDepth];
+};
+
+struct Args {
+    int n;
+    const double* f;       // smoothed iterate
+    const double* delta;   // Monte Carlo correction
+    double* x;
+    double* F;
+    double* Fold;
+    double* xold;
+    double* V;
+    double* Q;             // [m][n]
+    double* DX;            // [m][n]
+    const double* rp;      // residual at the updated iterate
+    double* part;
+    unsigned int* ticket;
+    AaState* st;
+    double* hist;
+    int hist_cap;
+    int* status;
+    cudaGraphConditionalHandle handle;
+    int use_cond;
+};
+
+inline int grid_for(long long work, int cap) {
+    long long g = (work + kThreads - 1) / kThreads;
+    if (g < 1) g = 1;
+    return int(g > cap ? cap : g);
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kThreads / 32; ++w) t += sh[w];
+    return t;
+}
+
+// Publish this block's sum of `v`; true in the block that finishes last,
+// whose thread 0 then holds the grid total in *total (block order, fixed
+// for a fixed launch).
+__device__ __forceinline__ bool grid_sum(double v, const Args& a, double* total) {
+    __shared__ double sh[kThreads / 32];
+    __shared__ bool last;
+    const double t = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        a.part[blockIdx.x] = t;
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double u = 0.0;
+    for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) u += a.part[k];
+    const double s = block_sum(u, sh);
+    if (threadIdx.x == 0) {
+        *total = s;
+        *a.ticket = 0u;
+    }
+    return true;
+}
+
+// Drop the oldest column (one thread): rotations that restore R's triangle
+// after its first column is removed, recorded for the next Q pass.
+__device__ void qr_delete(AaState* st) {
+    const int N = st->nstore;
+    for (int i = 0; i + 1 < N; ++i) {
+        const double a = st->R[i][i + 1], b = st->R[i + 1][i + 1];
+        const double t = sqrt(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+        const double c = a / t, s = b / t;
+        st->R[i][i + 1] = t;
+        st->R[i + 1][i + 1] = 0.0;
+        for (int j = i + 2; j < N; ++j) {
+            const double u = __dadd_rn(__dmul_rn(c, st->R[i][j]), __dmul_rn(s, st->R[i + 1][j]));
+            st->R[i + 1][j] =
+                __dadd_rn(__dmul_rn(-s, st->R[i][j]), __dmul_rn(c, st->R[i + 1][j]));
+            st->R[i][j] = u;
+        }
+        const int r = st->nrot++;
+        st->ri[r] = i;
+        st->rc[r] = c;
+        st->rs[r] = s;
+    }
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j + 1 < N; ++j) st->R[i][j] = st->R[i][j + 1];
+    for (int i = 0; i < N; ++i) st->R[i][N - 1] = 0.0;
+    st->nstore = N - 1;
+    st->dx_head = (st->dx_head + 1) % st->m;
+}
+
+// Reciprocal 1-norm condition number of the stored R (one thread).
+__device__ double rcond(const AaState* st) {
+    const int N = st->nstore;
+    double Ri[kMaxDepth][kMaxDepth];
+    for (int j = 0; j < N; ++j)
+        for (int i = j; i >= 0; --i) {
+            double s = i == j ? 1.0 : 0.0;
+            for (int k = i + 1; k <= j; ++k) s = __dadd_rn(s, -__dmul_rn(st->R[i][k], Ri[k][j]));
+            Ri[i][j] = s / st->R[i][i];
+        }
+    double n1 = 0.0, ni = 0.0;
+    for (int j = 0; j < N; ++j) {
+        double x = 0.0, y = 0.0;
+        for (int i = 0; i <= j; ++i) {
+            x += fabs(st->R[i][j]);
+            y += fabs(Ri[i][j]);
+        }
+        n1 = fmax(n1, x);
+        ni = fmax(ni, y);
+    }
+    return 1.0 / (n1 * ni);
+}
+
+// Apply the recorded rotations to element i of the Q columns.
+__device__ __forceinline__ void rotate_q(const Args& a, const AaState* st, int nrot, int i) {
+    for (int r = 0; r < nrot; ++r) {
+        const int c0 = st->ri[r];
+        const double c = st->rc[r], s = st->rs[r];
+        double* qa = a.Q + size_t(c0) * a.n;
+        double* qb = qa + a.n;
+        const double u = qa[i], v = qb[i];
+        qa[i] = __dadd_rn(__dmul_rn(c, u), __dmul_rn(s, v));
+        qb[i] = __dadd_rn(__dmul_rn(-s, u), __dmul_rn(c, v));
+    }
+}
+
+__global__ void k_aa_init(AaState* st, int max_iters, int m, int start, int adjust, double beta,
+                          double droptol, double tol, const double* b_sumsq,
+                          const double* r_sumsq, int* status) {
+    AaState s;
+    memset(&s, 0, sizeof(s));
+    s.max_iters = max_iters;
+    s.m = m;
+    s.start = start;
+    s.adjust = adjust;
+    s.beta = beta;
+    s.droptol = droptol;
+    s.bnorm = sqrt(*b_sumsq);
+    s.crit = tol * s.bnorm;
+    s.rnorm = sqrt(*r_sumsq);
+    s.converged = s.rnorm < s.crit;
+    if (!isfinite(s.rnorm)) atomicOr(status, DEV_ERR_NONFINITE);
+    s.done = s.converged || !isfinite(s.rnorm);
+    *st = s;
+}
+
+// F = (f + delta) - x and |F|^2; the last block plans the step.
+__global__ void __launch_bounds__(kThreads) k_aa_F(Args a) {
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double F = __dadd_rn(__dadd_rn(a.f[i], a.delta[i]), -a.x[i]);
+        a.F[i] = F;
+        acc = fma(F, F, acc);
+    }
+    double total;
+    if (!grid_sum(acc, a, &total) || threadIdx.x != 0) return;
+    AaState* st = a.st;
+    st->fnorm2 = total;
+    st->nrot = 0;
+    st->add = 0;
+    st->ok = 0;
+    if (st->m > 0 && st->k >= st->start) {
+        if (st->k == st->start) {
+            st->nstore = 0;
+            st->dx_head = 0;
+        } else if (st->nstore == st->m) {
+            qr_delete(st);
+        }
+        st->add = 1;
+        st->newcol = st->nstore;
+    }
+}
+
+// Gram-Schmidt pass j of the new column (modified Gram-Schmidt: one stored
+// column per pass).  Pass 0 also applies the drop's rotations to Q and forms
+// v = F - F_old and the new dX = x - x_old.
+__global__ void __launch_bounds__(kThreads) k_aa_mgs(Args a, int j) {
+    AaState* st = a.st;
+    const int add = st->add, nc = st->newcol;
+    if (!add || j > nc) return;  // uniform over the grid
+    const int nrot = st->nrot;
+    const double r_prev = j > 0 ? st->R[j - 1][nc] : 0.0;
+    const double* qprev = j > 0 ? a.Q + size_t(j - 1) * a.n : nullptr;
+    const double* qj = j < nc ? a.Q + size_t(j) * a.n : nullptr;
+    double* dxn = a.DX + size_t((st->dx_head + nc) % st->m) * a.n;
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double v;
+        if (j == 0) {
+            if (nrot) rotate_q(a, st, nrot, i);
+            v = __dadd_rn(a.F[i], -a.Fold[i]);
+            dxn[i] = __dadd_rn(a.x[i], -a.xold[i]);
+        } else {
+            v = __dadd_rn(a.V[i], __dmul_rn(-r_prev, qprev[i]));
+        }
+        a.V[i] = v;
+        acc = qj ? fma(qj[i], v, acc) : fma(v, v, acc);
+    }
+    double total;
+    if (!grid_sum(acc, a, &total) || threadIdx.x != 0) return;
+    if (j < nc)
+        st->R[j][nc] = total;
+    else
+        st->vnorm2 = total;
+}
+
+// New diagonal entry of R, then the drops for the condition number.
+__global__ void k_aa_ctrl(AaState* st) {
+    st->nrot = 0;
+    st->ok = 0;
+    if (st->add) {
+        const int nc = st->newcol;
+        const double rn = sqrt(st->vnorm2);
+        if (rn > 0.0 && isfinite(rn)) {
+            st->R[nc][nc] = rn;
+            st->inv_rnn = 1.0 / rn;
+            st->nstore = nc + 1;
+            st->ok = 1;
+        } else {
+            for (int j = 0; j < nc; ++j) st->R[j][nc] = 0.0;
+        }
+    }
+    if (st->adjust)
+        while (st->nstore > 1 && rcond(st) < st->droptol) qr_delete(st);
+}
+
+// q_new = v / |v|, the post-add rotations, <F, q_j>; the last block solves
+// R gamma = Q^T F and forms beta R gamma.
+__global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
+    __shared__ double sh[kThreads / 32];
+    __shared__ bool last;
+    AaState* st = a.st;
+    const int N = st->nstore, ok = st->ok, nc = st->newcol, nrot = st->nrot;
+    const double inv = st->inv_rnn;
+    double acc[kMaxDepth];
+#pragma unroll
+    for (int j = 0; j < kMaxDepth; ++j) acc[j] = 0.0;
+    double* qn = a.Q + size_t(nc) * a.n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        if (ok) qn[i] = __dmul_rn(inv, a.V[i]);
+        if (nrot) rotate_q(a, st, nrot, i);
+        const double F = a.F[i];
+#pragma unroll
+        for (int j = 0; j < kMaxDepth; ++j)
+            if (j < N) acc[j] = fma(F, a.Q[size_t(j) * a.n + i], acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kMaxDepth; ++j) {
+        if (j < N) {  // N is the same in every thread of the block
+            const double t = block_sum(acc[j], sh);
+            if (threadIdx.x == 0) a.part[size_t(blockIdx.x) * kMaxDepth + j] = t;
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double rhs[kMaxDepth];
+    for (int j = 0; j < N; ++j) {
+        double u = 0.0;
+        for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x)
+            u += a.part[size_t(k) * kMaxDepth + j];
+        const double t = block_sum(u, sh);
+        if (threadIdx.x == 0) rhs[j] = t;
+    }
+    if (threadIdx.x != 0) return;
+    *a.ticket = 0u;
+    for (int j = N - 1; j >= 0; --j) {
+        double g = rhs[j];
+        for (int i = j + 1; i < N; ++i) g = __dadd_rn(g, -__dmul_rn(st->R[j][i], st->gamma[i]));
+        st->gamma[j] = g / st->R[j][j];
+    }
+    for (int i = 0; i < N; ++i) {
+        double s = 0.0;
+        for (int j = i; j < N; ++j) s = __dadd_rn(s, __dmul_rn(st->R[i][j], st->gamma[j]));
+        st->rgamma[i] = __dmul_rn(st->beta, s);
+    }
+    st->nrot = 0;
+}
+
+// x_{k+1} = x_k + beta F - sum_j (gamma_j dX_j + (beta R gamma)_j q_j);
+// x_old = x_k, F_old = F.
+__global__ void __launch_bounds__(kThreads) k_aa_update(Args a) {
+    const AaState* st = a.st;
+    const int N = st->nstore, head = st->dx_head, m = st->m;
+    const double beta = st->beta;
+    double g[kMaxDepth], rg[kMaxDepth];
+    const double* dx[kMaxDepth];
+#pragma unroll
+    for (int j = 0; j < kMaxDepth; ++j) {
+        g[j] = j < N ? st->gamma[j] : 0.0;
+        rg[j] = j < N ? st->rgamma[j] : 0.0;
+        dx[j] = j < N ? a.DX + size_t((head + j) % m) * a.n : nullptr;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double xi = a.x[i], F = a.F[i];
+        double w = __dmul_rn(beta, F);
+#pragma unroll
+        for (int j = 0; j < kMaxDepth; ++j)
+            if (j < N)
+                w = __dadd_rn(__dadd_rn(w, __dmul_rn(-g[j], dx[j][i])),
+                              __dmul_rn(-rg[j], a.Q[size_t(j) * a.n + i]));
+        a.xold[i] = xi;
+        a.Fold[i] = F;
+        a.x[i] = __dadd_rn(xi, w);
+    }
+}
+
+// |rp|_2 and the status tests (MCSAStatusTest, MaxIters, FiniteValue).
+__global__ void __launch_bounds__(kThreads) k_aa_check(Args a) {
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+        acc = fma(a.rp[i], a.rp[i], acc);
+    double total;
+    if (!grid_sum(acc, a, &total) || threadIdx.x != 0) return;
+    AaState* st = a.st;
+    st->k += 1;
+    st->rnorm = sqrt(total);
+    if (a.hist && st->k <= a.hist_cap) a.hist[st->k - 1] = st->rnorm;
+    st->converged = st->rnorm < st->crit;
+    if (!isfinite(st->rnorm) || !isfinite(st->fnorm2)) atomicOr(a.status, DEV_ERR_NONFINITE);
+    const int keep = !st->converged && st->k < st->max_iters && !*a.status;
+    st->done = !keep;
+    if (a.use_cond) cudaGraphSetConditional(a.handle, keep ? 1u : 0u);
+}
+
+__global__ void k_axpy1(double* x, const double* r, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[i] = __dadd_rn(x[i], r[i]);
+}
+
+int check_params(mclsgpu_context* ctx, const mclsgpu_anderson_params* p,
+                 mclsgpu_anderson_params* out) {
+    mclsgpu_anderson_params d{};
+    d.size = sizeof(d);
+    d.max_iters = 1000;
+    d.tolerance = 1.0e-8;
+    d.smoother_steps = 1;
+    d.storage_depth = 2;
+    d.mixing = 1.0;
+    d.start_iteration = 1;
+    d.drop_tolerance = 1.0e-12;
+    if (p) {
+        if (p->size < sizeof(mclsgpu_anderson_params))
+            return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "anderson params: size mismatch");
+        d = *p;
+    }
+    if (d.max_iters < 1 || d.smoother_steps < 0 || !(d.tolerance >= 0.0) ||
+        d.storage_depth < 0 || d.storage_depth > kMaxDepth || d.start_iteration < 1 ||
+        !std::isfinite(d.mixing))
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "anderson params out of range");
+    *out = d;
+    return MCLSGPU_OK;
+}
+
+}  // namespace
+
+struct AndersonWork {
+    int n = 0;
+    int m = 0;
+    int grid = 1;
+    double* F = nullptr;
+    double* Fold = nullptr;
+    double* xold = nullptr;
+    double* V = nullptr;
+    double* delta = nullptr;
+    double* Q = nullptr;
+    double* DX = nullptr;
+    double* part = nullptr;
+    unsigned int* ticket = nullptr;
+    AaState* st = nullptr;
+    AaState* h_st = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    long long graph_key = -1;
+    const double* graph_hist = nullptr;  // residual history the graph writes
+    int body_kernels = 0;
+    ~AndersonWork() {
+        dfree(F);
+        dfree(Fold);
+        dfree(xold);
+        dfree(V);
+        dfree(delta);
+        dfree(Q);
+        dfree(DX);
+        dfree(part);
+        dfree(ticket);
+        dfree(st);
+        if (h_st) cudaFreeHost(h_st);
+        if (graph) cudaGraphExecDestroy(graph);
+    }
+};
+
+void release_anderson(mclsgpu_domain* dom) {
+    delete dom->aa;
+    dom->aa = nullptr;
+}
+
+namespace {
+
+int ensure_work(mclsgpu_domain* dom, int m) {
+    mclsgpu_context* ctx = dom->ctx;
+    const int mm = m > 0 ? m : 1;
+    if (dom->aa && dom->aa->m >= mm) return MCLSGPU_OK;
+    release_anderson(dom);
+    AndersonWork* w = new AndersonWork;
+    w->n = dom->n;
+    w->m = mm;
+    w->grid = grid_for(dom->n, ctx->num_sms * 4);
+    const size_t n = size_t(dom->n);
+    cudaError_t e;
+    if ((e = dmalloc(&w->F, n)) != cudaSuccess || (e = dmalloc(&w->Fold, n)) != cudaSuccess ||
+        (e = dmalloc(&w->xold, n)) != cudaSuccess || (e = dmalloc(&w->V, n)) != cudaSuccess ||
+        (e = dmalloc(&w->delta, n)) != cudaSuccess || (e = dmalloc(&w->Q, n * mm)) != cudaSuccess ||
+        (e = dmalloc(&w->DX, n * mm)) != cudaSuccess ||
+        (e = dmalloc(&w->part, size_t(w->grid) * kMaxDepth)) != cudaSuccess ||
+        (e = dmalloc(&w->ticket, 1)) != cudaSuccess || (e = dmalloc(&w->st, 1)) != cudaSuccess ||
+        (e = cudaMallocHost(reinterpret_cast<void**>(&w->h_st), sizeof(AaState))) != cudaSuccess) {
+        delete w;
+        return cuda_fail(ctx, e, "cudaMalloc anderson work space");
+    }
+    cudaMemsetAsync(w->ticket, 0, sizeof(unsigned int), ctx->stream);
+    dom->aa = w;
+    return MCLSGPU_OK;
+}
+
+// One Anderson step and its status test (captured into the graph body).
+void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
+                  cudaGraphConditionalHandle h, int use_cond) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    AndersonWork* w = dom->aa;
+    const int n = dom->n;
+    // MCSAModelEvaluator::evalModelImpl: f = x; f += r; r = PL (b - A f).
+    const double* f = dom->x;
+    const double* r = dom->rp;
+    if (p->smoother_steps == 1) {
+        richardson_residual(dom, dom->x, dom->rp, 1.0, dom->x2, dom->rp2);
+        f = dom->x2;
+        r = dom->rp2;
+    } else if (p->smoother_steps > 1) {
+        cudaMemcpyAsync(dom->x2, dom->x, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(dom->rp2, dom->rp, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice,
+                        s);
+        for (int l = 0; l < p->smoother_steps; ++l) {
+            k_axpy1<<<w->grid, kThreads, 0, s>>>(dom->x2, dom->rp2, n);
+            prec_residual(dom, dom->x2, dom->b, dom->rp2);
+        }
+        f = dom->x2;
+        r = dom->rp2;
+    }
+    mc_correction(dom, r, w->delta);
+    Args a{};
+    a.n = n;
+    a.f = f;
+    a.delta = w->delta;
+    a.x = dom->x;
+    a.F = w->F;
+    a.Fold = w->Fold;
+    a.xold = w->xold;
+    a.V = w->V;
+    a.Q = w->Q;
+    a.DX = w->DX;
+    a.rp = dom->rp;
+    a.part = w->part;
+    a.ticket = w->ticket;
+    a.st = w->st;
+    a.hist = dom->d_resid;
+    a.hist_cap = dom->resid_cap;
+    a.status = ctx->d_status;
+    a.handle = h;
+    a.use_cond = use_cond;
+    k_aa_F<<<w->grid, kThreads, 0, s>>>(a);
+    if (p->storage_depth > 0) {
+        for (int j = 0; j < p->storage_depth; ++j) k_aa_mgs<<<w->grid, kThreads, 0, s>>>(a, j);
+        k_aa_ctrl<<<1, 1, 0, s>>>(w->st);
+        k_aa_rhs<<<w->grid, kThreads, 0, s>>>(a);
+    }
+    k_aa_update<<<w->grid, kThreads, 0, s>>>(a);
+    prec_residual(dom, dom->x, dom->b, dom->rp);
+    k_aa_check<<<w->grid, kThreads, 0, s>>>(a);
+}
+
+int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
+                   const mclsgpu_anderson_params* p, mclsgpu_stats* stats) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    if (dom->right)
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
+                         "the Anderson solver applies the left preconditioner only");
+    int rc = ensure_work(dom, p->storage_depth);
+    if (rc) return rc;
+    AndersonWork* w = dom->aa;
+    if (p->max_iters > dom->resid_cap) {
+        dfree(dom->d_resid);
+        cudaError_t e = dmalloc(&dom->d_resid, size_t(p->max_iters));
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+        dom->resid_cap = p->max_iters;
+        // The captured MCSA graph holds the old history pointer.
+        if (dom->graph) cudaGraphExecDestroy(dom->graph);
+        dom->graph = nullptr;
+    }
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    cudaMemsetAsync(w->ticket, 0, sizeof(unsigned int), s);
+    mcsa_reset_counters(dom);
+    const long long key = (long long)p->smoother_steps * 64 + p->storage_depth;
+    if (!p->host_loop && (!w->graph || w->graph_key != key || w->graph_hist != dom->d_resid)) {
+        if (w->graph) cudaGraphExecDestroy(w->graph);
+        w->graph = nullptr;
+        rc = build_while_graph(
+            ctx, [&](cudaGraphConditionalHandle h) { enqueue_step(dom, p, h, 1); }, &w->graph,
+            &w->body_kernels);
+        if (rc) return rc;
+        w->graph_key = key;
+        w->graph_hist = dom->d_resid;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    if (b_dev != dom->b)
+        cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (x_dev != dom->x)
+        cudaMemcpyAsync(dom->x, x_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    // |b|_2 (MCSAStatusTest uses the unpreconditioned right-hand side) and
+    // the residual of the initial guess, tested before the first step.
+    sum_sq(s, dom->b, n, dom->part, dom->d_scalars + 6);
+    prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    k_aa_init<<<1, 1, 0, s>>>(w->st, p->max_iters, p->storage_depth, p->start_iteration,
+                              p->adjust_condition, p->mixing, p->drop_tolerance, p->tolerance,
+                              dom->d_scalars + 6, dom->d_scalars + 5, ctx->d_status);
+    cudaMemcpyAsync(w->h_st, w->st, sizeof(AaState), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && !w->h_st->done) {
+        if (!p->host_loop) {
+            e = cudaGraphLaunch(w->graph, s);
+        } else {
+            for (int it = 0; it < p->max_iters && e == cudaSuccess; ++it) {
+                enqueue_step(dom, p, cudaGraphConditionalHandle(0), 0);
+                cudaMemcpyAsync(w->h_st, w->st, sizeof(AaState), cudaMemcpyDeviceToHost, s);
+                e = cudaStreamSynchronize(s);
+                if (e == cudaSuccess && w->h_st->done) break;
+            }
+        }
+    }
+    if (e == cudaSuccess) {
+        if (x_dev != dom->x)
+            cudaMemcpyAsync(x_dev, dom->x, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaEventRecord(e1, s);
+        cudaMemcpyAsync(w->h_st, w->st, sizeof(AaState), cudaMemcpyDeviceToHost, s);
+        e = cudaStreamSynchronize(s);
+    }
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "anderson solve");
+    if ((rc = check_device_status(ctx))) return rc;
+    if (stats) {
+        const AaState& st = *w->h_st;
+        if ((rc = mcsa_read_stats(dom, stats))) return rc;
+        stats->iterations = st.k;
+        stats->converged = st.converged;
+        stats->residual_norm = st.rnorm;
+        stats->achieved_tol = st.bnorm > 0.0 ? st.rnorm / st.bnorm : st.rnorm;
+        stats->solve_ms = ms;
+        stats->fallback_taken = dom->left ? dom->left->fallback : 0;
+        stats->rho = dom->left ? dom->left->rho : -1.0;
+        stats->kernel_launches = int64_t(w->body_kernels) * st.k + 4;
+    }
+    return MCLSGPU_OK;
+}
+
+}  // namespace
+}  // namespace mclsgpu
+
+using namespace mclsgpu;
+
+extern "C" {
+
+int mclsgpu_anderson_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
+                               const mclsgpu_anderson_params* params, mclsgpu_stats* stats) {
+    if (!dom || !b_dev || !x_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_anderson_params p;
+    int rc = check_params(dom->ctx, params, &p);
+    if (rc) return rc;
+    cudaSetDevice(dom->ctx->device);
+    return anderson_solve(dom, b_dev, x_dev, &p, stats);
+}
+
+int mclsgpu_anderson_solve(mclsgpu_domain* dom, const double* b, double* x,
+                           const mclsgpu_anderson_params* params, mclsgpu_stats* stats) {
+    if (!dom || !b || !x) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = dom->ctx;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = size_t(dom->n) * sizeof(double);
+    // The domain's own vectors hold b and x for the solve.
+    cudaMemcpyAsync(dom->b, b, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(dom->x, x, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    int rc = mclsgpu_anderson_solve_dev(dom, dom->b, dom->x, params, stats);
+    if (!rc) {
+        cudaMemcpyAsync(x, dom->x, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "copy x");
+    }
+    return rc;
+}
+
+}  // extern "C"

@@ -123,6 +123,7 @@ int copy_csr_out(mclsgpu_context* ctx, const DevCsr& A, int64_t* nnz_out, int64_
 }
 
 void release_domain(mclsgpu_domain* d) {
+    release_anderson(d);
     d->D.release();
     d->DS.release();
     d->DT.release();

@@ -93,6 +93,8 @@ struct mclsgpu_precond {
 
 namespace mclsgpu {
 
+struct AndersonWork;
+
 struct McsaState {
     int iter;            // iterations completed
     int done;            // 1 once the loop must stop
@@ -176,6 +178,8 @@ struct mclsgpu_domain {
     // Step-wise MCSA (mclsgpu_mcsa_begin .. _finish).
     mclsgpu_mcsa_params step_p{};
     int step_ready = 0;
+    // Anderson-accelerated MCSA work space (anderson.cu), built on first use.
+    mclsgpu::AndersonWork* aa = nullptr;
 };
 
 namespace mclsgpu {
@@ -235,6 +239,19 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
 void prec_residual(mclsgpu_domain* dom, const double* x, const double* b, double* rp_out);
 // y = PL A PR x   (LinearProblem::apply); uses dom->tmp and dom->tmp2.
 void composite_apply(mclsgpu_domain* dom, const double* x, double* y);
+// x2 = x + w r; r2 = PL (b - A PR x2): one fused pass when PL is I, point
+// Jacobi or held on A's diagonals and there is no PR (x2 != x, r2 != r).
+void richardson_residual(mclsgpu_domain* dom, const double* x, const double* r, double w,
+                         double* x2, double* r2);
+// out = the Monte Carlo estimate for the source v (already left
+// preconditioned): one MC solve, advancing the domain's random stream.
+void mc_correction(mclsgpu_domain* dom, const double* v, double* out);
+// Walk statistics since the last reset (steps, histories, walk time).
+int mcsa_read_stats(mclsgpu_domain* dom, mclsgpu_stats* st);
+void mcsa_reset_counters(mclsgpu_domain* dom);
+
+// ---- Anderson-accelerated MCSA (anderson.cu) ------------------------------------
+void release_anderson(mclsgpu_domain* dom);
 
 // ---- fixed-point iterations (fixedpoint.cu) ------------------------------------
 // Transposes the RNSD iteration needs (set-up: never inside a stream capture).

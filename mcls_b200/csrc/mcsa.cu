@@ -592,6 +592,19 @@ static int mc_solve_device(mclsgpu_domain* dom, const double* rhs_dev, double* x
     return MCLSGPU_OK;
 }
 
+// x2 = x + w r (rounded as the reference's vector update)
+__global__ void k_axpy_to(const double* x, const double* r, double w, double* x2, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x2[i] = __dadd_rn(x[i], __dmul_rn(w, r[i]));
+}
+
+int mcsa_read_stats(mclsgpu_domain* dom, mclsgpu_stats* st) { return read_stats(dom, st); }
+void mcsa_reset_counters(mclsgpu_domain* dom) { reset_counters(dom); }
+
+void mc_correction(mclsgpu_domain* dom, const double* v, double* out) {
+    enqueue_mc(dom, v, out, 0, 0, nullptr, nullptr, nullptr, nullptr);
+}
+
 // The fused iteration covers one smoothing step, no right preconditioner and
 // a left preconditioner that is the identity or point Jacobi.
 static bool fused_iteration(const mclsgpu_domain* dom, const mclsgpu_mcsa_params* mp) {
@@ -605,6 +618,25 @@ static bool fused_iteration(const mclsgpu_domain* dom, const mclsgpu_mcsa_params
 // and k_residual_norm go to dom->part, sized for that many blocks.
 static int fused_grid(const mclsgpu_domain* dom) {
     return grid_for(dom->n, kFusedThreads, dom->ctx->num_sms * 8);
+}
+
+void richardson_residual(mclsgpu_domain* dom, const double* x, const double* r, double w,
+                         double* x2, double* r2) {
+    cudaStream_t s = dom->ctx->stream;
+    const mclsgpu_operator* op = dom->op;
+    const int grid = fused_grid(dom);
+    const mclsgpu_precond* L = dom->left;
+    if (!dom->right && (!L || L->kind == MCLSGPU_PREC_POINT_JACOBI)) {
+        MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_richardson_residual, dom->b,
+                          L ? L->diag : nullptr, x, r, w, x2, r2);
+    } else if (!dom->right && L->mdia && op->dia_k > 0) {
+        MCLSGPU_LAUNCH_OP(op, grid, kFusedThreads, s, k_richardson_residual, dom->b, nullptr, x,
+                          r, w, x2, dom->tmp);
+        MCLSGPU_LAUNCH_M(op, L->mdia, grid, kFusedThreads, s, k_dia_apply, dom->tmp, r2);
+    } else {
+        k_axpy_to<<<grid, kFusedThreads, 0, s>>>(x, r, w, x2, dom->n);
+        update_prec_residual(dom, x2, dom->b, r2);
+    }
 }
 
 // One MCSA iteration including its convergence check.  The fused form is

@@ -777,9 +777,226 @@ void fixed_point_step(Problem& P, int type, double omega, std::vector<double>& x
     }
 }
 
+// Anderson acceleration (Walker & Ni 2011, NOX's "Anderson Accelerated
+// Fixed-Point" solver): the least-squares problem min |F_k - dF gamma| is
+// solved through a QR factorisation of dF that is updated as columns come
+// and go.  Columns are kept oldest first.
+struct Anderson {
+    int m, start, adjust;
+    double beta, droptol;
+    int64_t n;
+    int nstore = 0;
+    std::vector<std::vector<double>> Q, DX;
+    std::vector<std::vector<double>> R;
+    std::vector<double> Fold, xold;
+    Anderson(const orc_anderson_params& p, int64_t n_)
+        : m(p.storage_depth), start(p.start_iteration), adjust(p.adjust_condition),
+          beta(p.mixing), droptol(p.drop_tolerance), n(n_),
+          R(size_t(std::max(m, 1)), std::vector<double>(size_t(std::max(m, 1)), 0.0)) {}
+    // Drop the oldest column: Givens rotations restore R's triangle after
+    // its first column is removed; Q takes the same rotations.
+    void qr_delete() {
+        for (int i = 0; i + 1 < nstore; ++i) {
+            const double a = R[i][i + 1], bb = R[i + 1][i + 1];
+            const double t = std::sqrt(a * a + bb * bb);
+            const double c = a / t, s = bb / t;
+            R[i][i + 1] = t;
+            R[i + 1][i + 1] = 0.0;
+            for (int j = i + 2; j < nstore; ++j) {
+                const double u = c * R[i][j] + s * R[i + 1][j];
+                R[i + 1][j] = (-s) * R[i][j] + c * R[i + 1][j];
+                R[i][j] = u;
+            }
+            for (int64_t e = 0; e < n; ++e) {
+                const double qa = Q[i][e], qb = Q[i + 1][e];
+                Q[i][e] = c * qa + s * qb;
+                Q[i + 1][e] = (-s) * qa + c * qb;
+            }
+        }
+        for (int i = 0; i < nstore; ++i)
+            for (int j = 0; j + 1 < nstore; ++j) R[i][j] = R[i][j + 1];
+        for (int i = 0; i < nstore; ++i) R[i][nstore - 1] = 0.0;
+        Q.pop_back();
+        DX.erase(DX.begin());
+        --nstore;
+    }
+    // Modified Gram-Schmidt of the new column against Q; false (and no
+    // column) when what is left of it has zero or non-finite norm.
+    bool qr_add(std::vector<double> v) {
+        const int N = nstore;
+        for (int j = 0; j < N; ++j) {
+            double r = 0.0;
+            for (int64_t e = 0; e < n; ++e) r = r + Q[j][e] * v[e];
+            R[j][N] = r;
+            for (int64_t e = 0; e < n; ++e) v[e] = v[e] + (-r) * Q[j][e];
+        }
+        double vv = 0.0;
+        for (int64_t e = 0; e < n; ++e) vv = vv + v[e] * v[e];
+        const double rn = std::sqrt(vv);
+        if (!(rn > 0.0) || !std::isfinite(rn)) {
+            for (int j = 0; j < N; ++j) R[j][N] = 0.0;
+            return false;
+        }
+        R[N][N] = rn;
+        const double inv = 1.0 / rn;
+        for (int64_t e = 0; e < n; ++e) v[e] = inv * v[e];
+        Q.push_back(std::move(v));
+        ++nstore;
+        return true;
+    }
+    // Reciprocal 1-norm condition number of the leading nstore x nstore R.
+    double rcond() const {
+        const int N = nstore;
+        std::vector<std::vector<double>> Ri(size_t(N), std::vector<double>(size_t(N), 0.0));
+        for (int j = 0; j < N; ++j) {
+            // column j of R^-1 by back substitution of e_j
+            for (int i = j; i >= 0; --i) {
+                double s = i == j ? 1.0 : 0.0;
+                for (int k = i + 1; k <= j; ++k) s = s - R[i][k] * Ri[k][j];
+                Ri[i][j] = s / R[i][i];
+            }
+        }
+        double n1 = 0.0, ni = 0.0;
+        for (int j = 0; j < N; ++j) {
+            double a = 0.0, c = 0.0;
+            for (int i = 0; i <= j; ++i) {
+                a = a + std::abs(R[i][j]);
+                c = c + std::abs(Ri[i][j]);
+            }
+            n1 = std::max(n1, a);
+            ni = std::max(ni, c);
+        }
+        return 1.0 / (n1 * ni);
+    }
+    // One step from x_k with F_k = g(x_k) - x_k (k = steps taken so far).
+    void step(int k, std::vector<double>& x, const std::vector<double>& F) {
+        if (m > 0 && k >= start) {
+            if (k == start) {
+                nstore = 0;
+                Q.clear();
+                DX.clear();
+            } else if (nstore == m) {
+                qr_delete();
+            }
+            std::vector<double> v(static_cast<size_t>(n)), dx(static_cast<size_t>(n));
+            for (int64_t e = 0; e < n; ++e) {
+                v[e] = F[e] - Fold[e];
+                dx[e] = x[e] - xold[e];
+            }
+            if (qr_add(std::move(v))) DX.push_back(std::move(dx));
+            if (adjust)
+                while (nstore > 1 && rcond() < droptol) qr_delete();
+        }
+        const int N = nstore;
+        std::vector<double> gamma(static_cast<size_t>(N)), rg(static_cast<size_t>(N));
+        for (int j = N - 1; j >= 0; --j) {
+            double rhs = 0.0;
+            for (int64_t e = 0; e < n; ++e) rhs = rhs + F[e] * Q[j][e];
+            double g = rhs;
+            for (int i = j + 1; i < N; ++i) g = g - R[j][i] * gamma[i];
+            gamma[j] = g / R[j][j];
+        }
+        for (int i = 0; i < N; ++i) {
+            double s = 0.0;
+            for (int j = i; j < N; ++j) s = s + R[i][j] * gamma[j];
+            rg[i] = beta * s;
+        }
+        Fold = F;
+        xold = x;
+        for (int64_t e = 0; e < n; ++e) {
+            double w = beta * F[e];
+            for (int j = 0; j < N; ++j) w = (w + (-gamma[j]) * DX[j][e]) + (-rg[j]) * Q[j][e];
+            x[e] = x[e] + w;
+        }
+    }
+};
+
 }  // namespace
 
 extern "C" {
+
+int orc_anderson_solve(const orc_csr* A, const orc_csr* PL, const orc_mc_params* mp,
+                       const orc_anderson_params* ap, const double* b, double* x, int* iters,
+                       double* achieved, int max_hist, double* res_hist, int64_t* total_steps) {
+    // AndersonSolverManager::solve (src/MCLS_AndersonSolverManager_impl.hpp:186-224) with
+    // MCSAStatusTest (src/MCLS_MCSAStatusTest_impl.hpp:65-110): converged when
+    // |PL (b - A x)|_2 < tolerance |b|_2, checked on the initial guess and after each step.
+    if (ap->storage_depth < 0 || ap->start_iteration < 1) return -1;
+    orc_mc* mc = orc_mc_create(A, PL, nullptr, mp);
+    if (!mc) return -1;
+    const int64_t n = A->m.n;
+    Problem P(A->m, PL ? &PL->m : nullptr, nullptr, b);
+    auto norm2 = [](const std::vector<double>& v) {
+        double s = 0.0;
+        for (double e : v) s += e * e;
+        return std::sqrt(s);
+    };
+    std::vector<double> xv(x, x + n), rp(n), f(n), delta(n), F(n), bv(b, b + n);
+    const double bnorm = norm2(bv);
+    const double crit = ap->tolerance * bnorm;
+    Anderson aa(*ap, n);
+    P.prec_residual(xv, rp);
+    double rnorm = norm2(rp);
+    int k = 0;
+    while (!(rnorm < crit) && k < ap->max_iters && std::isfinite(rnorm)) {
+        // MCSAModelEvaluator::evalModelImpl (src/MCLS_MCSAModelEvaluator_impl.hpp:306-350):
+        // f = x, smoothing f += r, Monte Carlo correction of the residual
+        // problem, F = f + delta - x.
+        f = xv;
+        for (int l = 0; l < ap->smoother_steps; ++l) {
+            for (int64_t i = 0; i < n; ++i) f[i] = f[i] + rp[i];
+            P.prec_residual(f, rp);
+        }
+        std::fill(delta.begin(), delta.end(), 0.0);
+        if (orc_mc_solve(mc, rp.data(), delta.data(), 1, 0, nullptr, nullptr, nullptr, nullptr) < 0) {
+            orc_mc_free(mc);
+            return -1;
+        }
+        for (int64_t i = 0; i < n; ++i) F[i] = (f[i] + delta[i]) - xv[i];
+        aa.step(k, xv, F);
+        ++k;
+        P.prec_residual(xv, rp);
+        rnorm = norm2(rp);
+        if (res_hist && k <= max_hist) res_hist[k - 1] = rnorm;
+    }
+    std::copy(xv.begin(), xv.end(), x);
+    if (iters) *iters = k;
+    if (achieved) *achieved = bnorm > 0.0 ? rnorm / bnorm : rnorm;
+    if (total_steps) *total_steps = mc->total_steps;
+    orc_mc_free(mc);
+    return rnorm < crit ? 1 : 0;
+}
+
+int orc_anderson_linear(const orc_csr* M, const double* c, const orc_anderson_params* ap,
+                        double* x, int* iters, int max_hist, double* iterates) {
+    const int64_t n = M->m.n;
+    std::vector<double> xv(x, x + n), g(n), F(n);
+    double cn = 0.0;
+    for (int64_t i = 0; i < n; ++i) cn += c[i] * c[i];
+    const double crit = ap->tolerance * std::sqrt(cn);
+    Anderson aa(*ap, n);
+    if (iterates) std::copy(xv.begin(), xv.end(), iterates);
+    int k = 0;
+    bool conv = false;
+    while (k < ap->max_iters) {
+        spmv(M->m, xv.data(), g.data());
+        double fn = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            F[i] = (g[i] + c[i]) - xv[i];
+            fn += F[i] * F[i];
+        }
+        if (std::sqrt(fn) < crit) {
+            conv = true;
+            break;
+        }
+        aa.step(k, xv, F);
+        ++k;
+        if (iterates && k <= max_hist) std::copy(xv.begin(), xv.end(), iterates + k * n);
+    }
+    std::copy(xv.begin(), xv.end(), x);
+    if (iters) *iters = k;
+    return conv ? 1 : 0;
+}
 
 int orc_fixed_point_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
                           const orc_mcsa_params* sp, const double* b, double* x, int* iters,

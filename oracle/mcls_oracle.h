@@ -119,6 +119,40 @@ int orc_fixed_point_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR
                           const orc_mcsa_params* sp, const double* b, double* x,
                           int* iters, double* achieved, int max_hist, double* res_hist);
 
+/* ---- Anderson-accelerated MCSA ----------------------------------------- */
+/* AndersonSolverManager (src/MCLS_AndersonSolverManager_impl.hpp:65-284):
+ * NOX's Anderson-accelerated fixed point on the MCSAModelEvaluator map
+ * (src/MCLS_MCSAModelEvaluator_impl.hpp:306-350).  NOX is not in the
+ * reference tree; its algorithm is restated from Walker & Ni, "Anderson
+ * acceleration for fixed-point iterations", SIAM J. Numer. Anal. 49 (2011),
+ * with the QR-updating least-squares solve (modified Gram-Schmidt to add a
+ * column, Givens rotations to drop the oldest) and NOX's parameter names. */
+typedef struct {
+    double tolerance;          /* "Convergence Tolerance" (default 1e-8)        */
+    int max_iters;             /* "Maximum Iterations" (default 1000)           */
+    int smoother_steps;        /* "Smoother Steps" (default 1)                  */
+    int storage_depth;         /* "Anderson Parameters"/"Storage Depth" (2)     */
+    double mixing;             /* "Mixing Parameter" (1.0)                      */
+    int start_iteration;       /* "Acceleration Start Iteration" (1)            */
+    int adjust_condition;      /* "Adjust Matrix for Condition Number" (0)      */
+    double drop_tolerance;     /* "Condition Number Drop Tolerance" (1e-12)     */
+} orc_anderson_params;
+
+/* Anderson-accelerated MCSA.  x holds x0 and receives the solution.  Stops
+ * when |PL (b - A x)|_2 < tolerance |b|_2 (MCSAStatusTest) or after
+ * max_iters steps.  res_hist gets |PL (b - A x_k)|_2 for k = 1.. (up to
+ * max_hist).  Returns 1 if converged, 0 if not, -1 on error. */
+int orc_anderson_solve(const orc_csr* A, const orc_csr* PL, const orc_mc_params* mp,
+                       const orc_anderson_params* ap, const double* b, double* x, int* iters,
+                       double* achieved, int max_hist, double* res_hist, int64_t* total_steps);
+
+/* The same acceleration of the linear map g(x) = M x + c (no Monte Carlo):
+ * stops when |g(x) - x|_2 < tolerance |c|_2 or after max_iters steps.
+ * iterates (optional, (max_hist + 1) x n) receives x_0, x_1, ...  Returns 1
+ * if converged. */
+int orc_anderson_linear(const orc_csr* M, const double* c, const orc_anderson_params* ap,
+                        double* x, int* iters, int max_hist, double* iterates);
+
 /* CPU baseline: independent histories on `threads` threads (one Xorshift per
  * thread, as one MPI rank per core with subdomain transport), adjoint
  * collision walks over the domain for `nh` histories of fixed length.

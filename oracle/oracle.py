@@ -50,6 +50,25 @@ class MCSAParams(C.Structure):
     ]
 
 
+class AndersonParams(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double),
+        ("max_iters", C.c_int),
+        ("smoother_steps", C.c_int),
+        ("storage_depth", C.c_int),
+        ("mixing", C.c_double),
+        ("start_iteration", C.c_int),
+        ("adjust_condition", C.c_int),
+        ("drop_tolerance", C.c_double),
+    ]
+
+
+def anderson_params(tolerance=1e-8, max_iters=1000, smoother_steps=1, storage_depth=2,
+                    mixing=1.0, start_iteration=1, adjust_condition=0, drop_tolerance=1e-12):
+    return AndersonParams(tolerance, max_iters, smoother_steps, storage_depth, mixing,
+                          start_iteration, adjust_condition, drop_tolerance)
+
+
 def build():
     """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
@@ -109,6 +128,13 @@ def lib():
                                             C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
                                             P]
         L.orc_fixed_point_solve.restype = C.c_int
+        L.orc_anderson_solve.argtypes = [P, P, C.POINTER(MCParams), C.POINTER(AndersonParams),
+                                         f64p, f64p, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                         C.c_int, P, C.POINTER(C.c_int64)]
+        L.orc_anderson_solve.restype = C.c_int
+        L.orc_anderson_linear.argtypes = [P, f64p, C.POINTER(AndersonParams), f64p,
+                                          C.POINTER(C.c_int), C.c_int, P]
+        L.orc_anderson_linear.restype = C.c_int
         L.orc_bench_walks.argtypes = [P, f64p, C.c_int64, C.c_int, P, C.POINTER(C.c_double)]
         L.orc_bench_walks.restype = C.c_int64
         _LIB = L
@@ -327,3 +353,37 @@ def fixed_point_solve(A: Csr, b, x0=None, PL=None, PR=None, tolerance=1.0, max_i
                                      C.byref(ach), max_iters, hist.ctypes.data)
     return dict(x=x, converged=bool(rc), iters=iters.value, achieved=ach.value,
                 residuals=hist[: iters.value])
+
+
+def anderson_solve(A: Csr, b, x0=None, PL=None, mc: MCParams | None = None,
+                   aa: AndersonParams | None = None, **kw):
+    """Anderson-accelerated MCSA restatement.  Keywords go to anderson_params
+    when they name one of its fields, else to mc_params."""
+    akeys = {f for f, _ in AndersonParams._fields_}
+    ap = aa if aa is not None else anderson_params(**{k: v for k, v in kw.items() if k in akeys})
+    mp = mc if mc is not None else mc_params(**{k: v for k, v in kw.items() if k not in akeys})
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+    iters = C.c_int(0)
+    ach = C.c_double(0.0)
+    steps = C.c_int64(0)
+    hist = np.zeros(max(ap.max_iters, 1), np.float64)
+    rc = lib().orc_anderson_solve(A.h, _h(PL), C.byref(mp), C.byref(ap), b, x, C.byref(iters),
+                                  C.byref(ach), ap.max_iters, hist.ctypes.data, C.byref(steps))
+    if rc < 0:
+        raise RuntimeError("oracle Anderson failed")
+    return dict(x=x, converged=bool(rc), iters=iters.value, achieved=ach.value,
+                residuals=hist[: iters.value], steps=steps.value)
+
+
+def anderson_linear(M: Csr, c, x0=None, **kw):
+    """Anderson acceleration of g(x) = M x + c: (x, iterations, converged,
+    iterates x_0..x_k)."""
+    ap = anderson_params(**kw)
+    c = np.ascontiguousarray(c, np.float64)
+    x = np.zeros_like(c) if x0 is None else np.array(x0, np.float64)
+    its = np.zeros((ap.max_iters + 1, c.size), np.float64)
+    iters = C.c_int(0)
+    rc = lib().orc_anderson_linear(M.h, c, C.byref(ap), x, C.byref(iters), ap.max_iters,
+                                   its.ctypes.data)
+    return x, iters.value, bool(rc), its[: iters.value + 1]

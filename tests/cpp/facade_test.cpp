@@ -109,7 +109,26 @@ static void cpu_checks() {
     EXPECT(Teuchos::nonnull(fp));
     EXPECT(fp->getValidParameters()->get<std::string>("Fixed Point Type") == "Richardson");
     EXPECT(fp->getValidParameters()->get<double>("Richardson Relaxation") == 1.0);
-    for (const char* name : {"Adjoint Anderson", "Forward Anderson", "Bogus"}) {
+    for (const char* name : {"Adjoint Anderson", "Forward Anderson"}) {
+        auto a = factory.create(name, pl);
+        EXPECT(Teuchos::nonnull(a));
+        auto va = a->getValidParameters();
+        EXPECT(va->get<double>("Convergence Tolerance") == 1.0e-8);
+        EXPECT(va->sublist("Anderson Parameters").get<int>("Storage Depth") == 2);
+        EXPECT(pl->get<std::string>("Nonlinear Solver") == "Anderson Accelerated Fixed-Point");
+    }
+    {
+        auto bad = mcsa_params();
+        bad->sublist("Anderson Parameters").set<int>("Storage Depth", 40);
+        bool threw = false;
+        try {
+            factory.create("Adjoint Anderson", bad);
+        } catch (const MCLS::Assertion&) {
+            threw = true;
+        }
+        EXPECT(threw);
+    }
+    for (const char* name : {"Bogus"}) {
         bool threw = false;
         try {
             factory.create(name, pl);
@@ -346,6 +365,33 @@ static void gpu_checks() {
         sm->setProblem(lp);
         EXPECT(sm->solve() && sm->getNumIters() < 20);
         EXPECT(rel_err(*x, direct(*A, *b)) < 1e-7);
+    }
+
+    // Anderson-accelerated MCSA: the reference's MCSA checks (signs, the
+    // direct solution) through the "Adjoint/Forward Anderson" managers, with
+    // the NOX sublist.
+    for (const char* name : {"Adjoint Anderson", "Forward Anderson"}) {
+        auto x = Teuchos::rcp(new Vec(n, 0.0));
+        auto b = Teuchos::rcp(new Vec(n, -1.0));
+        auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+        auto ms = Teuchos::rcp(new MCLS::MultiSetLinearProblem<Vec, Mat>(comm, 1, 0, lp));
+        auto pl = mcsa_params();
+        pl->set<int>("Maximum Iterations", 100);
+        pl->set<double>("Sample Ratio", 10.0);
+        pl->sublist("Anderson Parameters").set<int>("Storage Depth", 3);
+        MCLS::SolverFactory<Vec, Mat> factory;
+        auto sm = factory.create(name, pl);
+        for (double r : {-1.0, 2.0}) {
+            g_section = std::string(name) + ", b = " + std::to_string(r);
+            std::fill(b->begin(), b->end(), r);
+            std::fill(x->begin(), x->end(), 0.0);
+            sm->setProblem(lp);
+            EXPECT(sm->solve() && sm->getConvergedStatus());
+            EXPECT(sm->getNumIters() > 0 && sm->getNumIters() < 100);
+            EXPECT(sm->achievedTol() < 1e-8);
+            for (double xi : *x) EXPECT(r < 0 ? xi < 0.0 : xi > 0.0);
+            EXPECT(rel_err(*x, direct(*A, *b)) < 1e-7);
+        }
     }
 
     // Direct Monte Carlo: signs follow the source, sample ratio 10
