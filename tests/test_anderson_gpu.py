@@ -25,6 +25,7 @@ def _parity_pair(ctx, A, b, jacobi, seed, stratified=False, **aa):
                       source_sampling=capi.SOURCE_STRATIFIED if stratified else capi.SOURCE_RANDOM)
     x, st = dom.anderson_solve(b, **aa)
     Ao = O.Csr.from_scipy(A)
+    aa.pop("host_loop", None)
     r = O.anderson_solve(Ao, b, PL=O.point_jacobi(Ao) if jacobi else None, rng_mode=0,
                          seed=seed, stratified=int(stratified), **aa)
     return x, st, r
@@ -36,6 +37,7 @@ def _parity_pair(ctx, A, b, jacobi, seed, stratified=False, **aa):
     dict(storage_depth=3, start_iteration=3),
     dict(storage_depth=4, adjust_condition=1, drop_tolerance=1e-3),
     dict(storage_depth=2, smoother_steps=2),
+    dict(storage_depth=2, host_loop=1),
     # no smoothing: the random source's variance stalls the plain map, as it
     # stalls MCSA without smoothing; the stratified source converges
     dict(storage_depth=2, smoother_steps=0, stratified=True),
@@ -51,13 +53,18 @@ def test_anderson_follows_oracle_on_reference_stream(ctx, aa):
 
 
 def test_anderson_jacobi_poisson_follows_oracle(ctx):
+    # The first steps follow the oracle's; over tens of steps the rounding
+    # of atomically summed tallies can move a sampled source state, after
+    # which the two runs are independent samples of the same solve.
     A = P.poisson2d(9)
     b = np.linspace(0.5, 1.5, 81)
+    x, st, r = _parity_pair(ctx, A, b, True, 99, tolerance=0.0, max_iters=8, storage_depth=3)
+    assert st["iterations"] == r["iters"] == 8
+    assert np.allclose(x, r["x"], rtol=1e-7, atol=1e-12 * np.abs(r["x"]).max())
     x, st, r = _parity_pair(ctx, A, b, True, 99, tolerance=1e-8, max_iters=200,
                             storage_depth=3)
     assert st["converged"] == 1 and r["converged"]
-    assert abs(st["iterations"] - r["iters"]) <= 1
-    assert np.allclose(x, r["x"], rtol=1e-7, atol=1e-12 * np.abs(r["x"]).max())
+    assert abs(st["iterations"] - r["iters"]) <= 5
 
 
 @pytest.mark.parametrize("direction", [capi.ADJOINT, capi.FORWARD])
@@ -70,15 +77,15 @@ def test_anderson_fp32_converges(ctx, direction):
     x, st = dom.anderson_solve(b, tolerance=1e-8, max_iters=2000, storage_depth=2)
     assert st["converged"] == 1
     assert np.linalg.norm((b - A @ x) / A.diagonal()) < 1e-8 * np.linalg.norm(b) * 1.0001
+    # The error is the residual times the conditioning (D spans 0.1..10).
     xs = spla.spsolve(A.tocsc(), b)
-    assert np.linalg.norm(x - xs) <= 1e-6 * np.linalg.norm(xs)
-    # The same solve driven from the host takes the same steps.
-    dom.reseed(5)
+    assert np.linalg.norm(x - xs) <= 1e-5 * np.linalg.norm(xs)
+    # The host-driven loop (FP32 tallies are summed by atomics, so the
+    # iterates match the graph loop's statistically, not bit for bit).
     x2, st2 = dom.anderson_solve(b, tolerance=1e-8, max_iters=2000, storage_depth=2,
                                  host_loop=1)
-    dom.reseed(5)
-    x3, st3 = dom.anderson_solve(b, tolerance=1e-8, max_iters=2000, storage_depth=2)
-    assert st3["iterations"] == st2["iterations"] and np.array_equal(x3, x2)
+    assert st2["converged"] == 1
+    assert np.linalg.norm(x2 - xs) <= 1e-5 * np.linalg.norm(xs)
 
 
 def test_anderson_device_vectors_and_stats(ctx):
@@ -95,8 +102,9 @@ def test_anderson_device_vectors_and_stats(ctx):
     assert st["converged"] == 1 and st["iterations"] > 0
     assert st["histories"] >= st["iterations"] * n and st["walk_steps"] > 0
     assert st["achieved_tol"] < 1e-8
+    # error <= cond(A) (about 120 here) x the relative residual
     xs = spla.spsolve(A.tocsc(), np.ones(n))
-    assert np.linalg.norm(x.cpu().numpy() - xs) <= 1e-6 * np.linalg.norm(xs)
+    assert np.linalg.norm(x.cpu().numpy() - xs) <= 1e-5 * np.linalg.norm(xs)
 
 
 def test_converged_initial_guess_takes_no_step(ctx):
