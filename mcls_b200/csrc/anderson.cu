@@ -12,19 +12,23 @@
 //
 // One step on the device, all inside a captured graph with a WHILE node:
 //   smoothing + residual (one fused pass), the Monte Carlo correction,
-//   F pass         F = f + delta - x, |F|^2; the last block plans the step
-//                  (drop the oldest column when the store is full)
-//   MGS passes     the rotations of the drop on Q, the new column
-//                  v = F - F_old and dX = x - x_old, then one pass per
-//                  stored column: v -= r q_{j-1}, r = <q_j, v> (or |v|^2)
+//   first pass     F = f + delta - x and |F|^2; when a column is added also
+//                  the drop's rotations on Q, v = F - F_old, dX = x - x_old
+//                  and r = <q_0, v> (|v|^2 for an empty store)
+//   MGS passes     one per further stored column: v -= r q_{j-1},
+//                  r = <q_j, v> (|v|^2 after the last)
 //   control        R's new diagonal; optional drops for the condition number
 //   RHS pass       q_new = v / |v|, post-add rotations, <F, q_j>; the last
 //                  block back-solves R gamma = Q^T F
 //   update pass    x = x + beta F - sum (gamma_j dX_j + beta (R gamma)_j q_j)
-//   residual       rp = PL (b - A x), |rp|_2 and the status test.
-// Q and dX hold storage_depth vectors each; dX is a ring indexed from the
-// device state, so the captured graph never changes.
+//   residual       rp = PL (b - A x), |rp|_2, the status test, and (one
+//                  thread) the plan of the next step: whether it adds a
+//                  column and which one it drops first.
+// The passes move two elements per thread access (16 bytes).  Q and dX hold
+// storage_depth columns each at a stride rounded up to 32 elements; dX is a
+// ring indexed from the device state, so the captured graph never changes.
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "internal.h"
@@ -69,6 +73,7 @@ struct AaState {
 
 struct Args {
     int n;
+    size_t ld;             // column stride of Q and dX (n rounded up to 32)
     const double* f;       // smoothed iterate
     const double* delta;   // Monte Carlo correction
     double* x;
@@ -76,8 +81,8 @@ struct Args {
     double* Fold;
     double* xold;
     double* V;
-    double* Q;             // [m][n]
-    double* DX;            // [m][n]
+    double* Q;             // [m][ld]
+    double* DX;            // [m][ld] ring
     const double* rp;      // residual at the updated iterate
     double* part;
     unsigned int* ticket;
@@ -95,6 +100,42 @@ inline int grid_for(long long work, int cap) {
     return int(g > cap ? cap : g);
 }
 
+// W consecutive elements (W = 2: one 16-byte access; W = 1: the odd tail).
+template <int W>
+struct Vec {
+    double v[W];
+};
+template <int W>
+__device__ __forceinline__ Vec<W> ldv(const double* p, int i) {
+    Vec<W> r;
+    if constexpr (W == 2) {
+        const double2 t = *reinterpret_cast<const double2*>(p + i);
+        r.v[0] = t.x;
+        r.v[1] = t.y;
+    } else {
+        r.v[0] = p[i];
+    }
+    return r;
+}
+template <int W>
+__device__ __forceinline__ void stv(double* p, int i, const Vec<W>& r) {
+    if constexpr (W == 2)
+        *reinterpret_cast<double2*>(p + i) = make_double2(r.v[0], r.v[1]);
+    else
+        p[i] = r.v[0];
+}
+
+// body(integral_constant<int, W>, i) over the elements: pairs grid-stride,
+// then the odd last element in the last thread of the grid.
+template <class Body>
+__device__ __forceinline__ void for_elements(int n, Body body) {
+    const int np = n >> 1;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
+        body(std::integral_constant<int, 2>{}, 2 * p);
+    if ((n & 1) && blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1)
+        body(std::integral_constant<int, 1>{}, n - 1);
+}
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
     for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
     __syncthreads();
@@ -106,26 +147,34 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return t;
 }
 
-// Publish this block's sum of `v`; true in the block that finishes last,
-// whose thread 0 then holds the grid total in *total (block order, fixed
-// for a fixed launch).
-__device__ __forceinline__ bool grid_sum(double v, const Args& a, double* total) {
+// Publish this block's sums of v0 and v1; true in the block that finishes
+// last, whose thread 0 then holds the grid totals (block order, fixed for a
+// fixed launch).
+__device__ __forceinline__ bool grid_sum2(double v0, double v1, const Args& a, double* t0,
+                                          double* t1) {
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
-    const double t = block_sum(v, sh);
+    const double s0 = block_sum(v0, sh);
+    const double s1 = block_sum(v1, sh);
     if (threadIdx.x == 0) {
-        a.part[blockIdx.x] = t;
+        a.part[2 * blockIdx.x] = s0;
+        a.part[2 * blockIdx.x + 1] = s1;
         __threadfence();
         last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (!last) return false;
     __threadfence();
-    double u = 0.0;
-    for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) u += a.part[k];
-    const double s = block_sum(u, sh);
+    double u0 = 0.0, u1 = 0.0;
+    for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) {
+        u0 += a.part[2 * k];
+        u1 += a.part[2 * k + 1];
+    }
+    const double r0 = block_sum(u0, sh);
+    const double r1 = block_sum(u1, sh);
     if (threadIdx.x == 0) {
-        *total = s;
+        *t0 = r0;
+        *t1 = r1;
         *a.ticket = 0u;
     }
     return true;
@@ -182,16 +231,41 @@ __device__ double rcond(const AaState* st) {
     return 1.0 / (n1 * ni);
 }
 
-// Apply the recorded rotations to element i of the Q columns.
+// What step k does with the store (one thread): from the start iteration on
+// it adds a column, first dropping the oldest when the store is full.
+__device__ void plan(AaState* st) {
+    st->nrot = 0;
+    st->add = 0;
+    st->ok = 0;
+    if (st->m > 0 && st->k >= st->start) {
+        if (st->k == st->start) {
+            st->nstore = 0;
+            st->dx_head = 0;
+        } else if (st->nstore == st->m) {
+            qr_delete(st);
+        }
+        st->add = 1;
+        st->newcol = st->nstore;
+    }
+}
+
+// Apply the recorded rotations to elements i..i+W-1 of the Q columns.
+template <int W>
 __device__ __forceinline__ void rotate_q(const Args& a, const AaState* st, int nrot, int i) {
     for (int r = 0; r < nrot; ++r) {
         const int c0 = st->ri[r];
         const double c = st->rc[r], s = st->rs[r];
-        double* qa = a.Q + size_t(c0) * a.n;
-        double* qb = qa + a.n;
-        const double u = qa[i], v = qb[i];
-        qa[i] = __dadd_rn(__dmul_rn(c, u), __dmul_rn(s, v));
-        qb[i] = __dadd_rn(__dmul_rn(-s, u), __dmul_rn(c, v));
+        double* qa = a.Q + size_t(c0) * a.ld;
+        double* qb = qa + a.ld;
+        const Vec<W> u = ldv<W>(qa, i), v = ldv<W>(qb, i);
+        Vec<W> ua, vb;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            ua.v[w] = __dadd_rn(__dmul_rn(c, u.v[w]), __dmul_rn(s, v.v[w]));
+            vb.v[w] = __dadd_rn(__dmul_rn(-s, u.v[w]), __dmul_rn(c, v.v[w]));
+        }
+        stv<W>(qa, i, ua);
+        stv<W>(qb, i, vb);
     }
 }
 
@@ -212,67 +286,96 @@ __global__ void k_aa_init(AaState* st, int max_iters, int m, int start, int adju
     s.converged = s.rnorm < s.crit;
     if (!isfinite(s.rnorm)) atomicOr(status, DEV_ERR_NONFINITE);
     s.done = s.converged || !isfinite(s.rnorm);
+    plan(&s);
     *st = s;
 }
 
-// F = (f + delta) - x and |F|^2; the last block plans the step.
-__global__ void __launch_bounds__(kThreads) k_aa_F(Args a) {
-    double acc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        const double F = __dadd_rn(__dadd_rn(a.f[i], a.delta[i]), -a.x[i]);
-        a.F[i] = F;
-        acc = fma(F, F, acc);
-    }
-    double total;
-    if (!grid_sum(acc, a, &total) || threadIdx.x != 0) return;
-    AaState* st = a.st;
-    st->fnorm2 = total;
-    st->nrot = 0;
-    st->add = 0;
-    st->ok = 0;
-    if (st->m > 0 && st->k >= st->start) {
-        if (st->k == st->start) {
-            st->nstore = 0;
-            st->dx_head = 0;
-        } else if (st->nstore == st->m) {
-            qr_delete(st);
+// First pass of a step: F = (f + delta) - x and |F|^2; when the step adds a
+// column also the drop's rotations on Q, v = F - F_old, dX = x - x_old and
+// the first Gram-Schmidt product <q_0, v> (|v|^2 for an empty store).
+__global__ void __launch_bounds__(kThreads) k_aa_first(Args a) {
+    const AaState* st = a.st;
+    const int add = st->add, nc = st->newcol, nrot = st->nrot;
+    double* dxn = add ? a.DX + size_t((st->dx_head + nc) % st->m) * a.ld : nullptr;
+    const double* __restrict__ f = a.f;
+    const double* __restrict__ dl = a.delta;
+    double accF = 0.0, accV = 0.0;
+    for_elements(a.n, [&](auto wt, int i) {
+        constexpr int W = decltype(wt)::value;
+        const Vec<W> fv = ldv<W>(f, i), dv = ldv<W>(dl, i), xv = ldv<W>(a.x, i);
+        Vec<W> Fv;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            Fv.v[w] = __dadd_rn(__dadd_rn(fv.v[w], dv.v[w]), -xv.v[w]);
+            accF = fma(Fv.v[w], Fv.v[w], accF);
         }
-        st->add = 1;
-        st->newcol = st->nstore;
+        stv<W>(a.F, i, Fv);
+        if (!add) return;
+        if (nrot) rotate_q<W>(a, st, nrot, i);
+        const Vec<W> Fo = ldv<W>(a.Fold, i), xo = ldv<W>(a.xold, i);
+        Vec<W> v, dx;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            v.v[w] = __dadd_rn(Fv.v[w], -Fo.v[w]);
+            dx.v[w] = __dadd_rn(xv.v[w], -xo.v[w]);
+        }
+        stv<W>(a.V, i, v);
+        stv<W>(dxn, i, dx);
+        if (nc > 0) {
+            const Vec<W> q = ldv<W>(a.Q, i);
+#pragma unroll
+            for (int w = 0; w < W; ++w) accV = fma(q.v[w], v.v[w], accV);
+        } else {
+#pragma unroll
+            for (int w = 0; w < W; ++w) accV = fma(v.v[w], v.v[w], accV);
+        }
+    });
+    double tF, tV;
+    if (!grid_sum2(accF, accV, a, &tF, &tV) || threadIdx.x != 0) return;
+    AaState* sw = a.st;
+    sw->fnorm2 = tF;
+    if (add) {
+        if (nc > 0)
+            sw->R[0][nc] = tV;
+        else
+            sw->vnorm2 = tV;
     }
 }
 
-// Gram-Schmidt pass j of the new column (modified Gram-Schmidt: one stored
-// column per pass).  Pass 0 also applies the drop's rotations to Q and forms
-// v = F - F_old and the new dX = x - x_old.
+// Gram-Schmidt pass j >= 1 of the new column (modified Gram-Schmidt: one
+// stored column per pass): v -= R(j-1, new) q_{j-1}; R(j, new) = <q_j, v>,
+// or |v|^2 after the last stored column.
 __global__ void __launch_bounds__(kThreads) k_aa_mgs(Args a, int j) {
-    AaState* st = a.st;
+    const AaState* st = a.st;
     const int add = st->add, nc = st->newcol;
-    if (!add || j > nc) return;  // uniform over the grid
-    const int nrot = st->nrot;
-    const double r_prev = j > 0 ? st->R[j - 1][nc] : 0.0;
-    const double* qprev = j > 0 ? a.Q + size_t(j - 1) * a.n : nullptr;
-    const double* qj = j < nc ? a.Q + size_t(j) * a.n : nullptr;
-    double* dxn = a.DX + size_t((st->dx_head + nc) % st->m) * a.n;
+    if (!add || j > nc) return;  // the same in every block
+    const double r_prev = st->R[j - 1][nc];
+    const double* __restrict__ qprev = a.Q + size_t(j - 1) * a.ld;
+    const double* __restrict__ qj = j < nc ? a.Q + size_t(j) * a.ld : nullptr;
+    double* __restrict__ V = a.V;
     double acc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        double v;
-        if (j == 0) {
-            if (nrot) rotate_q(a, st, nrot, i);
-            v = __dadd_rn(a.F[i], -a.Fold[i]);
-            dxn[i] = __dadd_rn(a.x[i], -a.xold[i]);
+    for_elements(a.n, [&](auto wt, int i) {
+        constexpr int W = decltype(wt)::value;
+        const Vec<W> vo = ldv<W>(V, i), qp = ldv<W>(qprev, i);
+        Vec<W> v;
+#pragma unroll
+        for (int w = 0; w < W; ++w) v.v[w] = __dadd_rn(vo.v[w], __dmul_rn(-r_prev, qp.v[w]));
+        stv<W>(V, i, v);
+        if (qj) {
+            const Vec<W> q = ldv<W>(qj, i);
+#pragma unroll
+            for (int w = 0; w < W; ++w) acc = fma(q.v[w], v.v[w], acc);
         } else {
-            v = __dadd_rn(a.V[i], __dmul_rn(-r_prev, qprev[i]));
+#pragma unroll
+            for (int w = 0; w < W; ++w) acc = fma(v.v[w], v.v[w], acc);
         }
-        a.V[i] = v;
-        acc = qj ? fma(qj[i], v, acc) : fma(v, v, acc);
-    }
-    double total;
-    if (!grid_sum(acc, a, &total) || threadIdx.x != 0) return;
+    });
+    double t, unused;
+    if (!grid_sum2(acc, 0.0, a, &t, &unused) || threadIdx.x != 0) return;
     if (j < nc)
-        st->R[j][nc] = total;
+        a.st->R[j][nc] = t;
     else
-        st->vnorm2 = total;
+        a.st->vnorm2 = t;
 }
 
 // New diagonal entry of R, then the drops for the condition number.
@@ -300,21 +403,33 @@ __global__ void k_aa_ctrl(AaState* st) {
 __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
+    __shared__ double rhs[kMaxDepth];
     AaState* st = a.st;
     const int N = st->nstore, ok = st->ok, nc = st->newcol, nrot = st->nrot;
     const double inv = st->inv_rnn;
     double acc[kMaxDepth];
 #pragma unroll
     for (int j = 0; j < kMaxDepth; ++j) acc[j] = 0.0;
-    double* qn = a.Q + size_t(nc) * a.n;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        if (ok) qn[i] = __dmul_rn(inv, a.V[i]);
-        if (nrot) rotate_q(a, st, nrot, i);
-        const double F = a.F[i];
+    double* qn = a.Q + size_t(nc) * a.ld;
+    for_elements(a.n, [&](auto wt, int i) {
+        constexpr int W = decltype(wt)::value;
+        if (ok) {
+            const Vec<W> v = ldv<W>(a.V, i);
+            Vec<W> q;
+#pragma unroll
+            for (int w = 0; w < W; ++w) q.v[w] = __dmul_rn(inv, v.v[w]);
+            stv<W>(qn, i, q);
+        }
+        if (nrot) rotate_q<W>(a, st, nrot, i);
+        const Vec<W> F = ldv<W>(a.F, i);
 #pragma unroll
         for (int j = 0; j < kMaxDepth; ++j)
-            if (j < N) acc[j] = fma(F, a.Q[size_t(j) * a.n + i], acc[j]);
-    }
+            if (j < N) {
+                const Vec<W> q = ldv<W>(a.Q + size_t(j) * a.ld, i);
+#pragma unroll
+                for (int w = 0; w < W; ++w) acc[j] = fma(F.v[w], q.v[w], acc[j]);
+            }
+    });
 #pragma unroll
     for (int j = 0; j < kMaxDepth; ++j) {
         if (j < N) {  // N is the same in every thread of the block
@@ -329,7 +444,6 @@ __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    __shared__ double rhs[kMaxDepth];
     for (int j = 0; j < N; ++j) {
         double u = 0.0;
         for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x)
@@ -364,29 +478,45 @@ __global__ void __launch_bounds__(kThreads) k_aa_update(Args a) {
     for (int j = 0; j < kMaxDepth; ++j) {
         g[j] = j < N ? st->gamma[j] : 0.0;
         rg[j] = j < N ? st->rgamma[j] : 0.0;
-        dx[j] = j < N ? a.DX + size_t((head + j) % m) * a.n : nullptr;
+        dx[j] = j < N ? a.DX + size_t((head + j) % m) * a.ld : nullptr;
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        const double xi = a.x[i], F = a.F[i];
-        double w = __dmul_rn(beta, F);
+    for_elements(a.n, [&](auto wt, int i) {
+        constexpr int W = decltype(wt)::value;
+        const Vec<W> xv = ldv<W>(a.x, i), F = ldv<W>(a.F, i);
+        Vec<W> w;
+#pragma unroll
+        for (int e = 0; e < W; ++e) w.v[e] = __dmul_rn(beta, F.v[e]);
 #pragma unroll
         for (int j = 0; j < kMaxDepth; ++j)
-            if (j < N)
-                w = __dadd_rn(__dadd_rn(w, __dmul_rn(-g[j], dx[j][i])),
-                              __dmul_rn(-rg[j], a.Q[size_t(j) * a.n + i]));
-        a.xold[i] = xi;
-        a.Fold[i] = F;
-        a.x[i] = __dadd_rn(xi, w);
-    }
+            if (j < N) {
+                const Vec<W> d = ldv<W>(dx[j], i), q = ldv<W>(a.Q + size_t(j) * a.ld, i);
+#pragma unroll
+                for (int e = 0; e < W; ++e)
+                    w.v[e] = __dadd_rn(__dadd_rn(w.v[e], __dmul_rn(-g[j], d.v[e])),
+                                       __dmul_rn(-rg[j], q.v[e]));
+            }
+        Vec<W> xn;
+#pragma unroll
+        for (int e = 0; e < W; ++e) xn.v[e] = __dadd_rn(xv.v[e], w.v[e]);
+        stv<W>(a.xold, i, xv);
+        stv<W>(a.Fold, i, F);
+        stv<W>(a.x, i, xn);
+    });
 }
 
-// |rp|_2 and the status tests (MCSAStatusTest, MaxIters, FiniteValue).
+// |rp|_2 and the status tests (MCSAStatusTest, MaxIters, FiniteValue); the
+// last block also plans the next step.
 __global__ void __launch_bounds__(kThreads) k_aa_check(Args a) {
     double acc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
-        acc = fma(a.rp[i], a.rp[i], acc);
-    double total;
-    if (!grid_sum(acc, a, &total) || threadIdx.x != 0) return;
+    const double* __restrict__ rp = a.rp;
+    for_elements(a.n, [&](auto wt, int i) {
+        constexpr int W = decltype(wt)::value;
+        const Vec<W> r = ldv<W>(rp, i);
+#pragma unroll
+        for (int w = 0; w < W; ++w) acc = fma(r.v[w], r.v[w], acc);
+    });
+    double total, unused;
+    if (!grid_sum2(acc, 0.0, a, &total, &unused) || threadIdx.x != 0) return;
     AaState* st = a.st;
     st->k += 1;
     st->rnorm = sqrt(total);
@@ -395,6 +525,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_check(Args a) {
     if (!isfinite(st->rnorm) || !isfinite(st->fnorm2)) atomicOr(a.status, DEV_ERR_NONFINITE);
     const int keep = !st->converged && st->k < st->max_iters && !*a.status;
     st->done = !keep;
+    plan(st);
     if (a.use_cond) cudaGraphSetConditional(a.handle, keep ? 1u : 0u);
 }
 
@@ -433,6 +564,7 @@ struct AndersonWork {
     int n = 0;
     int m = 0;
     int grid = 1;
+    size_t ld = 0;
     double* F = nullptr;
     double* Fold = nullptr;
     double* xold = nullptr;
@@ -479,13 +611,14 @@ int ensure_work(mclsgpu_domain* dom, int m) {
     AndersonWork* w = new AndersonWork;
     w->n = dom->n;
     w->m = mm;
-    w->grid = grid_for(dom->n, ctx->num_sms * 4);
+    w->grid = grid_for((dom->n + 1) / 2, ctx->num_sms * 8);
+    w->ld = (size_t(dom->n) + 31) & ~size_t(31);
     const size_t n = size_t(dom->n);
     cudaError_t e;
     if ((e = dmalloc(&w->F, n)) != cudaSuccess || (e = dmalloc(&w->Fold, n)) != cudaSuccess ||
         (e = dmalloc(&w->xold, n)) != cudaSuccess || (e = dmalloc(&w->V, n)) != cudaSuccess ||
-        (e = dmalloc(&w->delta, n)) != cudaSuccess || (e = dmalloc(&w->Q, n * mm)) != cudaSuccess ||
-        (e = dmalloc(&w->DX, n * mm)) != cudaSuccess ||
+        (e = dmalloc(&w->delta, n)) != cudaSuccess || (e = dmalloc(&w->Q, w->ld * mm)) != cudaSuccess ||
+        (e = dmalloc(&w->DX, w->ld * mm)) != cudaSuccess ||
         (e = dmalloc(&w->part, size_t(w->grid) * kMaxDepth)) != cudaSuccess ||
         (e = dmalloc(&w->ticket, 1)) != cudaSuccess || (e = dmalloc(&w->st, 1)) != cudaSuccess ||
         (e = cudaMallocHost(reinterpret_cast<void**>(&w->h_st), sizeof(AaState))) != cudaSuccess) {
@@ -525,6 +658,7 @@ void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
     mc_correction(dom, r, w->delta);
     Args a{};
     a.n = n;
+    a.ld = w->ld;
     a.f = f;
     a.delta = w->delta;
     a.x = dom->x;
@@ -543,9 +677,9 @@ void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
     a.status = ctx->d_status;
     a.handle = h;
     a.use_cond = use_cond;
-    k_aa_F<<<w->grid, kThreads, 0, s>>>(a);
+    k_aa_first<<<w->grid, kThreads, 0, s>>>(a);
     if (p->storage_depth > 0) {
-        for (int j = 0; j < p->storage_depth; ++j) k_aa_mgs<<<w->grid, kThreads, 0, s>>>(a, j);
+        for (int j = 1; j < p->storage_depth; ++j) k_aa_mgs<<<w->grid, kThreads, 0, s>>>(a, j);
         k_aa_ctrl<<<1, 1, 0, s>>>(w->st);
         k_aa_rhs<<<w->grid, kThreads, 0, s>>>(a);
     }
