@@ -192,7 +192,7 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     train_s = time.perf_counter() - t0
     rl, rj = net.rho(op, iters=300)
     pc = capi.Precond(ctx, op, capi.PREC_LEARNED_SPAI, net=net)
-    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=1234,
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
                       direction=cfgd["direction"], history_length=cfgd["history_length"])
     mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
@@ -202,7 +202,7 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     tuned = dom.autotune(bt.data_ptr(), reps=1)
     stats = []
     for k in range(1 + args.steps):
-        dom.reseed(1234)
+        dom.reseed(args.seed)
         xt.zero_()
         torch.cuda.synchronize()
         st = dom.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
@@ -227,22 +227,27 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
                              "(seeds 1000-1007)" if args.config == "blocks256" else
                              "8 x 3D 7-pt var-coef diffusion 32^3 (seeds 1000-1007)"),
            "speedup_vs_jacobi": jacobi_ms / ms}
+    if not args.no_anderson:
+        M = pc.to_scipy(A.shape[0])
+        out["anderson"] = [anderson_arm(args, int(d), dom, bt, xt, A, b, args.seed, jacobi_ms,
+                                        PL=M) for d in args.anderson_depth.split(",")]
     dom.close()
     pc.close()
     net.close()
     return out
 
 
-def anderson_arm(args, dom, bt, xt, A, b, seed, jacobi_ms):
+def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None):
     """Anderson-accelerated MCSA (the "Adjoint/Forward Anderson" managers) on
-    the Jacobi arm's domain and right-hand side: one untimed warm-up solve,
-    then the timed solves, each from x = 0 on the same random stream."""
+    an MCSA arm's domain and right-hand side: one untimed warm-up solve, then
+    the timed solves, each from x = 0 on the same random stream.  PL: the
+    domain's left preconditioner as a scipy matrix (point Jacobi if None)."""
     import torch
 
     # The Anderson status test divides by |b|_2, MCSA's by |PL b|_2; the
     # tolerance below stops both at the same |PL (b - A x)|_2.
-    dinv = 1.0 / A.diagonal()
-    tol = 1e-8 * float(np.linalg.norm(dinv * b) / np.linalg.norm(b))
+    apply_pl = (lambda v: PL @ v) if PL is not None else (lambda v: v / A.diagonal())
+    tol = 1e-8 * float(np.linalg.norm(apply_pl(b)) / np.linalg.norm(b))
     stats = []
     for k in range(1 + args.steps):
         dom.reseed(seed)
@@ -250,19 +255,19 @@ def anderson_arm(args, dom, bt, xt, A, b, seed, jacobi_ms):
         torch.cuda.synchronize()
         st = dom.anderson_solve_dev(bt.data_ptr(), xt.data_ptr(), tolerance=tol,
                                     max_iters=args.max_iters,
-                                    storage_depth=args.anderson_depth,
+                                    storage_depth=depth,
                                     host_loop=1 if args.host_loop else 0)
         if k >= 1:
             stats.append(st)
     ms = sum(s["solve_ms"] for s in stats) / len(stats)
     rel = float(np.linalg.norm(b - A @ xt.cpu().numpy()) / np.linalg.norm(b))
     return {"time_to_1e-8_s": ms / 1e3, "iterations": stats[-1]["iterations"],
-            "converged": bool(stats[-1]["converged"]), "storage_depth": args.anderson_depth,
+            "converged": bool(stats[-1]["converged"]), "storage_depth": depth,
             "criterion": "|PL (b - A x)|_2 < tol |b|_2, tol = 1e-8 |PL b|_2 / |b|_2 "
                          "(the MCSA arm's |PL (b - A x)|_2 <= 1e-8 |PL b|_2)",
             "tolerance": tol,
-            "rel_prec_residual": float(np.linalg.norm(dinv * (b - A @ xt.cpu().numpy())) /
-                                       np.linalg.norm(dinv * b)),
+            "rel_prec_residual": float(np.linalg.norm(apply_pl(b - A @ xt.cpu().numpy())) /
+                                       np.linalg.norm(apply_pl(b))),
             "walk_steps_per_s": sum(s["walk_steps"] for s in stats) /
                                 (sum(s["solve_ms"] for s in stats) * 1e-3),
             "rel_residual_b_minus_Ax": rel, "speedup_vs_jacobi_mcsa": jacobi_ms / ms}
@@ -280,7 +285,7 @@ def run_batched(args, world, rank, local, pg):
     systems, nrhs, rhs, kinds = P.batch_sample(args.batch_systems, 1e3, args.batch_nmax,
                                                seed=rank)
     ctx = capi.Context(local)
-    seed = 1234 + rank
+    seed = args.seed + rank
     bt = capi.Batch(ctx, systems, nrhs, direction=capi.FORWARD, estimator=cfgd["estimator"],
                     precision=capi.FP32, sample_ratio=cfgd["sample_ratio"],
                     history_length=cfgd["history_length"], seed=seed)
@@ -446,8 +451,11 @@ def main():
                          "inside conditional graph nodes)")
     ap.add_argument("--no-anderson", action="store_true",
                     help="skip the Anderson-accelerated MCSA arm")
-    ap.add_argument("--anderson-depth", type=int, default=2,
-                    help="Anderson storage depth (NOX default 2)")
+    ap.add_argument("--anderson-depth", default="2,6",
+                    help="Anderson storage depths to time, comma separated (NOX's default "
+                         "is 2)")
+    ap.add_argument("--seed", type=int, default=1234,
+                    help="random-stream seed of the timed solves (rank r uses seed + r)")
     ap.add_argument("--spai-steps", type=int, default=2000,
                     help="training steps of the learned-SPAI network")
     ap.add_argument("--batch-systems", type=int, default=1024)
@@ -478,7 +486,7 @@ def main():
     ctx = capi.Context(local)
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
-    seed = 1234 + rank
+    seed = args.seed + rank
     dom = capi.Domain(ctx, op, pc, precision=fp, rng_mode=capi.RNG_COUNTER, seed=seed,
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
                       direction=cfgd["direction"],
@@ -578,8 +586,9 @@ def main():
         "wall_s": wall,
     }
     if world == 1 and not args.no_anderson:
-        line["config"]["anderson"] = anderson_arm(args, dom, bt, xt, A, b, seed,
-                                                  dev_ms_max / args.steps)
+        line["config"]["anderson"] = [
+            anderson_arm(args, int(d), dom, bt, xt, A, b, seed, dev_ms_max / args.steps)
+            for d in args.anderson_depth.split(",")]
     if world == 1 and args.config in ("diffusion128", "blocks256") and not args.no_learned:
         line["config"]["learned_spai"] = learned_arm(args, ctx, op, A, b, cfgd,
                                                      dev_ms_max / args.steps)
