@@ -417,6 +417,27 @@ int mclsgpu_anderson_solve(mclsgpu_domain* dom, const double* b, double* x,
                            const mclsgpu_anderson_params* params, mclsgpu_stats* stats);
 int mclsgpu_anderson_solve_dev(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
                                const mclsgpu_anderson_params* params, mclsgpu_stats* stats);
+/* The same solve one step at a time, for drivers that combine the Monte
+ * Carlo corrections of several sets (one set per GPU): the model
+ * evaluator's MultiSetLinearProblem::blockConstantVectorSum between the
+ * Monte Carlo solve and F (src/MCLS_MCSAModelEvaluator_impl.hpp:338-345).
+ *   begin:      x = x0; *rnorm = |PL (b - A x0)|_2, *bnorm = |b|_2,
+ *               *done = 1 when x0 already passes the status test
+ *   correction: smoothing, then delta_dev = this set's Monte Carlo correction
+ *   apply:      F = f + scale * delta_dev - x (scale = 1 / number of sets
+ *               after the caller summed delta over the sets), the
+ *               accelerated update, the new residual and the status test;
+ *               *done = 1 when the loop must stop
+ *   finish:     x_dev = x; stats of the steps since begin
+ * Device vectors of length n.  Every set takes the same steps: the update
+ * uses fixed-order reductions, so equal inputs give equal iterates. */
+int mclsgpu_anderson_begin(mclsgpu_domain* dom, const double* b_dev, const double* x0_dev,
+                           const mclsgpu_anderson_params* params, double* rnorm, double* bnorm,
+                           int32_t* done);
+int mclsgpu_anderson_correction(mclsgpu_domain* dom, double* delta_dev);
+int mclsgpu_anderson_apply(mclsgpu_domain* dom, const double* delta_dev, double scale,
+                           double* rnorm, int32_t* done);
+int mclsgpu_anderson_finish(mclsgpu_domain* dom, double* x_dev, mclsgpu_stats* stats);
 
 /* MCSA one iteration at a time, for drivers that combine the Monte Carlo
  * corrections of several sets (one set per GPU): the loop of

@@ -160,6 +160,8 @@ EXPORTS = [
     "mclsgpu_batch_mcsa_solve_dev", "mclsgpu_mcsa_begin", "mclsgpu_mcsa_correction",
     "mclsgpu_mcsa_apply", "mclsgpu_mcsa_finish", "mclsgpu_fixed_point_solve",
     "mclsgpu_fixed_point_solve_dev", "mclsgpu_anderson_solve", "mclsgpu_anderson_solve_dev",
+    "mclsgpu_anderson_begin", "mclsgpu_anderson_correction", "mclsgpu_anderson_apply",
+    "mclsgpu_anderson_finish",
 ]
 
 _LIB = None
@@ -226,6 +228,11 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_anderson_solve.argtypes = [P, P, P, C.POINTER(AndersonParams), C.POINTER(Stats)]
     L.mclsgpu_anderson_solve_dev.argtypes = [P, P, P, C.POINTER(AndersonParams),
                                              C.POINTER(Stats)]
+    L.mclsgpu_anderson_begin.argtypes = [P, P, P, C.POINTER(AndersonParams), C.POINTER(d),
+                                         C.POINTER(d), C.POINTER(C.c_int32)]
+    L.mclsgpu_anderson_correction.argtypes = [P, P]
+    L.mclsgpu_anderson_apply.argtypes = [P, P, d, C.POINTER(d), C.POINTER(C.c_int32)]
+    L.mclsgpu_anderson_finish.argtypes = [P, P, C.POINTER(Stats)]
     L.mclsgpu_fixed_point_solve.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
                                             C.POINTER(Stats)]
     L.mclsgpu_fixed_point_solve_dev.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
@@ -564,6 +571,33 @@ class Domain:
         self.ctx.check(self.ctx.L.mclsgpu_anderson_solve_dev(self.h, C.c_void_p(b_ptr),
                                                              C.c_void_p(x_ptr), C.byref(p),
                                                              C.byref(st)))
+        return st.as_dict()
+
+    def anderson_begin(self, b_ptr, x0_ptr, params: AndersonParams | None = None, **kw):
+        """Step-wise Anderson MCSA: (|PL (b - A x0)|_2, |b|_2, done)."""
+        p = params if params is not None else anderson_params(**kw)
+        rn, bn, done = C.c_double(), C.c_double(), C.c_int32()
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_begin(self.h, C.c_void_p(b_ptr),
+                                                         C.c_void_p(x0_ptr), C.byref(p),
+                                                         C.byref(rn), C.byref(bn),
+                                                         C.byref(done)))
+        return rn.value, bn.value, bool(done.value)
+
+    def anderson_correction(self, delta_ptr):
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_correction(self.h, C.c_void_p(delta_ptr)))
+
+    def anderson_apply(self, delta_ptr, scale=1.0):
+        """Returns (|PL (b - A x)|_2 after the step, done)."""
+        rn, done = C.c_double(), C.c_int32()
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_apply(self.h, C.c_void_p(delta_ptr), scale,
+                                                         C.byref(rn), C.byref(done)))
+        return rn.value, bool(done.value)
+
+    def anderson_finish(self, x_ptr):
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_finish(self.h, C.c_void_p(x_ptr),
+                                                          C.byref(st)))
         return st.as_dict()
 
     def mcsa_begin(self, b_ptr, x0_ptr, params: McsaParams | None = None, **kw):

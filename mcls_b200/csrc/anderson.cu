@@ -75,7 +75,8 @@ struct Args {
     int n;
     size_t ld;             // column stride of Q and dX (n rounded up to 32)
     const double* f;       // smoothed iterate
-    const double* delta;   // Monte Carlo correction
+    const double* delta;   // Monte Carlo correction (summed over the sets)
+    double dscale;         // 1 / number of sets
     double* x;
     double* F;
     double* Fold;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_first(Args a) {
         Vec<W> Fv;
 #pragma unroll
         for (int w = 0; w < W; ++w) {
-            Fv.v[w] = __dadd_rn(__dadd_rn(fv.v[w], dv.v[w]), -xv.v[w]);
+            Fv.v[w] = __dadd_rn(__dadd_rn(fv.v[w], __dmul_rn(a.dscale, dv.v[w])), -xv.v[w]);
             accF = fma(Fv.v[w], Fv.v[w], accF);
         }
         stv<W>(a.F, i, Fv);
@@ -580,6 +581,9 @@ struct AndersonWork {
     long long graph_key = -1;
     const double* graph_hist = nullptr;  // residual history the graph writes
     int body_kernels = 0;
+    // Step-wise solves (mclsgpu_anderson_begin .. _finish).
+    mclsgpu_anderson_params step_p{};
+    const double* step_f = nullptr;      // smoothed iterate of the pending step
     ~AndersonWork() {
         dfree(F);
         dfree(Fold);
@@ -630,14 +634,14 @@ int ensure_work(mclsgpu_domain* dom, int m) {
     return MCLSGPU_OK;
 }
 
-// One Anderson step and its status test (captured into the graph body).
-void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
-                  cudaGraphConditionalHandle h, int use_cond) {
-    mclsgpu_context* ctx = dom->ctx;
-    cudaStream_t s = ctx->stream;
+// The map's evaluation (MCSAModelEvaluator::evalModelImpl, :318-345):
+// f = x, "Smoother Steps" steps f += r, r = PL (b - A f), then this set's
+// Monte Carlo correction of the residual problem into delta.  Returns f.
+const double* enqueue_eval(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
+                           double* delta) {
+    cudaStream_t s = dom->ctx->stream;
     AndersonWork* w = dom->aa;
     const int n = dom->n;
-    // MCSAModelEvaluator::evalModelImpl: f = x; f += r; r = PL (b - A f).
     const double* f = dom->x;
     const double* r = dom->rp;
     if (p->smoother_steps == 1) {
@@ -655,12 +659,24 @@ void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
         f = dom->x2;
         r = dom->rp2;
     }
-    mc_correction(dom, r, w->delta);
+    mc_correction(dom, r, delta);
+    return f;
+}
+
+// The accelerated update from F = f + dscale * delta - x, the new residual
+// and the status test.
+void enqueue_accel(mclsgpu_domain* dom, const mclsgpu_anderson_params* p, const double* f,
+                   const double* delta, double dscale, cudaGraphConditionalHandle h,
+                   int use_cond) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    AndersonWork* w = dom->aa;
     Args a{};
-    a.n = n;
+    a.n = dom->n;
     a.ld = w->ld;
     a.f = f;
-    a.delta = w->delta;
+    a.delta = delta;
+    a.dscale = dscale;
     a.x = dom->x;
     a.F = w->F;
     a.Fold = w->Fold;
@@ -688,18 +704,23 @@ void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
     k_aa_check<<<w->grid, kThreads, 0, s>>>(a);
 }
 
-int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
-                   const mclsgpu_anderson_params* p, mclsgpu_stats* stats) {
+// One Anderson step and its status test (captured into the graph body).
+void enqueue_step(mclsgpu_domain* dom, const mclsgpu_anderson_params* p,
+                  cudaGraphConditionalHandle h, int use_cond) {
+    const double* f = enqueue_eval(dom, p, dom->aa->delta);
+    enqueue_accel(dom, p, f, dom->aa->delta, 1.0, h, use_cond);
+}
+
+// Work space and residual history buffer for a solve with these parameters.
+int anderson_prepare(mclsgpu_domain* dom, const mclsgpu_anderson_params* p) {
     mclsgpu_context* ctx = dom->ctx;
-    cudaStream_t s = ctx->stream;
-    const int n = dom->n;
     if (dom->right)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
                          "the Anderson solver applies the left preconditioner only");
     int rc = ensure_work(dom, p->storage_depth);
     if (rc) return rc;
-    AndersonWork* w = dom->aa;
     if (p->max_iters > dom->resid_cap) {
+        cudaStreamSynchronize(ctx->stream);
         dfree(dom->d_resid);
         cudaError_t e = dmalloc(&dom->d_resid, size_t(p->max_iters));
         if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
@@ -708,9 +729,55 @@ int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
         if (dom->graph) cudaGraphExecDestroy(dom->graph);
         dom->graph = nullptr;
     }
+    return MCLSGPU_OK;
+}
+
+// Counters, b and x0, the initial residual and state (the status test on
+// x0).  Leaves the state copying to the host, not synced.
+void anderson_begin(mclsgpu_domain* dom, const double* b_dev, const double* x_dev,
+                    const mclsgpu_anderson_params* p) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    AndersonWork* w = dom->aa;
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
     cudaMemsetAsync(w->ticket, 0, sizeof(unsigned int), s);
     mcsa_reset_counters(dom);
+    if (b_dev != dom->b)
+        cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (x_dev != dom->x)
+        cudaMemcpyAsync(dom->x, x_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    // |b|_2 (MCSAStatusTest uses the unpreconditioned right-hand side) and
+    // the residual of the initial guess, tested before the first step.
+    sum_sq(s, dom->b, n, dom->part, dom->d_scalars + 6);
+    prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    k_aa_init<<<1, 1, 0, s>>>(w->st, p->max_iters, p->storage_depth, p->start_iteration,
+                              p->adjust_condition, p->mixing, p->drop_tolerance, p->tolerance,
+                              dom->d_scalars + 6, dom->d_scalars + 5, ctx->d_status);
+    cudaMemcpyAsync(w->h_st, w->st, sizeof(AaState), cudaMemcpyDeviceToHost, s);
+}
+
+void fill_stats(mclsgpu_domain* dom, const AaState& st, double ms, mclsgpu_stats* stats) {
+    AndersonWork* w = dom->aa;
+    stats->iterations = st.k;
+    stats->converged = st.converged;
+    stats->residual_norm = st.rnorm;
+    stats->achieved_tol = st.bnorm > 0.0 ? st.rnorm / st.bnorm : st.rnorm;
+    stats->solve_ms = ms;
+    stats->fallback_taken = dom->left ? dom->left->fallback : 0;
+    stats->rho = dom->left ? dom->left->rho : -1.0;
+    stats->kernel_launches = int64_t(w->body_kernels) * st.k + 4;
+}
+
+int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
+                   const mclsgpu_anderson_params* p, mclsgpu_stats* stats) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    int rc = anderson_prepare(dom, p);
+    if (rc) return rc;
+    AndersonWork* w = dom->aa;
     const long long key = (long long)p->smoother_steps * 64 + p->storage_depth;
     if (!p->host_loop && (!w->graph || w->graph_key != key || w->graph_hist != dom->d_resid)) {
         if (w->graph) cudaGraphExecDestroy(w->graph);
@@ -726,19 +793,7 @@ int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    if (b_dev != dom->b)
-        cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
-    if (x_dev != dom->x)
-        cudaMemcpyAsync(dom->x, x_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
-    // |b|_2 (MCSAStatusTest uses the unpreconditioned right-hand side) and
-    // the residual of the initial guess, tested before the first step.
-    sum_sq(s, dom->b, n, dom->part, dom->d_scalars + 6);
-    prec_residual(dom, dom->x, dom->b, dom->rp);
-    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
-    k_aa_init<<<1, 1, 0, s>>>(w->st, p->max_iters, p->storage_depth, p->start_iteration,
-                              p->adjust_condition, p->mixing, p->drop_tolerance, p->tolerance,
-                              dom->d_scalars + 6, dom->d_scalars + 5, ctx->d_status);
-    cudaMemcpyAsync(w->h_st, w->st, sizeof(AaState), cudaMemcpyDeviceToHost, s);
+    anderson_begin(dom, b_dev, x_dev, p);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e == cudaSuccess && !w->h_st->done) {
         if (!p->host_loop) {
@@ -766,16 +821,8 @@ int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
     if (e != cudaSuccess) return cuda_fail(ctx, e, "anderson solve");
     if ((rc = check_device_status(ctx))) return rc;
     if (stats) {
-        const AaState& st = *w->h_st;
         if ((rc = mcsa_read_stats(dom, stats))) return rc;
-        stats->iterations = st.k;
-        stats->converged = st.converged;
-        stats->residual_norm = st.rnorm;
-        stats->achieved_tol = st.bnorm > 0.0 ? st.rnorm / st.bnorm : st.rnorm;
-        stats->solve_ms = ms;
-        stats->fallback_taken = dom->left ? dom->left->fallback : 0;
-        stats->rho = dom->left ? dom->left->rho : -1.0;
-        stats->kernel_launches = int64_t(w->body_kernels) * st.k + 4;
+        fill_stats(dom, *w->h_st, ms, stats);
     }
     return MCLSGPU_OK;
 }
@@ -795,6 +842,77 @@ int mclsgpu_anderson_solve_dev(mclsgpu_domain* dom, const double* b_dev, double*
     if (rc) return rc;
     cudaSetDevice(dom->ctx->device);
     return anderson_solve(dom, b_dev, x_dev, &p, stats);
+}
+
+int mclsgpu_anderson_begin(mclsgpu_domain* dom, const double* b_dev, const double* x0_dev,
+                           const mclsgpu_anderson_params* params, double* rnorm, double* bnorm,
+                           int32_t* done) {
+    if (!dom || !b_dev || !x0_dev) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_anderson_params p;
+    int rc = check_params(dom->ctx, params, &p);
+    if (rc) return rc;
+    cudaSetDevice(dom->ctx->device);
+    dom->aa_step_ready = 0;
+    if ((rc = anderson_prepare(dom, &p))) return rc;
+    anderson_begin(dom, b_dev, x0_dev, &p);
+    cudaError_t e = cudaStreamSynchronize(dom->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "anderson begin");
+    if ((rc = check_device_status(dom->ctx))) return rc;
+    const AaState& st = *dom->aa->h_st;
+    if (rnorm) *rnorm = st.rnorm;
+    if (bnorm) *bnorm = st.bnorm;
+    if (done) *done = st.done;
+    dom->aa->step_p = p;
+    dom->aa_step_ready = 1;
+    return MCLSGPU_OK;
+}
+
+int mclsgpu_anderson_correction(mclsgpu_domain* dom, double* delta_dev) {
+    if (!dom || !delta_dev) return MCLSGPU_ERR_INVALID_ARG;
+    if (!dom->aa_step_ready)
+        return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_anderson_begin first");
+    AndersonWork* w = dom->aa;
+    w->step_f = enqueue_eval(dom, &w->step_p, delta_dev);
+    cudaError_t e = cudaStreamSynchronize(dom->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "anderson correction");
+    return check_device_status(dom->ctx);
+}
+
+int mclsgpu_anderson_apply(mclsgpu_domain* dom, const double* delta_dev, double scale,
+                           double* rnorm, int32_t* done) {
+    if (!dom || !delta_dev) return MCLSGPU_ERR_INVALID_ARG;
+    if (!dom->aa_step_ready || !dom->aa->step_f)
+        return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG,
+                         "mclsgpu_anderson_correction first");
+    AndersonWork* w = dom->aa;
+    cudaStream_t s = dom->ctx->stream;
+    enqueue_accel(dom, &w->step_p, w->step_f, delta_dev, scale, cudaGraphConditionalHandle(0), 0);
+    w->step_f = nullptr;
+    cudaMemcpyAsync(w->h_st, w->st, sizeof(AaState), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "anderson apply");
+    int rc = check_device_status(dom->ctx);
+    if (rc) return rc;
+    if (rnorm) *rnorm = w->h_st->rnorm;
+    if (done) *done = w->h_st->done;
+    return MCLSGPU_OK;
+}
+
+int mclsgpu_anderson_finish(mclsgpu_domain* dom, double* x_dev, mclsgpu_stats* stats) {
+    if (!dom || !x_dev) return MCLSGPU_ERR_INVALID_ARG;
+    if (!dom->aa_step_ready)
+        return set_error(dom->ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_anderson_begin first");
+    cudaStream_t s = dom->ctx->stream;
+    if (x_dev != dom->x)
+        cudaMemcpyAsync(x_dev, dom->x, size_t(dom->n) * sizeof(double), cudaMemcpyDeviceToDevice,
+                        s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "anderson finish");
+    dom->aa_step_ready = 0;
+    if (!stats) return MCLSGPU_OK;
+    int rc = mcsa_read_stats(dom, stats);
+    if (!rc) fill_stats(dom, *dom->aa->h_st, 0.0, stats);
+    return rc;
 }
 
 int mclsgpu_anderson_solve(mclsgpu_domain* dom, const double* b, double* x,

@@ -180,6 +180,7 @@ struct mclsgpu_domain {
     int step_ready = 0;
     // Anderson-accelerated MCSA work space (anderson.cu), built on first use.
     mclsgpu::AndersonWork* aa = nullptr;
+    int aa_step_ready = 0;
 };
 
 namespace mclsgpu {

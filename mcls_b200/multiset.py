@@ -3,7 +3,9 @@ the Monte Carlo corrections summed over the sets by an all-reduce and
 divided by the set count -- the loop of MCSASolverManager::solve with
 MultiSetLinearProblem::blockConstantVectorSum
 (src/MCLS_MCSASolverManager_impl.hpp:344-400,
-src/MCLS_MultiSetLinearProblem_impl.hpp:102-120).
+src/MCLS_MultiSetLinearProblem_impl.hpp:102-120) -- and the same for the
+Anderson-accelerated solve, whose model evaluator sums the sets' corrections
+before forming F (src/MCLS_MCSAModelEvaluator_impl.hpp:338-345).
 
 The driver is written against a small engine interface so that the same
 host logic runs on GPUs (DeviceEngine: the library's step-wise MCSA entry
@@ -45,6 +47,25 @@ class DeviceEngine:
         stats = self.dom.mcsa_finish(self.x.data_ptr())
         return self.x, stats
 
+    # Anderson-accelerated MCSA (mclsgpu_anderson_begin/_correction/_apply/_finish)
+    def aa_begin(self, b, x0, params):
+        import torch
+
+        self.b = torch.as_tensor(b, dtype=torch.float64, device=self.dev).contiguous()
+        self.x = torch.as_tensor(x0, dtype=torch.float64, device=self.dev).clone().contiguous()
+        return self.dom.anderson_begin(self.b.data_ptr(), self.x.data_ptr(), params=params)
+
+    def aa_correction(self):
+        self.dom.anderson_correction(self.delta.data_ptr())
+        return self.delta
+
+    def aa_apply(self, delta, scale):
+        return self.dom.anderson_apply(delta.data_ptr(), scale)
+
+    def aa_finish(self):
+        stats = self.dom.anderson_finish(self.x.data_ptr())
+        return self.x, stats
+
 
 def solve(engine, b, x0, group=None, tolerance=1e-8, max_iters=1000, check_freq=1,
           smoother_steps=1, richardson_omega=1.0):
@@ -75,3 +96,37 @@ def solve(engine, b, x0, group=None, tolerance=1e-8, max_iters=1000, check_freq=
             converged = rnorm <= crit
     x, stats = engine.finish()
     return x, it, converged, rnorm / (bnorm if bnorm > 0.0 else 1.0), stats
+
+
+def solve_anderson(engine, b, x0, group=None, tolerance=1e-8, max_iters=1000, smoother_steps=1,
+                   storage_depth=2, mixing=1.0, start_iteration=1, adjust_condition=0,
+                   drop_tolerance=1e-12):
+    """Multi-set Anderson-accelerated MCSA on every rank of `group`: each step
+    sums the sets' Monte Carlo corrections (blockConstantVectorSum) and
+    scales by 1 / number of sets before the accelerated update.  Stops on
+    |PL (b - A x)|_2 < tolerance |b|_2 or max_iters steps.  Returns
+    (x, steps, converged, |PL (b - A x)|_2 / |b|_2, stats)."""
+    import torch
+
+    world = group.get_world_size() if group is not None else 1
+    params = capi.anderson_params(tolerance=tolerance, max_iters=max_iters,
+                                  smoother_steps=smoother_steps, storage_depth=storage_depth,
+                                  mixing=mixing, start_iteration=start_iteration,
+                                  adjust_condition=adjust_condition,
+                                  drop_tolerance=drop_tolerance)
+    rnorm, bnorm, done = engine.aa_begin(b, x0, params)
+    steps = 0
+    while not done:
+        steps += 1
+        delta = engine.aa_correction()
+        if world > 1:
+            group.all_reduce(delta)  # blockConstantVectorSum over the sets
+        rnorm, done = engine.aa_apply(delta, 1.0 / world)
+        if world > 1:
+            # Identical iterates give identical decisions; the MAX keeps the
+            # stopping decision common to all ranks regardless.
+            t = torch.tensor([rnorm, float(done)], dtype=torch.float64, device=delta.device)
+            group.all_reduce(t, op=group.ReduceOp.MAX)
+            rnorm, done = float(t[0].item()), bool(t[1].item())
+    x, stats = engine.aa_finish()
+    return x, steps, rnorm < tolerance * bnorm, rnorm / (bnorm if bnorm > 0.0 else 1.0), stats

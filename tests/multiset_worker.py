@@ -57,6 +57,49 @@ class OracleEngine:
     def finish(self):
         return self.x, {}
 
+    # Anderson-accelerated steps: the same map and acceleration in numpy
+    # (least squares on the stored differences, Walker & Ni 2011).
+    def aa_begin(self, b, x0, params):
+        self.b = np.asarray(b, np.float64)
+        self.x = np.array(x0, np.float64)
+        self.p = params
+        self.k = 0
+        self.Fs, self.Xs = [], []
+        self.rp = self._rp()
+        rn, bn = float(np.linalg.norm(self.rp)), float(np.linalg.norm(self.b))
+        return rn, bn, rn < params.tolerance * bn
+
+    def aa_correction(self):
+        self.f = self.x.copy()
+        r = self.rp
+        for _ in range(self.p.smoother_steps):
+            self.f = self.f + r
+            r = self.dinv * (self.b - self.A @ self.f)
+        delta, _ = self.mc.solve(r, internal=True)
+        return self.torch.tensor(delta)
+
+    def aa_apply(self, delta, scale):
+        p = self.p
+        F = self.f + scale * delta.numpy() - self.x
+        self.Fs.append(F)
+        self.Xs.append(self.x.copy())
+        k = self.k
+        if p.storage_depth > 0 and k >= p.start_iteration:
+            first = max(p.start_iteration - 1, k - p.storage_depth)
+            dF = np.column_stack([self.Fs[j + 1] - self.Fs[j] for j in range(first, k)])
+            dX = np.column_stack([self.Xs[j + 1] - self.Xs[j] for j in range(first, k)])
+            g = np.linalg.lstsq(dF, F, rcond=None)[0]
+            self.x = self.x + p.mixing * F - (dX + p.mixing * dF) @ g
+        else:
+            self.x = self.x + p.mixing * F
+        self.k += 1
+        self.rp = self._rp()
+        rn = float(np.linalg.norm(self.rp))
+        return rn, rn < p.tolerance * np.linalg.norm(self.b) or self.k >= p.max_iters
+
+    def aa_finish(self):
+        return self.x, {}
+
 
 def main(out_path):
     world, rank, _, pg = dist.init("gloo", timeout_s=60)
@@ -66,8 +109,14 @@ def main(out_path):
     eng = OracleEngine(A, seed)
     x, it, conv, rel, _ = multiset.solve(eng, b, np.zeros_like(b), group=pg, tolerance=1e-8,
                                          max_iters=3000)
+    eng_aa = OracleEngine(A, seed)
+    xa, ita, conva, rela, _ = multiset.solve_anderson(eng_aa, b, np.zeros_like(b), group=pg,
+                                                      tolerance=1e-10, max_iters=500,
+                                                      storage_depth=3)
     res = {"rank": rank, "world": world, "iters": it, "converged": bool(conv), "rel": rel,
            "x": list(map(float, x)), "seed": int(seed),
+           "aa_iters": ita, "aa_converged": bool(conva), "aa_rel": rela,
+           "aa_x": list(map(float, xa)),
            "allmax": dist.allmax(pg, rank + 1.0), "allsum": dist.allsum(pg, 1.0)}
     dist.barrier(pg)
     with open(out_path, "w") as f:

@@ -2,7 +2,7 @@
 
 Two ranks, one set each (the CPU oracle as each set's Monte Carlo engine,
 per-rank seeds as PRNG(rank) derives them), corrections summed by the
-product's multi-set driver.  Checks: both ranks end with the same iterate
+product's multi-set drivers (MCSA and Anderson-accelerated MCSA).  Checks: both ranks end with the same iterate
 and iteration count, the solution matches a direct solve, and the
 reduction helpers the benchmark's timing uses (max / sum over ranks) work.
 """
@@ -65,3 +65,8 @@ def test_two_sets_agree_and_converge(tmp_path):
     assert np.linalg.norm(np.array(r0["x"]) - xs) <= 1e-7 * np.linalg.norm(xs)
     assert r0["allmax"] == r1["allmax"] == 2.0
     assert r0["allsum"] == r1["allsum"] == 2.0
+    # Anderson-accelerated: the sets take identical steps to the solution.
+    assert r0["aa_converged"] and r1["aa_converged"]
+    assert r0["aa_iters"] == r1["aa_iters"] and r0["aa_iters"] < r0["iters"]
+    assert np.array_equal(np.array(r0["aa_x"]), np.array(r1["aa_x"]))
+    assert np.linalg.norm(np.array(r0["aa_x"]) - xs) <= 1e-7 * np.linalg.norm(xs)
