@@ -165,6 +165,43 @@ def allsum(pg, v):
     return dist.allsum(pg, v)
 
 
+def _learned_threshold_run(args, ctx, op, pc, A, b, cfgd, thr, jacobi_ms):
+    """Learned-SPAI MCSA with the composite operator M A filtered at `thr`
+    ("Composite Operator Threshold": entries |v| <= thr * row max dropped
+    before the domain is built), timed like the main learned solve."""
+    import torch
+
+    from mcls_b200 import capi
+
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
+                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
+                      direction=cfgd["direction"], history_length=cfgd["history_length"],
+                      composite_threshold=thr)
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
+    bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
+    xt = torch.zeros_like(bt)
+    dom.autotune(bt.data_ptr(), reps=1)
+    stats = []
+    for k in range(1 + args.steps):
+        dom.reseed(args.seed)
+        xt.zero_()
+        torch.cuda.synchronize()
+        st = dom.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
+        if k >= 1:
+            stats.append(st)
+    ms = sum(s["solve_ms"] for s in stats) / len(stats)
+    info = dom.info()
+    out = {"composite_threshold": thr, "time_to_1e-8_s": ms / 1e3,
+           "iterations": stats[-1]["iterations"], "converged": bool(stats[-1]["converged"]),
+           "record_bytes": info["record_bytes"], "h_entries_per_row": info["max_row_entries"],
+           "stencil_offsets": info["stencil_offsets"],
+           "rel_residual_b_minus_Ax": float(np.linalg.norm(b - A @ xt.cpu().numpy()) /
+                                            np.linalg.norm(b)),
+           "speedup_vs_jacobi": jacobi_ms / ms}
+    dom.close()
+    return out
+
+
 def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     """Learned-SPAI MCSA on the same system: train the per-row network on the
     GPU (untimed set-up, reported), build the learned preconditioner and its
@@ -192,9 +229,14 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     train_s = time.perf_counter() - t0
     rl, rj = net.rho(op, iters=300)
     pc = capi.Precond(ctx, op, capi.PREC_LEARNED_SPAI, net=net)
+    thresholds = [float(t) for t in args.learned_threshold.split(",")]
+    sweep = []
+    for thr in thresholds[1:]:
+        sweep.append(_learned_threshold_run(args, ctx, op, pc, A, b, cfgd, thr, jacobi_ms))
     dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
-                      direction=cfgd["direction"], history_length=cfgd["history_length"])
+                      direction=cfgd["direction"], history_length=cfgd["history_length"],
+                      composite_threshold=thresholds[0])
     mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
                           host_loop=1 if args.host_loop else 0)
     bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
@@ -226,7 +268,10 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
            "train_systems": ("8 x 3D 7-pt diffusion-reaction 32^3 on 4^3 random blocks "
                              "(seeds 1000-1007)" if args.config == "blocks256" else
                              "8 x 3D 7-pt var-coef diffusion 32^3 (seeds 1000-1007)"),
-           "speedup_vs_jacobi": jacobi_ms / ms}
+           "speedup_vs_jacobi": jacobi_ms / ms,
+           "composite_threshold": thresholds[0]}
+    if sweep:
+        out["threshold_sweep"] = sweep
     if not args.no_anderson:
         M = pc.to_scipy(A.shape[0])
         out["anderson"] = [anderson_arm(args, int(d), dom, bt, xt, A, b, args.seed, jacobi_ms,
@@ -454,6 +499,10 @@ def main():
     ap.add_argument("--anderson-depth", default="2,6",
                     help="Anderson storage depths to time, comma separated (NOX's default "
                          "is 2)")
+    ap.add_argument("--learned-threshold", default="0",
+                    help="Composite Operator Threshold(s) of the learned-SPAI domain, comma "
+                         "separated: the first is the reported learned solve, the others a "
+                         "sweep")
     ap.add_argument("--seed", type=int, default=1234,
                     help="random-stream seed of the timed solves (rank r uses seed + r)")
     ap.add_argument("--spai-steps", type=int, default=2000,
