@@ -161,7 +161,9 @@ EXPORTS = [
     "mclsgpu_mcsa_apply", "mclsgpu_mcsa_finish", "mclsgpu_fixed_point_solve",
     "mclsgpu_fixed_point_solve_dev", "mclsgpu_anderson_solve", "mclsgpu_anderson_solve_dev",
     "mclsgpu_anderson_begin", "mclsgpu_anderson_correction", "mclsgpu_anderson_apply",
-    "mclsgpu_anderson_finish",
+    "mclsgpu_anderson_finish", "mclsgpu_history_wire_size", "mclsgpu_subdomain_build",
+    "mclsgpu_subdomain_destroy", "mclsgpu_subdomain_info", "mclsgpu_subdomain_begin",
+    "mclsgpu_subdomain_transport", "mclsgpu_subdomain_finish",
 ]
 
 _LIB = None
@@ -233,6 +235,15 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_anderson_correction.argtypes = [P, P]
     L.mclsgpu_anderson_apply.argtypes = [P, P, d, C.POINTER(d), C.POINTER(C.c_int32)]
     L.mclsgpu_anderson_finish.argtypes = [P, P, C.POINTER(Stats)]
+    L.mclsgpu_history_wire_size.restype = C.c_int32
+    L.mclsgpu_subdomain_build.argtypes = [P, i64, C.c_int32, P, C.c_int32, P, P, P,
+                                          C.POINTER(McParams), PP]
+    L.mclsgpu_subdomain_destroy.argtypes = [P]
+    L.mclsgpu_subdomain_info.argtypes = [P, C.POINTER(i64), C.POINTER(i64),
+                                         C.POINTER(C.c_int32)]
+    L.mclsgpu_subdomain_begin.argtypes = [P, P, C.POINTER(i64), C.POINTER(i64)]
+    L.mclsgpu_subdomain_transport.argtypes = [P, P, i64, P, i64, P]
+    L.mclsgpu_subdomain_finish.argtypes = [P, P, C.POINTER(Stats)]
     L.mclsgpu_fixed_point_solve.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
                                             C.POINTER(Stats)]
     L.mclsgpu_fixed_point_solve_dev.argtypes = [P, P, P, P, P, P, C.POINTER(McsaParams),
@@ -793,6 +804,65 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             self.ctx.L.mclsgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Subdomain:
+    """One part of a row-partitioned adjoint domain (mclsgpu_subdomain_*).
+
+    `rows` is the part's rows of the transposed composite operator
+    (PL A PR)^T with global column indices (scipy CSR, n_global columns)."""
+
+    def __init__(self, ctx: Context, n_global: int, bounds, part: int, rows,
+                 params: McParams | None = None, **kw):
+        self.ctx = ctx
+        self.p = params if params is not None else mc_params(**kw)
+        self.bounds = np.ascontiguousarray(bounds, np.int64)
+        self.nparts = len(self.bounds) - 1
+        self.part = part
+        R = sp.csr_matrix(rows)
+        R.sort_indices()
+        rp = np.ascontiguousarray(R.indptr, np.int64)
+        ci = np.ascontiguousarray(R.indices, np.int64)
+        v = np.ascontiguousarray(R.data, np.float64)
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_subdomain_build(ctx.h, n_global, self.nparts, _ptr(self.bounds),
+                                                part, _ptr(rp), _ptr(ci), _ptr(v),
+                                                C.byref(self.p), C.byref(h)))
+        self.h = h
+        ctx._adopt(self)
+        b, r, rb = C.c_int64(), C.c_int64(), C.c_int32()
+        ctx.check(ctx.L.mclsgpu_subdomain_info(self.h, C.byref(b), C.byref(r), C.byref(rb)))
+        self.row_begin, self.rows, self.record_bytes = b.value, r.value, rb.value
+
+    def begin(self, rhs_ptr):
+        """Returns (histories starting in this part, histories in the solve)."""
+        ns, nt = C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.L.mclsgpu_subdomain_begin(self.h, C.c_void_p(rhs_ptr),
+                                                          C.byref(ns), C.byref(nt)))
+        return ns.value, nt.value
+
+    def transport(self, inbox_ptr, n_in, outbox_ptr, capacity):
+        """One round; returns the departures per destination part."""
+        counts = np.zeros(self.nparts, np.int64)
+        self.ctx.check(self.ctx.L.mclsgpu_subdomain_transport(
+            self.h, C.c_void_p(inbox_ptr) if inbox_ptr else None, n_in, C.c_void_p(outbox_ptr),
+            capacity, _ptr(counts)))
+        return counts
+
+    def finish(self, x_ptr):
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_subdomain_finish(self.h, C.c_void_p(x_ptr),
+                                                           C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_subdomain_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -36,12 +36,12 @@ __device__ __forceinline__ double iteration_value(int row, int col, double m, do
     return col == row ? __dsub_rn(1.0, prod) : -prod;
 }
 
-__global__ void k_domain_count(const int* rp, const int* ci, const double* v, int n,
+__global__ void k_domain_count(const int* rp, const int* ci, const double* v, int n, int row0,
                                double relax, int* cnt, int* status, int* max_len) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int c = 0;
         for (int k = rp[i]; k < rp[i + 1]; ++k) {
-            double h = iteration_value(i, ci[k], v[k], relax);
+            double h = iteration_value(row0 + i, ci[k], v[k], relax);
             if (!(fabs(h) < DBL_EPSILON)) ++c;  // :312-317
         }
         cnt[i] = c;
@@ -50,7 +50,7 @@ __global__ void k_domain_count(const int* rp, const int* ci, const double* v, in
     }
 }
 
-__global__ void k_domain_fill(const int* rp, const int* ci, const double* v, int n,
+__global__ void k_domain_fill(const int* rp, const int* ci, const double* v, int n, int row0,
                               double relax, const int* drp, int* dcol, double* dh,
                               double* dcdf, double* dw, int* status) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -58,7 +58,7 @@ __global__ void k_domain_fill(const int* rp, const int* ci, const double* v, int
         double c = 0.0;
         const int o0 = o;
         for (int k = rp[i]; k < rp[i + 1]; ++k) {
-            double h = iteration_value(i, ci[k], v[k], relax);
+            double h = iteration_value(row0 + i, ci[k], v[k], relax);
             if (fabs(h) < DBL_EPSILON) continue;
             dcol[o] = ci[k];
             dh[o] = h;
@@ -176,7 +176,7 @@ int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int max_k, int* offse
 
 // Build the FP64 domain arrays and FP32 records from the composite M.
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
-                        mclsgpu_domain* dom) {
+                        mclsgpu_domain* dom, int row0) {
     cudaStream_t s = ctx->stream;
     const int n = M.n;
     int* cnt = nullptr;
@@ -188,8 +188,8 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     }
     cudaMemsetAsync(maxlen, 0, sizeof(int), s);
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
-    k_domain_count<<<grid_for(n), 256, 0, s>>>(M.rp, M.ci, M.v, n, relax, cnt, ctx->d_status,
-                                               maxlen);
+    k_domain_count<<<grid_for(n), 256, 0, s>>>(M.rp, M.ci, M.v, n, row0, relax, cnt,
+                                               ctx->d_status, maxlen);
     DevCsr& D = dom->D;
     D.release();
     D.n = n;
@@ -212,7 +212,7 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     if ((e = dmalloc(&D.ci, tot + 1)) != cudaSuccess || (e = dmalloc(&D.v, tot + 1)) != cudaSuccess ||
         (e = dmalloc(&dom->cdf, tot + 1)) != cudaSuccess || (e = dmalloc(&dom->w, n + 1)) != cudaSuccess)
         return cuda_fail(ctx, e, "cudaMalloc");
-    k_domain_fill<<<grid_for(n), 256, 0, s>>>(M.rp, M.ci, M.v, n, relax, D.rp, D.ci, D.v,
+    k_domain_fill<<<grid_for(n), 256, 0, s>>>(M.rp, M.ci, M.v, n, row0, relax, D.rp, D.ci, D.v,
                                               dom->cdf, dom->w, ctx->d_status);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "domain fill");
@@ -232,7 +232,7 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     // for offsets the row lacks: 2 + K words instead of 2 + 2 * row length.
     dom->stencil_k = 0;
     const int fmt = dom->p.record_format;
-    if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED) {
+    if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED && row0 == 0) {
         int K = 0;
         if ((rc = collect_offsets(ctx, D, 30, dom->stencil_off, &K))) return rc;
         // 32-, 64- or 128-byte records.

@@ -201,8 +201,9 @@ inline void dfree(T*& p) {
 
 // ---- sparse (sparse.cu) ----------------------------------------------------
 // Upload a host CSR (int64 indices) to a DevCsr (int32).  Validates.
+// ncols < 0: square (ncols = n).
 int upload_csr(mclsgpu_context* ctx, int64_t n, const int64_t* rp,
-               const int64_t* ci, const double* v, DevCsr& out);
+               const int64_t* ci, const double* v, DevCsr& out, int64_t ncols = -1);
 int csr_transpose(mclsgpu_context* ctx, const DevCsr& A, DevCsr& T);
 // C = A*B (accumulated over A's row entries in column order) then filtered
 // by `threshold` relative to the signed row max.
@@ -232,8 +233,10 @@ void sell_spmv(cudaStream_t s, const DevSell& A, const double* x, double* y);
 int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int* d_rp,
                               long long* total);
 // Domain arrays and FP32 records from the composite operator (domain.cu).
+// row0: global index of M's first row (rows of one part of a row-partitioned
+// domain; its columns are global).
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
-                        mclsgpu_domain* dom);
+                        mclsgpu_domain* dom, int row0 = 0);
 
 // ---- MCSA helpers (mcsa.cu) ----------------------------------------------------
 // rp_out = PL (b - A PR x)   (LinearProblem::updatePrecResidual)
@@ -265,6 +268,47 @@ void enqueue_fixed_point_step(mclsgpu_domain* dom, int type, double omega);
 int build_while_graph(mclsgpu_context* ctx,
                       const std::function<void(cudaGraphConditionalHandle)>& body,
                       cudaGraphExec_t* exec, int* body_kernels);
+
+// ---- row-partitioned domains (walk.cu, subdomain.cu) ---------------------------
+constexpr int kMaxParts = 64;
+
+// One history crossing between parts (24 bytes, the C ABI's
+// mclsgpu_history_wire).
+struct HistoryWire {
+    uint64_t rng;     // Xorshift state after the last draw
+    int32_t state;    // the global state it moved to
+    int32_t step;     // transitions taken
+    float weight;
+    int32_t id;       // its index in the global source
+};
+static_assert(sizeof(HistoryWire) == 24, "history wire format");
+
+struct PartWalk {
+    const uint2* rec;       // packed FP32 records of rows [row0, row0 + n)
+    int slots;
+    int row0;
+    int n;
+    int L;
+    // first round: the histories e_begin <= e < e_end of the global source
+    const int* start;
+    long long e_begin, e_end;
+    const double* sc;       // [0] = starting weight |b|_1
+    uint64_t seed;
+    const unsigned long long* d_epoch;
+    // later rounds: histories handed over by other parts
+    const HistoryWire* in;
+    long long n_in;
+    // departures: out[q * cap + slot] for the owner q of the new state
+    HistoryWire* out;
+    long long cap;
+    unsigned long long* out_cnt;
+    int nparts;
+    const int* bounds;      // nparts + 1 global row bounds (device)
+    double* y;              // tallies of the part's rows
+    unsigned long long* d_steps;
+    int* status;
+};
+void launch_walk_part(const PartWalk& p, mclsgpu_context* ctx);
 
 // ---- scans and reductions (scan.cu) ------------------------------------------
 int scan_partials_needed(int n);

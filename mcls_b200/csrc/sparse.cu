@@ -278,8 +278,10 @@ __global__ void k_block_jacobi(const int* rp, const int* ci, const double* v, in
 
 // ---------------------------------------------------------------------------
 int upload_csr(mclsgpu_context* ctx, int64_t n, const int64_t* rp, const int64_t* ci,
-               const double* v, DevCsr& out) {
-    if (n <= 0 || n >= (int64_t(1) << 31) || !rp || !ci || !v)
+               const double* v, DevCsr& out, int64_t ncols) {
+    if (ncols < 0) ncols = n;
+    if (n <= 0 || n >= (int64_t(1) << 31) || ncols <= 0 || ncols >= (int64_t(1) << 31) || !rp ||
+        !ci || !v)
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "operator: bad size or null array");
     if (rp[0] != 0) return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "operator: rowptr[0] != 0");
     const int64_t nnz = rp[n];
@@ -299,7 +301,7 @@ int upload_csr(mclsgpu_context* ctx, int64_t n, const int64_t* rp, const int64_t
         row.clear();
         bool sorted = true;
         for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-            if (ci[k] < 0 || ci[k] >= n)
+            if (ci[k] < 0 || ci[k] >= ncols)
                 return set_error(ctx, MCLSGPU_ERR_INVALID_ARG,
                                  "operator: column %lld out of range in row %lld",
                                  (long long)ci[k], (long long)i);

@@ -60,6 +60,7 @@ struct WalkArgs {
     unsigned long long* d_steps;
     unsigned long long* d_tim;  // [0] first warp start, [1] last warp end (ns)
     int* status;
+    int row0;                   // global index of the first record / tally row
     int stoff[32];              // stencil records: column offset of each slot
     // trace (FP64 only)
     long long max_trace;
@@ -112,13 +113,13 @@ __device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, in
                                           uint64_t& x, float& acc, float& comp, int k) {
     // One record: S/4 256-bit loads that bypass L1 (each step touches exactly
     // the record's own sectors).
-    const char* r = rec + size_t(s) * (S * 8);
+    const char* r = rec + size_t(s - a.row0) * (S * 8);
     uint32_t q[2 * S];
 #pragma unroll
     for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
     if (DIR == MCLSGPU_ADJOINT) {
         // FP32 weight, FP64 reduction (fire-and-forget RED.ADD.F64).
-        if (k > 0) atomicAdd(&a.y64[s], double(w));
+        if (k > 0) atomicAdd(&a.y64[s - a.row0], double(w));
     } else {
         // Kahan-compensated FP32 history sum; the tally source of the state
         // rides in the record header (slot 0, second word).
@@ -665,6 +666,105 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
             walk64<MCLSGPU_ADJOINT><<<grid, 128, 0, st>>>(a);
         else
             walk64<MCLSGPU_FORWARD><<<grid, 128, 0, st>>>(a);
+    }
+}
+
+// ---- row-partitioned domains (domain-decomposed transport) -----------------
+//
+// One part holds the records and tallies of rows [row0, row0 + n).  A
+// history walks while its state stays in the part; when a transition takes
+// it to another part's row with steps left, it is written to that part's
+// outbox (HistoryWire: Xorshift state, state, step, weight) and continues
+// there in a later round, on the same random stream.  Every transition and
+// tally is therefore the one the whole-domain walk would make.
+namespace {
+
+template <int S>
+__global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
+    __shared__ int sb[kMaxParts + 1];
+    for (int t = threadIdx.x; t <= p.nparts; t += blockDim.x) sb[t] = p.bounds[t];
+    __syncthreads();
+    WalkArgs a{};
+    a.y64 = p.y;
+    a.row0 = p.row0;
+    const uint64_t ekey = epoch_key(p.seed, *p.d_epoch);
+    const float wnorm = float(p.sc[0]);
+    const long long nwork = p.in ? p.n_in : p.e_end - p.e_begin;
+    const char* rec = reinterpret_cast<const char*>(p.rec);
+    const int hi = p.row0 + p.n;
+    unsigned steps = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nwork;
+         t += (long long)gridDim.x * blockDim.x) {
+        int s, k, id;
+        float w;
+        uint64_t x;
+        if (p.in) {
+            const HistoryWire h = p.in[t];
+            s = h.state;
+            k = h.step;
+            w = h.weight;
+            x = h.rng;
+            id = h.id;
+        } else {
+            const long long e = p.e_begin + t;
+            const int sv = p.start[e];
+            s = sv & 0x7fffffff;
+            w = sv < 0 ? -wnorm : wnorm;
+            x = counter_state(ekey, 2, uint64_t(e));
+            k = 0;
+            id = int(e);
+        }
+        if (s < p.row0 || s >= hi) {  // not this part's history
+            atomicOr(p.status, DEV_ERR_BOUNDS);
+            continue;
+        }
+        float acc = 0.f, comp = 0.f;
+        while (k < p.L) {
+            walk_step<S, MCLSGPU_ADJOINT, false>(a, rec, s, w, x, acc, comp, k);
+            ++k;
+            ++steps;
+            if (k < p.L && (s < p.row0 || s >= hi)) {
+                int lo = 0, up = p.nparts;  // owner: sb[lo] <= s < sb[lo + 1]
+                while (up - lo > 1) {
+                    const int mid = (lo + up) >> 1;
+                    if (sb[mid] <= s) lo = mid; else up = mid;
+                }
+                const unsigned long long slot = atomicAdd(&p.out_cnt[lo], 1ULL);
+                if (slot < (unsigned long long)p.cap) {
+                    HistoryWire h;
+                    h.rng = x;
+                    h.state = s;
+                    h.step = k;
+                    h.weight = w;
+                    h.id = id;
+                    p.out[size_t(lo) * size_t(p.cap) + slot] = h;
+                } else {
+                    atomicOr(p.status, DEV_ERR_CAPACITY);
+                }
+                break;
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) steps += __shfl_down_sync(kFull, steps, d);
+    if ((threadIdx.x & 31) == 0 && steps) atomicAdd(p.d_steps, (unsigned long long)steps);
+}
+
+}  // namespace
+
+void launch_walk_part(const PartWalk& p, mclsgpu_context* ctx) {
+    const long long nwork = p.in ? p.n_in : p.e_end - p.e_begin;
+    if (nwork <= 0) return;
+    long long g = (nwork + 255) / 256;
+    const int grid = int(g < ctx->num_sms * 8 ? g : ctx->num_sms * 8);
+    cudaStream_t st = ctx->stream;
+    switch (p.slots) {
+        case 4: walk32_part<4><<<grid, 256, 0, st>>>(p); break;
+        case 8: walk32_part<8><<<grid, 256, 0, st>>>(p); break;
+        case 12: walk32_part<12><<<grid, 256, 0, st>>>(p); break;
+        case 16: walk32_part<16><<<grid, 256, 0, st>>>(p); break;
+        case 24: walk32_part<24><<<grid, 256, 0, st>>>(p); break;
+        default: walk32_part<32><<<grid, 256, 0, st>>>(p); break;
     }
 }
 
