@@ -212,8 +212,9 @@ int csr_multiply(mclsgpu_context* ctx, const DevCsr& A, const DevCsr& B,
 int csr_copy(mclsgpu_context* ctx, const DevCsr& A, DevCsr& B);
 // Column scaling: T.v[k] *= s[T.ci[k]] (composite with a diagonal factor).
 void csr_scale_cols(mclsgpu_context* ctx, DevCsr& T, const double* s);
+// ncols: A's column count (< 0: square).
 int csr_filter(mclsgpu_context* ctx, const DevCsr& A, double threshold,
-               DevCsr& out);
+               DevCsr& out, int ncols = -1);
 void spmv(cudaStream_t s, const DevCsr& A, const double* x, double* y);
 int reciprocal_diagonal(mclsgpu_context* ctx, const DevCsr& A, double* dinv);
 int block_jacobi(mclsgpu_context* ctx, const DevCsr& A, int bs, DevCsr& P);

@@ -466,18 +466,22 @@ void csr_scale_cols(mclsgpu_context* ctx, DevCsr& T, const double* sc) {
     k_scale_cols<<<grid_for(T.nnz), 256, 0, ctx->stream>>>(T.ci, T.v, T.nnz, sc);
 }
 
-int csr_filter(mclsgpu_context* ctx, const DevCsr& A, double threshold, DevCsr& out) {
+int csr_filter(mclsgpu_context* ctx, const DevCsr& A, double threshold, DevCsr& out,
+               int ncols) {
     // Filtering is a product with the identity: reuse the SpGEMM row builder
-    // with B = I so that the reference filter code path is shared.
+    // with B = I (ncols x ncols: A's columns index its rows) so that the
+    // reference filter code path is shared.
+    if (ncols < 0) ncols = A.n;
     DevCsr I;
-    I.n = A.n;
-    I.nnz = A.n;
+    I.n = ncols;
+    I.nnz = ncols;
     cudaError_t e;
     double* ones = nullptr;
-    if ((e = dmalloc(&ones, A.n)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
-    std::vector<double> h(A.n, 1.0);
-    cudaMemcpyAsync(ones, h.data(), A.n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
-    int rc = point_jacobi_csr(ctx, A.n, ones, I);
+    if ((e = dmalloc(&ones, ncols)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    std::vector<double> h(ncols, 1.0);
+    cudaMemcpyAsync(ones, h.data(), size_t(ncols) * sizeof(double), cudaMemcpyHostToDevice,
+                    ctx->stream);
+    int rc = point_jacobi_csr(ctx, ncols, ones, I);
     if (!rc) rc = csr_multiply(ctx, A, I, threshold, out);
     I.release();
     dfree(ones);

@@ -172,7 +172,7 @@ int mclsgpu_subdomain_build(mclsgpu_context* ctx, int64_t n_global, int32_t npar
     {
         DevCsr M, F;
         rc = upload_csr(ctx, sd->n, rowptr, colind, values, M, n_global);
-        if (!rc) rc = csr_filter(ctx, M, p->composite_threshold, F);
+        if (!rc) rc = csr_filter(ctx, M, p->composite_threshold, F, N);
         M.release();
         mclsgpu_domain& r = sd->recs;
         r.ctx = ctx;
