@@ -91,9 +91,12 @@ def test_small_outbox_is_reported(ctx):
 def test_partitioned_mc_drives_mcsa(ctx):
     # MCSA with the Monte Carlo correction from three parts: Richardson,
     # residual, partitioned correction, update; converges to the solution.
+    # (2D Poisson: the adjoint collision estimator's variance makes MCSA
+    # diverge on the strongly varying 3D coefficients, whole domain or not.)
     import torch
 
-    A, b = P.diffusion3d_varcoef(10, seed=5)
+    A = P.poisson2d(20)
+    b = np.ones(A.shape[0])
     n = A.shape[0]
     dinv = 1.0 / A.diagonal()
     parts = _parts(ctx, A, 3, 11)
@@ -110,4 +113,4 @@ def test_partitioned_mc_drives_mcsa(ctx):
         rp = dinv * (b - A @ x)
     assert np.linalg.norm(rp) <= crit
     xs = spla.spsolve(A.tocsc(), b)
-    assert np.linalg.norm(x - xs) <= 1e-5 * np.linalg.norm(xs)
+    assert np.linalg.norm(x - xs) <= 1e-6 * np.linalg.norm(xs)
