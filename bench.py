@@ -318,6 +318,60 @@ def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None):
             "rel_residual_b_minus_Ax": rel, "speedup_vs_jacobi_mcsa": jacobi_ms / ms}
 
 
+def partition_arm(args, ctx, A, b):
+    """One adjoint-collision Monte Carlo solve (FP32 packed records, the
+    Jacobi-preconditioned source) on the whole domain and on P row parts on
+    this GPU (domain-decomposed transport: rounds of walks with the crossing
+    histories handed between the parts).  Same histories, same transitions;
+    the difference is the cost of the rounds and the hand-over."""
+    import torch
+
+    from mcls_b200 import capi, partition
+
+    P = args.partition_parts
+    n = A.shape[0]
+    dinv = 1.0 / A.diagonal()
+    mc = dict(precision=capi.FP32, rng_mode=capi.RNG_COUNTER, direction=capi.ADJOINT,
+              estimator=capi.COLLISION, history_length=10, sample_ratio=1.0,
+              record_format=capi.RECORD_PACKED, seed=args.seed)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    dom = capi.Domain(ctx, op, pc, **mc)
+    rt = torch.tensor(dinv * b, device=ctx_device(), dtype=torch.float64)
+    xt = torch.zeros_like(rt)
+    T = partition.transposed_composite(A, dinv)
+    bounds = partition.row_bounds(n, P)
+    parts = [partition.DevicePart(capi.Subdomain(ctx, n, bounds, q, T[bounds[q]:bounds[q + 1]],
+                                                 params=capi.mc_params(**mc)),
+                                  n // P + n // 4 + 1024, ctx_device())
+             for q in range(P)]
+    whole_ms, part_ms, steps, rounds, moved = [], [], 0, 0, 0
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        st = dom.mc_solve_dev(rt.data_ptr(), xt.data_ptr(), internal=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xp, rounds, moved, steps = partition.solve_local(parts, rt)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            whole_ms.append(st["solve_ms"])
+            part_ms.append((time.perf_counter() - t0) * 1e3)
+    err = float((xp - xt).abs().max() / xt.abs().max())
+    wm, pm = sum(whole_ms) / len(whole_ms), sum(part_ms) / len(part_ms)
+    out = {"parts": P, "histories": int(st["histories"]), "walk_steps": int(steps),
+           "whole_ms": wm, "parts_ms": pm, "whole_steps_per_s": steps / (wm * 1e-3),
+           "parts_steps_per_s": steps / (pm * 1e-3), "rounds": rounds,
+           "histories_handed_over": moved, "max_rel_diff_vs_whole": err,
+           "timing": "whole: device time of the library call; parts: wall time of the "
+                     "host-driven rounds (synchronised)"}
+    for p in parts:
+        p.sub.close()
+    dom.close()
+    pc.close()
+    op.close()
+    return out
+
+
 def run_batched(args, world, rank, local, pg):
     """Batched workload: every step solves all (system, rhs) pairs to 1e-8."""
     import torch
@@ -499,6 +553,9 @@ def main():
     ap.add_argument("--anderson-depth", default="2,6",
                     help="Anderson storage depths to time, comma separated (NOX's default "
                          "is 2)")
+    ap.add_argument("--partition-parts", type=int, default=0,
+                    help="also time one Monte Carlo solve on this many row parts of the "
+                         "domain (domain-decomposed transport) against the whole domain")
     ap.add_argument("--learned-threshold", default="0",
                     help="Composite Operator Threshold(s) of the learned-SPAI domain, comma "
                          "separated: the first is the reported learned solve, the others a "
@@ -634,6 +691,8 @@ def main():
                      "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
         "wall_s": wall,
     }
+    if world == 1 and args.partition_parts > 1:
+        line["config"]["partitioned_mc"] = partition_arm(args, ctx, A, b)
     if world == 1 and not args.no_anderson:
         line["config"]["anderson"] = [
             anderson_arm(args, int(d), dom, bt, xt, A, b, seed, dev_ms_max / args.steps)

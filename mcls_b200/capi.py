@@ -528,6 +528,15 @@ class Domain:
                                                    C.byref(st)))
         return x, st.as_dict()
 
+    def mc_solve_dev(self, rhs_ptr, x_ptr, internal=False):
+        """Device-pointer Monte Carlo solve (mclsgpu_mc_solve_dev)."""
+        st = Stats()
+        st.size = C.sizeof(Stats)
+        self.ctx.check(self.ctx.L.mclsgpu_mc_solve_dev(self.h, C.c_void_p(rhs_ptr),
+                                                       C.c_void_p(x_ptr), int(internal),
+                                                       C.byref(st)))
+        return st.as_dict()
+
     def mc_trace(self, rhs, max_trace, internal=False):
         rhs = np.ascontiguousarray(rhs, np.float64)
         x = np.empty_like(rhs)
