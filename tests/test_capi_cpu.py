@@ -50,6 +50,13 @@ int main(void) {
   F(mclsgpu_mc_params, seed) F(mclsgpu_mc_params, rng_mode) F(mclsgpu_mc_params, precision)
   F(mclsgpu_mcsa_params, richardson_omega) F(mclsgpu_precond_params, rho_fallback)
   F(mclsgpu_stats, rho) F(mclsgpu_stats, walk_steps)
+  F(mclsgpu_mcsa_params, fixed_point_type)
+  printf("anderson %zu\\nwire %zu\\n", sizeof(mclsgpu_anderson_params),
+         sizeof(mclsgpu_history_wire));
+  F(mclsgpu_anderson_params, mixing) F(mclsgpu_anderson_params, drop_tolerance)
+  F(mclsgpu_anderson_params, host_loop)
+  F(mclsgpu_history_wire, state) F(mclsgpu_history_wire, step)
+  F(mclsgpu_history_wire, weight) F(mclsgpu_history_wire, id)
   return 0;
 }
 """)
@@ -69,6 +76,17 @@ int main(void) {
     assert int(out["mclsgpu_precond_params.rho_fallback"]) == capi.PrecondParams.rho_fallback.offset
     assert int(out["mclsgpu_stats.rho"]) == capi.Stats.rho.offset
     assert int(out["mclsgpu_stats.walk_steps"]) == capi.Stats.walk_steps.offset
+    assert int(out["mclsgpu_mcsa_params.fixed_point_type"]) == \
+        capi.McsaParams.fixed_point_type.offset
+    assert int(out["anderson"]) == C.sizeof(capi.AndersonParams)
+    for f in ("mixing", "drop_tolerance", "host_loop"):
+        assert int(out["mclsgpu_anderson_params." + f]) == getattr(capi.AndersonParams, f).offset
+    # The history record the partition driver moves between parts.
+    from mcls_b200 import partition
+
+    assert int(out["wire"]) == partition.WIRE_BYTES == capi.load().mclsgpu_history_wire_size()
+    for f in ("state", "step", "weight", "id"):
+        assert int(out["mclsgpu_history_wire." + f]) == partition.WIRE_DTYPE.fields[f][1]
 
 
 def test_rank_seed_matches_oracle():
@@ -86,6 +104,12 @@ def test_null_arguments_are_rejected_without_a_device():
     assert L.mclsgpu_mcsa_solve(None, None, None, None, None) == capi.ERR_INVALID_ARG
     assert L.mclsgpu_domain_build(None, None, None, None, None, None) == capi.ERR_INVALID_ARG
     assert L.mclsgpu_context_destroy(None) == capi.OK
+    assert L.mclsgpu_anderson_solve(None, None, None, None, None) == capi.ERR_INVALID_ARG
+    assert L.mclsgpu_fixed_point_solve(None, None, None, None, None, None, None,
+                                       None) == capi.ERR_INVALID_ARG
+    assert L.mclsgpu_subdomain_build(None, 0, 0, None, 0, None, None, None, None,
+                                     None) == capi.ERR_INVALID_ARG
+    assert L.mclsgpu_subdomain_destroy(None) == capi.OK
 
 
 def test_context_reports_missing_device():
