@@ -498,9 +498,20 @@ def cpu_baseline(cfg, A, b, seconds_target=15.0):
     # scale the sample to ~seconds_target of CPU work
     nh2 = int(min(1 << 26, nh * max(1.0, seconds_target / max(secs, 1e-3))))
     steps, secs, _ = mc.bench_walks(src, nh2, threads)
-    return {"value": steps / secs, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{nh2} adjoint histories x {c['history_length']} steps on the "
-                      f"{A.shape[0]}-row Jacobi domain, {secs:.1f} s"}
+    out = {"value": steps / secs, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"{nh2} adjoint histories x {c['history_length']} steps on the "
+                     f"{A.shape[0]}-row Jacobi domain, {secs:.1f} s"}
+    if cfg == "poisson100":
+        # The whole solve on one core, as one MPI rank of the reference runs
+        # it: MCSA to 1e-8 with FP64 adjoint collision walks.
+        t0 = time.perf_counter()
+        r = O.mcsa_solve(Ao, b, PL=O.point_jacobi(Ao), tolerance=1e-8, max_iters=20000,
+                         rng_mode=1, seed=1234, sample_ratio=c["sample_ratio"],
+                         history_length=c["history_length"])
+        out["mcsa_one_core"] = {"time_to_1e-8_s": time.perf_counter() - t0,
+                                "iterations": r["iters"], "converged": bool(r["converged"]),
+                                "walk_steps": int(r["steps"])}
+    return out
 
 
 def run_reference(args, world, rank, pg):
