@@ -51,3 +51,25 @@ def test_partitioned_walk_equals_whole_walk(tmp_path, world):
     assert np.allclose(x, whole, rtol=1e-15, atol=0)
     assert all(r["rounds"] == res[0]["rounds"] for r in res) and res[0]["rounds"] >= 3
     assert sum(r["sent"] for r in res) > 0
+
+
+def test_host_composite_rows_match_the_oracle():
+    # The host helper that forms a part's rows: (PL A)^T with point Jacobi,
+    # entry (i, j) = A_ji * (1 / A_jj), against the oracle's restatement of
+    # LinearProblem's composite operator (exact values, zeros aside).
+    import scipy.sparse as sp
+
+    from mcls_b200 import partition
+    from mcls_b200 import problems as P
+    from oracle import oracle as O
+
+    A, _ = P.diffusion3d_varcoef(6, seed=3)
+    T = partition.transposed_composite(A, 1.0 / A.diagonal())
+    Ao = O.Csr.from_scipy(A)
+    ref = O.composite(Ao, PL=O.point_jacobi(Ao), transpose_=True).to_scipy()
+    D = (T - ref).tocsr()
+    D.eliminate_zeros()
+    assert D.nnz == 0
+    b = partition.row_bounds(A.shape[0], 5)
+    assert b[0] == 0 and b[-1] == A.shape[0] and np.all(np.diff(b) > 0)
+    assert isinstance(T, sp.csr_matrix) and T.has_sorted_indices
