@@ -400,7 +400,9 @@ __global__ void k_aa_ctrl(AaState* st) {
 }
 
 // q_new = v / |v|, the post-add rotations, <F, q_j>; the last block solves
-// R gamma = Q^T F and forms beta R gamma.
+// R gamma = Q^T F and forms beta R gamma.  MD >= the storage depth bounds the
+// per-thread accumulators (registers, hence occupancy).
+template <int MD>
 __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
     __shared__ double sh[kThreads / 32];
     __shared__ bool last;
@@ -408,9 +410,9 @@ __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
     AaState* st = a.st;
     const int N = st->nstore, ok = st->ok, nc = st->newcol, nrot = st->nrot;
     const double inv = st->inv_rnn;
-    double acc[kMaxDepth];
+    double acc[MD];
 #pragma unroll
-    for (int j = 0; j < kMaxDepth; ++j) acc[j] = 0.0;
+    for (int j = 0; j < MD; ++j) acc[j] = 0.0;
     double* qn = a.Q + size_t(nc) * a.ld;
     for_elements(a.n, [&](auto wt, int i) {
         constexpr int W = decltype(wt)::value;
@@ -424,7 +426,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
         if (nrot) rotate_q<W>(a, st, nrot, i);
         const Vec<W> F = ldv<W>(a.F, i);
 #pragma unroll
-        for (int j = 0; j < kMaxDepth; ++j)
+        for (int j = 0; j < MD; ++j)
             if (j < N) {
                 const Vec<W> q = ldv<W>(a.Q + size_t(j) * a.ld, i);
 #pragma unroll
@@ -432,7 +434,7 @@ __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
             }
     });
 #pragma unroll
-    for (int j = 0; j < kMaxDepth; ++j) {
+    for (int j = 0; j < MD; ++j) {
         if (j < N) {  // N is the same in every thread of the block
             const double t = block_sum(acc[j], sh);
             if (threadIdx.x == 0) a.part[size_t(blockIdx.x) * kMaxDepth + j] = t;
@@ -468,34 +470,36 @@ __global__ void __launch_bounds__(kThreads) k_aa_rhs(Args a) {
 }
 
 // x_{k+1} = x_k + beta F - sum_j (gamma_j dX_j + (beta R gamma)_j q_j);
-// x_old = x_k, F_old = F.
+// x_old = x_k, F_old = F.  The coefficients and the ring slots of dX sit in
+// shared memory, so the thread keeps only its loads in flight.
 __global__ void __launch_bounds__(kThreads) k_aa_update(Args a) {
+    __shared__ double sg[kMaxDepth], srg[kMaxDepth];
+    __shared__ const double* sdx[kMaxDepth];
     const AaState* st = a.st;
-    const int N = st->nstore, head = st->dx_head, m = st->m;
+    const int N = st->nstore;
     const double beta = st->beta;
-    double g[kMaxDepth], rg[kMaxDepth];
-    const double* dx[kMaxDepth];
-#pragma unroll
-    for (int j = 0; j < kMaxDepth; ++j) {
-        g[j] = j < N ? st->gamma[j] : 0.0;
-        rg[j] = j < N ? st->rgamma[j] : 0.0;
-        dx[j] = j < N ? a.DX + size_t((head + j) % m) * a.ld : nullptr;
+    if (threadIdx.x < N) {
+        const int j = threadIdx.x;
+        sg[j] = st->gamma[j];
+        srg[j] = st->rgamma[j];
+        sdx[j] = a.DX + size_t((st->dx_head + j) % st->m) * a.ld;
     }
+    __syncthreads();
     for_elements(a.n, [&](auto wt, int i) {
         constexpr int W = decltype(wt)::value;
         const Vec<W> xv = ldv<W>(a.x, i), F = ldv<W>(a.F, i);
         Vec<W> w;
 #pragma unroll
         for (int e = 0; e < W; ++e) w.v[e] = __dmul_rn(beta, F.v[e]);
+#pragma unroll 4
+        for (int j = 0; j < N; ++j) {
+            const Vec<W> d = ldv<W>(sdx[j], i), q = ldv<W>(a.Q + size_t(j) * a.ld, i);
+            const double g = sg[j], rg = srg[j];
 #pragma unroll
-        for (int j = 0; j < kMaxDepth; ++j)
-            if (j < N) {
-                const Vec<W> d = ldv<W>(dx[j], i), q = ldv<W>(a.Q + size_t(j) * a.ld, i);
-#pragma unroll
-                for (int e = 0; e < W; ++e)
-                    w.v[e] = __dadd_rn(__dadd_rn(w.v[e], __dmul_rn(-g[j], d.v[e])),
-                                       __dmul_rn(-rg[j], q.v[e]));
-            }
+            for (int e = 0; e < W; ++e)
+                w.v[e] = __dadd_rn(__dadd_rn(w.v[e], __dmul_rn(-g, d.v[e])),
+                                   __dmul_rn(-rg, q.v[e]));
+        }
         Vec<W> xn;
 #pragma unroll
         for (int e = 0; e < W; ++e) xn.v[e] = __dadd_rn(xv.v[e], w.v[e]);
@@ -697,7 +701,12 @@ void enqueue_accel(mclsgpu_domain* dom, const mclsgpu_anderson_params* p, const 
     if (p->storage_depth > 0) {
         for (int j = 1; j < p->storage_depth; ++j) k_aa_mgs<<<w->grid, kThreads, 0, s>>>(a, j);
         k_aa_ctrl<<<1, 1, 0, s>>>(w->st);
-        k_aa_rhs<<<w->grid, kThreads, 0, s>>>(a);
+        if (p->storage_depth <= 4)
+            k_aa_rhs<4><<<w->grid, kThreads, 0, s>>>(a);
+        else if (p->storage_depth <= 8)
+            k_aa_rhs<8><<<w->grid, kThreads, 0, s>>>(a);
+        else
+            k_aa_rhs<kMaxDepth><<<w->grid, kThreads, 0, s>>>(a);
     }
     k_aa_update<<<w->grid, kThreads, 0, s>>>(a);
     prec_residual(dom, dom->x, dom->b, dom->rp);
