@@ -247,11 +247,15 @@ int mclsgpu_operator_upload(mclsgpu_context* ctx, int64_t n, const int64_t* rowp
     if (!rc && K > 0 && double(K) * op->A.n <= 1.25 * op->A.nnz + op->A.n) {
         rc = csr_to_dia(ctx, op->A, K, op->dia_off, &op->dia_val);
         if (!rc) op->dia_k = K;
+        if (!rc && K <= 9)
+            rc = dia_symmetric(ctx, op->A.n, K, op->dia_off, op->dia_val, &op->sym_val,
+                               &op->sym_h, op->sym_off);
     }
     if (rc) {
         op->A.release();
         op->S.release();
         dfree(op->dia_val);
+        dfree(op->sym_val);
         delete op;
         return rc;
     }
@@ -265,6 +269,7 @@ int mclsgpu_operator_destroy(mclsgpu_operator* op) {
     op->AT.release();
     op->S.release();
     dfree(op->dia_val);
+    dfree(op->sym_val);
     dfree(op->dinv);
     delete op;
     return MCLSGPU_OK;

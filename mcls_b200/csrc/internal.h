@@ -74,6 +74,12 @@ struct mclsgpu_operator {
     int dia_k = 0;
     int dia_off[16] = {0};
     double* dia_val = nullptr;
+    // Symmetric stencil operators (A(r, r - o) == A(r - o, r) for every offset)
+    // also keep the diagonal and the positive-offset diagonals only:
+    // sym_val[0 * n + r] = A(r, r), sym_val[(1 + h) * n + r] = A(r, r + sym_off[h]).
+    int sym_h = 0;
+    int sym_off[8] = {0};
+    double* sym_val = nullptr;
     double* dinv = nullptr;       // reciprocal diagonal (built on demand)
     mclsgpu::DevCsr AT;           // A^T (built on demand: RNSD iterations)
     uint64_t serial = 0;          // identity for "operator changed" checks
@@ -228,6 +234,11 @@ int collect_offsets(mclsgpu_context* ctx, const DevCsr& A, int max_k, int* offse
 // Diagonal-offset values of a stencil matrix (K offsets): val[j*n + r].
 int csr_to_dia(mclsgpu_context* ctx, const DevCsr& A, int K, const int* offsets,
                double** val);
+// The diagonal and positive-offset diagonals of a DIA matrix whose K offsets
+// are symmetric about 0 and whose values are (bit for bit) symmetric; *kh = 0
+// and no allocation otherwise.
+int dia_symmetric(mclsgpu_context* ctx, int n, int K, const int* offsets, const double* val,
+                  double** sym, int* kh, int* sym_off);
 // y = A x over a SELL-32 matrix.
 void sell_spmv(cudaStream_t s, const DevSell& A, const double* x, double* y);
 // Exclusive scan of set-up counts into rp[0..n]; *total = sum.

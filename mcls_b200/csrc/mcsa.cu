@@ -93,6 +93,34 @@ struct DiaViewT {
 };
 using DiaView = DiaViewT<0>;
 
+// Symmetric stencil operator (A(r, r - o) == A(r - o, r)): only the diagonal
+// and the H positive-offset diagonals are read; A(r, r - o_h) is taken as
+// A(r - o_h, r).  The products are the same as DiaViewT's, in the same
+// (ascending column) order, so the sums are bit for bit the same with
+// (1 + H) / (1 + 2H) of the matrix bytes.
+template <int H>
+struct DiaSymView {
+    const double* val;  // [(1 + H) * n]: diagonal, then positive offsets ascending
+    int n;
+    int off[H];
+    template <class F>
+    __device__ __forceinline__ double dot(int r, F f) const {
+        double s = 0.0;
+#pragma unroll
+        for (int h = H - 1; h >= 0; --h) {
+            const int c = r - off[h];
+            if (c >= 0) s = fma(val[size_t(1 + h) * n + c], f(c), s);
+        }
+        s = fma(val[r], f(r), s);
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const int c = r + off[h];
+            if (c < n) s = fma(val[size_t(1 + h) * n + r], f(c), s);
+        }
+        return s;
+    }
+};
+
 // rp = (b - A x) [* dinv]   (LinearProblem::updatePrecResidual, :410-442)
 template <class Op>
 __global__ void __launch_bounds__(256) k_residual(Op A, const double* x, const double* b,
@@ -377,6 +405,15 @@ static SellView sell_view(const mclsgpu_operator* op) {
     return SellView{op->S.off, op->S.col, op->S.val, op->S.n};
 }
 
+template <int H>
+static DiaSymView<H> sym_view(const mclsgpu_operator* op) {
+    DiaSymView<H> v{};
+    v.val = op->sym_val;
+    v.n = op->A.n;
+    for (int h = 0; h < H; ++h) v.off[h] = op->sym_off[h];
+    return v;
+}
+
 template <int KK>
 static DiaViewT<KK> dia_view(const mclsgpu_operator* op) {
     DiaViewT<KK> v{};
@@ -417,8 +454,9 @@ static DiaViewT<KK> dia_view_vals(const mclsgpu_operator* op, const double* vals
     } while (0)
 
 // Launch `kern<Op>` on the operator's fastest layout: diagonal-offset values
-// for stencil operators (unrolled for the 5-, 7- and 9-point stencils),
-// SELL-32 otherwise.
+// for stencil operators (unrolled for the 5-, 7- and 9-point stencils; only
+// the diagonal and upper diagonals when the values are symmetric), SELL-32
+// otherwise.
 #define MCLSGPU_LAUNCH_OP(op, grid, threads, stream, kern, ...)                              \
     do {                                                                                     \
         switch ((op)->dia_k) {                                                               \
@@ -426,13 +464,28 @@ static DiaViewT<KK> dia_view_vals(const mclsgpu_operator* op, const double* vals
                 kern<SellView><<<grid, threads, 0, stream>>>(sell_view(op), __VA_ARGS__);    \
                 break;                                                                       \
             case 5:                                                                          \
-                kern<DiaViewT<5>><<<grid, threads, 0, stream>>>(dia_view<5>(op), __VA_ARGS__); \
+                if ((op)->sym_h == 2)                                                        \
+                    kern<DiaSymView<2>><<<grid, threads, 0, stream>>>(sym_view<2>(op),        \
+                                                                      __VA_ARGS__);          \
+                else                                                                         \
+                    kern<DiaViewT<5>><<<grid, threads, 0, stream>>>(dia_view<5>(op),          \
+                                                                    __VA_ARGS__);            \
                 break;                                                                       \
             case 7:                                                                          \
-                kern<DiaViewT<7>><<<grid, threads, 0, stream>>>(dia_view<7>(op), __VA_ARGS__); \
+                if ((op)->sym_h == 3)                                                        \
+                    kern<DiaSymView<3>><<<grid, threads, 0, stream>>>(sym_view<3>(op),        \
+                                                                      __VA_ARGS__);          \
+                else                                                                         \
+                    kern<DiaViewT<7>><<<grid, threads, 0, stream>>>(dia_view<7>(op),          \
+                                                                    __VA_ARGS__);            \
                 break;                                                                       \
             case 9:                                                                          \
-                kern<DiaViewT<9>><<<grid, threads, 0, stream>>>(dia_view<9>(op), __VA_ARGS__); \
+                if ((op)->sym_h == 4)                                                        \
+                    kern<DiaSymView<4>><<<grid, threads, 0, stream>>>(sym_view<4>(op),        \
+                                                                      __VA_ARGS__);          \
+                else                                                                         \
+                    kern<DiaViewT<9>><<<grid, threads, 0, stream>>>(dia_view<9>(op),          \
+                                                                    __VA_ARGS__);            \
                 break;                                                                       \
             default:                                                                         \
                 kern<DiaView><<<grid, threads, 0, stream>>>(dia_view<0>(op), __VA_ARGS__);   \

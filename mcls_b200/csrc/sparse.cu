@@ -622,7 +622,61 @@ __global__ void k_fill_dia(const int* rp, const int* ci, const double* v, int n,
     }
 }
 
+// Symmetry of a diagonal pair: val[jneg][r] == val[jpos][r - o] bit for bit
+// (A(r, r - o) == A(r - o, r)); rows without the column hold 0.
+__global__ void k_dia_symmetric(const double* val, int n, int jneg, int jpos, int o, int* bad) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const double a = val[size_t(jneg) * n + r];
+        const double b = r >= o ? val[size_t(jpos) * n + r - o] : 0.0;
+        if (__double_as_longlong(a) != __double_as_longlong(b)) atomicOr(bad, 1);
+    }
+}
+
 }  // namespace
+
+int dia_symmetric(mclsgpu_context* ctx, int n, int K, const int* offsets, const double* val,
+                  double** sym, int* kh, int* sym_off) {
+    *sym = nullptr;
+    *kh = 0;
+    // Offsets -o_h < ... < -o_1 < 0 < o_1 < ... < o_h (ascending).
+    if (K < 3 || (K & 1) == 0 || offsets[K / 2] != 0) return MCLSGPU_OK;
+    const int H = K / 2;
+    for (int h = 0; h < H; ++h)
+        if (offsets[K / 2 + 1 + h] <= 0 || offsets[K / 2 - 1 - h] != -offsets[K / 2 + 1 + h])
+            return MCLSGPU_OK;
+    cudaStream_t s = ctx->stream;
+    int* bad = nullptr;
+    cudaError_t e = dmalloc(&bad, 1);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    cudaMemsetAsync(bad, 0, sizeof(int), s);
+    for (int h = 0; h < H; ++h) {
+        const int jpos = K / 2 + 1 + h, jneg = K / 2 - 1 - h;
+        k_dia_symmetric<<<grid_for(n), 256, 0, s>>>(val, n, jneg, jpos, offsets[jpos], bad);
+    }
+    int hb = 1;
+    cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    dfree(bad);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "DIA symmetry");
+    if (hb) return MCLSGPU_OK;
+    // Diagonal first, then the positive offsets in ascending order.
+    if ((e = dmalloc(sym, size_t(1 + H) * n)) != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaMalloc symmetric DIA");
+    cudaMemcpyAsync(*sym, val + size_t(K / 2) * n, size_t(n) * sizeof(double),
+                    cudaMemcpyDeviceToDevice, s);
+    for (int h = 0; h < H; ++h) {
+        cudaMemcpyAsync(*sym + size_t(1 + h) * n, val + size_t(K / 2 + 1 + h) * n,
+                        size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        sym_off[h] = offsets[K / 2 + 1 + h];
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        dfree(*sym);
+        return cuda_fail(ctx, e, "symmetric DIA");
+    }
+    *kh = H;
+    return MCLSGPU_OK;
+}
 
 int csr_to_dia(mclsgpu_context* ctx, const DevCsr& A, int K, const int* offsets, double** val) {
     *val = nullptr;

@@ -392,3 +392,31 @@ def test_smoother_steps_and_relaxation(ctx):
     assert st["converged"] == 1
     Dinv = 1.0 / A.diagonal()
     assert np.linalg.norm(Dinv * (b - A @ x)) <= 1e-8 * np.linalg.norm(Dinv * b) * 1.0001
+
+
+@pytest.mark.parametrize("name", ["tridiag", "poisson2d", "varcoef3d", "aniso9pt", "nonsym"])
+def test_stencil_residual_is_bitwise_the_csr_one(ctx, name):
+    # The MCSA residual kernels read a symmetric stencil operator through its
+    # diagonal and upper diagonals only (the lower ones are the upper ones'
+    # mirror); the sums must equal the CSR product's bit for bit, with the
+    # full diagonal layout for a nonsymmetric operator.
+    import torch
+
+    systems = _systems()
+    if name == "nonsym":
+        A = sp.csr_matrix(P.poisson2d(9) + 0.1 * sp.eye(81, k=1))
+    else:
+        A = systems[name][0]
+    n = A.shape[0]
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n)
+    b = rng.standard_normal(n)
+    dom, op, pc = _gpu_domain(ctx, A, "jacobi", precision=capi.FP32)
+    bt = torch.tensor(b, device="cuda:0")
+    xt = torch.tensor(x, device="cuda:0")
+    rp = torch.empty_like(bt)
+    dom.mcsa_begin(bt.data_ptr(), xt.data_ptr(), tolerance=1e-8)
+    dom.residual(rp.data_ptr())
+    dom.mcsa_finish(xt.data_ptr())
+    ref = (1.0 / A.diagonal()) * (b - op.apply(x))
+    assert np.array_equal(rp.cpu().numpy(), ref)
