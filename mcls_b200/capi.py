@@ -271,6 +271,17 @@ def load(path: str = LIB_PATH):
     return L
 
 
+def _torch_ready():
+    """Device vectors handed to the library are often torch tensors written by
+    kernels on torch's current stream; the library works on its own
+    non-blocking stream, so wait for torch's stream first."""
+    import sys
+
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.current_stream().synchronize()
+
+
 def _ptr(a):
     return a.ctypes.data if a is not None else None
 
@@ -510,6 +521,7 @@ class Domain:
 
     def autotune(self, rhs_dev_ptr, reps=3):
         """Pick the fastest FP32 walk launch shape on a device right-hand side."""
+        _torch_ready()
         hpl, blk, ms = C.c_int(), C.c_int(), C.c_double()
         self.ctx.check(self.ctx.L.mclsgpu_domain_autotune(self.h, C.c_void_p(rhs_dev_ptr), reps,
                                                           C.byref(hpl), C.byref(blk),
@@ -530,6 +542,7 @@ class Domain:
 
     def mc_solve_dev(self, rhs_ptr, x_ptr, internal=False):
         """Device-pointer Monte Carlo solve (mclsgpu_mc_solve_dev)."""
+        _torch_ready()
         st = Stats()
         st.size = C.sizeof(Stats)
         self.ctx.check(self.ctx.L.mclsgpu_mc_solve_dev(self.h, C.c_void_p(rhs_ptr),
@@ -565,6 +578,7 @@ class Domain:
 
     def mcsa_solve_dev(self, b_ptr, x_ptr, params: McsaParams | None = None, **kw):
         """Device-pointer variant (e.g. torch tensors' data_ptr())."""
+        _torch_ready()
         p = params if params is not None else mcsa_params(**kw)
         st = Stats()
         st.size = C.sizeof(Stats)
@@ -585,6 +599,7 @@ class Domain:
         return x, st.as_dict()
 
     def anderson_solve_dev(self, b_ptr, x_ptr, params: AndersonParams | None = None, **kw):
+        _torch_ready()
         p = params if params is not None else anderson_params(**kw)
         st = Stats()
         st.size = C.sizeof(Stats)
@@ -595,6 +610,7 @@ class Domain:
 
     def anderson_begin(self, b_ptr, x0_ptr, params: AndersonParams | None = None, **kw):
         """Step-wise Anderson MCSA: (|PL (b - A x0)|_2, |b|_2, done)."""
+        _torch_ready()
         p = params if params is not None else anderson_params(**kw)
         rn, bn, done = C.c_double(), C.c_double(), C.c_int32()
         self.ctx.check(self.ctx.L.mclsgpu_anderson_begin(self.h, C.c_void_p(b_ptr),
@@ -604,16 +620,19 @@ class Domain:
         return rn.value, bn.value, bool(done.value)
 
     def anderson_correction(self, delta_ptr):
+        _torch_ready()
         self.ctx.check(self.ctx.L.mclsgpu_anderson_correction(self.h, C.c_void_p(delta_ptr)))
 
     def anderson_apply(self, delta_ptr, scale=1.0):
         """Returns (|PL (b - A x)|_2 after the step, done)."""
+        _torch_ready()
         rn, done = C.c_double(), C.c_int32()
         self.ctx.check(self.ctx.L.mclsgpu_anderson_apply(self.h, C.c_void_p(delta_ptr), scale,
                                                          C.byref(rn), C.byref(done)))
         return rn.value, bool(done.value)
 
     def anderson_finish(self, x_ptr):
+        _torch_ready()
         st = Stats()
         st.size = C.sizeof(Stats)
         self.ctx.check(self.ctx.L.mclsgpu_anderson_finish(self.h, C.c_void_p(x_ptr),
@@ -622,6 +641,7 @@ class Domain:
 
     def mcsa_begin(self, b_ptr, x0_ptr, params: McsaParams | None = None, **kw):
         """Step-wise MCSA: initial residual; returns (|rp|_2, |PL b|_2)."""
+        _torch_ready()
         p = params if params is not None else mcsa_params(**kw)
         rn, bn = C.c_double(), C.c_double()
         self.ctx.check(self.ctx.L.mclsgpu_mcsa_begin(self.h, C.c_void_p(b_ptr), C.c_void_p(x0_ptr),
@@ -629,15 +649,18 @@ class Domain:
         return rn.value, bn.value
 
     def mcsa_correction(self, delta_ptr):
+        _torch_ready()
         self.ctx.check(self.ctx.L.mclsgpu_mcsa_correction(self.h, C.c_void_p(delta_ptr)))
 
     def mcsa_apply(self, delta_ptr, scale=1.0):
+        _torch_ready()
         rn = C.c_double()
         self.ctx.check(self.ctx.L.mclsgpu_mcsa_apply(self.h, C.c_void_p(delta_ptr), scale,
                                                      C.byref(rn)))
         return rn.value
 
     def mcsa_finish(self, x_ptr):
+        _torch_ready()
         st = Stats()
         st.size = C.sizeof(Stats)
         self.ctx.check(self.ctx.L.mclsgpu_mcsa_finish(self.h, C.c_void_p(x_ptr), C.byref(st)))
@@ -645,6 +668,7 @@ class Domain:
 
     def residual(self, rp_dev_ptr):
         """Copy the last MCSA solve's preconditioned residual to a device vector."""
+        _torch_ready()
         self.ctx.check(self.ctx.L.mclsgpu_domain_residual(self.h, C.c_void_p(rp_dev_ptr)))
 
     def spectral_radius(self, which=0, max_iters=2000, tol=1e-8, seed=7):
@@ -699,6 +723,7 @@ class SpaiNet:
 
     def gradient(self, op: Operator, v_dev_ptr, nvec):
         """(loss, FP32 parameter gradient) for nvec device vectors."""
+        _torch_ready()
         loss = C.c_double()
         g = np.empty(self.nparams, np.float32)
         self.ctx.check(self.ctx.L.mclsgpu_spai_gradient(self.h, op.h, C.c_void_p(v_dev_ptr), nvec,
@@ -707,6 +732,7 @@ class SpaiNet:
 
     def train_step(self, op: Operator, v_dev_ptr, nvec, lr=1e-3, beta1=0.9, beta2=0.999,
                    eps=1e-8, grad_clip=0.0):
+        _torch_ready()
         a = SpaiAdam()
         a.size = C.sizeof(SpaiAdam)
         a.lr, a.beta1, a.beta2, a.eps, a.grad_clip = lr, beta1, beta2, eps, grad_clip
@@ -717,6 +743,7 @@ class SpaiNet:
 
     def smooth_vectors(self, op: Operator, v_dev_ptr, nvec, iters):
         """In place: iters applications of I - M A (normalised) to each vector."""
+        _torch_ready()
         self.ctx.check(self.ctx.L.mclsgpu_spai_smooth_vectors(self.h, op.h, C.c_void_p(v_dev_ptr),
                                                               nvec, iters))
 
@@ -790,6 +817,7 @@ class Batch:
         self.ctx.check(self.ctx.L.mclsgpu_batch_set_launch(self.h, block_size))
 
     def autotune(self, b_ptr, x_ptr, reps=3):
+        _torch_ready()
         blk, ms = C.c_int(), C.c_double()
         self.ctx.check(self.ctx.L.mclsgpu_batch_autotune(self.h, C.c_void_p(b_ptr),
                                                          C.c_void_p(x_ptr), reps, C.byref(blk),
@@ -800,6 +828,7 @@ class Batch:
         """Solve in place on device [rows, width] arrays; returns (stats,
         per-pair convergence iterations [nsys, width], final relative
         preconditioned residuals [nsys, width])."""
+        _torch_ready()
         p = params if params is not None else mcsa_params(**kw)
         st = Stats()
         st.size = C.sizeof(Stats)
@@ -849,6 +878,7 @@ class Subdomain:
 
     def begin(self, rhs_ptr):
         """Returns (histories starting in this part, histories in the solve)."""
+        _torch_ready()
         ns, nt = C.c_int64(), C.c_int64()
         self.ctx.check(self.ctx.L.mclsgpu_subdomain_begin(self.h, C.c_void_p(rhs_ptr),
                                                           C.byref(ns), C.byref(nt)))
@@ -856,6 +886,7 @@ class Subdomain:
 
     def transport(self, inbox_ptr, n_in, outbox_ptr, capacity):
         """One round; returns the departures per destination part."""
+        _torch_ready()
         counts = np.zeros(self.nparts, np.int64)
         self.ctx.check(self.ctx.L.mclsgpu_subdomain_transport(
             self.h, C.c_void_p(inbox_ptr) if inbox_ptr else None, n_in, C.c_void_p(outbox_ptr),
@@ -863,6 +894,7 @@ class Subdomain:
         return counts
 
     def finish(self, x_ptr):
+        _torch_ready()
         st = Stats()
         st.size = C.sizeof(Stats)
         self.ctx.check(self.ctx.L.mclsgpu_subdomain_finish(self.h, C.c_void_p(x_ptr),

@@ -53,18 +53,21 @@ def test_anderson_follows_oracle_on_reference_stream(ctx, aa):
 
 
 def test_anderson_jacobi_poisson_follows_oracle(ctx):
-    # The first steps follow the oracle's; over tens of steps the rounding
-    # of atomically summed tallies can move a sampled source state, after
-    # which the two runs are independent samples of the same solve.
+    # The first steps follow the oracle's.  The least-squares fits amplify
+    # the last-bit differences of atomically summed tallies from step to
+    # step, so within a few more steps a history count or a sampled source
+    # state can change, after which the two runs are independent samples of
+    # the same solve: they still reach the same solution.
     A = P.poisson2d(9)
     b = np.linspace(0.5, 1.5, 81)
-    x, st, r = _parity_pair(ctx, A, b, True, 99, tolerance=0.0, max_iters=8, storage_depth=3)
-    assert st["iterations"] == r["iters"] == 8
+    x, st, r = _parity_pair(ctx, A, b, True, 99, tolerance=0.0, max_iters=3, storage_depth=3)
+    assert st["iterations"] == r["iters"] == 3
     assert np.allclose(x, r["x"], rtol=1e-7, atol=1e-12 * np.abs(r["x"]).max())
     x, st, r = _parity_pair(ctx, A, b, True, 99, tolerance=1e-8, max_iters=200,
                             storage_depth=3)
     assert st["converged"] == 1 and r["converged"]
     assert abs(st["iterations"] - r["iters"]) <= 5
+    assert np.allclose(x, r["x"], rtol=1e-6, atol=0)
 
 
 @pytest.mark.parametrize("direction", [capi.ADJOINT, capi.FORWARD])
