@@ -67,7 +67,8 @@ def test_anderson_jacobi_poisson_follows_oracle(ctx):
                             storage_depth=3)
     assert st["converged"] == 1 and r["converged"]
     assert abs(st["iterations"] - r["iters"]) <= 5
-    assert np.allclose(x, r["x"], rtol=1e-6, atol=0)
+    # independent runs stopped at |PL r| < 1e-8 |b| differ by about 2e-6 here
+    assert np.allclose(x, r["x"], rtol=1e-5, atol=0)
 
 
 @pytest.mark.parametrize("direction", [capi.ADJOINT, capi.FORWARD])
