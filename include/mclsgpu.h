@@ -13,6 +13,10 @@
  * Threading: one context owns one CUDA stream; calls on one context must be
  * serialised by the caller (the reference is single-threaded per rank).
  * Distinct contexts may be used from distinct host threads.
+ * Streams: the context's stream does not wait for the legacy default stream,
+ * so device vectors given to the *_dev entry points must be complete when
+ * the call is made (synchronise the stream that wrote them); every call
+ * returns after its own work has finished, so its outputs are complete.
  * Ownership: host arrays are borrowed for the duration of a call and copied;
  * the *_dev variants borrow caller device memory for the duration of the
  * call.  Handles are owned by the caller and released with *_destroy.
