@@ -8,6 +8,7 @@
   tpetra/test/tstTpetraDomainTransporter.cpp:97-172 (Cutoff),
   tpetra/test/tstTpetraAdjointTally.cpp:83-167 (normalize),
   tpetra/test/tstTpetraUniformAdjointSource.cpp:75-161 (counts, weight),
+  tpetra/test/tstTpetraUniformForwardSource.cpp:75-260 (counts, weight 1),
   tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations),
   tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345 (Richardson: 15
   iterations, solution sign).
@@ -125,6 +126,29 @@ def test_adjoint_source_counts_and_weight():
     assert np.all(tr["start"] >= 1)
     W = d["weights"][tr["start"]]
     assert np.all(tr["final_weight"] == -float(n) * W)
+
+
+@pytest.mark.parametrize("mult", [1, 10])
+def test_forward_source_counts_and_weight(mult):
+    # tstTpetraUniformForwardSource nh_not_set / nh_set: Sample Ratio = mult
+    # gives mult * N histories, mult starting in every state, each of weight
+    # 1 (the forward source does not scale by |b|_1).  History Length 1: the
+    # final weight is W_i times the sign of the one transition's entry.  The
+    # reference builds its forward domain from A^T; the forward oracle walks
+    # the rows of the operator it is given, so it is given A^T.
+    n = 10
+    A = sp.lil_matrix((n, n))
+    for i in range(1, n):
+        A[i, i - 1] = -0.5
+    A[n - 1, n - 1] = -0.5
+    mc = O.MC(O.Csr.from_scipy(sp.csr_matrix(A.T)), history_length=1, direction=1,
+              sample_ratio=float(mult))
+    x, nh, tr = mc.solve(np.full(n, -1.0), trace=mult * n)
+    assert nh == mult * n
+    assert np.array_equal(np.bincount(tr["start"], minlength=n), np.full(n, mult))
+    d = mc.domain()
+    W = d["weights"][tr["start"]]
+    assert np.allclose(np.abs(tr["final_weight"]), W, rtol=0, atol=0)
 
 
 @pytest.mark.parametrize("b", [-1.0, 2.0, -2.0])
