@@ -9,6 +9,7 @@
   tpetra/test/tstTpetraAdjointTally.cpp:83-167 (normalize),
   tpetra/test/tstTpetraUniformAdjointSource.cpp:75-161 (counts, weight),
   tpetra/test/tstTpetraUniformForwardSource.cpp:75-260 (counts, weight 1),
+  tpetra/test/tstTpetraForwardTally.cpp:83-235 (tally, finalize, normalize),
   tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations),
   tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345 (Richardson: 15
   iterations, solution sign).
@@ -149,6 +150,25 @@ def test_forward_source_counts_and_weight(mult):
     d = mc.domain()
     W = d["weights"][tr["start"]]
     assert np.allclose(np.abs(tr["final_weight"]), W, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 4])
+def test_forward_tally_known_answer(L):
+    # tstTpetraForwardTally TallyHistory / Normalize: a history tallies
+    # weight x b at each state it visits before its cutoff, the sum goes to
+    # its starting state, finalize divides by the histories per state and
+    # normalize leaves the forward result alone.  A = 2 I gives H = -I
+    # (W = 1, every transition flips the sign and stays put), so L steps
+    # give x = sum_{k<L} (-1)^k b: b for odd L, 0 for even L.
+    n = 8
+    A = sp.csr_matrix(2.0 * sp.identity(n))
+    b = np.linspace(-1.0, 2.0, n)
+    for ratio in (1.0, 3.0):
+        mc = O.MC(O.Csr.from_scipy(A), history_length=L, direction=1, sample_ratio=ratio)
+        x, nh = mc.solve(b)
+        assert nh == int(ratio) * n
+        # sum / count: exact for one history per state, one rounding for 3
+        assert np.allclose(x, b if L % 2 else np.zeros(n), rtol=1e-15, atol=0)
 
 
 @pytest.mark.parametrize("b", [-1.0, 2.0, -2.0])
