@@ -45,6 +45,7 @@ class AndersonSolverManager : public SolverManager<Vector, Matrix> {
     }
 
     const LinearProblem<Vector, Matrix>& getProblem() const override { return *d_problem; }
+    std::string description() const override { return std::string(std::is_same<MonteCarloTag, ForwardTag>::value ? "Forward" : "Adjoint") + " Anderson (GPU)"; }
 
     // The Monte Carlo keys and the loop's own (the reference returns an empty
     // list here, :113-121).

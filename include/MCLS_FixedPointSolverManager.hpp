@@ -33,6 +33,7 @@ class FixedPointSolverManager : public SolverManager<Vector, Matrix> {
     }
 
     const LinearProblem<Vector, Matrix>& getProblem() const override { return *d_problem; }
+    std::string description() const override { return std::string("Fixed Point (GPU)"); }
 
     // src/MCLS_FixedPointSolverManager_impl.hpp:106-126 (with the
     // Richardson iteration's "Richardson Relaxation").

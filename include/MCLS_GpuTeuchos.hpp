@@ -6,8 +6,9 @@
 // used.  Otherwise this header supplies a small stand-in with the same
 // spelling for what user code of the managers touches: RCP / rcp / null /
 // nonnull / is_null, ParameterList (set, get, get-with-default,
-// isParameter, isType, setParameters), parameterList(), ScalarTraits,
-// Describable, as<>, and a serial Comm<int>.
+// isParameter, isType, sublist, setParameters, validateParameters and
+// validateParametersAndSetDefaults without validators), parameterList(),
+// sublist(), ScalarTraits, Describable, as<>, and a serial Comm<int>.
 #ifndef MCLS_GPUTEUCHOS_HPP
 #define MCLS_GPUTEUCHOS_HPP
 
@@ -89,6 +90,9 @@ struct InvalidParameterName : InvalidParameter {
 struct InvalidParameterType : InvalidParameter {
     using InvalidParameter::InvalidParameter;
 };
+struct InvalidParameterValue : InvalidParameter {
+    using InvalidParameter::InvalidParameter;
+};
 }  // namespace Exceptions
 
 // Name -> typed value map.  Typing is strict as in Teuchos: get<int> on an
@@ -161,7 +165,49 @@ class ParameterList {
     int numParams() const { return static_cast<int>(names_.size()); }
     const std::vector<std::string>& names() const { return names_; }
 
+    // Every entry must be named in `valid` with the same type
+    // (InvalidParameterName / InvalidParameterType otherwise); sublists
+    // present in both lists are checked `depth` levels further down.
+    void validateParameters(const ParameterList& valid, int depth = 1000) const {
+        for (const auto& k : names_) {
+            const std::any& a = entries_.at(k);
+            const std::any& v = valid.checked(name_, k, a);
+            if (depth > 0 && a.type() == typeid(ParameterList))
+                std::any_cast<const ParameterList&>(a).validateParameters(
+                    std::any_cast<const ParameterList&>(v), depth - 1);
+        }
+    }
+    // validateParameters, then copies in every entry of `valid` missing here
+    // (a missing sublist arrives whole, with all its defaults).
+    void validateParametersAndSetDefaults(const ParameterList& valid, int depth = 1000) {
+        for (const auto& k : names_) {
+            std::any& a = entries_.at(k);
+            const std::any& v = valid.checked(name_, k, a);
+            if (depth > 0 && a.type() == typeid(ParameterList))
+                std::any_cast<ParameterList&>(a).validateParametersAndSetDefaults(
+                    std::any_cast<const ParameterList&>(v), depth - 1);
+        }
+        for (const auto& k : valid.names_)
+            if (!isParameter(k)) {
+                entries_[k] = valid.entries_.at(k);
+                order(k);
+            }
+    }
+
   private:
+    // The entry of this (valid) list that `value`, named `key` in the list
+    // `owner`, must match by name and type.
+    const std::any& checked(const std::string& owner, const std::string& key,
+                            const std::any& value) const {
+        auto it = entries_.find(key);
+        if (it == entries_.end())
+            throw Exceptions::InvalidParameterName("ParameterList '" + owner + "': parameter \"" +
+                                                   key + "\" is not a valid parameter");
+        if (it->second.type() != value.type())
+            throw Exceptions::InvalidParameterType("ParameterList '" + owner + "': parameter \"" +
+                                                   key + "\" has the wrong type");
+        return it->second;
+    }
     std::any& find(const std::string& key) {
         auto it = entries_.find(key);
         if (it == entries_.end())
@@ -191,6 +237,14 @@ class ParameterList {
 inline RCP<ParameterList> parameterList() { return RCP<ParameterList>(new ParameterList); }
 inline RCP<ParameterList> parameterList(const std::string& name) {
     return RCP<ParameterList>(new ParameterList(name));
+}
+// Handle to the sublist `name` of `parent` that keeps `parent` alive.
+inline RCP<ParameterList> sublist(const RCP<ParameterList>& parent, const std::string& name,
+                                  bool mustAlreadyExist = false) {
+    if (mustAlreadyExist && !parent->isSublist(name))
+        throw Exceptions::InvalidParameterName("ParameterList '" + parent->name() +
+                                               "': no sublist \"" + name + "\"");
+    return RCP<ParameterList>(std::shared_ptr<ParameterList>(parent, &parent->sublist(name)));
 }
 
 // Serial communicator: one process, rank 0.

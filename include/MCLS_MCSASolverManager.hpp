@@ -40,6 +40,7 @@ class MCSASolverManager : public SolverManager<Vector, Matrix> {
     }
 
     const LinearProblem<Vector, Matrix>& getProblem() const override { return *d_problem; }
+    std::string description() const override { return std::string(std::is_same<MonteCarloTag, ForwardTag>::value ? "Forward" : "Adjoint") + " MCSA (GPU)"; }
 
     // Monte Carlo keys plus the MCSA defaults
     // (src/MCLS_MCSASolverManager_impl.hpp:116-133).

@@ -43,6 +43,7 @@ class MonteCarloSolverManager : public SolverManager<Vector, Matrix> {
     }
 
     const LinearProblem<Vector, Matrix>& getProblem() const override { return *d_problem; }
+    std::string description() const override { return std::string(std::is_same<MonteCarloTag, ForwardTag>::value ? "Forward" : "Adjoint") + " MC (GPU)"; }
 
     // Defaults (src/MCLS_MonteCarloSolverManager_impl.hpp:99-110) and this
     // library's own keys.
