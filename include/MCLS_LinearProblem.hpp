@@ -1,20 +1,91 @@
 // MCLS_LinearProblem.hpp -- A x = b with optional left/right preconditioners.
 //
 // Same constructor, setters and getters as the reference's LinearProblem
-// (src/MCLS_LinearProblem.hpp:73-154).  The composite operators
-// PL*A*PR and (PL*A*PR)^T (src/MCLS_LinearProblem_impl.hpp:141-221) are not
-// formed on the host: mclsgpu_domain_build forms them on the device.  The
-// host-side apply/residual helpers below serve callers that inspect the
-// problem; the solve itself runs on the GPU.
+// (src/MCLS_LinearProblem.hpp:73-154).  The solvers never form the
+// composite operators PL*A*PR and (PL*A*PR)^T on the host:
+// mclsgpu_domain_build forms them on the device.  getCompositeOperator /
+// getTransposeCompositeOperator and the apply/residual helpers below serve
+// callers that inspect the problem; the solve itself runs on the GPU.
 #ifndef MCLS_LINEARPROBLEM_HPP
 #define MCLS_LINEARPROBLEM_HPP
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "MCLS_GpuTraits.hpp"
 
 namespace MCLS {
+
+namespace detail {
+
+// Square host CSR used by the composite-operator helpers.
+struct Csr {
+    std::int64_t n = 0;
+    std::vector<std::int64_t> rp{0}, ci;
+    std::vector<double> v;
+};
+
+// C = A B row by row: the products of row i of A, taken in A's column order,
+// accumulate into a dense row; columns come out sorted.  Then the reference
+// filter (tpetra/src/MCLS_TpetraHelpers.hpp:196-259): entries with
+// |c| <= threshold * (signed row max) and exact zeros are dropped.
+inline Csr multiply(const Csr& A, const Csr& B, double threshold) {
+    Csr C;
+    C.n = A.n;
+    std::vector<double> acc(size_t(A.n), 0.0);
+    std::vector<char> used(size_t(A.n), 0);
+    std::vector<std::int64_t> cols;
+    for (std::int64_t i = 0; i < A.n; ++i) {
+        cols.clear();
+        for (std::int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+            const std::int64_t k = A.ci[p];
+            for (std::int64_t q = B.rp[k]; q < B.rp[k + 1]; ++q) {
+                const std::int64_t j = B.ci[q];
+                if (!used[j]) {
+                    used[j] = 1;
+                    acc[j] = 0.0;
+                    cols.push_back(j);
+                }
+                acc[j] += A.v[p] * B.v[q];
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        double rmax = 0.0;
+        for (size_t t = 0; t < cols.size(); ++t)
+            rmax = t == 0 ? acc[cols[t]] : std::max(rmax, acc[cols[t]]);
+        const double row_threshold = rmax * threshold;
+        for (std::int64_t j : cols) {
+            used[j] = 0;
+            if (std::abs(acc[j]) <= row_threshold || acc[j] == 0.0) continue;
+            C.ci.push_back(j);
+            C.v.push_back(acc[j]);
+        }
+        C.rp.push_back(std::int64_t(C.ci.size()));
+    }
+    return C;
+}
+
+inline Csr transpose(const Csr& A) {
+    Csr T;
+    T.n = A.n;
+    T.rp.assign(size_t(A.n) + 1, 0);
+    for (std::int64_t j : A.ci) ++T.rp[size_t(j) + 1];
+    for (std::int64_t i = 0; i < A.n; ++i) T.rp[i + 1] += T.rp[i];
+    T.ci.resize(A.ci.size());
+    T.v.resize(A.v.size());
+    std::vector<std::int64_t> next(T.rp.begin(), T.rp.end() - 1);
+    for (std::int64_t i = 0; i < A.n; ++i)
+        for (std::int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+            const std::int64_t q = next[size_t(A.ci[p])]++;
+            T.ci[q] = i;
+            T.v[q] = A.v[p];
+        }
+    return T;
+}
+
+}  // namespace detail
 
 template <class Vector, class Matrix>
 class LinearProblem {
@@ -54,6 +125,25 @@ class LinearProblem {
     // Bumped whenever the operator or a preconditioner is replaced; the
     // managers rebuild their device domain when it changes.
     std::uint64_t generation() const { return d_generation; }
+
+    // PL A PR, the products filtered with `threshold` (no preconditioner:
+    // A itself) (src/MCLS_LinearProblem_impl.hpp:141-176).
+    Teuchos::RCP<const Matrix> getCompositeOperator(double threshold = 0.0) const {
+        if (!isLeftPrec() && !isRightPrec()) return d_A;
+        detail::Csr C = csr(*d_A);
+        if (isRightPrec()) C = detail::multiply(C, csr(*d_PR), threshold);
+        if (isLeftPrec()) C = detail::multiply(csr(*d_PL), C, threshold);
+        return fromCsr(std::move(C));
+    }
+    // (PL A PR)^T = PR^T A^T PL^T, formed from the transposes as the
+    // reference does (src/MCLS_LinearProblem_impl.hpp:182-221); no
+    // preconditioner: a copy of A^T.
+    Teuchos::RCP<const Matrix> getTransposeCompositeOperator(double threshold = 0.0) const {
+        detail::Csr C = detail::transpose(csr(*d_A));
+        if (isLeftPrec()) C = detail::multiply(C, detail::transpose(csr(*d_PL)), threshold);
+        if (isRightPrec()) C = detail::multiply(detail::transpose(csr(*d_PR)), C, threshold);
+        return fromCsr(std::move(C));
+    }
 
     // y = PL A PR x (src/MCLS_LinearProblem_impl.hpp:252-287).
     void apply(const Vector& x, Vector& y) const {
@@ -96,6 +186,16 @@ class LinearProblem {
     }
 
   private:
+    static detail::Csr csr(const Matrix& M) {
+        detail::Csr c;
+        c.n = MT::getGlobalNumRows(M);
+        MT::getCsr(M, c.rp, c.ci, c.v);
+        return c;
+    }
+    static Teuchos::RCP<const Matrix> fromCsr(detail::Csr c) {
+        return MT::fromCsr(c.n, std::move(c.rp), std::move(c.ci), std::move(c.v));
+    }
+
     Teuchos::RCP<const Matrix> d_A;
     Teuchos::RCP<Vector> d_x;
     Teuchos::RCP<const Vector> d_b;

@@ -3,8 +3,9 @@
 // preconditioners, ParameterList keys) over libmclsgpu.
 //
 //   facade_test cpu   checks that need no device: valid parameter lists,
-//                     factory names, ParameterList typing, and that a solve
-//                     without a device throws MCLS::Assertion.
+//                     factory names, ParameterList typing, LinearProblem's
+//                     host helpers (tpetra/test/tstTpetraLinearProblem.cpp),
+//                     and that a solve without a device throws MCLS::Assertion.
 //   facade_test gpu   the solves, after the reference's manager tests
 //                     (tpetra/test/tstTpetraMCSASolverManager.cpp:72-355,
 //                     tpetra/test/tstTpetraMonteCarloSolverManager.cpp:73-197,
@@ -89,7 +90,163 @@ static Teuchos::RCP<Teuchos::ParameterList> mcsa_params() {
     return pl;
 }
 
+static Teuchos::RCP<Mat> identity(int n) {
+    auto I = Teuchos::rcp(new Mat);
+    I->n = n;
+    for (int i = 0; i < n; ++i) {
+        I->colind.push_back(i);
+        I->values.push_back(1.0);
+        I->rowptr.push_back(i + 1);
+    }
+    return I;
+}
+
+static std::vector<double> dense(const Mat& A) {
+    std::vector<double> D(size_t(A.n * A.n), 0.0);
+    for (std::int64_t i = 0; i < A.n; ++i)
+        for (auto p = A.rowptr[i]; p < A.rowptr[i + 1]; ++p)
+            D[size_t(i * A.n + A.colind[p])] += A.values[p];
+    return D;
+}
+
+static std::vector<double> dense_mul(const std::vector<double>& X, const std::vector<double>& Y,
+                                     int n, bool tx = false, bool ty = false) {
+    std::vector<double> Z(size_t(n) * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < n; ++k)
+                s += (tx ? X[size_t(k) * n + i] : X[size_t(i) * n + k]) *
+                     (ty ? Y[size_t(j) * n + k] : Y[size_t(k) * n + j]);
+            Z[size_t(i) * n + j] = s;
+        }
+    return Z;
+}
+
+// LinearProblem's host helpers, after tpetra/test/tstTpetraLinearProblem.cpp:
+// Apply (:118-217), ResidualUpdate (:218-280), CompositeOperator (:281-330).
+static void linear_problem_checks() {
+    g_section = "LinearProblem apply";
+    const int n = 10;
+    {
+        auto A = identity(n);
+        auto X = Teuchos::rcp(new Vec(n, 2.0));
+        auto B = Teuchos::rcp(new Vec(n, 5.0));
+        MCLS::LinearProblem<Vec, Mat> lp(A, X, B);
+        Vec Y(n, 0.0);
+        lp.applyOp(*X, Y);
+        for (double y : Y) EXPECT(y == 2.0);
+        lp.updateSolution(X);  // the update aliases the LHS: X doubles
+        lp.apply(*X, Y);
+        for (double y : Y) EXPECT(y == 4.0);
+        lp.setRightPrec(A);
+        lp.applyRightPrec(*X, Y);
+        for (double y : Y) EXPECT(y == 4.0);
+        lp.apply(*X, Y);
+        for (double y : Y) EXPECT(y == 4.0);
+        lp.setLeftPrec(A);
+        lp.applyLeftPrec(*X, Y);
+        for (double y : Y) EXPECT(y == 4.0);
+        lp.apply(*X, Y);
+        for (double y : Y) EXPECT(y == 4.0);
+        lp.updateSolution(X);
+        auto composite = lp.getCompositeOperator();
+        MCLS::MatrixTraits<Vec, Mat>::apply(*composite, *X, Y);
+        for (double y : Y) EXPECT(y == 8.0);
+    }
+    g_section = "LinearProblem residual update";
+    {
+        auto A = identity(n);
+        auto X = Teuchos::rcp(new Vec(n, 2.0));
+        auto B = Teuchos::rcp(new Vec(n, 5.0));
+        MCLS::LinearProblem<Vec, Mat> lp(A, X, B);
+        lp.updateResidual();
+        for (double r : *lp.getResidual()) EXPECT(r == 3.0);
+        for (double r : *lp.getPrecResidual()) EXPECT(r == 0.0);
+        lp.setLeftPrec(A);
+        lp.updateResidual();
+        for (double r : *lp.getResidual()) EXPECT(r == 3.0);
+        lp.updatePrecResidual();
+        for (double r : *lp.getPrecResidual()) EXPECT(r == 3.0);
+    }
+    g_section = "LinearProblem composite operator";
+    {
+        // A: 1 on the diagonal and 2 right of it, last row empty; PL = A^T:
+        // interior rows of PL A are (2, 5, 2).
+        auto A = Teuchos::rcp(new Mat);
+        A->n = n;
+        for (int i = 0; i < n - 1; ++i) {
+            A->colind.push_back(i);
+            A->values.push_back(1.0);
+            A->colind.push_back(i + 1);
+            A->values.push_back(2.0);
+            A->rowptr.push_back(std::int64_t(A->colind.size()));
+        }
+        A->rowptr.push_back(std::int64_t(A->colind.size()));
+        auto X = Teuchos::rcp(new Vec(n, 2.0));
+        MCLS::LinearProblem<Vec, Mat> lp0(A, X, X);
+        EXPECT(lp0.getCompositeOperator() == A);  // no preconditioner: A itself
+        MCLS::LinearProblem<Vec, Mat> tp(A, X, X);
+        auto C = tp.getTransposeCompositeOperator();
+        MCLS::LinearProblem<Vec, Mat> lp(A, X, X);
+        lp.setLeftPrec(C);
+        auto D = lp.getCompositeOperator();
+        for (int i = 1; i < n - 1; ++i) {
+            EXPECT(D->rowptr[i + 1] - D->rowptr[i] == 3);
+            const auto p = D->rowptr[i];
+            EXPECT(D->colind[p] == i - 1 && D->colind[p + 1] == i && D->colind[p + 2] == i + 1);
+            EXPECT(D->values[p] == 2.0 && D->values[p + 1] == 5.0 && D->values[p + 2] == 2.0);
+        }
+        // Both preconditioners, and the transposed composite, against dense
+        // products of a nonsymmetric case; the threshold drops the small
+        // products of each row.
+        auto T = tridiag(n);
+        auto P = Teuchos::rcp(new Mat(*T));
+        for (auto& v : P->values) v = v == 1.0 ? 0.5 : v * 3.0;
+        MCLS::LinearProblem<Vec, Mat> both(A, X, X);
+        both.setLeftPrec(T);
+        both.setRightPrec(P);
+        const auto dA = dense(*A), dT = dense(*T), dP = dense(*P);
+        const auto ref = dense_mul(dT, dense_mul(dA, dP, n), n);
+        const auto got = dense(*both.getCompositeOperator());
+        const auto gotT = dense(*both.getTransposeCompositeOperator());
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                EXPECT(std::fabs(got[size_t(i) * n + j] - ref[size_t(i) * n + j]) < 1e-14);
+                EXPECT(std::fabs(gotT[size_t(j) * n + i] - ref[size_t(i) * n + j]) < 1e-14);
+            }
+        // Each product is filtered (|c| <= 0.3 * signed row max and zeros
+        // dropped) before the next one, as the reference's multiply does.
+        auto filt = [n](std::vector<double> M) {
+            for (int i = 0; i < n; ++i) {
+                double rmax = 0.0;
+                bool first = true;
+                for (int j = 0; j < n; ++j)
+                    if (M[size_t(i) * n + j] != 0.0) {
+                        rmax = first ? M[size_t(i) * n + j] : std::max(rmax, M[size_t(i) * n + j]);
+                        first = false;
+                    }
+                for (int j = 0; j < n; ++j)
+                    if (std::fabs(M[size_t(i) * n + j]) <= 0.3 * rmax) M[size_t(i) * n + j] = 0.0;
+            }
+            return M;
+        };
+        const auto reff = filt(dense_mul(dT, filt(dense_mul(dA, dP, n)), n));
+        auto F = both.getCompositeOperator(0.3);
+        const auto gotf = dense(*F);
+        int kept = 0;
+        for (int i = 0; i < n * n; ++i) {
+            EXPECT(std::fabs(gotf[size_t(i)] - reff[size_t(i)]) < 1e-14);
+            kept += reff[size_t(i)] != 0.0;
+        }
+        int unfiltered = 0;
+        for (double r : ref) unfiltered += r != 0.0;
+        EXPECT(std::int64_t(F->values.size()) == kept && kept < unfiltered);
+    }
+}
+
 static void cpu_checks() {
+    linear_problem_checks();
     MCLS::SolverFactory<Vec, Mat> factory;
     auto pl = mcsa_params();
     for (const char* name : {"Adjoint MC", "Forward MC", "Adjoint MCSA", "Forward MCSA"}) {

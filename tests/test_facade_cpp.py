@@ -2,7 +2,9 @@
 
 tests/cpp/facade_test.cpp is compiled with g++ against the headers and the
 in-tree library.  Its `cpu` mode checks parameter lists, factory names and
-ParameterList typing and that a solve without a device throws
+ParameterList typing, LinearProblem's host helpers against the reference's
+tests (tpetra/test/tstTpetraLinearProblem.cpp: apply, residual update,
+composite operator), and that a solve without a device throws
 MCLS::Assertion; its `gpu` mode runs the reference's manager tests (signs,
 fewer than 20 MCSA iterations, four successive solves, device-built Jacobi
 and block-Jacobi preconditioners) through the facade on the GPU.
