@@ -414,6 +414,41 @@ static void gpu_checks() {
         EXPECT(rel_err(*x, direct(*B, *b)) < 1e-7);
     }
 
+    // The reference's block inversion known answer
+    // (test/tstBlockInversion.cpp:46-105) through a block of size 4.
+    {
+        g_section = "block inversion";
+        const double B[16] = {3.2,  -1.43, 2.98, 0.32,  -4.12, -7.53, 1.44, -3.72,
+                              4.24, -6.42, 1.82, 2.67, -0.23, 5.8,   1.13, -3.73};
+        const double inv[16] = {-0.461356423424245, -0.060920073472551, 0.547244760641934,
+                                0.412904055961420,  0.154767451798665,  -0.056225122550555,
+                                -0.174451348828054, -0.055523340725809, 0.848746201780808,
+                                0.045927762119214,  -0.618485718805259, -0.415712965073367,
+                                0.526232280383953,  -0.069757566407458, -0.492378815120724,
+                                -0.505833501236923};
+        auto M4 = Teuchos::rcp(new Mat);
+        M4->n = 4;
+        for (int i = 0; i < 4; ++i) {
+            for (int j = 0; j < 4; ++j) {
+                M4->colind.push_back(j);
+                M4->values.push_back(B[4 * i + j]);
+            }
+            M4->rowptr.push_back(4 * (i + 1));
+        }
+        auto params = Teuchos::parameterList();
+        params->set<int>("Jacobi Block Size", 4);
+        MCLS::BlockJacobiPreconditioner<Vec, Mat> prec(params);
+        prec.setOperator(M4);
+        prec.buildPreconditioner();
+        auto PL = prec.getLeftPreconditioner();
+        EXPECT(PL->n == 4 && PL->values.size() == 16);
+        double got[16] = {0};
+        for (int i = 0; i < 4; ++i)
+            for (auto p = PL->rowptr[i]; p < PL->rowptr[i + 1]; ++p)
+                got[4 * i + PL->colind[p]] = PL->values[p];
+        for (int k = 0; k < 16; ++k) EXPECT(std::fabs(got[k] - inv[k]) <= 1e-13 * std::fabs(inv[k]));
+    }
+
     // Learned SPAI with a network whose output layer is zero: M is point
     // Jacobi, the rho gate keeps the plain preconditioner, the solve converges.
     {

@@ -261,6 +261,24 @@ def test_block_jacobi_known_answers():
     assert np.allclose(Pm, want, rtol=1e-14, atol=1e-14)
 
 
+# test/tstBlockInversion.cpp:46-105: a 4x4 block and its GETRF/GETRI inverse.
+BLOCK_INVERSION = (
+    [[3.2, -1.43, 2.98, 0.32], [-4.12, -7.53, 1.44, -3.72], [4.24, -6.42, 1.82, 2.67],
+     [-0.23, 5.8, 1.13, -3.73]],
+    [[-0.461356423424245, -0.060920073472551, 0.547244760641934, 0.412904055961420],
+     [0.154767451798665, -0.056225122550555, -0.174451348828054, -0.055523340725809],
+     [0.848746201780808, 0.045927762119214, -0.618485718805259, -0.415712965073367],
+     [0.526232280383953, -0.069757566407458, -0.492378815120724, -0.505833501236923]])
+
+
+def test_block_inversion_known_answer():
+    # One block of size 4 is the whole matrix: the preconditioner is its
+    # inverse, to the reference's relative 1e-14.
+    B, want = (np.array(m) for m in BLOCK_INVERSION)
+    Pm = O.block_jacobi(O.Csr.from_scipy(sp.csr_matrix(B)), 4).to_scipy().toarray()
+    assert np.all(np.abs(Pm - want) <= 1e-14 * np.abs(want))
+
+
 def test_filter_relative_threshold():
     # TpetraMatrixHelpers::filter: drop |v| <= threshold * (signed row max).
     A = sp.csr_matrix(np.array([[4.0, 0.1, -0.3], [0.2, 1.0, 0.05], [1.0, 1.0, 1.0]]))
