@@ -51,8 +51,9 @@ CONFIGS = {
                         "FP64 walks, N histories per iteration",
                n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0),
 }
-# DRAM bytes (read + write) of one walk launch on each workload, from the ncu
-# capture summarised in profiles/walk32_stencil_diffusion128.md.
+# DRAM bytes (read + write) of one walk launch on each workload: ncu's
+# dram__bytes_read.sum (83.90 MB) + dram__bytes_write.sum (7.82 MB) for the
+# stencil forward expected-value walk32 launch at 128^3.
 WALK_DRAM_BYTES_PER_LAUNCH = {"diffusion128": 91.72e6}
 
 

@@ -42,7 +42,7 @@ typedef enum {
     MCLSGPU_ERR_NOT_CONVERGED = 5,/* informational: max iterations reached        */
     MCLSGPU_ERR_DEGENERATE = 6,   /* empty or zero-weight domain row (MCLS_CHECK) */
     MCLSGPU_ERR_NO_DEVICE = 7,    /* no usable CUDA device                        */
-    MCLSGPU_ERR_UNSUPPORTED = 8   /* configuration outside this build's limits    */
+    MCLSGPU_ERR_UNSUPPORTED = 8   /* configuration outside the library's limits  */
 } mclsgpu_status;
 
 /* Monte Carlo direction (MonteCarloTag of the reference managers). */

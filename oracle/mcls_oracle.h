@@ -30,7 +30,9 @@ void orc_xorshift_uniforms(uint64_t seed, int64_t n, double* out);
 /* Seed of rank `rank` derived as in src/MCLS_PRNG_impl.hpp:56-75 with the
  * std::random_device draw replaced by `master_seed`. */
 uint64_t orc_rank_seed(uint64_t master_seed, int rank);
-/* Counter-based generator (no reference counterpart). */
+/* Counter-based generator of the FP32 walks (no reference counterpart): the
+ * Xorshift stream started from the state hashed from (seed, epoch, kind, idx),
+ * n uniforms in the reference's canonical mapping. */
 void orc_counter_uniforms(uint64_t seed, uint64_t epoch, int kind, int64_t idx,
                           int64_t n, double* out);
 /* src/MCLS_SamplingTools.hpp:67-80 */
