@@ -648,6 +648,15 @@ class LinearOpWithSolveFactory : public virtual Teuchos::Describable {
                                     ESupportSolveUse use = SUPPORT_SOLVE_UNSPECIFIED) const {
         selectOp(A, Teuchos::null, prec, false, op, use);
     }
+    // With left and right preconditioner matrices built elsewhere (either
+    // may be null), as a GivenPreconditioner.
+    void initializePreconditionedOp(const Teuchos::RCP<const Matrix>& A,
+                                    const Teuchos::RCP<const Matrix>& PL,
+                                    const Teuchos::RCP<const Matrix>& PR, Op* op,
+                                    ESupportSolveUse use = SUPPORT_SOLVE_UNSPECIFIED) const {
+        selectOp(A, Teuchos::null, Teuchos::rcp(new GivenPreconditioner<Matrix>(PL, PR)), false,
+                 op, use);
+    }
     // The factory's preconditioner built from approx_A instead of A.
     void initializeApproxPreconditionedOp(const Teuchos::RCP<const Matrix>& A,
                                           const Teuchos::RCP<const Matrix>& approx_A, Op* op,

@@ -35,6 +35,38 @@ class PreconditionerFactoryBase : public virtual Teuchos::Describable {
     virtual void initializePrec(const Teuchos::RCP<const Matrix>& A, Prec* prec) const = 0;
 };
 
+// A preconditioner built elsewhere (a Thyra preconditioner's operators, a
+// user's own M^-1): its left and right matrices as given; either may be null.
+template <class Matrix>
+class GivenPreconditioner : public Preconditioner<Matrix> {
+  public:
+    GivenPreconditioner(const Teuchos::RCP<const Matrix>& left,
+                        const Teuchos::RCP<const Matrix>& right)
+        : d_left(left), d_right(right) {
+        if (!Teuchos::nonnull(left) && !Teuchos::nonnull(right))
+            throw Assertion("GivenPreconditioner: no left or right matrix");
+    }
+    Teuchos::RCP<const Teuchos::ParameterList> getValidParameters() const override {
+        return Teuchos::parameterList();
+    }
+    Teuchos::RCP<const Teuchos::ParameterList> getCurrentParameters() const override {
+        return Teuchos::parameterList();
+    }
+    void setParameters(const Teuchos::RCP<Teuchos::ParameterList>&) override {}
+    void setOperator(const Teuchos::RCP<const Matrix>& A) override { d_A = A; }
+    const Matrix& getOperator() const override {
+        if (!Teuchos::nonnull(d_A)) throw Assertion("GivenPreconditioner: no operator set");
+        return *d_A;
+    }
+    void buildPreconditioner() override {}
+    Teuchos::RCP<const Matrix> getLeftPreconditioner() const override { return d_left; }
+    Teuchos::RCP<const Matrix> getRightPreconditioner() const override { return d_right; }
+    std::string description() const override { return "MCLS::GivenPreconditioner"; }
+
+  private:
+    Teuchos::RCP<const Matrix> d_left, d_right, d_A;
+};
+
 template <class Vector, class Matrix>
 class PreconditionerFactory : public PreconditionerFactoryBase<Matrix> {
   public:

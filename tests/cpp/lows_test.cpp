@@ -579,6 +579,15 @@ static void cpu_checks(const std::string& dir) {
         Teuchos::RCP<MCLS::Preconditioner<Mat>> P_out;
         f.uninitializeOp(op.get(), &A_out, &P_out);
         EXPECT(A_out == A && P_out == mine && !op->isInitialized());
+        // Matrices built elsewhere, right side only.
+        auto PR = mine->getLeftPreconditioner();
+        f.initializePreconditionedOp(A, Teuchos::null, PR, op.get());
+        EXPECT(op->isExternalPrec() && op->problem()->getLeftPrec().is_null() &&
+               op->problem()->getRightPrec() == PR && pf->built == 3);
+        EXPECT(throws<MCLS::Assertion>([&] {
+            f.initializePreconditionedOp(A, Teuchos::null, Teuchos::null, op.get());
+        }));
+        f.uninitializeOp(op.get());
         f.initializeOp(A, op.get());
         f.uninitializeOp(op.get(), &A_out, &P_out);
         EXPECT(P_out.is_null());  // the factory's own preconditioner is not handed out
