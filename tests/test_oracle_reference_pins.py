@@ -12,7 +12,9 @@
   tpetra/test/tstTpetraForwardTally.cpp:83-235 (tally, finalize, normalize),
   tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations),
   tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345 (Richardson: 15
-  iterations, solution sign).
+  iterations, solution sign), tpetra/test/tstTpetraMCSolver.cpp:68-156
+  (signs on one domain), tpetra/test/tstTpetraBlockJacobiPreconditioner.cpp
+  and test/tstBlockInversion.cpp:46-105 (block inverses).
 """
 import json
 import os
@@ -238,6 +240,21 @@ def test_monte_carlo_solve_sign():
         for b in (-1.0, 2.0):
             x, _ = mc.solve(np.full(10, b))
             assert np.all(np.sign(x) == np.sign(b))
+
+
+def test_mc_solver_signs_on_one_source():
+    # tpetra/test/tstTpetraMCSolver.cpp:68-156: Sample Ratio 100, the
+    # reference's own stream ("Reproducible MC Mode"), b = -2 then b = 2 on
+    # the same domain: the solution takes b's sign, whatever x held before.
+    A = O.Csr.from_scipy(P.tridiag_test(10))
+    # The source's CDF starts from the signed b[0]
+    # (src/MCLS_UniformAdjointSource_impl.hpp:185), so b = -2 draws
+    # 1000 * (-2 + 9 * 2) / 20 = 800 histories and b = 2 all 1000.
+    mc = O.MC(A, sample_ratio=100.0, rng_mode=0, seed=5)
+    x, nh = mc.solve(np.full(10, -2.0))
+    assert nh == 800 and np.all(x < 0.0)
+    x, nh = mc.solve(np.full(10, 2.0))
+    assert nh == 1000 and np.all(x > 0.0)
 
 
 def test_point_jacobi_and_composite():
