@@ -13,7 +13,8 @@
   tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations),
   tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345 (Richardson: 15
   iterations, solution sign), tpetra/test/tstTpetraMCSolver.cpp:68-156
-  (signs on one domain), tpetra/test/tstTpetraBlockJacobiPreconditioner.cpp
+  (signs on one domain), tpetra/test/tstTpetraPointJacobiPreconditioner.cpp,
+  tpetra/test/tstTpetraBlockJacobiPreconditioner.cpp
   and test/tstBlockInversion.cpp:46-105 (block inverses).
 """
 import json
@@ -255,6 +256,21 @@ def test_mc_solver_signs_on_one_source():
     assert nh == 800 and np.all(x < 0.0)
     x, nh = mc.solve(np.full(10, 2.0))
     assert nh == 1000 and np.all(x > 0.0)
+
+
+@pytest.mark.parametrize("tridiagonal", [False, True])
+def test_point_jacobi_known_answers(tridiagonal):
+    # tpetra/test/tstTpetraPointJacobiPreconditioner.cpp diag_matrix /
+    # tridiag_matrix: every entry 2 (the first and last rows hold only their
+    # diagonal) gives M^-1 = diag(1/2), diagonal only.
+    n = 10
+    A = sp.lil_matrix((n, n))
+    for i in range(n):
+        cols = [i] if not tridiagonal or i in (0, n - 1) else [i - 1, i, i + 1]
+        for c in cols:
+            A[i, c] = 2.0
+    M = O.point_jacobi(O.Csr.from_scipy(sp.csr_matrix(A))).to_scipy()
+    assert M.nnz == n and np.array_equal(M.toarray(), np.diag(np.full(n, 0.5)))
 
 
 def test_point_jacobi_and_composite():
