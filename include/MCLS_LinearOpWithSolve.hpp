@@ -457,12 +457,12 @@ class LinearOpWithSolve : public virtual Teuchos::Describable {
         for (int j = 0; j < MVT::getNumVectors(X); ++j) {
             auto x = MVT::getVector(X, j);
             auto y = MVT::getVectorNonConst(*Y, j);
-            Vector ax = *x;
-            MT::apply(A, *x, ax);
+            auto ax = VT::clone(*x);
+            MT::apply(A, *x, *ax);
             const std::int64_t n = VT::getGlobalLength(*y);
-            if (VT::getGlobalLength(ax) != n)
+            if (VT::getGlobalLength(*ax) != n)
                 throw Assertion("LinearOpWithSolve::apply: Y has the wrong length");
-            const double* a = VT::view(ax);
+            const double* a = VT::view(*ax);
             double* yv = VT::viewNonConst(*y);
             for (std::int64_t i = 0; i < n; ++i)
                 yv[i] = beta == 0.0 ? alpha * a[i] : alpha * a[i] + beta * yv[i];

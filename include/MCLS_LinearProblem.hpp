@@ -145,14 +145,23 @@ class LinearProblem {
         return fromCsr(std::move(C));
     }
 
-    // y = PL A PR x (src/MCLS_LinearProblem_impl.hpp:252-287).
+    // y = PL A PR x (src/MCLS_LinearProblem_impl.hpp:252-287).  The
+    // intermediate vectors are VT::clone'd, never copy-constructed: a
+    // vector type may copy by view (Tpetra does).
     void apply(const Vector& x, Vector& y) const {
-        Vector t = x;
-        if (isRightPrec()) MT::apply(*d_PR, x, t);
-        MT::apply(*d_A, t, y);
+        const Vector* in = &x;
+        Teuchos::RCP<Vector> t;
+        if (isRightPrec()) {
+            t = VT::clone(x);
+            MT::apply(*d_PR, x, *t);
+            in = t.get();
+        }
         if (isLeftPrec()) {
-            Vector u = y;
-            MT::apply(*d_PL, u, y);
+            auto u = VT::clone(y);
+            MT::apply(*d_A, *in, *u);
+            MT::apply(*d_PL, *u, y);
+        } else {
+            MT::apply(*d_A, *in, y);
         }
     }
     void applyOp(const Vector& x, Vector& y) const { MT::apply(*d_A, x, y); }
@@ -161,27 +170,33 @@ class LinearProblem {
 
     // r = b - A x (src/MCLS_LinearProblem_impl.hpp:390-405).
     void updateResidual() {
-        Vector ax = *d_r;
-        MT::apply(*d_A, *d_x, ax);
+        auto ax = VT::clone(*d_r);
+        MT::apply(*d_A, *d_x, *ax);
         const double* b = VT::view(*d_b);
-        const double* a = VT::view(ax);
+        const double* a = VT::view(*ax);
         double* r = VT::viewNonConst(*d_r);
         for (std::int64_t i = 0; i < VT::getGlobalLength(*d_r); ++i) r[i] = b[i] - a[i];
     }
     // rp = PL (b - A x) (src/MCLS_LinearProblem_impl.hpp:410-442).
     void updatePrecResidual() {
         updateResidual();
-        if (isLeftPrec())
+        if (isLeftPrec()) {
             MT::apply(*d_PL, *d_r, *d_rp);
-        else
-            *d_rp = *d_r;
+        } else {
+            const double* r = VT::view(*d_r);
+            double* rp = VT::viewNonConst(*d_rp);
+            for (std::int64_t i = 0; i < VT::getGlobalLength(*d_r); ++i) rp[i] = r[i];
+        }
     }
     // x += PR update (src/MCLS_LinearProblem_impl.hpp:228-247).
     void updateSolution(const Teuchos::RCP<Vector>& update) {
-        Vector u = *update;
-        if (isRightPrec()) MT::apply(*d_PR, *update, u);
+        Teuchos::RCP<Vector> u;
+        if (isRightPrec()) {
+            u = VT::clone(*update);
+            MT::apply(*d_PR, *update, *u);
+        }
+        const double* p = VT::view(isRightPrec() ? *u : *update);
         double* x = VT::viewNonConst(*d_x);
-        const double* p = VT::view(u);
         for (std::int64_t i = 0; i < VT::getGlobalLength(*d_x); ++i) x[i] += p[i];
     }
 
