@@ -486,21 +486,25 @@ def ctx_device():
 
 
 def cpu_baseline(cfg, A, b, seconds_target=15.0):
-    """Oracle port: multi-threaded adjoint walks on the same domain."""
+    """Oracle port: multi-threaded walks on the same domain, in the
+    workload's direction with its estimator."""
     from oracle import oracle as O
 
     c = CONFIGS[cfg]
     Ao = O.Csr.from_scipy(A)
-    mc = O.MC(Ao, PL=O.point_jacobi(Ao), history_length=c["history_length"], rng_mode=1)
+    mc = O.MC(Ao, PL=O.point_jacobi(Ao), history_length=c["history_length"], rng_mode=1,
+              direction=c["direction"], estimator=c["estimator"])
     threads = os.cpu_count() or 1
     src = (1.0 / A.diagonal()) * b
     nh = 1 << 18
     steps, secs, _ = mc.bench_walks(src, nh, threads)
     # scale the sample to ~seconds_target of CPU work
-    nh2 = int(min(1 << 26, nh * max(1.0, seconds_target / max(secs, 1e-3))))
+    nh2 = int(min(1 << 30, nh * max(1.0, seconds_target / max(secs, 1e-3))))
     steps, secs, _ = mc.bench_walks(src, nh2, threads)
+    kind = ("forward " + ("expected-value" if c["estimator"] else "collision")
+            if c["direction"] else "adjoint " + ("expected-value" if c["estimator"] else "collision"))
     out = {"value": steps / secs, "unit": UNIT, "cores": threads, "kind": "port",
-           "sample": f"{nh2} adjoint histories x {c['history_length']} steps on the "
+           "sample": f"{nh2} {kind} histories x {c['history_length']} steps on the "
                      f"{A.shape[0]}-row Jacobi domain, {secs:.1f} s"}
     if cfg == "poisson100":
         # The whole solve on one core, as one MPI rank of the reference runs

@@ -1103,8 +1103,81 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
     return rnorm <= criteria ? 1 : 0;
 }
 
+namespace {
+
+// Forward histories laid out as the forward source lays them out
+// (src/MCLS_UniformForwardSource_impl.hpp:60-148): history e starts at state
+// e mod n with weight 1.  Each step adds w * b[s] (collision) or
+// w * (H b)_s (expected value) to the history's sum
+// (src/MCLS_ForwardTally.hpp:123-132), which goes to its start state
+// (src/MCLS_ForwardTally_impl.hpp:84-110); x_i is the mean over the
+// histories started at i, plus b_i for the expected value, as the forward
+// solve finishes it.
+int64_t bench_walks_forward(const orc_mc* mc, const double* rhs, int64_t nh, int threads,
+                            double* x, double* secs) {
+    const Domain& D = mc->D;
+    const int64_t n = D.n;
+    const int L = mc->p.history_length;
+    const bool ev = mc->p.estimator == 1;
+    std::vector<double> hb;
+    if (ev) {
+        hb.assign(n, 0.0);
+        for (int64_t i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int64_t k = D.rp[i]; k < D.rp[i + 1]; ++k) s = s + D.h[k] * rhs[D.col[k]];
+            hb[i] = s;
+        }
+    }
+    const double* tsrc = ev ? hb.data() : rhs;
+    if (threads < 1) threads = 1;
+    std::vector<std::vector<double>> sums(threads, std::vector<double>(n, 0.0));
+    std::vector<int64_t> steps(threads, 0);
+    auto t0 = std::chrono::steady_clock::now();
+    auto work = [&](int t) {
+        Xorshift64 xs(orc_rank_seed(0x5EEDULL, t) | 1ULL);
+        std::vector<double>& sm = sums[t];
+        int64_t lo = nh * t / threads, hi = nh * (t + 1) / threads;
+        int64_t st = 0;
+        for (int64_t e = lo; e < hi; ++e) {
+            const int64_t s0 = e % n;
+            int64_t s = s0;
+            double w = 1.0, h = 0.0;
+            for (int k = 0; k < L; ++k) {
+                h += w * tsrc[s];
+                int64_t r0 = D.rp[s];
+                int j = sample_cdf(&D.cdf[r0], int(D.rp[s + 1] - r0), canonical(xs()));
+                w *= D.w[s] * (D.h[r0 + j] > 0.0 ? 1.0 : -1.0);
+                s = D.col[r0 + j];
+                ++st;
+            }
+            sm[s0] += h;
+        }
+        steps[t] = st;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    auto t1 = std::chrono::steady_clock::now();
+    if (secs) *secs = std::chrono::duration<double>(t1 - t0).count();
+    int64_t total = 0;
+    for (int t = 0; t < threads; ++t) total += steps[t];
+    if (x) {
+        for (int64_t i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int t = 0; t < threads; ++t) s += sums[t][i];
+            const int64_t count = nh / n + (i < nh % n ? 1 : 0);
+            x[i] = (count ? s / double(count) : 0.0) + (ev ? rhs[i] : 0.0);
+        }
+    }
+    return total;
+}
+
+}  // namespace
+
 int64_t orc_bench_walks(const orc_mc* mc, const double* rhs, int64_t nh,
                         int threads, double* x, double* secs) {
+    if (mc->p.direction == 1) return bench_walks_forward(mc, rhs, nh, threads, x, secs);
     // Independent adjoint collision histories, one Xorshift per thread, the
     // source sampled per thread from the |rhs| CDF (buildRandomSource), the
     // per-thread tallies summed at the end.

@@ -156,8 +156,10 @@ int orc_anderson_linear(const orc_csr* M, const double* c, const orc_anderson_pa
                         double* x, int* iters, int max_hist, double* iterates);
 
 /* CPU baseline: independent histories on `threads` threads (one Xorshift per
- * thread, as one MPI rank per core with subdomain transport), adjoint
- * collision walks over the domain for `nh` histories of fixed length.
+ * thread, as one MPI rank per core with subdomain transport), `nh` histories
+ * of fixed length in the domain's direction: adjoint collision walks from
+ * the |rhs| CDF, or forward walks (history e starts at state e mod n; the
+ * domain's estimator, collision or expected value).  x gets the estimate.
  * Returns walk steps performed; elapsed seconds through *secs. */
 int64_t orc_bench_walks(const orc_mc*, const double* rhs, int64_t nh,
                         int threads, double* x, double* secs);

@@ -1,0 +1,56 @@
+"""The CPU baseline walks (oracle/mcls_oracle.cpp orc_bench_walks) that
+bench.py times beside the GPU: they walk the workload's own direction and
+estimator, so the baseline's walk steps are the GPU's.
+
+* Forward, H = -I (A = 2I): every transition stays put and flips the sign,
+  so each estimate is exact and equals the oracle's forward solve.
+* Forward collision and expected value on a small contraction: the mean
+  over many histories matches the truncated Neumann sums
+  sum_{k<L} H^k b and b + sum_{k<L} H^{k+1} b.
+* Adjoint: nh histories of L steps each.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from mcls_b200 import problems as P
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("L", [1, 2, 3])
+@pytest.mark.parametrize("threads", [1, 3])
+def test_forward_walks_on_minus_identity_are_exact(L, threads):
+    n = 8
+    b = np.linspace(-1.0, 2.0, n)
+    A = O.Csr.from_scipy(sp.csr_matrix(2.0 * sp.identity(n)))
+    for est in (0, 1):
+        mc = O.MC(A, history_length=L, direction=1, estimator=est)
+        steps, _, x = mc.bench_walks(b, 5 * n, threads)
+        xs, _ = mc.solve(b)
+        assert steps == 5 * n * L
+        assert np.allclose(x, xs, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("est", [0, 1])
+def test_forward_walk_means_are_the_neumann_sums(est):
+    A = P.poisson2d(4)
+    n = A.shape[0]
+    b = np.linspace(0.5, 1.5, n)
+    Ao = O.Csr.from_scipy(A)
+    L = 4
+    mc = O.MC(Ao, PL=O.point_jacobi(Ao), history_length=L, direction=1, estimator=est)
+    d = mc.domain()
+    H = sp.csr_matrix((d["h"], d["col"], d["rowptr"]), shape=(n, n)).toarray()
+    terms = [np.linalg.matrix_power(H, k + est) @ b for k in range(L)]
+    want = sum(terms) + (b if est else 0.0)
+    steps, _, x = mc.bench_walks(b, 20000 * n, 4)
+    assert steps == 20000 * n * L
+    assert np.abs(x - want).max() <= 0.02 * np.abs(want).max()
+
+
+def test_adjoint_walk_steps():
+    A = P.tridiag_test(10)
+    Ao = O.Csr.from_scipy(A)
+    mc = O.MC(Ao, history_length=7)
+    steps, secs, x = mc.bench_walks(np.ones(10), 1000, 2)
+    assert steps == 7000 and secs >= 0.0 and np.all(np.isfinite(x))
