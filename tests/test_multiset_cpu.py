@@ -13,7 +13,6 @@ import subprocess
 import sys
 
 import numpy as np
-import pytest
 import scipy.sparse.linalg as spla
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
