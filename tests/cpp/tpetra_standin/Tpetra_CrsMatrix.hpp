@@ -13,8 +13,15 @@
 
 namespace Tpetra {
 
+// The operator base a Thyra wrapper holds (Tpetra_Operator.hpp).
 template <class S = double, class LO = int, class GO = long long, class Node = DefaultNode>
-class CrsMatrix {
+class Operator {
+  public:
+    virtual ~Operator() = default;
+};
+
+template <class S = double, class LO = int, class GO = long long, class Node = DefaultNode>
+class CrsMatrix : public Operator<S, LO, GO, Node> {
   public:
     typedef Map<LO, GO, Node> map_type;
     typedef MultiVector<S, LO, GO, Node> mv_type;

@@ -16,6 +16,9 @@ struct DefaultNode {};
 template <class LO = int, class GO = long long, class Node = DefaultNode>
 class Map {
   public:
+    typedef LO local_ordinal_type;
+    typedef GO global_ordinal_type;
+    typedef Node node_type;
     // Contiguous: local i holds global indexBase + i.
     Map(std::size_t numGlobal, GO indexBase, const Teuchos::RCP<const Teuchos::Comm<int>>& comm)
         : d_comm(comm) {
