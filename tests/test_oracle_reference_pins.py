@@ -5,7 +5,8 @@
   (tests/golden/make_golden.py via oracle/_ref).
 * test/tstSamplingTools.cpp:65-101 known-answer table.
 * tpetra/test/tstTpetraAlmostOptimalDomain.cpp:204-259 (Diagonal),
-  tpetra/test/tstTpetraDomainTransporter.cpp:97-172 (Cutoff),
+  tpetra/test/tstTpetraDomainTransporter.cpp:97-172 (Cutoff) and :175-242
+  (Boundary, as trajectories leaving their block of rows),
   tpetra/test/tstTpetraAdjointTally.cpp:83-167 (normalize),
   tpetra/test/tstTpetraUniformAdjointSource.cpp:75-161 (counts, weight),
   tpetra/test/tstTpetraUniformForwardSource.cpp:75-260 (counts, weight 1),
@@ -256,6 +257,32 @@ def test_mc_solver_signs_on_one_source():
     assert nh == 800 and np.all(x < 0.0)
     x, nh = mc.solve(np.full(10, 2.0))
     assert nh == 1000 and np.all(x > 0.0)
+
+
+@pytest.mark.parametrize("parts", [2, 4])
+def test_long_histories_leave_their_part(parts):
+    # tpetra/test/tstTpetraDomainTransporter.cpp:175-242 (Boundary): on the
+    # 1 / -0.499 tridiagonal with History Length 10000, every history started
+    # in a rank's rows ends in a BOUNDARY event.  One domain here (the
+    # adjoint one, on A^T as the reference builds it; stratified, so one
+    # history starts in every row), so the pin is on the trajectories: each
+    # one reaches a row outside the block of 10 rows it started in.
+    n = 10 * parts
+    rows = np.arange(n)
+    A = sp.lil_matrix(P.tridiag_test(n, off=-0.499))
+    A[0, 1] = A[0, 2] = -0.499  # the reference's first and last rows
+    A[n - 1, n - 3] = A[n - 1, n - 2] = -0.499
+    A = sp.csr_matrix(A)
+    A.eliminate_zeros()
+    L = 10000
+    mc = O.MC(O.Csr.from_scipy(A), history_length=L, stratified=1, seed=3)
+    _, nh, tr = mc.solve(np.ones(n), trace=n)
+    assert nh == n
+    for h in range(n):
+        states = tr["states"][h]
+        block = tr["start"][h] // 10
+        assert np.any(states // 10 != block), h
+    assert np.array_equal(np.sort(tr["start"]), rows)
 
 
 @pytest.mark.parametrize("tridiagonal", [False, True])
