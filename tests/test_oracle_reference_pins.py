@@ -202,6 +202,21 @@ def test_mcsa_forward_tridiagonal(b):
     assert np.all(np.sign(r["x"]) == np.sign(b))
 
 
+def test_mcsa_forward_prec_identity_successive_solves():
+    # tstTpetraMCSASolverManager prec_forward (:391-510): forward, PL = PR =
+    # I, Sample Ratio 1, four solves from x = 0 with b = -1, 2, 2, -2: each
+    # converges in fewer than 20 iterations with the sign of b.  (The
+    # reference runs them on one manager, one continuing stream; each solve
+    # here starts a stream of its own.)
+    A = O.Csr.from_scipy(P.tridiag_test(10))
+    I = O.Csr.from_scipy(sp.identity(10, format="csr"))
+    for k, b in enumerate((-1.0, 2.0, 2.0, -2.0)):
+        r = O.mcsa_solve(A, np.full(10, b), PL=I, PR=I, tolerance=1e-8, max_iters=20,
+                         seed=17 + k, direction=1, sample_ratio=1.0)
+        assert r["converged"] and r["iters"] < 20 and r["achieved"] > 0, b
+        assert np.all(np.sign(r["x"]) == np.sign(b))
+
+
 @pytest.mark.parametrize("b", [-1.0, 2.0, -2.0])
 @pytest.mark.parametrize("prec", [False, True])
 def test_fixed_point_richardson_known_answer(b, prec):
