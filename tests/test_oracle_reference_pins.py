@@ -11,7 +11,8 @@
   tpetra/test/tstTpetraUniformAdjointSource.cpp:75-161 (counts, weight),
   tpetra/test/tstTpetraUniformForwardSource.cpp:75-260 (counts, weight 1),
   tpetra/test/tstTpetraForwardTally.cpp:83-235 (tally, finalize, normalize),
-  tpetra/test/tstTpetraMCSASolverManager.cpp:72-204 (MCSA < 20 iterations),
+  tpetra/test/tstTpetraMCSASolverManager.cpp:72-510 (MCSA < 20 iterations:
+  adjoint, forward, PL = PR = I),
   tpetra/test/tstTpetraFixedPointSolverManager.cpp:72-345 (Richardson: 15
   iterations, solution sign), tpetra/test/tstTpetraMCSolver.cpp:68-156
   (signs on one domain), tpetra/test/tstTpetraPointJacobiPreconditioner.cpp,
