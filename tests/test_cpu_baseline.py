@@ -7,7 +7,8 @@ estimator, so the baseline's walk steps are the GPU's.
 * Forward collision and expected value on a small contraction: the mean
   over many histories matches the truncated Neumann sums
   sum_{k<L} H^k b and b + sum_{k<L} H^{k+1} b.
-* Adjoint: nh histories of L steps each.
+* Adjoint: nh histories of L steps each, and the adjoint solve's mean over
+  independent streams within 5 standard errors of the Neumann sums.
 """
 import numpy as np
 import pytest
@@ -54,3 +55,24 @@ def test_adjoint_walk_steps():
     mc = O.MC(Ao, history_length=7)
     steps, secs, x = mc.bench_walks(np.ones(10), 1000, 2)
     assert steps == 7000 and secs >= 0.0 and np.all(np.isfinite(x))
+
+
+@pytest.mark.parametrize("est", [0, 1])
+def test_adjoint_solve_means_are_the_neumann_sums(est):
+    # The oracle's adjoint solve is unbiased: over 30 independent streams the
+    # mean of x lies within 5 standard errors of sum_{k<L} H^k PL b
+    # (collision) or sum_{k<=L} H^k PL b (expected value) in every entry.
+    A = P.poisson2d(4)
+    n = A.shape[0]
+    b = np.linspace(0.5, 1.5, n)
+    Ao = O.Csr.from_scipy(A)
+    L = 4
+    D = np.diag(1.0 / A.diagonal())
+    H = np.eye(n) - D @ A.toarray()
+    src = D @ b
+    want = sum(np.linalg.matrix_power(H, k) @ src for k in range(L + est))
+    E = np.array([O.MC(Ao, PL=O.point_jacobi(Ao), history_length=L, sample_ratio=50.0,
+                       seed=100 + s, rng_mode=1, estimator=est).solve(b)[0]
+                  for s in range(30)])
+    se = E.std(0, ddof=1) / np.sqrt(len(E))
+    assert np.all(np.abs(E.mean(0) - want) <= 5.0 * se)
