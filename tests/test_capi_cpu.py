@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from mcls_b200 import capi
@@ -95,6 +96,11 @@ def test_rank_seed_matches_oracle():
         for rank in range(4):
             assert capi.rank_seed(master, rank) == O.rank_seed(master, rank)
     assert len({capi.rank_seed(5, r) for r in range(16)}) == 16
+    # test/tstPRNG.cpp:66-104: the k-th draws of different ranks differ.
+    U = np.array([O.xorshift_uniforms(capi.rank_seed(5, r), 100) for r in range(8)])
+    for r in range(8):
+        for q in range(r + 1, 8):
+            assert np.all(U[r] != U[q])
 
 
 def test_null_arguments_are_rejected_without_a_device():
