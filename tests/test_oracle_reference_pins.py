@@ -8,7 +8,8 @@
   tpetra/test/tstTpetraDomainTransporter.cpp:97-172 (Cutoff) and :175-242
   (Boundary, as trajectories leaving their block of rows),
   tpetra/test/tstTpetraAdjointTally.cpp:83-167 (normalize),
-  tpetra/test/tstTpetraUniformAdjointSource.cpp:75-161 (counts, weight),
+  tpetra/test/tstTpetraUniformAdjointSource.cpp:75-240 (counts, weight;
+  nh_not_set and nh_set),
   tpetra/test/tstTpetraUniformForwardSource.cpp:75-260 (counts, weight 1),
   tpetra/test/tstTpetraForwardTally.cpp:83-235 (tally, finalize, normalize),
   tpetra/test/tstTpetraMCSASolverManager.cpp:72-510 (MCSA < 20 iterations:
@@ -102,33 +103,35 @@ def test_cutoff_known_answer():
     assert np.allclose(x * nh, 3.0, rtol=0, atol=1e-15)
 
 
-def test_adjoint_source_counts_and_weight():
-    # tstTpetraUniformAdjointSource nh_not_set: b = -1 gives N histories, all
-    # local states, weight -|b|_1 = -N.  The reference's operator has no entry
-    # in row 0 and keeps the identity only where A has a diagonal entry.
+@pytest.mark.parametrize("mult", [1, 10])
+def test_adjoint_source_counts_and_weight(mult):
+    # tstTpetraUniformAdjointSource nh_not_set / nh_set (Sample Ratio mult):
+    # b = -1 gives mult * N histories, all local states, weight -|b|_1 = -N.
+    # The reference's operator has no entry in row 0 and keeps the identity
+    # only where A has a diagonal entry.
     n = 10
     A = sp.lil_matrix((n, n))
     for i in range(1, n):
         A[i, i - 1] = -0.5
     A[n - 1, n - 1] = -0.5
-    mc = O.MC(O.Csr.from_scipy(sp.csr_matrix(A)), history_length=1)
+    mc = O.MC(O.Csr.from_scipy(sp.csr_matrix(A)), history_length=1, sample_ratio=float(mult))
     d = mc.domain()
     # Row i of A^T holds A(i+1, i) = -0.5 -> h = +0.5 (no identity term: the
     # diagonal is absent); the last row holds A(n-1,n-1) -> h = 1 + 0.5.
     assert np.all(d["h"][:-1] == 0.5) and d["h"][-1] == 1.5
-    # b > 0: nh = N histories, weight +|b|_1 = N.
-    x, nh, tr = mc.solve(np.full(n, 1.0), trace=n)
-    assert nh == n
+    # b > 0: nh = mult * N histories, weight +|b|_1 = N.
+    x, nh, tr = mc.solve(np.full(n, 1.0), trace=mult * n)
+    assert nh == mult * n
     W = d["weights"][tr["start"]]
     assert np.all(tr["final_weight"] == float(n) * W)
     # b = -1: the source code seeds its CDF with the signed b[0]
     # (src/MCLS_UniformAdjointSource_impl.hpp:185), so cdf.back() = N - 2 and
-    # nh = int(N * (N-2)/N) = 8, and state 0 is never sampled.  The reference
-    # unit test still expects N here; it predates that code (it also builds
-    # the source before setting its RNG) and is stale -- the oracle follows
-    # the source code.
-    x, nh, tr = mc.solve(np.full(n, -1.0), trace=n)
-    assert nh == n - 2
+    # nh = int(mult * N * (N-2)/N) = 8 mult, and state 0 is never sampled.
+    # The reference unit test still expects mult * N here; it predates that
+    # code (it also builds the source before setting its RNG) and is stale --
+    # the oracle follows the source code.
+    x, nh, tr = mc.solve(np.full(n, -1.0), trace=mult * n)
+    assert nh == mult * (n - 2)
     assert np.all(tr["start"] >= 1)
     W = d["weights"][tr["start"]]
     assert np.all(tr["final_weight"] == -float(n) * W)
