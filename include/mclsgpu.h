@@ -168,6 +168,11 @@ int mclsgpu_abi_version(void);
 /* Library build information (architecture, options). */
 const char* mclsgpu_build_info(void);
 
+/* Diagnostics, no counterpart in the reference: the number of device
+ * allocations (cudaMalloc) and releases (cudaFree) the library has made since
+ * it was loaded, over all contexts and devices (either pointer may be NULL). */
+int mclsgpu_debug_device_allocations(int64_t* allocs, int64_t* frees);
+
 /* ---- context ------------------------------------------------------------ */
 /* Replaces the Teuchos::Comm / rank plumbing of the managers: one context per
  * device.  `device` < 0 selects the current device. */
@@ -176,6 +181,14 @@ int mclsgpu_context_destroy(mclsgpu_context* ctx);
 const char* mclsgpu_last_error(const mclsgpu_context* ctx);
 /* Synchronise the context stream and report any pending device error. */
 int mclsgpu_context_sync(mclsgpu_context* ctx);
+/* Failure detection, no counterpart in the reference.  The library's kernels
+ * wait on tensor-core completion barriers with a bounded number of polls
+ * (default 1,048,576); a wait that runs out ends its kernel early, the call
+ * returns MCLSGPU_ERR_TIMEOUT and the context stays usable.  This sets that
+ * bound on the context's device for every later launch (polls < 0 restores
+ * the default; 0 makes every such wait give up at once, which failure-
+ * detection tests use). */
+int mclsgpu_set_wait_limit(mclsgpu_context* ctx, int32_t polls);
 
 /* ---- operator (LinearProblem's A) --------------------------------------- */
 /* Replaces LinearProblem(A, x, b)'s operator handle

@@ -164,6 +164,7 @@ EXPORTS = [
     "mclsgpu_anderson_finish", "mclsgpu_history_wire_size", "mclsgpu_subdomain_build",
     "mclsgpu_subdomain_destroy", "mclsgpu_subdomain_info", "mclsgpu_subdomain_begin",
     "mclsgpu_subdomain_transport", "mclsgpu_subdomain_finish",
+    "mclsgpu_debug_device_allocations", "mclsgpu_set_wait_limit",
 ]
 
 _LIB = None
@@ -194,6 +195,8 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_last_error.argtypes = [P]
     L.mclsgpu_last_error.restype = C.c_char_p
     L.mclsgpu_context_sync.argtypes = [P]
+    L.mclsgpu_debug_device_allocations.argtypes = [C.POINTER(i64), C.POINTER(i64)]
+    L.mclsgpu_set_wait_limit.argtypes = [P, C.c_int32]
     L.mclsgpu_operator_upload.argtypes = [P, i64, P, P, P, PP]
     L.mclsgpu_operator_destroy.argtypes = [P]
     L.mclsgpu_operator_rows.argtypes = [P]
@@ -303,6 +306,11 @@ class Context:
     def check(self, rc):
         if rc != OK:
             raise MclsError(rc, self.L.mclsgpu_last_error(self.h).decode())
+
+    def set_wait_limit(self, polls: int):
+        """Polls a bounded device wait makes before it gives up (< 0: the
+        default)."""
+        self.check(self.L.mclsgpu_set_wait_limit(self.h, int(polls)))
 
     def _adopt(self, child):
         import weakref
@@ -908,6 +916,14 @@ class Subdomain:
 
     def __del__(self):
         self.close()
+
+
+def device_allocations():
+    """(allocations, releases) of device memory the library has made."""
+    L = load()
+    a, f = C.c_int64(), C.c_int64()
+    L.mclsgpu_debug_device_allocations(C.byref(a), C.byref(f))
+    return a.value, f.value
 
 
 def rank_seed(master: int, rank: int) -> int:

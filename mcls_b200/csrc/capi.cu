@@ -12,6 +12,9 @@
 
 namespace mclsgpu {
 
+std::atomic<long long> g_device_allocs{0};
+std::atomic<long long> g_device_frees{0};
+
 int set_error(mclsgpu_context* ctx, int code, const char* fmt, ...) {
     if (ctx) {
         char buf[512];
@@ -180,6 +183,12 @@ const char* mclsgpu_build_info(void) {
     return "mclsgpu sm_100a; walk records FP32 {4,8,12,16,24,32} slots; FP64 parity walk";
 }
 
+int mclsgpu_debug_device_allocations(int64_t* allocs, int64_t* frees) {
+    if (allocs) *allocs = g_device_allocs.load(std::memory_order_relaxed);
+    if (frees) *frees = g_device_frees.load(std::memory_order_relaxed);
+    return MCLSGPU_OK;
+}
+
 int mclsgpu_context_create(int device, mclsgpu_context** out) {
     if (!out) return MCLSGPU_ERR_INVALID_ARG;
     *out = nullptr;
@@ -288,13 +297,24 @@ int mclsgpu_operator_apply(mclsgpu_operator* op, const double* x, double* y) {
         dfree(dx);
         return cuda_fail(ctx, e, "cudaMalloc");
     }
-    cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, ctx->stream);
-    spmv(ctx->stream, op->A, dx, dy);
-    cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-    e = cudaStreamSynchronize(ctx->stream);
+    const char* what = "copy x";
+    e = cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        spmv(ctx->stream, op->A, dx, dy);
+        what = "apply: spmv launch";
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        what = "copy y";
+        e = cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (e == cudaSuccess) {
+        what = "apply";
+        e = cudaStreamSynchronize(ctx->stream);
+    }
     dfree(dx);
     dfree(dy);
-    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "apply");
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, what);
 }
 
 // ---- preconditioner ----------------------------------------------------------

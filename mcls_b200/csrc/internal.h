@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <functional>
 #include <string>
@@ -195,13 +196,21 @@ namespace mclsgpu {
 int set_error(mclsgpu_context* ctx, int code, const char* fmt, ...);
 int cuda_fail(mclsgpu_context* ctx, cudaError_t e, const char* what);
 int check_device_status(mclsgpu_context* ctx);
+// Every device allocation and release of the library goes through dmalloc and
+// dfree; the counters behind mclsgpu_debug_device_allocations count them.
+extern std::atomic<long long> g_device_allocs;
+extern std::atomic<long long> g_device_frees;
 template <class T>
 inline cudaError_t dmalloc(T** p, size_t count) {
+    g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T) + 16);
 }
 template <class T>
 inline void dfree(T*& p) {
-    if (p) cudaFree(p);
+    if (p) {
+        g_device_frees.fetch_add(1, std::memory_order_relaxed);
+        cudaFree(p);
+    }
     p = nullptr;
 }
 

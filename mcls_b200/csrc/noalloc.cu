@@ -19,7 +19,12 @@
 //     context or stream on the same device) race on it; serialise them.
 //   * The first call on a device looks up the array's device address (once
 //     per device, with that device current).  Make that first call before
-//     any stream capture begins.
+//     any stream capture begins.  The address is cached together with the
+//     device's current CUDA context; after cudaDeviceReset (or any other
+//     teardown of the primary context) the module is loaded again, the
+//     context handle changes and the next call looks the address up anew.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "internal.h"
@@ -36,17 +41,44 @@ static __device__ __align__(256) double g_apply_stage[2 * kStaticApplyMaxRows];
 
 std::mutex g_addr_mutex;
 double* g_addr[kMaxDevices] = {nullptr};
+CUcontext g_addr_ctx[kMaxDevices] = {nullptr};
 
-// Device address of the staging array on `device` (the current device).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+// cuCtxGetCurrent through the runtime's driver entry point table, so the
+// library needs no link against libcuda.  Called with g_addr_mutex held.
+int current_context(mclsgpu_context* ctx, CUcontext* out) {
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000,
+                                                         cudaEnableDefault, &q);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "driver entry point cuCtxGetCurrent");
+        if (q != cudaDriverEntryPointSuccess || !f)
+            return set_error(ctx, MCLSGPU_ERR_CUDA, "driver entry point cuCtxGetCurrent not found");
+        fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    }
+    if (fn(out) != CUDA_SUCCESS || !*out)
+        return set_error(ctx, MCLSGPU_ERR_CUDA, "no current CUDA context");
+    return MCLSGPU_OK;
+}
+
+// Device address of the staging array on `device` (the current device), looked
+// up once per device and again whenever the device's context has changed.
 int stage_address(mclsgpu_context* ctx, double** out) {
     std::lock_guard<std::mutex> lock(g_addr_mutex);
     if (ctx->device < 0 || ctx->device >= kMaxDevices)
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "device ordinal out of range");
-    if (!g_addr[ctx->device]) {
+    CUcontext cur = nullptr;
+    int rc = current_context(ctx, &cur);
+    if (rc) return rc;
+    if (!g_addr[ctx->device] || g_addr_ctx[ctx->device] != cur) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_apply_stage);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(staging array)");
         g_addr[ctx->device] = static_cast<double*>(p);
+        g_addr_ctx[ctx->device] = cur;
     }
     *out = g_addr[ctx->device];
     return MCLSGPU_OK;
@@ -76,7 +108,10 @@ extern "C" int mclsgpu_operator_apply_static(mclsgpu_operator* op, const double*
     e = cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "copy x");
     spmv(ctx->stream, op->A, dx, dy);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "static apply: spmv launch");
     e = cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy y");
+    e = cudaStreamSynchronize(ctx->stream);
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "static apply");
 }

@@ -130,9 +130,15 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// Bounded wait for the phase `parity` of an mbarrier to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int it = 0; it < (1 << 20); ++it) {
+// Polls a bounded mbarrier wait makes before it gives up (host-settable
+// through mclsgpu_set_wait_limit; 0 makes every such wait give up at once).
+constexpr int kDefaultWaitPolls = 1 << 20;
+__device__ int g_wait_polls = kDefaultWaitPolls;
+
+// Bounded wait for the phase `parity` of an mbarrier to complete, at most
+// `polls` polls.
+__device__ __forceinline__ bool mbar_wait_n(uint32_t mbar, uint32_t parity, int polls) {
+    for (int it = 0; it < polls; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred P1;\n\t"
@@ -144,6 +150,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
         if (ok) return true;
     }
     return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    return mbar_wait_n(mbar, parity, *reinterpret_cast<volatile int*>(&g_wait_polls));
+}
+// After a wait gave up, the MMAs of the phase it waited for may still be
+// writing tensor memory.  The thread that issued them waits for that phase
+// (with the default bound, whatever the host limit) before the columns are
+// released.
+__device__ __forceinline__ void mbar_drain(uint32_t mbar, uint32_t parity) {
+    mbar_wait_n(mbar, parity, kDefaultWaitPolls);
 }
 __device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
@@ -282,6 +298,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
     const float* b3 = a.params + kB3;
     uint32_t phase = 0;
     bool ok = true;
+    // Thread 0 issues the MMAs, and only while its own waits succeed, so at
+    // most one committed phase is outstanding when a wait gives up.
+    bool pend = false;
+    uint32_t pend_parity = 0;
+    auto wait_mma = [&]() {
+        const bool got = ok && mbar_wait(mbar, phase);
+        if (ok && !got) {
+            pend = true;
+            pend_parity = phase;
+        }
+        ok = got;
+        phase ^= 1;
+        fence_after_sync();
+    };
     const int ntiles = (a.n + kTileRows - 1) / kTileRows;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int row = tile * kTileRows + tid;
@@ -295,15 +325,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
         fence_before_sync();
         __syncthreads();
         // Layer 1: Z1 = X W1^T  (M 128, N 64, K 16).
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             mma_bf16(tmem, desc_kmajor(sX, kTileRows, 0), desc_kmajor(sW1, kH, 0),
                      idesc_bf16(128, kH, 0, 0), 0);
             mma_commit(mbar);
         }
-        ok = mbar_wait(mbar, phase);
-        phase ^= 1;
-        fence_after_sync();
+        wait_mma();
 #pragma unroll 1
         for (int c = 0; c < kH; c += 16) {
             float z[16];
@@ -317,16 +345,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
         fence_before_sync();
         __syncthreads();
         // Layer 2: Z2 = H1 W2^T  (M 128, N 64, K 64).
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
                 mma_bf16(tmem + 64, desc_kmajor(sH, kTileRows, ks), desc_kmajor(sW2, kH, ks),
                          idesc_bf16(128, kH, 0, 0), ks > 0);
             mma_commit(mbar);
         }
-        ok = ok && mbar_wait(mbar, phase);
-        phase ^= 1;
-        fence_after_sync();
+        wait_mma();
         // H2 overwrites H1: layer 2's operands are consumed (its MMAs are
         // complete once the barrier phase has flipped).
         float h2[kH];
@@ -340,23 +366,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
         fence_before_sync();
         __syncthreads();
         // Layer 3: out = H2 W3^T  (M 128, N 16, K 64).
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
                 mma_bf16(tmem, desc_kmajor(sH, kTileRows, ks), desc_kmajor(sW3, kO, ks),
                          idesc_bf16(128, kO, 0, 0), ks > 0);
             mma_commit(mbar);
         }
-        ok = ok && mbar_wait(mbar, phase);
-        phase ^= 1;
-        fence_after_sync();
+        wait_mma();
         float o[kO];
         tmem_ld16(lane_base, o);
         fence_before_sync();
         // The next tile's layer 1 reuses these columns; a timed-out wait on
         // any thread ends the loop on all of them.
         ok = __syncthreads_and(ok);
-        if (row < a.n) {
+        if (ok && row < a.n) {
 #pragma unroll
             for (int k = 0; k < kO; ++k) o[k] += b3[k];
             if (a.out) {
@@ -377,6 +401,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
         }
     }
     if (!ok && tid == 0) atomicExch(a.status, MCLSGPU_ERR_TIMEOUT);
+    if (tid == 0 && pend) mbar_drain(mbar, pend_parity);
     fence_before_sync();
     __syncthreads();
     if (warp == 0) {
@@ -462,6 +487,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
     uint32_t phase = 0;
     bool ok = true;
     int done = 0;
+    // Thread 0 issues the MMAs only while its own waits succeed (at most one
+    // committed phase outstanding when a wait gives up).
+    bool pend = false;
+    uint32_t pend_parity = 0;
     const int ntiles = (a.n + kTileRows - 1) / kTileRows;
     auto stage_sync = [&]() {
         fence_async_smem();
@@ -469,7 +498,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
         __syncthreads();
     };
     auto wait_mma = [&]() {
-        ok = ok && mbar_wait(mbar, phase);
+        const bool got = ok && mbar_wait(mbar, phase);
+        if (ok && !got) {
+            pend = true;
+            pend_parity = phase;
+        }
+        ok = got;
         phase ^= 1;
         fence_after_sync();
     };
@@ -482,7 +516,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
             store8(smem + kBwX, tid, 8, kTileRows, f + 8);
         }
         stage_sync();
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             mma_bf16(tmem + kTA, desc_kmajor(sX, kTileRows, 0), desc_kmajor(sW1, kH, 0),
                      idesc_bf16(128, kH, 0, 0), 0);
@@ -499,7 +533,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
             store8(smem + kBwH1, tid, c + 8, kTileRows, z + 8);
         }
         stage_sync();
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
                 mma_bf16(tmem + kTB, desc_kmajor(sH1, kTileRows, ks), desc_kmajor(sW2, kH, ks),
@@ -545,7 +579,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
         stage_sync();
         // dH2 = G W3 (B = W3 read MN-major: N 64 = h2, K 16 = o) and
         // dW3^T += H2^T G (A = H2 MN-major, B = G MN-major; K = 128 rows).
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             mma_bf16(tmem + kTA, desc_kmajor(sG, kTileRows, 0), desc_mnmajor(sW3, kO, 0),
                      idesc_bf16(128, kH, 0, 1), 0);
@@ -570,7 +604,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
         stage_sync();
         // dH1 = dZ2 W2 (B = W2 MN-major: N 64 = h1, K 64 = h2) and
         // [dW2 | db2] += dZ2^T [H1 | 1] (K = 128 rows).
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
                 mma_bf16(tmem + kTB, desc_kmajor(sDZ2, kTileRows, ks), desc_mnmajor(sW2, kH, ks),
@@ -595,7 +629,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
         }
         stage_sync();
         // [dW1 | db1] += dZ1^T [X | 1] (K = 128 rows).
-        if (tid == 0) {
+        if (tid == 0 && ok) {
             fence_after_sync();
             for (int ks = 0; ks < kTileRows / 16; ++ks)
                 mma_bf16(tmem + kTdW1, desc_mnmajor(sDZ1, kTileRows, ks),
@@ -610,6 +644,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_backward(SpaiBwdArgs a) {
         ok = __syncthreads_and(ok);
     }
     if (!ok && tid == 0) atomicExch(a.status, MCLSGPU_ERR_TIMEOUT);
+    if (tid == 0 && pend) mbar_drain(mbar, pend_parity);
     if (ok && done > 0) {
         fence_after_sync();
         // M = 64 accumulators: row 16w + t of the product sits in lane
@@ -1058,6 +1093,17 @@ int spai_build(mclsgpu_context* ctx, mclsgpu_operator* op, const mclsgpu_precond
 using namespace mclsgpu;
 
 extern "C" {
+
+int mclsgpu_set_wait_limit(mclsgpu_context* ctx, int32_t polls) {
+    if (!ctx) return MCLSGPU_ERR_INVALID_ARG;
+    const int v = polls < 0 ? kDefaultWaitPolls : polls;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess)
+        e = cudaMemcpyToSymbolAsync(g_wait_polls, &v, sizeof(int), 0, cudaMemcpyHostToDevice,
+                                    ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "set wait limit");
+}
 
 int mclsgpu_spai_num_params(void) { return kParams; }
 

@@ -70,10 +70,12 @@ def anderson_params(tolerance=1e-8, max_iters=1000, smoother_steps=1, storage_de
 
 
 def build():
-    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    """Compile liboracle.so, and oracle/_ref when the environment variable
+    MCLS_REFERENCE_ROOT names an MCLS source tree."""
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    ref = os.environ.get("MCLS_REFERENCE_ROOT", "")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF_ROOT=" + ref], check=True)
 
 
 def lib():

@@ -1,12 +1,12 @@
 """Generate golden vectors from the reference's own RNG and CDF sampler.
 
-Run in a container that has the MCLS reference tree: it builds oracle/_ref
+Run with MCLS_REFERENCE_ROOT naming an MCLS source tree: it builds oracle/_ref
 (src/MCLS_Xorshift.hpp, src/MCLS_RNGTraits.hpp, src/MCLS_SamplingTools.hpp,
 src/MCLS_DBC.cpp compiled where they lie) and writes reference_rng.json next
 to this script.  The tests compare the oracle against this file, so the GPU
 box (which has no reference tree) still checks the oracle's pin.
 
-    python tests/golden/make_golden.py
+    MCLS_REFERENCE_ROOT=<MCLS tree> python tests/golden/make_golden.py
 """
 import json
 import os

@@ -44,6 +44,29 @@ def test_static_apply_smaller_operator_after_larger(ctx):
 
 
 @pytest.mark.gpu
+def test_static_apply_makes_no_device_allocation(ctx):
+    # The library counts every cudaMalloc/cudaFree it makes.  The allocating
+    # apply moves the counters (which shows they count); repeated static
+    # applies after the first must leave them where they were.
+    A, _ = P.diffusion3d_varcoef(16, seed=8)
+    op = capi.Operator(ctx, A)
+    try:
+        x = np.random.default_rng(9).standard_normal(A.shape[0])
+        a0, f0 = capi.device_allocations()
+        op.apply(x)
+        a1, f1 = capi.device_allocations()
+        assert a1 - a0 == 2 and f1 - f0 == 2
+        first = op.apply_static(x)
+        a2, f2 = capi.device_allocations()
+        for _ in range(5):
+            np.testing.assert_array_equal(op.apply_static(x), first)
+        assert capi.device_allocations() == (a2, f2)
+        assert (a2, f2) == (a1, f1)
+    finally:
+        op.close()
+
+
+@pytest.mark.gpu
 def test_static_apply_rejects_operator_above_limit(ctx):
     n = (1 << 20) + 1
     A = sp.identity(n, format="csr")
