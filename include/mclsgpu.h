@@ -325,6 +325,20 @@ int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps
                             int* histories_per_lane, int* block_size,
                             double* walk_ms);
 
+/* Precision check of the FP32 walk, no counterpart in the reference: runs
+ * `histories` histories of History Length transitions (history e starts at
+ * state e mod n on its own counter stream keyed by `seed`) along the FP64
+ * domain, selecting each transition with std::lower_bound over the FP64 CDF
+ * for u = the 53-bit canonical uniform of the draw, as the reference
+ * samples (src/MCLS_SamplingTools.hpp:67-80); at every transition the FP32
+ * record of the same state is searched as the production walk does, with
+ * the 24-bit uniform of the same draw.  Reports the histories with at least
+ * one transition where the two select a different column or sign, and the
+ * number of such transitions (of histories * History Length).  Needs an
+ * FP32 domain. */
+int mclsgpu_domain_walk_agreement(mclsgpu_domain* dom, int64_t histories, uint64_t seed,
+                                  int64_t* histories_differing, int64_t* transitions_differing);
+
 /* Replace the stream seed/position (restart the reproducible stream). */
 int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed);
 /* Per-rank Xorshift seed as PRNG<RNG>(rank) derives it

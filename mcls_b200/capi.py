@@ -165,6 +165,7 @@ EXPORTS = [
     "mclsgpu_subdomain_destroy", "mclsgpu_subdomain_info", "mclsgpu_subdomain_begin",
     "mclsgpu_subdomain_transport", "mclsgpu_subdomain_finish",
     "mclsgpu_debug_device_allocations", "mclsgpu_set_wait_limit",
+    "mclsgpu_domain_walk_agreement",
 ]
 
 _LIB = None
@@ -212,6 +213,8 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_domain_destroy.argtypes = [P]
     L.mclsgpu_domain_export.argtypes = [P, C.POINTER(i64), P, P, P, P, P]
     L.mclsgpu_domain_reseed.argtypes = [P, C.c_uint64]
+    L.mclsgpu_domain_walk_agreement.argtypes = [P, i64, C.c_uint64, C.POINTER(i64),
+                                                C.POINTER(i64)]
     L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
     L.mclsgpu_domain_set_launch.argtypes = [P, C.c_int, C.c_int]
     L.mclsgpu_domain_autotune.argtypes = [P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -535,6 +538,14 @@ class Domain:
                                                           C.byref(hpl), C.byref(blk),
                                                           C.byref(ms)))
         return {"histories_per_lane": hpl.value, "block_size": blk.value, "walk_ms": ms.value}
+
+    def walk_agreement(self, histories, seed=1):
+        """FP32 walk against the FP64 selection on the same draws: (histories
+        with a differing transition, differing transitions)."""
+        h, t = C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.L.mclsgpu_domain_walk_agreement(self.h, int(histories), seed,
+                                                                C.byref(h), C.byref(t)))
+        return h.value, t.value
 
     def reseed(self, seed):
         self.ctx.check(self.ctx.L.mclsgpu_domain_reseed(self.h, seed))

@@ -788,7 +788,9 @@ int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
     if (rc) return rc;
     AndersonWork* w = dom->aa;
     const long long key = (long long)p->smoother_steps * 64 + p->storage_depth;
-    if (!p->host_loop && (!w->graph || w->graph_key != key || w->graph_hist != dom->d_resid)) {
+    // Variable-length reference-stream walks synchronise with the host.
+    const bool host_loop = p->host_loop || walk_needs_rounds(dom);
+    if (!host_loop && (!w->graph || w->graph_key != key || w->graph_hist != dom->d_resid)) {
         if (w->graph) cudaGraphExecDestroy(w->graph);
         w->graph = nullptr;
         rc = build_while_graph(
@@ -805,7 +807,7 @@ int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
     anderson_begin(dom, b_dev, x_dev, p);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e == cudaSuccess && !w->h_st->done) {
-        if (!p->host_loop) {
+        if (!host_loop) {
             e = cudaGraphLaunch(w->graph, s);
         } else {
             for (int it = 0; it < p->max_iters && e == cudaSuccess; ++it) {

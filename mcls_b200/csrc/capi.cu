@@ -51,6 +51,8 @@ int check_device_status(mclsgpu_context* ctx) {
 }
 
 void prepare_walk(mclsgpu_domain* dom);
+int walk_agreement(mclsgpu_domain* dom, long long histories, uint64_t seed, long long* hist_diff,
+                   long long* trans_diff);
 void prepare_source(mclsgpu_domain* dom);
 int spai_build(mclsgpu_context* ctx, mclsgpu_operator* op, const mclsgpu_precond_params* p,
                mclsgpu_precond* pc);
@@ -136,6 +138,10 @@ void release_domain(mclsgpu_domain* d) {
     dfree(d->rec);
     dfree(d->d_jump);
     dfree(d->d_pos);
+    dfree(d->hoff);
+    dfree(d->hlen);
+    dfree(d->hoff2);
+    dfree(d->y_save);
     dfree(d->d_epoch);
     dfree(d->src);
     dfree(d->scdf);
@@ -411,9 +417,10 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "bad precision");
     if (p->rng_mode != MCLSGPU_RNG_REFERENCE && p->rng_mode != MCLSGPU_RNG_COUNTER)
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "bad rng mode");
-    if (p->rng_mode == MCLSGPU_RNG_REFERENCE && p->weight_cutoff > 0.0)
+    if (p->rng_mode == MCLSGPU_RNG_REFERENCE && p->weight_cutoff > 0.0 &&
+        p->precision != MCLSGPU_FP64)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
-                         "the reference stream needs fixed-length histories (no Weight Cutoff)");
+                         "a Weight Cutoff on the reference stream needs the FP64 walk");
     if ((left && left->P.n != op->A.n) || (right && right->P.n != op->A.n))
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "preconditioner size mismatch");
     if (left && left->kind == MCLSGPU_PREC_NONE) left = nullptr;
@@ -531,6 +538,12 @@ int mclsgpu_domain_build(mclsgpu_context* ctx, mclsgpu_operator* op, mclsgpu_pre
         const unsigned long long tim0[4] = {~0ULL, 0ULL, 0ULL, 0ULL};
         cudaMemcpyAsync(dom->d_tim, tim0, sizeof(tim0), cudaMemcpyHostToDevice, ctx->stream);
         cudaStreamSynchronize(ctx->stream);
+        if (!rc && walk_needs_rounds(dom) &&
+            ((e = dmalloc(&dom->hoff, size_t(dom->nh_cap) + 1)) != cudaSuccess ||
+             (e = dmalloc(&dom->hlen, size_t(dom->nh_cap) + 1)) != cudaSuccess ||
+             (e = dmalloc(&dom->hoff2, size_t(dom->nh_cap) + 2)) != cudaSuccess ||
+             (e = dmalloc(&dom->y_save, n)) != cudaSuccess))
+            rc = cuda_fail(ctx, e, "cudaMalloc history offsets");
         if (p->rng_mode == MCLSGPU_RNG_REFERENCE) {
             std::vector<uint64_t> tab(64 * 64);
             xs_jump_tables(tab.data());
@@ -585,6 +598,17 @@ int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info) {
     info->max_row_entries = dom->max_row;
     info->stencil_offsets = dom->stencil_k;
     info->operator_dia = dom->op->dia_k;
+    return MCLSGPU_OK;
+}
+
+int mclsgpu_domain_walk_agreement(mclsgpu_domain* dom, int64_t histories, uint64_t seed,
+                                  int64_t* histories_differing, int64_t* transitions_differing) {
+    if (!dom || !histories_differing || !transitions_differing) return MCLSGPU_ERR_INVALID_ARG;
+    long long h = 0, t = 0;
+    int rc = walk_agreement(dom, histories, seed, &h, &t);
+    if (rc) return rc;
+    *histories_differing = h;
+    *transitions_differing = t;
     return MCLSGPU_OK;
 }
 

@@ -185,6 +185,14 @@ struct mclsgpu_domain {
     // Step-wise MCSA (mclsgpu_mcsa_begin .. _finish).
     mclsgpu_mcsa_params step_p{};
     int step_ready = 0;
+    // Reference stream with a weight cutoff (variable-length histories): each
+    // history's first draw is the sum of the earlier histories' lengths,
+    // found by rounds of FP64 walks (walk.cu).
+    int* hoff = nullptr;           // per-history stream offsets (nh_cap)
+    int* hlen = nullptr;           // per-history lengths of the last round
+    int* hoff2 = nullptr;          // offsets recomputed from hlen (nh_cap + 1)
+    double* y_save = nullptr;      // tallies before the first round (n)
+    int walk_rounds = 0;           // rounds the last Monte Carlo solve took
     // Anderson-accelerated MCSA work space (anderson.cu), built on first use.
     mclsgpu::AndersonWork* aa = nullptr;
     int aa_step_ready = 0;
@@ -271,6 +279,12 @@ void richardson_residual(mclsgpu_domain* dom, const double* x, const double* r, 
 // out = the Monte Carlo estimate for the source v (already left
 // preconditioned): one MC solve, advancing the domain's random stream.
 void mc_correction(mclsgpu_domain* dom, const double* v, double* out);
+// True when the domain walks variable-length histories on the reference
+// stream: those walks synchronise with the host (rounds), so the MCSA and
+// Anderson loops run from the host instead of a captured graph.
+inline bool walk_needs_rounds(const mclsgpu_domain* dom) {
+    return dom->p.rng_mode == MCLSGPU_RNG_REFERENCE && dom->p.weight_cutoff > 0.0;
+}
 // Walk statistics since the last reset (steps, histories, walk time).
 int mcsa_read_stats(mclsgpu_domain* dom, mclsgpu_stats* st);
 void mcsa_reset_counters(mclsgpu_domain* dom);

@@ -871,7 +871,9 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
         cudaEventDestroy(e1);
         return rc;
     }
-    if (!mp->host_loop && (!dom->graph || dom->graph_key != key)) {
+    // Variable-length reference-stream walks synchronise with the host.
+    const bool host_loop = mp->host_loop || walk_needs_rounds(dom);
+    if (!host_loop && (!dom->graph || dom->graph_key != key)) {
         int rc = build_mcsa_graph(dom, mp);
         if (rc) {
             cudaEventDestroy(e0);
@@ -898,7 +900,7 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
                                 mp->max_iters, dom->d_scalars + 5);
     if (fused_iteration(dom, mp) && dom->p.direction == MCLSGPU_FORWARD) launch_forward_setup(dom);
     cudaError_t e = cudaSuccess;
-    if (!mp->host_loop) {
+    if (!host_loop) {
         e = cudaGraphLaunch(dom->graph, s);
     } else {
         // Host-driven loop: the same iteration, one state read-back each.

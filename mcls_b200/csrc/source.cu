@@ -572,7 +572,9 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
 }
 
 void launch_advance_walk_pos(mclsgpu_domain* dom) {
-    if (dom->p.rng_mode == MCLSGPU_RNG_REFERENCE)
+    // Variable-length histories advance the stream by their summed lengths
+    // in the walk itself.
+    if (dom->p.rng_mode == MCLSGPU_RNG_REFERENCE && !walk_needs_rounds(dom))
         k_advance_pos<<<1, 1, 0, dom->ctx->stream>>>(dom->d_pos, dom->d_nh, dom->p.history_length);
 }
 

@@ -62,6 +62,10 @@ struct WalkArgs {
     int* status;
     int row0;                   // global index of the first record / tally row
     int stoff[32];              // stencil records: column offset of each slot
+    // variable-length histories on the reference stream (FP64 only): history
+    // e's first draw is *d_pos + hoff[e]; hlen[e] receives its length
+    const int* hoff;
+    int* hlen;
     // trace (FP64 only)
     long long max_trace;
     long long* tr_states;
@@ -92,7 +96,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 __device__ __forceinline__ uint64_t history_state(const WalkArgs& a, uint64_t ekey, long long e) {
     if (a.rng_mode == MCLSGPU_RNG_COUNTER) return counter_state(ekey, 2, uint64_t(e));
-    return xs_jump(a.jump, a.seed, *a.d_pos + uint64_t(e) * uint64_t(a.L));
+    const uint64_t off = a.hoff ? uint64_t(a.hoff[e]) : uint64_t(e) * uint64_t(a.L);
+    return xs_jump(a.jump, a.seed, *a.d_pos + off);
 }
 
 // Small records (up to 8 slots) run at full occupancy: 8 blocks of 256 threads
@@ -103,6 +108,56 @@ template <int S>
 struct WalkOccupancy {
     static constexpr int kMinBlocks = S <= 8 ? 8 : (S <= 24 ? 4 : 2);
 };
+
+// Selection in one FP32 record (the S-slot words q of state s) for the
+// uniform u: the first entry whose CDF value is >= u (sampleDiscreteCDF's
+// lower_bound).  s becomes the selected column; neg is the sign bit of the
+// selected h.
+template <int S, bool ST>
+__device__ __forceinline__ void select32(const WalkArgs& a, const uint32_t* q, float u, int& s,
+                                         unsigned& neg) {
+    if constexpr (!ST) {
+        unsigned sel = q[3];  // slot 1 (first entry)
+        bool found = __uint_as_float(q[2]) >= u;
+#pragma unroll
+        for (int t = 2; t < S; ++t) {
+            const bool c = !found && __uint_as_float(q[2 * t]) >= u;
+            sel = c ? q[2 * t + 1] : sel;
+            found = found || c;
+        }
+        neg = sel & 0x80000000u;
+        s = int(sel & 0x7fffffffu);
+    } else {
+        // Stencil slots: first |cdf_j| >= u (NaN slots never match); the next
+        // state is s + offset_j, the sign of h_j is the sign bit of the slot.
+        int dsel = 0;
+        unsigned ng = 0u;
+        bool found = false;
+#pragma unroll
+        for (int j = 0; j < 2 * S - 2; ++j) {
+            const bool c = !found && fabsf(__uint_as_float(q[2 + j])) >= u;
+            dsel = c ? a.stoff[j] : dsel;
+            ng = c ? (q[2 + j] & 0x80000000u) : ng;
+            found = found || c;
+        }
+        neg = ng;
+        s += dsel;
+    }
+}
+
+// Selection in the FP64 domain row of state s for the uniform u
+// (std::lower_bound over the row's CDF, as the reference samples it).
+// Returns the entry index within the row; the caller checks it is < len.
+__device__ __forceinline__ int select64(const WalkArgs& a, int s, double u, int& r0, int& len) {
+    r0 = a.rp[s];
+    len = a.rp[s + 1] - r0;
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a.cdf[r0 + mid] < u) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
 
 // One transition of a history at state s (DomainTransporter::transport's
 // loop body): tally at the pre-transition state, read the state's record,
@@ -131,33 +186,9 @@ __device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, in
     x = xs_step(x);
     const float u = canonical32(x);
     const float Wt = __uint_as_float(q[0]);
-    if constexpr (!ST) {
-        unsigned sel = q[3];  // slot 1 (first entry)
-        bool found = __uint_as_float(q[2]) >= u;
-#pragma unroll
-        for (int t = 2; t < S; ++t) {
-            const bool c = !found && __uint_as_float(q[2 * t]) >= u;
-            sel = c ? q[2 * t + 1] : sel;
-            found = found || c;
-        }
-        w = (sel & 0x80000000u) ? -(w * Wt) : w * Wt;
-        s = int(sel & 0x7fffffffu);
-    } else {
-        // Stencil slots: first |cdf_j| >= u (NaN slots never match); the next
-        // state is s + offset_j, the sign of h_j is the sign bit of the slot.
-        int dsel = 0;
-        unsigned neg = 0u;
-        bool found = false;
-#pragma unroll
-        for (int j = 0; j < 2 * S - 2; ++j) {
-            const bool c = !found && fabsf(__uint_as_float(q[2 + j])) >= u;
-            dsel = c ? a.stoff[j] : dsel;
-            neg = c ? (q[2 + j] & 0x80000000u) : neg;
-            found = found || c;
-        }
-        w = neg ? -(w * Wt) : w * Wt;
-        s += dsel;
-    }
+    unsigned neg;
+    select32<S, ST>(a, q, u, s, neg);
+    w = neg ? -(w * Wt) : w * Wt;
 }
 
 // Starting state, weight and stream of history e.
@@ -331,12 +362,8 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
             }
             x = xs_step(x);
             const double u = canonical64(x);
-            const int r0 = a.rp[s], len = a.rp[s + 1] - r0;
-            int lo = 0, hi = len;
-            while (lo < hi) {
-                int mid = (lo + hi) >> 1;
-                if (a.cdf[r0 + mid] < u) lo = mid + 1; else hi = mid;
-            }
+            int r0, len;
+            int lo = select64(a, s, u, r0, len);
             if (lo >= len) {
                 atomicOr(a.status, DEV_ERR_BOUNDS);
                 lo = len - 1;
@@ -350,6 +377,7 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
             if (k >= L || fabs(w) < wcut) break;
         }
         if (!isfinite(w)) atomicOr(a.status, DEV_ERR_NONFINITE);
+        if (a.hlen) a.hlen[e] = k;
         if (DIR == MCLSGPU_FORWARD) atomicAdd(&a.y64[s0], acc);
         if (e < a.max_trace) {
             if (a.tr_w) a.tr_w[e] = w;
@@ -627,6 +655,74 @@ int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y, co
     return MCLSGPU_OK;
 }
 
+__global__ void k_fill_offsets(int* hoff, const int* d_nh, int L) {
+    const int nh = *d_nh;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nh; e += gridDim.x * blockDim.x)
+        hoff[e] = e * L;
+}
+
+// hoff2 (exclusive prefix of the lengths) against hoff: *changed = 1 when
+// any offset moved; hoff takes the new offsets.
+__global__ void k_update_offsets(int* hoff, const int* hoff2, const int* d_nh, int* changed) {
+    const int nh = *d_nh;
+    int c = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nh; e += gridDim.x * blockDim.x) {
+        if (hoff[e] != hoff2[e]) {
+            c = 1;
+            hoff[e] = hoff2[e];
+        }
+    }
+    if (__syncthreads_or(c) && threadIdx.x == 0) atomicOr(changed, 1);
+}
+
+__global__ void k_advance_pos_by(unsigned long long* d_pos, long long draws) { *d_pos += draws; }
+
+// Variable-length histories on the reference stream (a Weight Cutoff with
+// "Reproducible MC Mode"): the reference draws history e's uniforms right
+// after history e-1's, so e's first draw depends on every earlier length.
+// Round 1 walks with offsets e * L; each later round walks again with the
+// offsets the previous round's lengths give, until no offset moves.  The
+// histories before the first moved offset are final after each round, so the
+// rounds end (at most one more than the histories); in practice lengths
+// repeat and a few rounds suffice.  Tallies and the step count are restored
+// before each repeated round.  Host-synchronous.
+static void walk_reference_rounds(mclsgpu_domain* dom, WalkArgs a, int grid) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t st = ctx->stream;
+    const int n = dom->n;
+    const int L = dom->p.history_length;
+    int nh = 0;
+    unsigned long long steps0 = 0;
+    cudaMemcpyAsync(&nh, dom->d_nh, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&steps0, dom->d_steps, sizeof(steps0), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(dom->y_save, dom->y64, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice,
+                    st);
+    k_fill_offsets<<<grid, 128, 0, st>>>(dom->hoff, dom->d_nh, L);
+    a.hoff = dom->hoff;
+    a.hlen = dom->hlen;
+    int* changed = reinterpret_cast<int*>(dom->hoff2 + dom->nh_cap + 1);
+    long long total = 0;
+    int rounds = 0;
+    for (;;) {
+        ++rounds;
+        if (dom->p.direction == MCLSGPU_ADJOINT)
+            walk64<MCLSGPU_ADJOINT><<<grid, 128, 0, st>>>(a);
+        else
+            walk64<MCLSGPU_FORWARD><<<grid, 128, 0, st>>>(a);
+        if (nh == 0 || exclusive_scan_counts_dev(ctx, dom->hlen, nh, dom->hoff2, &total)) break;
+        cudaMemsetAsync(changed, 0, sizeof(int), st);
+        k_update_offsets<<<grid, 128, 0, st>>>(dom->hoff, dom->hoff2, dom->d_nh, changed);
+        int h_changed = 0;
+        cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess || !h_changed || rounds > nh) break;
+        cudaMemcpyAsync(dom->y64, dom->y_save, size_t(n) * sizeof(double),
+                        cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(dom->d_steps, &steps0, sizeof(steps0), cudaMemcpyHostToDevice, st);
+    }
+    dom->walk_rounds = rounds;
+    k_advance_pos_by<<<1, 1, 0, st>>>(dom->d_pos, total);
+}
+
 // Launch the walks of the current source.  Trace arrays only with FP64.
 // `fused`: the work-queue counter reset and the timing accumulation are done
 // by the fused residual kernel that follows the walk (MCSA loop).
@@ -662,7 +758,9 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
         long long g = (dom->nh_cap + 127) / 128;
         if (g < 1) g = 1;
         const int grid = int(g < ctx->num_sms * 8 ? g : ctx->num_sms * 8);
-        if (p.direction == MCLSGPU_ADJOINT)
+        if (walk_needs_rounds(dom))
+            walk_reference_rounds(dom, a, grid);
+        else if (p.direction == MCLSGPU_ADJOINT)
             walk64<MCLSGPU_ADJOINT><<<grid, 128, 0, st>>>(a);
         else
             walk64<MCLSGPU_FORWARD><<<grid, 128, 0, st>>>(a);
@@ -750,7 +848,117 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
     if ((threadIdx.x & 31) == 0 && steps) atomicAdd(p.d_steps, (unsigned long long)steps);
 }
 
+// FP32-versus-FP64 transition agreement.  History e starts at state e mod n
+// on its counter stream and walks `L` transitions along the FP64 domain
+// (walk64's selection with u = canonical64(x)); at every transition the FP32
+// record of the same state is searched with u = canonical32(x) of the same
+// draw (walk32's selection).  A transition disagrees when the two select a
+// different column or sign; out[0] += histories with at least one
+// disagreement, out[1] += disagreeing transitions.
+template <int S, bool ST>
+__global__ void __launch_bounds__(256) k_walk_agreement(WalkArgs a, long long nh, uint64_t ekey,
+                                                        unsigned long long* out) {
+    const char* rec = reinterpret_cast<const char*>(a.rec);
+    unsigned long long hd = 0, td = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nh;
+         e += (long long)gridDim.x * blockDim.x) {
+        int s = int(e % a.n);
+        uint64_t x = counter_state(ekey, 2, uint64_t(e));
+        bool differ = false;
+        for (int k = 0; k < a.L; ++k) {
+            uint32_t q[2 * S];
+            const char* r = rec + size_t(s) * (S * 8);
+#pragma unroll
+            for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
+            x = xs_step(x);
+            int s32 = s;
+            unsigned neg32;
+            select32<S, ST>(a, q, canonical32(x), s32, neg32);
+            int r0, len;
+            int j = select64(a, s, canonical64(x), r0, len);
+            if (j >= len) {
+                atomicOr(a.status, DEV_ERR_BOUNDS);
+                j = len - 1;
+            }
+            const int s64 = a.col[r0 + j];
+            const bool neg64 = !(a.h[r0 + j] > 0.0);
+            if (s32 != s64 || (neg32 != 0u) != neg64) {
+                ++td;
+                differ = true;
+            }
+            s = s64;
+        }
+        hd += differ ? 1 : 0;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        hd += __shfl_down_sync(kFull, hd, d);
+        td += __shfl_down_sync(kFull, td, d);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (hd) atomicAdd(&out[0], hd);
+        if (td) atomicAdd(&out[1], td);
+    }
+}
+
 }  // namespace
+
+int walk_agreement(mclsgpu_domain* dom, long long histories, uint64_t seed, long long* hist_diff,
+                   long long* trans_diff) {
+    mclsgpu_context* ctx = dom->ctx;
+    if (dom->p.precision != MCLSGPU_FP32 || !dom->rec)
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "walk agreement needs FP32 records");
+    if (histories < 1) return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "histories < 1");
+    WalkArgs a{};
+    fill_walk_args(dom, a);
+    a.rp = dom->D.rp;
+    a.col = dom->D.ci;
+    a.h = dom->D.v;
+    a.cdf = dom->cdf;
+    a.W = dom->w;
+    unsigned long long* d_out = nullptr;
+    cudaError_t e = dmalloc(&d_out, 2);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    cudaStream_t st = ctx->stream;
+    cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), st);
+    const long long g = (histories + 255) / 256;
+    const int grid = int(g < ctx->num_sms * 8 ? g : ctx->num_sms * 8);
+    const uint64_t ekey = epoch_key(seed, 0);
+    bool ok = true;
+#define MCLSGPU_AGREE(SL, STV) k_walk_agreement<SL, STV><<<grid, 256, 0, st>>>(a, histories, ekey, d_out)
+    if (dom->stencil_k) {
+        switch (dom->slots) {
+            case 4: MCLSGPU_AGREE(4, true); break;
+            case 8: MCLSGPU_AGREE(8, true); break;
+            case 16: MCLSGPU_AGREE(16, true); break;
+            default: ok = false;
+        }
+    } else {
+        switch (dom->slots) {
+            case 4: MCLSGPU_AGREE(4, false); break;
+            case 8: MCLSGPU_AGREE(8, false); break;
+            case 12: MCLSGPU_AGREE(12, false); break;
+            case 16: MCLSGPU_AGREE(16, false); break;
+            case 24: MCLSGPU_AGREE(24, false); break;
+            case 32: MCLSGPU_AGREE(32, false); break;
+            default: ok = false;
+        }
+    }
+#undef MCLSGPU_AGREE
+    unsigned long long h[2] = {0, 0};
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    dfree(d_out);
+    if (!ok) return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "walk agreement: %d-slot records",
+                              dom->slots);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "walk agreement");
+    int rc = check_device_status(ctx);
+    if (rc) return rc;
+    *hist_diff = (long long)h[0];
+    *trans_diff = (long long)h[1];
+    return MCLSGPU_OK;
+}
 
 void launch_walk_part(const PartWalk& p, mclsgpu_context* ctx) {
     const long long nwork = p.in ? p.n_in : p.e_end - p.e_begin;

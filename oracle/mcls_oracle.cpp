@@ -13,6 +13,7 @@
 #include "mcls_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <chrono>
 #include <climits>
@@ -204,13 +205,50 @@ Csr composite(const Csr& A, const Csr* PL, const Csr* PR, bool trans,
     return transpose(A);
 }
 
+// Host threads for the oracle's long row loops (orc_set_threads; 1 = one
+// thread, as one reference rank runs).  Every row is computed exactly as the
+// one-thread loop computes it, so results do not depend on the count.
+int g_threads = 1;
+
+// f(lo, hi) over contiguous row ranges [lo, hi) of [0, n), one per thread.
+template <class F>
+void parallel_ranges(int64_t n, const F& f) {
+    const int T = g_threads;
+    if (T <= 1 || n < (1 << 16)) {
+        f(int64_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(f, n * t / T, n * (t + 1) / T);
+    f(int64_t(0), n / T);
+    for (auto& th : pool) th.join();
+}
+
+// Sum over threads of g(lo, hi) on the ranges parallel_ranges uses, added in
+// range order (deterministic for a given thread count).
+template <class G>
+double parallel_sum(int64_t n, const G& g) {
+    const int T = (g_threads <= 1 || n < (1 << 16)) ? 1 : g_threads;
+    std::vector<double> part(T, 0.0);
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t)
+        pool.emplace_back([&, t]() { part[t] = g(n * t / T, n * (t + 1) / T); });
+    part[0] = g(int64_t(0), n / T);
+    for (auto& th : pool) th.join();
+    double s = 0.0;
+    for (double v : part) s += v;
+    return s;
+}
+
 // Tpetra CrsMatrix::apply on one rank: y_i = sum_j a_ij x_j in column order.
 void spmv(const Csr& A, const double* x, double* y) {
-    for (int64_t i = 0; i < A.n; ++i) {
-        double s = 0.0;
-        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) s = s + A.v[k] * x[A.ci[k]];
-        y[i] = s;
-    }
+    parallel_ranges(A.n, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            double s = 0.0;
+            for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) s = s + A.v[k] * x[A.ci[k]];
+            y[i] = s;
+        }
+    });
 }
 
 // TpetraPointJacobiPreconditioner::buildPreconditioner
@@ -577,18 +615,59 @@ int64_t orc_mc_solve(orc_mc* mc, const double* rhs, double* x, int internal,
     std::vector<double> hb;
     if (p.direction == 1 && p.estimator == 1) {
         hb.assign(n, 0.0);
-        for (int64_t i = 0; i < n; ++i) {
-            double s = 0.0;
-            for (int64_t k = D.rp[i]; k < D.rp[i + 1]; ++k) s = s + D.h[k] * src[D.col[k]];
-            hb[i] = s;
-        }
+        parallel_ranges(n, [&](int64_t lo, int64_t hi) {
+            for (int64_t i = lo; i < hi; ++i) {
+                double s = 0.0;
+                for (int64_t k = D.rp[i]; k < D.rp[i + 1]; ++k) s = s + D.h[k] * src[D.col[k]];
+                hb[i] = s;
+            }
+        });
     }
     std::vector<double> fsum, fcount;
     if (p.direction == 1) { fsum.assign(n, 0.0); fcount.assign(n, 0.0); }
 
     // DomainTransporter::transport (src/MCLS_DomainTransporter_impl.hpp:70-119)
     const int64_t nh = int64_t(starts.size());
-    for (int64_t e = 0; e < nh; ++e) {
+    const bool threaded = p.direction == 1 && rng.mode == 1 && !trace_states && !final_weight &&
+                          !events && !start_state && g_threads > 1;
+    if (threaded) {
+        // Forward histories on the counter stream are independent: threads
+        // take contiguous ranges of start states (all histories of a state in
+        // one thread, in emission order), so every sum is the one-thread sum.
+        const int per = int(nh / (n > 0 ? n : 1));
+        std::atomic<int64_t> total{0};
+        parallel_ranges(n, [&](int64_t lo, int64_t hi) {
+            int64_t st = 0;
+            for (int64_t e = lo * per; e < hi * per; ++e) {
+                int64_t state = starts[e];
+                double w = w0[e];
+                const double wabs0 = std::abs(w0[e]);
+                uint64_t cs = counter_state(rng.seed, rng.epoch, 2, uint64_t(e));
+                int steps = 0;
+                double htally = 0.0;
+                while (true) {
+                    htally += w * (p.estimator == 0 ? src[state] : hb[state]);
+                    cs = xs_step(cs);
+                    const double u = canonical(cs);
+                    int64_t r0 = D.rp[state];
+                    int j = sample_cdf(&D.cdf[r0], int(D.rp[state + 1] - r0), u);
+                    int sign = (D.h[r0 + j] > 0.0) ? 1 : -1;
+                    w *= D.w[state] * double(sign);
+                    state = D.col[r0 + j];
+                    ++steps;
+                    if (steps >= L ||
+                        (p.weight_cutoff > 0.0 && std::abs(w) < p.weight_cutoff * wabs0))
+                        break;
+                }
+                st += steps;
+                fsum[starts[e]] += htally;
+                fcount[starts[e]] += 1.0;
+            }
+            total += st;
+        });
+        mc->total_steps += total.load();
+    }
+    for (int64_t e = 0; e < nh && !threaded; ++e) {
         int64_t state = starts[e];
         double w = w0[e];
         const double wabs0 = std::abs(w0[e]);
@@ -1042,11 +1121,86 @@ int orc_fixed_point_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR
     return rnorm <= criteria ? 1 : 0;
 }
 
+void orc_set_threads(int threads) { g_threads = threads < 1 ? 1 : threads; }
+
+int orc_pcg(const orc_csr* A, const double* b, double* x, double tol, int max_iters,
+            int* iters, double* relres) {
+    // Conjugate gradients with the diagonal as preconditioner (Hestenes and
+    // Stiefel; M = diag(A)), FP64, for symmetric positive definite A.  Not a
+    // reference routine: the FP64 solve MCSA results are measured against.
+    const Csr& M = A->m;
+    const int64_t n = M.n;
+    std::vector<double> dinv(n), r(n), z(n), p(n), q(n);
+    for (int64_t i = 0; i < n; ++i) {
+        double d = 0.0;
+        for (int64_t k = M.rp[i]; k < M.rp[i + 1]; ++k)
+            if (M.ci[k] == i) d = M.v[k];
+        if (d <= 0.0) return -1;
+        dinv[i] = 1.0 / d;
+    }
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& c) {
+        return parallel_sum(n, [&](int64_t lo, int64_t hi) {
+            double t = 0.0;
+            for (int64_t i = lo; i < hi; ++i) t += a[i] * c[i];
+            return t;
+        });
+    };
+    std::vector<double> bv(b, b + n);
+    const double bn = std::sqrt(dot(bv, bv));
+    int it = 0;
+    double rn = 0.0;
+    // The recursively updated residual drifts from b - A x; CG restarts from
+    // the true residual until that one meets the tolerance.
+    for (int restart = 0; restart < 8; ++restart) {
+        spmv(M, x, q.data());
+        for (int64_t i = 0; i < n; ++i) {
+            r[i] = b[i] - q[i];
+            z[i] = dinv[i] * r[i];
+            p[i] = z[i];
+        }
+        double rz = dot(r, z);
+        rn = std::sqrt(dot(r, r));
+        if (rn <= tol * bn || it >= max_iters) break;
+        while (rn > tol * bn && it < max_iters) {
+            ++it;
+            spmv(M, p.data(), q.data());
+            const double alpha = rz / dot(p, q);
+            parallel_ranges(n, [&](int64_t lo, int64_t hi) {
+                for (int64_t i = lo; i < hi; ++i) {
+                    x[i] += alpha * p[i];
+                    r[i] -= alpha * q[i];
+                    z[i] = dinv[i] * r[i];
+                }
+            });
+            rn = std::sqrt(dot(r, r));
+            const double rz2 = dot(r, z);
+            const double beta = rz2 / rz;
+            rz = rz2;
+            parallel_ranges(n, [&](int64_t lo, int64_t hi) {
+                for (int64_t i = lo; i < hi; ++i) p[i] = z[i] + beta * p[i];
+            });
+        }
+    }
+    if (iters) *iters = it;
+    if (relres) *relres = bn > 0.0 ? rn / bn : rn;
+    return rn <= tol * bn ? 1 : 0;
+}
+
+namespace {
+double g_mcsa_setup_s = 0.0, g_mcsa_loop_s = 0.0;
+}
+
+void orc_mcsa_last_timing(double* setup_s, double* loop_s) {
+    if (setup_s) *setup_s = g_mcsa_setup_s;
+    if (loop_s) *loop_s = g_mcsa_loop_s;
+}
+
 int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
                    const orc_mc_params* mp, const orc_mcsa_params* sp,
                    const double* b, double* x, int* iters, double* achieved,
                    int max_hist, double* res_hist, int64_t* total_steps) {
     // MCSASolverManager::solve (src/MCLS_MCSASolverManager_impl.hpp:278-432)
+    const auto t_setup = std::chrono::steady_clock::now();
     orc_mc* mc = orc_mc_create(A, PL, PR, mp);
     if (!mc) return -1;
     const Csr& Am = A->m;
@@ -1076,6 +1230,8 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
     double rnorm = norm2(rp);
     int it = 0;
     bool go = true;
+    const auto t_loop = std::chrono::steady_clock::now();
+    g_mcsa_setup_s = std::chrono::duration<double>(t_loop - t_setup).count();
     while (go) {
         ++it;
         for (int l = 0; l < sp->smoother_steps; ++l)
@@ -1091,6 +1247,8 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
         if (res_hist && it <= max_hist) res_hist[it - 1] = rnorm;
         if (it % sp->check_freq == 0) go = (rnorm > criteria) && (it < sp->max_iters);
     }
+    g_mcsa_loop_s =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop).count();
     if (PR) {
         spmv(PR->m, xv.data(), tmp.data());
         xv = tmp;

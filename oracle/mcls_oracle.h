@@ -113,6 +113,10 @@ int orc_mcsa_solve(const orc_csr* A, const orc_csr* PL, const orc_csr* PR,
                    const double* b, double* x, int* iters, double* achieved,
                    int max_hist, double* res_hist, int64_t* total_steps);
 
+/* Wall seconds of the last orc_mcsa_solve: set-up (domain build, initial
+ * residual) and the iteration loop. */
+void orc_mcsa_last_timing(double* setup_s, double* loop_s);
+
 /* FixedPointSolverManager::solve restatement: sp->fixed_point_type
  * iterations alone until |rp|_inf <= tolerance |PL b|_inf (or max_iters).
  * x is updated in place (x = PR x at the end).  res_hist gets |rp|_inf per
@@ -154,6 +158,20 @@ int orc_anderson_solve(const orc_csr* A, const orc_csr* PL, const orc_mc_params*
  * if converged. */
 int orc_anderson_linear(const orc_csr* M, const double* c, const orc_anderson_params* ap,
                         double* x, int* iters, int max_hist, double* iterates);
+
+/* Host threads for the oracle's long loops: the SpMVs, the expected-value
+ * source and forward walks on the counter stream (histories partitioned by
+ * start state, as ranks own rows).  Results do not depend on the count;
+ * default 1 (one reference rank). */
+void orc_set_threads(int threads);
+
+/* FP64 conjugate gradients with the diagonal as preconditioner (no reference
+ * counterpart): the oracle solve MCSA results are measured against, for
+ * symmetric positive definite A.  x holds x0 and receives the solution;
+ * stops when |b - A x|_2 <= tol |b|_2 or after max_iters.  Returns 1 if
+ * converged, 0 if not, -1 for a non-positive diagonal. */
+int orc_pcg(const orc_csr* A, const double* b, double* x, double tol, int max_iters,
+            int* iters, double* relres);
 
 /* CPU baseline: independent histories on `threads` threads (one Xorshift per
  * thread, as one MPI rank per core with subdomain transport), `nh` histories

@@ -139,6 +139,11 @@ def lib():
         L.orc_anderson_linear.restype = C.c_int
         L.orc_bench_walks.argtypes = [P, f64p, C.c_int64, C.c_int, P, C.POINTER(C.c_double)]
         L.orc_bench_walks.restype = C.c_int64
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_mcsa_last_timing.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_pcg.argtypes = [P, f64p, f64p, C.c_double, C.c_int, C.POINTER(C.c_int),
+                              C.POINTER(C.c_double)]
+        L.orc_pcg.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -338,8 +343,30 @@ def mcsa_solve(A: Csr, b, x0=None, PL=None, PR=None, mc: MCParams | None = None,
                               C.byref(steps))
     if rc < 0:
         raise RuntimeError("oracle MCSA failed")
+    t_setup, t_loop = C.c_double(), C.c_double()
+    lib().orc_mcsa_last_timing(C.byref(t_setup), C.byref(t_loop))
     return dict(x=x, converged=bool(rc), iters=iters.value, achieved=ach.value,
-                residuals=hist[: iters.value], steps=steps.value)
+                residuals=hist[: iters.value], steps=steps.value, setup_s=t_setup.value,
+                loop_s=t_loop.value)
+
+
+def set_threads(threads: int):
+    """Host threads of the oracle's SpMVs and counter-stream forward walks
+    (results do not depend on the count)."""
+    lib().orc_set_threads(int(threads))
+
+
+def pcg(A: Csr, b, x0=None, tolerance=1e-12, max_iters=100000):
+    """FP64 diagonal-preconditioned conjugate gradients (SPD A): the oracle
+    solve MCSA solutions are measured against."""
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+    it = C.c_int(0)
+    rr = C.c_double(0.0)
+    rc = lib().orc_pcg(A.h, b, x, tolerance, max_iters, C.byref(it), C.byref(rr))
+    if rc < 0:
+        raise RuntimeError("oracle CG: non-positive diagonal")
+    return dict(x=x, converged=bool(rc), iters=it.value, rel_residual=rr.value)
 
 
 def fixed_point_solve(A: Csr, b, x0=None, PL=None, PR=None, tolerance=1.0, max_iters=1000,

@@ -76,3 +76,40 @@ def test_adjoint_solve_means_are_the_neumann_sums(est):
                   for s in range(30)])
     se = E.std(0, ddof=1) / np.sqrt(len(E))
     assert np.all(np.abs(E.mean(0) - want) <= 5.0 * se)
+
+
+def test_oracle_cg_matches_direct_solve():
+    # The FP64 solve MCSA results are measured against: conjugate gradients
+    # to 1e-13 agree with a sparse direct solve, with one or several threads.
+    import scipy.sparse.linalg as spla
+
+    from mcls_b200 import problems as P
+    from oracle import oracle as O
+
+    A, b = P.diffusion3d_varcoef(42, seed=2)  # 74,088 rows: the threaded loops run
+    xs = spla.spsolve(A.tocsc(), b)
+    for threads in (1, 4):
+        O.set_threads(threads)
+        r = O.pcg(O.Csr.from_scipy(A), b, tolerance=1e-13)
+        assert r["converged"] and r["rel_residual"] <= 1e-13
+        assert np.linalg.norm(r["x"] - xs) / np.linalg.norm(xs) < 1e-11
+    O.set_threads(1)
+
+
+def test_threaded_forward_walks_equal_one_thread():
+    # The oracle's forward counter-stream walks partitioned over threads give
+    # the one-thread result bit for bit (histories grouped by start state).
+    from mcls_b200 import problems as P
+    from oracle import oracle as O
+
+    A, b = P.diffusion3d_varcoef(42, seed=1)
+    Ao = O.Csr.from_scipy(A)
+    out = []
+    for threads in (1, 8):
+        O.set_threads(threads)
+        r = O.mcsa_solve(Ao, b, PL=O.point_jacobi(Ao), tolerance=1e-8, max_iters=3,
+                         estimator=1, direction=1, sample_ratio=2.0, rng_mode=1, seed=3)
+        out.append(r)
+    O.set_threads(1)
+    assert np.array_equal(out[0]["x"], out[1]["x"])
+    assert out[0]["steps"] == out[1]["steps"]

@@ -366,3 +366,25 @@ def test_filter_relative_threshold():
     assert C[0, 1] == 0.0 and C[0, 2] == -0.3   # 0.1 <= 0.2 dropped, 0.3 kept
     assert C[1, 2] == 0.0 and C[1, 0] == 0.2
     assert np.all(C[2] == 1.0)
+
+
+def test_composite_threshold_uses_the_signed_row_maximum():
+    # tpetra/src/MCLS_TpetraHelpers.hpp:226-233 takes the row maximum of the
+    # signed values.  With PL = -D^-1 every row of the composite operator has
+    # a negative diagonal, so the signed maximum is the largest positive
+    # off-diagonal entry and the filter keeps more than a magnitude-based
+    # threshold would.
+    A = P.anisotropic2d(8, 20.0, 0.6)
+    thr = 0.3
+    neg = sp.diags(-1.0 / A.diagonal(), format="csr")
+    M = (neg @ A).T.tocsr()  # transposed composite operator (adjoint)
+    kept_signed = kept_abs = 0
+    for i in range(M.shape[0]):
+        v = M.data[M.indptr[i]:M.indptr[i + 1]]
+        kept_signed += int(np.sum(np.abs(v) > thr * v.max()))
+        kept_abs += int(np.sum(np.abs(v) > thr * np.abs(v).max()))
+    assert kept_signed > kept_abs
+    o = O.MC(O.Csr.from_scipy(A), PL=O.Csr.from_scipy(neg), direction=0,
+             composite_threshold=thr).domain()
+    # H = I - M keeps every retained entry of M (its diagonal becomes 2).
+    assert len(o["col"]) == kept_signed

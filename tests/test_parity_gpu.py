@@ -289,12 +289,45 @@ def test_invalid_operator_is_rejected(ctx):
     assert e.value.code == capi.ERR_INVALID_ARG
 
 
-def test_reference_stream_rejects_weight_cutoff(ctx):
+def test_reference_stream_weight_cutoff_needs_fp64(ctx):
+    # Variable-length histories on the reference stream are walked by the
+    # FP64 parity walk only.
     A = P.poisson2d(4)
     op = capi.Operator(ctx, A)
     with pytest.raises(capi.MclsError) as e:
-        capi.Domain(ctx, op, None, rng_mode=capi.RNG_REFERENCE, weight_cutoff=1e-4)
+        capi.Domain(ctx, op, None, rng_mode=capi.RNG_REFERENCE, weight_cutoff=1e-4,
+                    precision=capi.FP32)
     assert e.value.code == capi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("name,L,cutoff", [("tridiag", 10, 1e-4), ("varcoef3d", 200, 0.05),
+                                           ("poisson2d", 40, 1e-4), ("aniso9pt", 30, 1e-3)])
+def test_weight_cutoff_trajectories_reference_stream(ctx, name, L, cutoff):
+    # "Weight Cutoff" with "Reproducible MC Mode": histories end at different
+    # steps, so each history's draws start where the previous one's ended in
+    # the reference's single stream; trajectories, events and final weights
+    # are bit-exact against the oracle over successive solves.
+    A, b = _systems()[name]
+    _trace_compare(ctx, A, b, "jacobi", rng_mode=capi.RNG_REFERENCE, seed=31, history_length=L,
+                   weight_cutoff=cutoff, sample_ratio=2.0)
+
+
+@pytest.mark.parametrize("direction", [0, 1])
+def test_mcsa_weight_cutoff_reference_stream_matches_oracle(ctx, direction):
+    # MCSA with the cutoff in the reproducible mode follows the oracle's
+    # iterates (the residual rounds differently, as in the fixed-length test).
+    A = P.poisson2d(10)
+    b = np.ones(A.shape[0])
+    kw = dict(history_length=40, weight_cutoff=1e-4, sample_ratio=1.0)
+    dom, op, pc = _gpu_domain(ctx, A, "jacobi", precision=capi.FP64,
+                              rng_mode=capi.RNG_REFERENCE, seed=77, direction=direction, **kw)
+    x, st = dom.mcsa_solve(b, tolerance=1e-8, max_iters=400)
+    Ao = O.Csr.from_scipy(A)
+    r = O.mcsa_solve(Ao, b, PL=O.point_jacobi(Ao), tolerance=1e-8, max_iters=400, rng_mode=0,
+                     seed=77, direction=direction, **kw)
+    assert st["converged"] == 1 and r["converged"]
+    assert abs(st["iterations"] - r["iters"]) <= 1
+    assert np.allclose(x, r["x"], rtol=1e-7, atol=1e-12 * np.abs(r["x"]).max())
 
 
 def test_device_vectors_entry_point(ctx):

@@ -1,0 +1,82 @@
+"""How far a sparse approximate inverse on A's own 7-point pattern can take
+MCSA on 3D diffusion, checked numerically (CPU, dense eigensolves).
+
+On the constant-coefficient 3D Laplacian, with D = diag(A), N = D - A and
+T = D^-1 N (the Jacobi iteration matrix), every M on A's pattern that is
+symmetric in the six neighbours is M = D^-1 (alpha I + beta T) (T's pattern
+is A's off-diagonal one).  Then
+
+    H = I - M A = (1 - alpha) I + (alpha - beta) T + beta T^2
+
+whose row sums of |H| -- the factor by which a walk's weight changes at
+each step, which keeps the Monte Carlo variance bounded when it is <= 1 --
+are |1 - alpha + beta/6| + |alpha - beta| + 5 beta/6.  Near the smooth end of
+the spectrum (T's eigenvalue t -> 1), 1 - lambda(H) = (alpha + beta)(1 - t),
+against (1 - t) for Jacobi.  Maximising alpha + beta under row sums <= 1 gives
+alpha = 1 + beta/6, beta <= 6/5: at most 2.4 times the Jacobi spectral gap,
+hence at most 2.4 times fewer MCSA iterations where the iteration count is
+set by rho(H)^(History Length + 1).
+"""
+import numpy as np
+import scipy.sparse as sp
+
+from mcls_b200 import problems as P
+
+
+def _laplacian3d(n):
+    D = np.ones((n, n, n))
+    return P._diffusion3d(D, np.zeros((n, n, n)), 1.0 / (n + 1))
+
+
+def _poly_spai(A, alpha, beta):
+    d = A.diagonal()
+    T = sp.diags(1.0 / d) @ (sp.diags(d) - A)
+    return sp.diags(1.0 / d) @ (alpha * sp.identity(A.shape[0]) + beta * T)
+
+
+def _gap_and_rowsum(A, M):
+    H = (sp.identity(A.shape[0]) - M @ A).toarray()
+    lam = np.linalg.eigvals(H)
+    return 1.0 - np.abs(lam).max(), np.abs(H).sum(1)
+
+
+def _t_eigs(A):
+    # T = D^-1 N is symmetric for a constant diagonal; H is a polynomial in T.
+    d = A.diagonal()
+    T = (sp.diags(1.0 / d) @ (sp.diags(d) - A)).toarray()
+    return np.linalg.eigvalsh(0.5 * (T + T.T))
+
+
+def test_row_sums_stay_at_one_on_the_optimal_line():
+    A = _laplacian3d(8)
+    for beta in (0.3, 0.6, 1.0, 1.2):
+        M = _poly_spai(A, 1.0 + beta / 6.0, beta)
+        _, W = _gap_and_rowsum(A, M)
+        assert W.max() <= 1.0 + 1e-12, (beta, W.max())
+    # past beta = 6/5 the neighbour term changes sign and the row sums exceed 1
+    _, W = _gap_and_rowsum(A, _poly_spai(A, 1.0 + 1.5 / 6.0, 1.5))
+    assert W.max() > 1.0 + 1e-3
+
+
+def test_spectral_gap_gain_is_at_most_2_4():
+    A = _laplacian3d(8)
+    t = _t_eigs(A)
+    gap_j = 1.0 - np.abs(t).max()
+    # the polynomial form agrees with the matrix it describes
+    gap_m, _ = _gap_and_rowsum(A, _poly_spai(A, 1.1, 0.6))
+    lam = (1.0 - 1.1) + (1.1 - 0.6) * t + 0.6 * t * t
+    assert abs(gap_m - (1.0 - np.abs(lam).max())) < 1e-10
+    best, arg = 0.0, None
+    for alpha in np.linspace(0.8, 1.4, 61):
+        for beta in np.linspace(0.0, 1.6, 81):
+            W = abs(1.0 - alpha + beta / 6.0) + abs(alpha - beta) + 5.0 * beta / 6.0
+            if W > 1.0 + 1e-12:
+                continue
+            lam = (1.0 - alpha) + (alpha - beta) * t + beta * t * t
+            gain = (1.0 - np.abs(lam).max()) / gap_j
+            if gain > best:
+                best, arg = gain, (alpha, beta)
+    assert 2.2 < best <= 2.4 + 1e-3, (best, arg)
+    # the interior row-sum formula is the matrix's own
+    _, W = _gap_and_rowsum(A, _poly_spai(A, *arg))
+    assert W.max() <= 1.0 + 1e-12
