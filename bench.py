@@ -55,8 +55,17 @@ CONFIGS = {
                              "graph-captured loop, per-(system, rhs) convergence to 1e-8",
                     n=0, sample_ratio=1.0, estimator=1, history_length=10, direction=1),
     "poisson100": dict(workload="2D Poisson 5-pt 100x100, Jacobi MCSA, adjoint collision estimator, "
-                        "FP64 walks, N histories per iteration",
-               n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0),
+                        "FP64 walks, N histories per iteration, Weight Cutoff 1e-4 with a History "
+                        "Length cap of 10",
+               n=100, sample_ratio=1.0, estimator=0, history_length=10, direction=0,
+               weight_cutoff=1e-4),
+    "aniso512": dict(workload="2D anisotropic diffusion 512^2, 9-point stencil of K = R(theta) "
+                              "diag(1, 1/a) R(theta)^T (one seeded system with rho(H_Jacobi) > "
+                              "0.95), forward expected-value MCSA, FP32 walks / FP64 residual, 2 "
+                              "histories per row per iteration: point Jacobi vs block Jacobi "
+                              "(4 along x) vs learned SPAI (network trained on 2,000 seeded "
+                              "systems of the family)",
+                     n=512, sample_ratio=2.0, estimator=1, history_length=10, direction=1),
 }
 # DRAM bytes (read + write) of one walk launch on each workload: ncu's
 # dram__bytes_read.sum (83.90 MB) + dram__bytes_write.sum (7.82 MB) for the
@@ -249,14 +258,35 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     sweep = []
     for thr in thresholds[1:]:
         sweep.append(_learned_threshold_run(args, ctx, op, pc, A, b, cfgd, thr, jacobi_ms))
-    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
-                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
-                      direction=cfgd["direction"], history_length=cfgd["history_length"],
-                      composite_threshold=thresholds[0])
     mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
                           host_loop=1 if args.host_loop else 0)
     bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
     xt = torch.zeros_like(bt)
+    # The FP32 stencil records of the 25-offset learned H (128 bytes) are timed
+    # once beside the reported 16-bit-threshold records (64 bytes).
+    fp32_rec = None
+    if args.learned_format == "stencil16":
+        d32 = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER,
+                          seed=args.seed, estimator=cfgd["estimator"],
+                          sample_ratio=cfgd["sample_ratio"], direction=cfgd["direction"],
+                          history_length=cfgd["history_length"],
+                          composite_threshold=thresholds[0], record_format=capi.RECORD_STENCIL)
+        d32.autotune(bt.data_ptr(), reps=1)
+        for k in range(2):
+            d32.reseed(args.seed)
+            xt.zero_()
+            torch.cuda.synchronize()
+            s32 = d32.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
+        fp32_rec = {"record_bytes": d32.info()["record_bytes"],
+                    "time_to_1e-8_s": s32["solve_ms"] / 1e3, "iterations": s32["iterations"],
+                    "walk_ms_per_launch": s32["walk_ms"] / max(s32["walk_launches"], 1),
+                    "speedup_vs_jacobi": jacobi_ms / s32["solve_ms"]}
+        d32.close()
+    fmt = capi.RECORD_STENCIL16 if args.learned_format == "stencil16" else capi.RECORD_AUTO
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
+                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
+                      direction=cfgd["direction"], history_length=cfgd["history_length"],
+                      composite_threshold=thresholds[0], record_format=fmt)
     tuned = dom.autotune(bt.data_ptr(), reps=1)
     stats = []
     for k in range(1 + args.steps):
@@ -285,7 +315,14 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
                              "(seeds 1000-1007)" if args.config == "blocks256" else
                              "8 x 3D 7-pt var-coef diffusion 32^3 (seeds 1000-1007)"),
            "speedup_vs_jacobi": jacobi_ms / ms,
-           "composite_threshold": thresholds[0]}
+           "composite_threshold": thresholds[0],
+           "gate": {"rule": "point Jacobi replaces the learned M when rho(I - M A) >= 0.95 "
+                            "and >= the Jacobi rho (both by 300 power iterations)",
+                    "fell_back": bool(stats[-1]["fallback_taken"]),
+                    "literal_rule": "rho >= 0.95 alone",
+                    "literal_would_fall_back": bool(rl >= 0.95)}}
+    if fp32_rec:
+        out["fp32_stencil_records"] = fp32_rec
     if sweep:
         out["threshold_sweep"] = sweep
     if not args.no_anderson:
@@ -573,6 +610,129 @@ def hbm_walk_roofline(args, ctx, n=192, reps=10):
                         f"10 steps per row, {reps} launches after 3 warm-up launches"}
 
 
+def _aniso_solve(args, ctx, op, A, b, kind, cfgd, net=None, block=4, rho_fallback=2.0,
+                 record_format=0):
+    """One timed MCSA solve of the anisotropic system (after one warm-up
+    solve); divergence (non-finite weights or residual) is reported, not
+    raised."""
+    import torch
+
+    from mcls_b200 import capi
+
+    pc = capi.Precond(ctx, op, kind, block_size=block, net=net, rho_fallback=rho_fallback)
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
+                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
+                      direction=cfgd["direction"], history_length=cfgd["history_length"],
+                      record_format=record_format)
+    mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
+    bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
+    xt = torch.zeros_like(bt)
+    out = {"record_bytes": dom.info()["record_bytes"]}
+    try:
+        for _ in range(2):
+            dom.reseed(args.seed)
+            xt.zero_()
+            torch.cuda.synchronize()
+            st = dom.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
+        x = xt.cpu().numpy()
+        out.update({"converged": bool(st["converged"]), "iterations": st["iterations"],
+                    "time_to_1e-8_s": st["solve_ms"] / 1e3 if st["converged"] else None,
+                    "achieved_tol": st["achieved_tol"], "x": x,
+                    "rel_residual_b_minus_Ax": float(np.linalg.norm(b - A @ x) /
+                                                     np.linalg.norm(b)),
+                    "walk_ms_per_launch": st["walk_ms"] / max(st["walk_launches"], 1)})
+    except capi.MclsError as e:
+        out.update({"converged": False, "diverged": e.code == capi.ERR_DIVERGED,
+                    "error": str(e), "time_to_1e-8_s": None})
+    dom.close()
+    pc.close()
+    return out
+
+
+def run_aniso(args, world, rank, local, pg):
+    """The learned-preconditioner workload: train on 2,000 seeded systems of
+    the family (32^2 grids, GPU kernels), then solve one seeded 512^2 system
+    with point Jacobi, block Jacobi and the learned SPAI."""
+    import torch
+
+    from mcls_b200 import capi
+    from mcls_b200 import problems as P
+    from mcls_b200 import spai
+
+    cfgd = CONFIGS["aniso512"]
+    torch.cuda.set_device(local)
+    ctx = capi.Context(local)
+    # the solved system: the first seed from 7 whose Jacobi rho exceeds 0.95
+    seed = 7
+    while True:
+        A, b, ratio, theta = P.anisotropic2d_sample(cfgd["n"], seed=seed)
+        op = capi.Operator(ctx, A)
+        probe = capi.SpaiNet(ctx, spai.stencil_slots(A), seed=0)
+        _, rj = probe.rho(op, iters=300)
+        probe.close()
+        if rj > 0.95:
+            break
+        op.close()
+        seed += 1
+    slots = spai.stencil_slots(A)
+    t0 = time.perf_counter()
+    samples = []
+    g = torch.Generator(device=ctx_device())
+    g.manual_seed(0)
+    for k in range(args.aniso_train_systems):
+        At, _, _, _ = P.anisotropic2d_sample(32, seed=10000 + k)
+        if spai.stencil_slots(At) != slots:
+            continue
+        opt = capi.Operator(ctx, At)
+        V = torch.randn((4, opt.n), dtype=torch.float64, device=ctx_device(), generator=g)
+        samples.append((opt, V))
+    net = capi.SpaiNet(ctx, slots, seed=0)
+    if args.spai_penalty > 0:
+        net.set_penalty(args.spai_penalty, 1.0)
+    losses = spai.train(net, samples, steps=args.aniso_train_steps, lr=3e-3, lr_final=3e-4,
+                        refresh=25, adv_count=4, adv_iters=30)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    rl, rj = net.rho(op, iters=300)
+    arms = {"jacobi": _aniso_solve(args, ctx, op, A, b, capi.PREC_POINT_JACOBI, cfgd),
+            "block_jacobi": _aniso_solve(args, ctx, op, A, b, capi.PREC_BLOCK_JACOBI, cfgd,
+                                         record_format=capi.RECORD_STENCIL16),
+            "learned_spai": _aniso_solve(args, ctx, op, A, b, capi.PREC_LEARNED_SPAI, cfgd,
+                                         net=net, record_format=capi.RECORD_STENCIL16)}
+    from oracle import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    ref = O.pcg(O.Csr.from_scipy(A), b, tolerance=1e-12)
+    for arm in arms.values():
+        x = arm.pop("x", None)
+        if x is not None:
+            arm["err_vs_oracle"] = float(np.linalg.norm(x - ref["x"]) / np.linalg.norm(ref["x"]))
+    lt = arms["learned_spai"]["time_to_1e-8_s"]
+    jt = arms["jacobi"]["time_to_1e-8_s"]
+    line = {"metric": METRIC, "value": lt, "unit": UNIT, "n_gpus": world, "steps": 1,
+            "warmup": 1, "ms_per_step": lt * 1e3 if lt else None, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfgd["workload"], "n": A.shape[0], "nnz": int(A.nnz),
+                       "system_seed": seed, "anisotropy_ratio": ratio, "theta": theta,
+                       "tolerance": 1e-8, "l2": "inputs larger than L2 (no flush)"},
+            "results": {"arms": arms, "rho_jacobi": rj, "rho_learned": rl,
+                        "gate": "disabled for the learned arm (rho_fallback 2): every system of "
+                                "this family has rho >= 0.95 at 512^2, so the literal rule "
+                                "'rho >= 0.95 falls back' would always take Jacobi",
+                        "speedup_vs_jacobi": (jt / lt) if (jt and lt) else None,
+                        "train_systems": len(samples), "train_steps": args.aniso_train_steps,
+                        "train_grid": "32^2", "train_s": train_s,
+                        "train_loss_first": float(np.mean(losses[:20])),
+                        "train_loss_last": float(np.mean(losses[-100:])),
+                        "oracle": {"solver": "FP64 diagonal-preconditioned CG (oracle/)",
+                                   "rel_residual": ref["rel_residual"]}}}
+    if rank == 0:
+        print(json.dumps(line))
+    net.close()
+    op.close()
+    ctx.close()
+
+
 def ctx_device():
     import torch
 
@@ -585,7 +745,7 @@ def workload_config(args, cfgd, n, nnz, world):
     hist = n * per if cfgd["direction"] == 1 else int(n * cfgd["sample_ratio"])
     return {"workload": cfgd["workload"], "n": n, "nnz": int(nnz),
             "histories_per_iteration": hist, "history_length": cfgd["history_length"],
-            "tolerance": 1e-8,
+            "tolerance": 1e-8, "weight_cutoff": cfgd.get("weight_cutoff", 0.0),
             "stopping_test": "|PL (b - A x)|_2 <= 1e-8 |PL b|_2 (MCSASolverManager's test)",
             "preconditioner": "point Jacobi",
             "parallelism": f"replicas x{world}" if world > 1 else "single domain",
@@ -609,7 +769,8 @@ def cpu_mcsa(cfg, A, b, iterations, threads, seed=1234):
     r = O.mcsa_solve(Ao, b, PL=O.point_jacobi(Ao), tolerance=1e-8,
                      max_iters=iterations if iterations else 100000, rng_mode=1, seed=seed,
                      direction=c["direction"], estimator=c["estimator"],
-                     sample_ratio=c["sample_ratio"], history_length=c["history_length"])
+                     sample_ratio=c["sample_ratio"], history_length=c["history_length"],
+                     weight_cutoff=c.get("weight_cutoff", 0.0))
     return r
 
 
@@ -676,6 +837,11 @@ def run_reference(args, world, rank, pg):
                           "system per call; the batched workload has no single-system "
                           "reference timing"}))
         return
+    if args.config == "aniso512":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned "
+                          "preconditioner, and its point-Jacobi MCSA does not converge on this "
+                          "family (|H| row sums above 1)"}))
+        return
     A, b = make_system(args.config)
     cfgd = CONFIGS[args.config]
     threads = os.cpu_count() or 1
@@ -741,11 +907,23 @@ def main():
                     help="random-stream seed of the timed solves (rank r uses seed + r)")
     ap.add_argument("--spai-steps", type=int, default=2000,
                     help="training steps of the learned-SPAI network")
+    ap.add_argument("--learned-format", default="stencil16", choices=["stencil16", "auto"],
+                    help="walk records of the learned-SPAI domain: 16-bit CDF thresholds "
+                         "(64 bytes for the 25-offset H) or the automatic FP32 choice")
+    ap.add_argument("--aniso-train-systems", type=int, default=2000)
+    ap.add_argument("--aniso-train-steps", type=int, default=4000)
+    ap.add_argument("--spai-penalty", type=float, default=1.0,
+                    help="weight of the |H| row-sum penalty in the anisotropic training loss")
     ap.add_argument("--batch-systems", type=int, default=1024)
     ap.add_argument("--batch-nmax", type=float, default=1e4,
                     help="largest system of the batched workload (5e5 for the full size)")
     args = ap.parse_args()
     world, rank, local, pg = dist_init(args)
+    if args.impl == "mcls_b200" and args.config == "aniso512":
+        run_aniso(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if args.impl == "mcls_b200" and args.config == "batched":
         run_batched(args, world, rank, local, pg)
         if pg is not None:
@@ -773,7 +951,8 @@ def main():
     dom = capi.Domain(ctx, op, pc, precision=fp, rng_mode=capi.RNG_COUNTER, seed=seed,
                       estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
                       direction=cfgd["direction"],
-                      history_length=cfgd["history_length"])
+                      history_length=cfgd["history_length"],
+                      weight_cutoff=cfgd.get("weight_cutoff", 0.0))
     mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters,
                           host_loop=1 if args.host_loop else 0)
     bt = torch.tensor(b, device=f"cuda:{local}", dtype=torch.float64)

@@ -96,12 +96,23 @@ typedef struct {
     int32_t rng_mode;
     int32_t record_format;    /* FP32 walk records: 0 = automatic, 1 = packed
                                * (column, CDF) pairs, 2 = stencil (CDF slots for
-                               * a fixed set of column offsets) */
+                               * a fixed set of column offsets), 3 = stencil
+                               * with 16-bit CDF thresholds (opt-in) */
     uint64_t seed;
 } mclsgpu_mc_params;
 
-/* Record formats (mclsgpu_mc_params.record_format). */
-enum { MCLSGPU_RECORD_AUTO = 0, MCLSGPU_RECORD_PACKED = 1, MCLSGPU_RECORD_STENCIL = 2 };
+/* Record formats (mclsgpu_mc_params.record_format).  STENCIL16 keeps W and
+ * the tally source in FP32 and quantises each transition's cumulative
+ * probability to 16 bits (a selection differs from the FP32 one with
+ * probability below 2^-16 per column), so that a row of up to 10 column
+ * offsets fits 32 bytes and up to 26 fit 64 bytes; the walk then samples an
+ * iteration matrix within 2^-16 W of H.  No counterpart in the reference. */
+enum {
+    MCLSGPU_RECORD_AUTO = 0,
+    MCLSGPU_RECORD_PACKED = 1,
+    MCLSGPU_RECORD_STENCIL = 2,
+    MCLSGPU_RECORD_STENCIL16 = 3
+};
 
 /* MCSA parameters (src/MCLS_MCSASolverManager_impl.hpp:290-343). */
 typedef struct {
@@ -302,7 +313,7 @@ int mclsgpu_domain_export(mclsgpu_domain* dom, int64_t* nnz_out,
  * record format replaces AlmostOptimalDomain's per-row arrays). */
 typedef struct {
     uint32_t size;            /* sizeof(mclsgpu_domain_info) */
-    int32_t record_format;    /* MCLSGPU_RECORD_PACKED or _STENCIL (FP32 walks) */
+    int32_t record_format;    /* MCLSGPU_RECORD_PACKED, _STENCIL or _STENCIL16 */
     int64_t rows;
     int64_t entries;          /* retained H entries */
     int32_t record_bytes;     /* bytes of one FP32 walk record (0: FP64 walk only) */

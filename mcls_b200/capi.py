@@ -22,7 +22,7 @@ COLLISION, EXPECTED_VALUE = 0, 1
 SOURCE_RANDOM, SOURCE_STRATIFIED = 0, 1
 FP64, FP32 = 0, 1
 RNG_REFERENCE, RNG_COUNTER = 0, 1
-RECORD_AUTO, RECORD_PACKED, RECORD_STENCIL = 0, 1, 2
+RECORD_AUTO, RECORD_PACKED, RECORD_STENCIL, RECORD_STENCIL16 = 0, 1, 2, 3
 PREC_NONE, PREC_POINT_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED_SPAI, PREC_USER_CSR = range(5)
 FIXED_POINT_RICHARDSON, FIXED_POINT_STEEPEST_DESCENT, FIXED_POINT_MINRES, FIXED_POINT_RNSD = range(4)
 #: "Fixed Point Type" names (FixedPointIterationFactory) to the C enum.

@@ -591,7 +591,9 @@ int mclsgpu_domain_export(mclsgpu_domain* dom, int64_t* nnz_out, int64_t* rowptr
 
 int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info) {
     if (!dom || !info || info->size < sizeof(mclsgpu_domain_info)) return MCLSGPU_ERR_INVALID_ARG;
-    info->record_format = dom->stencil_k ? MCLSGPU_RECORD_STENCIL : MCLSGPU_RECORD_PACKED;
+    info->record_format = !dom->stencil_k ? MCLSGPU_RECORD_PACKED
+                          : dom->rec_q16  ? MCLSGPU_RECORD_STENCIL16
+                                          : MCLSGPU_RECORD_STENCIL;
     info->rows = dom->n;
     info->entries = dom->D.nnz;
     info->record_bytes = dom->p.precision == MCLSGPU_FP32 ? dom->slots * 8 : 0;

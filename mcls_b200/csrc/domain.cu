@@ -138,6 +138,32 @@ __global__ void k_pack_stencil(const int* drp, const int* dcol, const double* dh
     }
 }
 
+// Stencil record with 16-bit thresholds (stencil16): word 0 = W, word 1 =
+// tally source, word 2 = sign bits of h (bit j), slot j's threshold t_j =
+// round(65536 cdf_j) (65535 for the row's last entry; 0, never selected, for
+// offsets the row lacks) in the 16-bit half j of words 3...
+__global__ void k_pack_stencil16(const int* drp, const int* dcol, const double* dh,
+                                 const double* dcdf, const double* dw, int n, int K,
+                                 const int* off, int words, uint32_t* rec) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t* r = rec + size_t(i) * words;
+        r[0] = __float_as_uint(__double2float_rn(dw[i]));
+        r[1] = 0u;
+        for (int j = 2; j < words; ++j) r[j] = 0u;
+        const int last = drp[i + 1] - 1;
+        for (int k = drp[i]; k <= last; ++k) {
+            const int d = dcol[k] - i;
+            int j = 0;
+            while (j < K && off[j] != d) ++j;
+            if (j == K) continue;  // cannot happen: every offset is in the table
+            double t = rint(dcdf[k] * 65536.0);
+            if (k == last || t > 65535.0) t = 65535.0;
+            r[3 + j / 2] |= uint32_t(t) << (16 * (j & 1));
+            if (!(dh[k] > 0.0)) r[2] |= 1u << j;
+        }
+    }
+}
+
 __global__ void k_to_float(const double* a, float* b, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         b[i] = __double2float_rn(a[i]);
@@ -235,16 +261,21 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED && row0 == 0) {
         int K = 0;
         if ((rc = collect_offsets(ctx, D, 30, dom->stencil_off, &K))) return rc;
-        // 32-, 64- or 128-byte records.
-        const int words = K <= 0 ? 0 : (K <= 6 ? 8 : (K <= 14 ? 16 : (K <= 30 ? 32 : 0)));
+        // 32-, 64- or 128-byte records; stencil16: 3 words + K halves in 32 or
+        // 64 bytes.
+        const bool q16 = fmt == MCLSGPU_RECORD_STENCIL16;
+        const int words = K <= 0 ? 0
+                          : q16  ? (K <= 10 ? 8 : (K <= 26 ? 16 : 0))
+                                 : (K <= 6 ? 8 : (K <= 14 ? 16 : (K <= 30 ? 32 : 0)));
         const int packed_words = slots ? 2 * slots : 1 << 30;
-        if (words && (fmt == MCLSGPU_RECORD_STENCIL || words < packed_words)) {
+        if (words && (fmt == MCLSGPU_RECORD_STENCIL || q16 || words < packed_words)) {
             dom->stencil_k = K;
+            dom->rec_q16 = q16 ? 1 : 0;
             slots = words / 2;
-        } else if (fmt == MCLSGPU_RECORD_STENCIL) {
+        } else if (fmt == MCLSGPU_RECORD_STENCIL || q16) {
             return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
-                             "stencil records need at most 30 distinct column offsets (found %d)",
-                             K);
+                             "stencil records need at most %d distinct column offsets (found %d)",
+                             q16 ? 26 : 30, K);
         }
     }
     dom->slots = slots;  // 0: rows too long for packed records (FP64 walk only)
@@ -255,9 +286,14 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
             int* doff = nullptr;
             if ((e = dmalloc(&doff, 32)) != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
             cudaMemcpyAsync(doff, dom->stencil_off, 32 * sizeof(int), cudaMemcpyHostToDevice, s);
-            k_pack_stencil<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n,
-                                                       dom->stencil_k, doff, 2 * slots,
-                                                       reinterpret_cast<uint32_t*>(dom->rec));
+            if (dom->rec_q16)
+                k_pack_stencil16<<<grid_for(n), 256, 0, s>>>(
+                    D.rp, D.ci, D.v, dom->cdf, dom->w, n, dom->stencil_k, doff, 2 * slots,
+                    reinterpret_cast<uint32_t*>(dom->rec));
+            else
+                k_pack_stencil<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n,
+                                                           dom->stencil_k, doff, 2 * slots,
+                                                           reinterpret_cast<uint32_t*>(dom->rec));
             e = cudaStreamSynchronize(s);
             dfree(doff);
             if (e != cudaSuccess) return cuda_fail(ctx, e, "stencil records");

@@ -140,6 +140,7 @@ struct mclsgpu_domain {
     int walk_block = 256;
     // Stencil records (stencil_k > 0): row r's slot j is column r + stencil_off[j].
     int stencil_k = 0;
+    int rec_q16 = 0;               // stencil records with 16-bit CDF thresholds
     int stencil_off[32] = {0};
     // Random stream.
     uint64_t seed = 1;

@@ -261,14 +261,52 @@ __device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, const dou
                  : "memory");
 }
 
+// The same for a stencil16 record: slot j carries |h_j| = W (t_j - t_prev) /
+// 65536 (the last entry's 65535 standing for 65536), the transition
+// probabilities the walk samples, and the sign in bit j of word 2.
+template <int WORDS>
+__device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, const double* v,
+                                                     double omega, int has, int K,
+                                                     const StencilOffsets& so) {
+    uint32_t q[WORDS];
+#pragma unroll
+    for (int t = 0; t < WORDS / 8; ++t)
+        asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(q[8 * t]), "=r"(q[8 * t + 1]), "=r"(q[8 * t + 2]), "=r"(q[8 * t + 3]),
+                       "=r"(q[8 * t + 4]), "=r"(q[8 * t + 5]), "=r"(q[8 * t + 6]),
+                       "=r"(q[8 * t + 7])
+                     : "l"(r + 8 * t));
+    const float W = __uint_as_float(q[0]);
+    unsigned prev = 0u;
+    double c = 0.0;
+#pragma unroll
+    for (int j = 0; j < 2 * (WORDS - 3); ++j) {
+        if (j >= K) break;
+        unsigned t = (q[3 + j / 2] >> (16 * (j & 1))) & 0xffffu;
+        if (t == 0u) continue;
+        if (t == 65535u) t = 65536u;
+        const float h = W * (float(t - prev) * 0x1p-16f);
+        prev = t;
+        c = fma(double(((q[2] >> j) & 1u) ? -h : h), load_src(v, i + so.off[j], omega, has), c);
+    }
+    q[1] = __float_as_uint(__double2float_rn(c));
+    asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
+                 "r"(q[1]), "r"(q[2]), "r"(q[3]), "r"(q[4]), "r"(q[5]), "r"(q[6]), "r"(q[7])
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, double omega,
                                                              int has, int ev, int K,
                                                              StencilOffsets so, int words,
-                                                             uint32_t* rec, double* y) {
+                                                             int q16, uint32_t* rec, double* y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* r = rec + size_t(i) * words;
         if (!ev) {
             r[1] = __float_as_uint(__double2float_rn(load_src(v, i, omega, has)));
+        } else if (q16 && words == 8) {
+            rec_stencil16_source<8>(r, i, v, omega, has, K, so);
+        } else if (q16) {
+            rec_stencil16_source<16>(r, i, v, omega, has, K, so);
         } else if (words == 8) {
             rec_stencil_source<8>(r, i, v, omega, has, K, so);
         } else if (words == 16) {
@@ -556,7 +594,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
             StencilOffsets so{};
             for (int j = 0; j < 32; ++j) so.off[j] = dom->stencil_off[j];
             k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
-                v, n, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots,
+                v, n, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots, dom->rec_q16,
                 reinterpret_cast<uint32_t*>(dom->rec), dom->y64);
         } else {
             k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, omega, has_omega, ev,

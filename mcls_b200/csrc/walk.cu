@@ -109,14 +109,29 @@ struct WalkOccupancy {
     static constexpr int kMinBlocks = S <= 8 ? 8 : (S <= 24 ? 4 : 2);
 };
 
-// Selection in one FP32 record (the S-slot words q of state s) for the
-// uniform u: the first entry whose CDF value is >= u (sampleDiscreteCDF's
-// lower_bound).  s becomes the selected column; neg is the sign bit of the
-// selected h.
-template <int S, bool ST>
-__device__ __forceinline__ void select32(const WalkArgs& a, const uint32_t* q, float u, int& s,
+// Record kinds of the FP32 walk (template parameter ST).
+//   0 packed:      slot 0 = {W, len or tally source}, slots 1.. = {cdf (f32),
+//                  column | sign << 31}, padding CDF 2.0
+//   1 stencil:     word 0 = W, word 1 = tally source, word 2 + j = the CDF at
+//                  column offset off[j] with the sign of h_j in its sign bit,
+//                  NaN where the row has no entry at that offset
+//   2 stencil16:   word 0 = W, word 1 = tally source, word 2 = the signs of
+//                  h_j (bit j), then 16-bit thresholds t_j two to a word
+//                  (slot j in word 3 + j/2, bits 16 (j % 2)..): t_j =
+//                  round(65536 cdf_j), 65535 for the row's last entry, 0 where
+//                  the row has no entry at off[j]
+constexpr int kPacked = 0, kStencil = 1, kStencil16 = 2;
+
+// Selection in one FP32 record (the S-slot words q of state s) for the draw
+// x: the first entry whose CDF value is >= u (sampleDiscreteCDF's
+// lower_bound) with u the draw's 24-bit uniform, or for stencil16 the first
+// slot with u16 < t_j, u16 = min(top 16 bits, 65534).  s becomes the selected
+// column; neg is the sign bit of the selected h.
+template <int S, int ST>
+__device__ __forceinline__ void select32(const WalkArgs& a, const uint32_t* q, uint64_t x, int& s,
                                          unsigned& neg) {
-    if constexpr (!ST) {
+    if constexpr (ST == kPacked) {
+        const float u = canonical32(x);
         unsigned sel = q[3];  // slot 1 (first entry)
         bool found = __uint_as_float(q[2]) >= u;
 #pragma unroll
@@ -127,9 +142,10 @@ __device__ __forceinline__ void select32(const WalkArgs& a, const uint32_t* q, f
         }
         neg = sel & 0x80000000u;
         s = int(sel & 0x7fffffffu);
-    } else {
+    } else if constexpr (ST == kStencil) {
         // Stencil slots: first |cdf_j| >= u (NaN slots never match); the next
         // state is s + offset_j, the sign of h_j is the sign bit of the slot.
+        const float u = canonical32(x);
         int dsel = 0;
         unsigned ng = 0u;
         bool found = false;
@@ -141,6 +157,20 @@ __device__ __forceinline__ void select32(const WalkArgs& a, const uint32_t* q, f
             found = found || c;
         }
         neg = ng;
+        s += dsel;
+    } else {
+        const unsigned u16 = min(unsigned(x >> 48), 65534u);
+        int dsel = 0, jsel = 0;
+        bool found = false;
+#pragma unroll
+        for (int j = 0; j < 2 * (2 * S - 3); ++j) {
+            const unsigned t = (q[3 + j / 2] >> (16 * (j & 1))) & 0xffffu;
+            const bool c = !found && u16 < t;
+            dsel = c ? a.stoff[j] : dsel;
+            jsel = c ? j : jsel;
+            found = found || c;
+        }
+        neg = ((q[2] >> jsel) & 1u) << 31;
         s += dsel;
     }
 }
@@ -163,7 +193,7 @@ __device__ __forceinline__ int select64(const WalkArgs& a, int s, double u, int&
 // loop body): tally at the pre-transition state, read the state's record,
 // draw u, select the first entry whose CDF value is >= u, update the state
 // and the weight.
-template <int S, int DIR, bool ST>
+template <int S, int DIR, int ST>
 __device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, int& s, float& w,
                                           uint64_t& x, float& acc, float& comp, int k) {
     // One record: S/4 256-bit loads that bypass L1 (each step touches exactly
@@ -184,10 +214,9 @@ __device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, in
         acc = t;
     }
     x = xs_step(x);
-    const float u = canonical32(x);
     const float Wt = __uint_as_float(q[0]);
     unsigned neg;
-    select32<S, ST>(a, q, u, s, neg);
+    select32<S, ST>(a, q, x, s, neg);
     w = neg ? -(w * Wt) : w * Wt;
 }
 
@@ -211,7 +240,7 @@ __device__ __forceinline__ void walk_start(const WalkArgs& a, int e, uint64_t ek
 // the warp takes 32 histories at a time and runs them without per-step
 // termination checks.  Otherwise lanes refill one by one from the queue as
 // their histories terminate.
-template <int S, int DIR, bool ST, bool FIXED, int ILP = 1>
+template <int S, int DIR, int ST, bool FIXED, int ILP = 1>
 __global__ void __launch_bounds__(256, ILP == 1 ? WalkOccupancy<S>::kMinBlocks : 5)
     walk32(WalkArgs a) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
@@ -392,7 +421,7 @@ __global__ void __launch_bounds__(128) walk64(WalkArgs a) {
     if ((threadIdx.x & 31) == 0 && steps) atomicAdd(a.d_steps, steps);
 }
 
-template <int S, int DIR, bool ST, bool FX, int ILP>
+template <int S, int DIR, int ST, bool FX, int ILP>
 int blocks_per_sm(int block) {
     static int cached[5] = {0, 0, 0, 0, 0};  // block sizes 128..1024 by log2
     const int slot = block <= 128 ? 0 : block <= 256 ? 1 : block <= 512 ? 2 : 3;
@@ -406,7 +435,7 @@ int blocks_per_sm(int block) {
 
 // Dispatch on the record stride; `launch` false only caches the occupancy.
 // Persistent grid: as many blocks as fit on every SM at once.
-template <int DIR, bool ST, bool FX, int ILP>
+template <int DIR, int ST, bool FX, int ILP>
 void launch32_slots(int slots, const WalkArgs& a, int sms, int block, cudaStream_t st,
                     bool launch) {
 #define MCLSGPU_WALK_CASE(SL)                                                             \
@@ -417,13 +446,13 @@ void launch32_slots(int slots, const WalkArgs& a, int sms, int block, cudaStream
         else                                                                              \
             blocks_per_sm<SL, DIR, ST, FX, ILP>(block);                                   \
         break;
-    if (ILP > 1) {
+    if constexpr (ILP > 1 || ST == kStencil16) {
         switch (slots) {
             MCLSGPU_WALK_CASE(4)
             default:
                 MCLSGPU_WALK_CASE(8)
         }
-    } else if (ST) {
+    } else if constexpr (ST == kStencil) {
         switch (slots) {
             MCLSGPU_WALK_CASE(4)
             MCLSGPU_WALK_CASE(8)
@@ -457,12 +486,15 @@ void dispatch_walk32(const mclsgpu_domain* dom, const WalkArgs& a, bool launch) 
     (ilp2 ? launch32_slots<DIRV, STV, true, 2>(dom->slots, a, sms, block, st, launch)         \
           : fixed ? launch32_slots<DIRV, STV, true, 1>(dom->slots, a, sms, block, st, launch) \
                   : launch32_slots<DIRV, STV, false, 1>(dom->slots, a, sms, block, st, launch))
-    if (dom->stencil_k) {
-        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, true);
-        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, true);
+    if (dom->stencil_k && dom->rec_q16) {
+        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, kStencil16);
+        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, kStencil16);
+    } else if (dom->stencil_k) {
+        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, kStencil);
+        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, kStencil);
     } else {
-        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, false);
-        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, false);
+        if (adj) MCLSGPU_WALK_DIR(MCLSGPU_ADJOINT, kPacked);
+        else MCLSGPU_WALK_DIR(MCLSGPU_FORWARD, kPacked);
     }
 #undef MCLSGPU_WALK_DIR
 }
@@ -549,7 +581,7 @@ __global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* 
                     acc[r] = t;
                 }
                 float da = 0.f, dc = 0.f;  // the record header's own tally is unused here
-                walk_step<S, MCLSGPU_FORWARD, ST>(a, rec, s, w, x, da, dc, k);
+                walk_step<S, MCLSGPU_FORWARD, ST ? kStencil : kPacked>(a, rec, s, w, x, da, dc, k);
             }
             steps += L;
 #pragma unroll
@@ -624,8 +656,10 @@ static void fill_walk_args(mclsgpu_domain* dom, WalkArgs& a) {
 int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y, const int* rsys,
                       const int* sys_done) {
     mclsgpu_context* ctx = dom->ctx;
-    if (dom->p.precision != MCLSGPU_FP32 || dom->p.direction != MCLSGPU_FORWARD || !dom->slots)
-        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batched walks need FP32 forward records");
+    if (dom->p.precision != MCLSGPU_FP32 || dom->p.direction != MCLSGPU_FORWARD || !dom->slots ||
+        dom->rec_q16)
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
+                         "batched walks need FP32 forward packed or stencil records");
     WalkArgs a{};
     fill_walk_args(dom, a);
     const int sms = ctx->num_sms;
@@ -818,7 +852,7 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
         }
         float acc = 0.f, comp = 0.f;
         while (k < p.L) {
-            walk_step<S, MCLSGPU_ADJOINT, false>(a, rec, s, w, x, acc, comp, k);
+            walk_step<S, MCLSGPU_ADJOINT, kPacked>(a, rec, s, w, x, acc, comp, k);
             ++k;
             ++steps;
             if (k < p.L && (s < p.row0 || s >= hi)) {
@@ -855,7 +889,7 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
 // draw (walk32's selection).  A transition disagrees when the two select a
 // different column or sign; out[0] += histories with at least one
 // disagreement, out[1] += disagreeing transitions.
-template <int S, bool ST>
+template <int S, int ST>
 __global__ void __launch_bounds__(256) k_walk_agreement(WalkArgs a, long long nh, uint64_t ekey,
                                                         unsigned long long* out) {
     const char* rec = reinterpret_cast<const char*>(a.rec);
@@ -873,7 +907,7 @@ __global__ void __launch_bounds__(256) k_walk_agreement(WalkArgs a, long long nh
             x = xs_step(x);
             int s32 = s;
             unsigned neg32;
-            select32<S, ST>(a, q, canonical32(x), s32, neg32);
+            select32<S, ST>(a, q, x, s32, neg32);
             int r0, len;
             int j = select64(a, s, canonical64(x), r0, len);
             if (j >= len) {
@@ -926,21 +960,27 @@ int walk_agreement(mclsgpu_domain* dom, long long histories, uint64_t seed, long
     const uint64_t ekey = epoch_key(seed, 0);
     bool ok = true;
 #define MCLSGPU_AGREE(SL, STV) k_walk_agreement<SL, STV><<<grid, 256, 0, st>>>(a, histories, ekey, d_out)
-    if (dom->stencil_k) {
+    if (dom->stencil_k && dom->rec_q16) {
         switch (dom->slots) {
-            case 4: MCLSGPU_AGREE(4, true); break;
-            case 8: MCLSGPU_AGREE(8, true); break;
-            case 16: MCLSGPU_AGREE(16, true); break;
+            case 4: MCLSGPU_AGREE(4, kStencil16); break;
+            case 8: MCLSGPU_AGREE(8, kStencil16); break;
+            default: ok = false;
+        }
+    } else if (dom->stencil_k) {
+        switch (dom->slots) {
+            case 4: MCLSGPU_AGREE(4, kStencil); break;
+            case 8: MCLSGPU_AGREE(8, kStencil); break;
+            case 16: MCLSGPU_AGREE(16, kStencil); break;
             default: ok = false;
         }
     } else {
         switch (dom->slots) {
-            case 4: MCLSGPU_AGREE(4, false); break;
-            case 8: MCLSGPU_AGREE(8, false); break;
-            case 12: MCLSGPU_AGREE(12, false); break;
-            case 16: MCLSGPU_AGREE(16, false); break;
-            case 24: MCLSGPU_AGREE(24, false); break;
-            case 32: MCLSGPU_AGREE(32, false); break;
+            case 4: MCLSGPU_AGREE(4, kPacked); break;
+            case 8: MCLSGPU_AGREE(8, kPacked); break;
+            case 12: MCLSGPU_AGREE(12, kPacked); break;
+            case 16: MCLSGPU_AGREE(16, kPacked); break;
+            case 24: MCLSGPU_AGREE(24, kPacked); break;
+            case 32: MCLSGPU_AGREE(32, kPacked); break;
             default: ok = false;
         }
     }

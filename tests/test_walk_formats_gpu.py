@@ -130,3 +130,58 @@ def test_fp32_weight_cutoff_walks(ctx, direction):
     # Jacobi-Poisson interior weights stay 1, so the cutoff only trims walks
     # that lose weight at the boundary: the two estimates agree to MC noise.
     assert np.linalg.norm(x - xf) / np.linalg.norm(xf) < 0.2
+
+
+def _wide_preconditioner(A, beta=0.3):
+    import scipy.sparse as sp
+
+    d = 1.0 / A.diagonal()
+    N = sp.diags(d) @ (sp.diags(A.diagonal()) - A)
+    return (sp.diags(d) @ (sp.identity(A.shape[0]) + beta * N)).tocsr()
+
+
+def test_stencil16_record_layouts(ctx):
+    # 25 offsets (H = I - M A, M on A's 7-point pattern): 64 bytes instead of
+    # 128; the 9-point Jacobi H (8 offsets): 32 bytes instead of 64.
+    A, _ = P.diffusion3d_varcoef(10, seed=4)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_USER_CSR, user=_wide_preconditioner(A))
+    d = capi.Domain(ctx, op, pc, precision=capi.FP32, direction=capi.FORWARD,
+                    record_format=capi.RECORD_STENCIL16)
+    i = d.info()
+    assert i["record_format"] == capi.RECORD_STENCIL16
+    assert i["stencil_offsets"] == 25 and i["record_bytes"] == 64
+    Aa = P.anisotropic2d(24, 15.0, 0.4)
+    opa = capi.Operator(ctx, Aa)
+    pca = capi.Precond(ctx, opa, capi.PREC_POINT_JACOBI)
+    da = capi.Domain(ctx, opa, pca, precision=capi.FP32, direction=capi.FORWARD,
+                     record_format=capi.RECORD_STENCIL16)
+    ia = da.info()
+    assert ia["stencil_offsets"] == 8 and ia["record_bytes"] == 32
+
+
+@pytest.mark.parametrize("direction", [capi.FORWARD, capi.ADJOINT])
+@pytest.mark.parametrize("estimator", [capi.COLLISION, capi.EXPECTED_VALUE])
+def test_stencil16_selection_rate_and_solution(ctx, direction, estimator):
+    # 16-bit CDF thresholds: a transition can differ from the FP64 selection
+    # only when u falls within 2^-16 of a CDF boundary (plus the FP32 rounding
+    # the other formats have), at most (K + 1) 2^-16 per transition; MCSA
+    # still converges to the tolerance (the residual is FP64).
+    A, b = P.diffusion3d_varcoef(12, seed=6)
+    op = capi.Operator(ctx, A)
+    M = _wide_preconditioner(A)
+    pc = capi.Precond(ctx, op, capi.PREC_USER_CSR, user=M)
+    kw = dict(precision=capi.FP32, direction=direction, estimator=estimator, sample_ratio=2.0,
+              seed=9)
+    d16 = capi.Domain(ctx, op, pc, record_format=capi.RECORD_STENCIL16, **kw)
+    nh = 1 << 20
+    hd, td = d16.walk_agreement(nh, seed=3)
+    assert td / (nh * 10) <= 26 * 2.0 ** -16
+    x, st = d16.mcsa_solve(b, tolerance=1e-8, max_iters=3000)
+    assert st["converged"] == 1
+    r = M @ (b - A @ x)
+    assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(M @ b) * 1.0001
+    d32 = capi.Domain(ctx, op, pc, record_format=capi.RECORD_STENCIL, **kw)
+    x32, st32 = d32.mcsa_solve(b, tolerance=1e-8, max_iters=3000)
+    assert st32["converged"] == 1
+    assert abs(st["iterations"] - st32["iterations"]) <= 0.1 * st32["iterations"] + 2
