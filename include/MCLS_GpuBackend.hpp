@@ -304,6 +304,7 @@ inline mclsgpu_mc_params mcParams(const Teuchos::ParameterList& pl, int directio
     if (fmt == "Auto") p.record_format = MCLSGPU_RECORD_AUTO;
     else if (fmt == "Packed") p.record_format = MCLSGPU_RECORD_PACKED;
     else if (fmt == "Stencil") p.record_format = MCLSGPU_RECORD_STENCIL;
+    else if (fmt == "Stencil16") p.record_format = MCLSGPU_RECORD_STENCIL16;
     else throw Assertion("Walk Record Format \"" + fmt + "\" not supported");
     p.seed = std::uint64_t(numeric(pl, "Random Seed", 433494437.0));
     // "Transport Type" (Global | Subdomain), "MC Check Frequency" and "MC

@@ -57,6 +57,7 @@ class MCSASolverManager : public SolverManager<Vector, Matrix> {
         pl->set<double>("Richardson Relaxation", 1.0);
         pl->set<int>("Smoother Steps", 1);
         pl->set<bool>("Print Iterations", true);
+        pl->set<int>("Number of Sets", 1);
         return pl;
     }
     Teuchos::RCP<const Teuchos::ParameterList> getCurrentParameters() const override {
@@ -70,11 +71,13 @@ class MCSASolverManager : public SolverManager<Vector, Matrix> {
     }
     int getNumIters() const override { return d_stats.iterations; }
 
+    // Several sets need the problem's set reducer, which sums the sets'
+    // corrections each iteration (MultiSetLinearProblem::setSetReducer).
     void setMultiSetProblem(const Teuchos::RCP<MultiSetType>& multiset_problem) {
         if (!Teuchos::nonnull(multiset_problem)) throw Assertion("MCSASolverManager: null problem");
-        if (multiset_problem->getNumSets() != 1)
-            throw Assertion("MCSASolverManager: one set per process on the GPU path; "
-                            "sum corrections across sets with the multi-set driver");
+        if (multiset_problem->getNumSets() != 1 && !multiset_problem->hasSetReducer())
+            throw Assertion("MCSASolverManager: a problem of several sets needs a set reducer "
+                            "(MultiSetLinearProblem::setSetReducer)");
         d_multiset = multiset_problem;
         setProblem(multiset_problem->getProblem());
     }
@@ -94,6 +97,21 @@ class MCSASolverManager : public SolverManager<Vector, Matrix> {
         gpu::Domain& dom = d_device.prepare(*d_problem, *d_plist, direction());
         d_stats = mclsgpu_stats{};
         d_stats.size = sizeof(d_stats);
+        const int sets = Teuchos::nonnull(d_multiset) ? d_multiset->getNumSets() : 1;
+        // "Number of Sets", when given, must agree with the problem's layout.
+        if (d_plist->isParameter("Number of Sets") &&
+            int(gpu::numeric(*d_plist, "Number of Sets", 1.0)) != sets)
+            throw Assertion("MCSASolverManager: \"Number of Sets\" differs from the problem's");
+        if (sets > 1) {
+            int32_t on_device = 0;
+            dom.context().check(
+                mclsgpu_mcsa_solve_sets(dom.get(), &d_multiset->setReducer(),
+                                        VT::view(*d_problem->getRHS()),
+                                        VT::viewNonConst(*d_problem->getLHS()), &mp, &d_stats,
+                                        &on_device),
+                "mclsgpu_mcsa_solve_sets");
+            return d_stats.converged != 0;
+        }
         dom.context().check(mclsgpu_mcsa_solve(dom.get(), VT::view(*d_problem->getRHS()),
                                                VT::viewNonConst(*d_problem->getLHS()), &mp,
                                                &d_stats),

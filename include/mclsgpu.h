@@ -500,6 +500,55 @@ int mclsgpu_mcsa_correction(mclsgpu_domain* dom, double* delta_dev);
 int mclsgpu_mcsa_apply(mclsgpu_domain* dom, const double* delta_dev, double scale,
                        double* rnorm);
 int mclsgpu_mcsa_finish(mclsgpu_domain* dom, double* x_dev, mclsgpu_stats* stats);
+/* ---- multi-set MCSA ---------------------------------------------------------- */
+/* Replaces MCSASolverManager::solve on a MultiSetLinearProblem with more than
+ * one set (src/MCLS_MCSASolverManager_impl.hpp:344-400 with
+ * MultiSetLinearProblem::blockConstantVectorSum,
+ * src/MCLS_MultiSetLinearProblem_impl.hpp:102-120): every set (one call per
+ * set, typically one process and GPU each, all with the same b, x0, domain
+ * parameters and MCSA parameters but their own random streams) transports
+ * its own histories; each iteration the sets' Monte Carlo corrections are
+ * summed by `reduce` and divided by num_sets.  The sets apply the same sum,
+ * so their iterates, residuals and stopping decisions are identical; the sum
+ * is the only exchange.
+ *   reduce(user, data_dev, n, stream): sum the n doubles at data_dev over
+ *   all sets, in place, identically on every set, either enqueued on the
+ *   CUDA stream `stream` (a cudaStream_t) or finished before returning;
+ *   returns 0 on success.
+ *   capturable = 1: reduce only enqueues stream work that a CUDA graph
+ *   capture may record (NCCL); the whole loop then runs on the device in a
+ *   captured WHILE graph, with no host round trip per iteration.  Otherwise
+ *   (a host reduction such as MPI or gloo on host copies) the loop runs from
+ *   the host.  *device_loop (may be NULL) receives which one ran. */
+typedef int (*mclsgpu_set_reduce_fn)(void* user, double* data_dev, int64_t n, void* stream);
+typedef struct {
+    uint32_t size;                  /* sizeof(mclsgpu_set_params) */
+    int32_t num_sets;               /* "Number of Sets" */
+    mclsgpu_set_reduce_fn reduce;
+    void* user;
+    int32_t capturable;
+    int32_t reserved0;
+} mclsgpu_set_params;
+int mclsgpu_mcsa_solve_sets(mclsgpu_domain* dom, const mclsgpu_set_params* sets, const double* b,
+                            double* x, const mclsgpu_mcsa_params* params, mclsgpu_stats* stats,
+                            int32_t* device_loop);
+int mclsgpu_mcsa_solve_sets_dev(mclsgpu_domain* dom, const mclsgpu_set_params* sets,
+                                const double* b_dev, double* x_dev,
+                                const mclsgpu_mcsa_params* params, mclsgpu_stats* stats,
+                                int32_t* device_loop);
+/* An NCCL communicator of nranks sets (no counterpart in the reference, whose
+ * sets talk over MPI): the library loads libnccl.so.2 at run time.  One rank
+ * makes the 128-byte unique id and the caller sends it to the others (any
+ * channel); every rank then creates its communicator with its own context's
+ * device.  mclsgpu_comm_set_params fills set params whose reducer is an
+ * in-place ncclAllReduce (sum) on the solve's stream, capturable. */
+typedef struct mclsgpu_comm mclsgpu_comm;
+int mclsgpu_comm_unique_id(uint8_t* id128);
+int mclsgpu_comm_create(mclsgpu_context* ctx, int nranks, int rank, const uint8_t* id128,
+                        mclsgpu_comm** out);
+int mclsgpu_comm_destroy(mclsgpu_comm* comm);
+int mclsgpu_comm_set_params(mclsgpu_comm* comm, mclsgpu_set_params* out);
+
 /* The preconditioned residual PL (b - A x) at the end of the last MCSA
  * solve, copied to the device vector rp_dev (LinearProblem::getPrecResidual,
  * src/MCLS_LinearProblem.hpp:121-122). */

@@ -140,6 +140,21 @@ class DomainInfo(C.Structure):
     ]
 
 
+#: Multi-set reducer: (user, data_dev, n, cudaStream_t) -> status.
+SET_REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
+
+
+class SetParams(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("num_sets", C.c_int32),
+        ("reduce", C.c_void_p),
+        ("user", C.c_void_p),
+        ("capturable", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
 #: Every entry point declared in include/mclsgpu.h.
 EXPORTS = [
     "mclsgpu_abi_version", "mclsgpu_build_info", "mclsgpu_context_create",
@@ -165,7 +180,9 @@ EXPORTS = [
     "mclsgpu_subdomain_destroy", "mclsgpu_subdomain_info", "mclsgpu_subdomain_begin",
     "mclsgpu_subdomain_transport", "mclsgpu_subdomain_finish",
     "mclsgpu_debug_device_allocations", "mclsgpu_set_wait_limit",
-    "mclsgpu_domain_walk_agreement",
+    "mclsgpu_domain_walk_agreement", "mclsgpu_mcsa_solve_sets", "mclsgpu_mcsa_solve_sets_dev",
+    "mclsgpu_comm_unique_id", "mclsgpu_comm_create", "mclsgpu_comm_destroy",
+    "mclsgpu_comm_set_params",
 ]
 
 _LIB = None
@@ -215,6 +232,15 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_domain_reseed.argtypes = [P, C.c_uint64]
     L.mclsgpu_domain_walk_agreement.argtypes = [P, i64, C.c_uint64, C.POINTER(i64),
                                                 C.POINTER(i64)]
+    L.mclsgpu_mcsa_solve_sets.argtypes = [P, C.POINTER(SetParams), P, P, C.POINTER(McsaParams),
+                                          C.POINTER(Stats), C.POINTER(C.c_int32)]
+    L.mclsgpu_mcsa_solve_sets_dev.argtypes = [P, C.POINTER(SetParams), P, P,
+                                              C.POINTER(McsaParams), C.POINTER(Stats),
+                                              C.POINTER(C.c_int32)]
+    L.mclsgpu_comm_unique_id.argtypes = [P]
+    L.mclsgpu_comm_create.argtypes = [P, C.c_int, C.c_int, P, PP]
+    L.mclsgpu_comm_destroy.argtypes = [P]
+    L.mclsgpu_comm_set_params.argtypes = [P, C.POINTER(SetParams)]
     L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
     L.mclsgpu_domain_set_launch.argtypes = [P, C.c_int, C.c_int]
     L.mclsgpu_domain_autotune.argtypes = [P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -290,6 +316,12 @@ def _torch_ready():
 
 def _ptr(a):
     return a.ctypes.data if a is not None else None
+
+
+def _stats():
+    st = Stats()
+    st.size = C.sizeof(Stats)
+    return st
 
 
 class Context:
@@ -538,6 +570,31 @@ class Domain:
                                                           C.byref(hpl), C.byref(blk),
                                                           C.byref(ms)))
         return {"histories_per_lane": hpl.value, "block_size": blk.value, "walk_ms": ms.value}
+
+    def mcsa_solve_sets_dev(self, sets: "SetParams", b_ptr, x_ptr,
+                            params: McsaParams | None = None, **kw):
+        """Multi-set MCSA with device vectors: (stats, ran on the device)."""
+        _torch_ready()
+        p = params if params is not None else mcsa_params(**kw)
+        st = _stats()
+        dl = C.c_int32(0)
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_solve_sets_dev(
+            self.h, C.byref(sets), C.c_void_p(b_ptr), C.c_void_p(x_ptr), C.byref(p),
+            C.byref(st), C.byref(dl)))
+        return st.as_dict(), bool(dl.value)
+
+    def mcsa_solve_sets(self, sets: "SetParams", b, x0=None, params: McsaParams | None = None,
+                        **kw):
+        """Multi-set MCSA with host vectors: (x, stats, ran on the device)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+        p = params if params is not None else mcsa_params(**kw)
+        st = _stats()
+        dl = C.c_int32(0)
+        self.ctx.check(self.ctx.L.mclsgpu_mcsa_solve_sets(self.h, C.byref(sets), _ptr(b), _ptr(x),
+                                                          C.byref(p), C.byref(st),
+                                                          C.byref(dl)))
+        return x, st.as_dict(), bool(dl.value)
 
     def walk_agreement(self, histories, seed=1):
         """FP32 walk against the FP64 selection on the same draws: (histories
@@ -927,6 +984,65 @@ class Subdomain:
 
     def __del__(self):
         self.close()
+
+
+class Comm:
+    """The library's NCCL communicator of `nranks` sets (multi-set MCSA)."""
+
+    @staticmethod
+    def unique_id() -> bytes:
+        buf = (C.c_uint8 * 128)()
+        rc = load().mclsgpu_comm_unique_id(buf)
+        if rc != OK:
+            raise MclsError(rc, "NCCL unique id")
+        return bytes(buf)
+
+    def __init__(self, ctx: Context, nranks: int, rank: int, uid: bytes):
+        self.ctx = ctx
+        buf = (C.c_uint8 * 128).from_buffer_copy(uid)
+        h = C.c_void_p()
+        ctx.check(ctx.L.mclsgpu_comm_create(ctx.h, nranks, rank, buf, C.byref(h)))
+        self.h = h
+        ctx._adopt(self)
+
+    def set_params(self) -> SetParams:
+        sp = SetParams()
+        self.ctx.check(self.ctx.L.mclsgpu_comm_set_params(self.h, C.byref(sp)))
+        return sp
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mclsgpu_comm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def set_params(num_sets: int, reduce, capturable: bool = False) -> SetParams:
+    """Set params around a Python reducer reduce(data_ptr, n, stream_ptr) ->
+    None that sums the n doubles at data_ptr over the sets in place.  The
+    returned structure keeps the callback alive."""
+
+    def _cb(user, data, n, stream):
+        try:
+            reduce(int(data or 0), int(n), int(stream or 0))
+            return 0
+        except Exception:  # reported to the library as a failed reduction
+            import traceback
+
+            traceback.print_exc()
+            return ERR_INVALID_ARG
+
+    fn = SET_REDUCE_FN(_cb)
+    sp = SetParams()
+    sp.size = C.sizeof(SetParams)
+    sp.num_sets = num_sets
+    sp.reduce = C.cast(fn, C.c_void_p).value
+    sp.user = None
+    sp.capturable = 1 if capturable else 0
+    sp._keep = fn
+    return sp
 
 
 def device_allocations():

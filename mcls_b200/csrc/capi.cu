@@ -142,6 +142,9 @@ void release_domain(mclsgpu_domain* d) {
     dfree(d->hlen);
     dfree(d->hoff2);
     dfree(d->y_save);
+    dfree(d->delta);
+    if (d->set_graph) cudaGraphExecDestroy(d->set_graph);
+    d->set_graph = nullptr;
     dfree(d->d_epoch);
     dfree(d->src);
     dfree(d->scdf);

@@ -194,6 +194,15 @@ struct mclsgpu_domain {
     int* hoff2 = nullptr;          // offsets recomputed from hlen (nh_cap + 1)
     double* y_save = nullptr;      // tallies before the first round (n)
     int walk_rounds = 0;           // rounds the last Monte Carlo solve took
+    // Multi-set MCSA (multiset.cu): this set's correction and the device-side
+    // loop captured for one reducer.
+    double* delta = nullptr;
+    cudaGraphExec_t set_graph = nullptr;
+    void* set_graph_reduce = nullptr;
+    void* set_graph_user = nullptr;
+    int set_graph_sets = 0;
+    long long set_graph_key = -1;
+    int set_body_kernels = 0;
     // Anderson-accelerated MCSA work space (anderson.cu), built on first use.
     mclsgpu::AndersonWork* aa = nullptr;
     int aa_step_ready = 0;

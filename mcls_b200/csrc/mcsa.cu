@@ -966,9 +966,92 @@ static int mcsa_solve_device(mclsgpu_domain* dom, const double* b_dev, double* x
     return MCLSGPU_OK;
 }
 
+// ---- multi-set loop pieces (multiset.cu) ------------------------------------
+// Start of an MCSA loop on dom->x and dom->b: |PL b|_2, the initial
+// preconditioned residual and its norm, the loop state.
+void mcsa_loop_begin(mclsgpu_domain* dom, const double* b_dev, const double* x_dev,
+                     const mclsgpu_mcsa_params* mp) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
+    reset_counters(dom);
+    if (b_dev != dom->b)
+        cudaMemcpyAsync(dom->b, b_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (x_dev != dom->x)
+        cudaMemcpyAsync(dom->x, x_dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    const double* pb = dom->b;
+    if (dom->left) {
+        spmv(s, dom->left->P, dom->b, dom->tmp);
+        pb = dom->tmp;
+    }
+    sum_sq(s, pb, n, dom->part, dom->d_scalars + 6);
+    update_prec_residual(dom, dom->x, dom->b, dom->rp);
+    sum_sq(s, dom->rp, n, dom->part, dom->d_scalars + 5);
+    k_mcsa_init<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 6, mp->tolerance, mp->check_freq,
+                                mp->max_iters, dom->d_scalars + 5);
+}
+
+// The convergence check on |rp|_2 (d_scalars[5]), ending a device-side loop
+// through `handle` when use_cond.
+void mcsa_loop_check(mclsgpu_domain* dom, cudaGraphConditionalHandle handle, int use_cond) {
+    cudaStream_t s = dom->ctx->stream;
+    if (use_cond)
+        k_mcsa_check<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid,
+                                     dom->resid_cap, dom->ctx->d_status, handle);
+    else
+        k_mcsa_check_host<<<1, 1, 0, s>>>(dom->d_state, dom->d_scalars + 5, dom->d_resid,
+                                           dom->resid_cap, dom->ctx->d_status);
+}
+
+// End of the loop: x_dev = PR x, the loop state and the statistics.
+int mcsa_loop_finish(mclsgpu_domain* dom, double* x_dev, float ms, int kernels_per_iter,
+                     mclsgpu_stats* stats) {
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const size_t bytes = size_t(dom->n) * sizeof(double);
+    if (dom->right) {
+        spmv(s, dom->right->P, dom->x, dom->tmp);
+        cudaMemcpyAsync(x_dev, dom->tmp, bytes, cudaMemcpyDeviceToDevice, s);
+    } else if (x_dev != dom->x) {
+        cudaMemcpyAsync(x_dev, dom->x, bytes, cudaMemcpyDeviceToDevice, s);
+    }
+    cudaMemcpyAsync(dom->h_state, dom->d_state, sizeof(McsaState), cudaMemcpyDeviceToHost, s);
+    double src_sumsq = 0.0;
+    cudaMemcpyAsync(&src_sumsq, dom->d_scalars + 6, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mcsa loop");
+    int rc = check_device_status(ctx);
+    if (rc) return rc;
+    const McsaState st = *dom->h_state;
+    if (stats) {
+        if ((rc = read_stats(dom, stats))) return rc;
+        stats->iterations = st.iter;
+        stats->converged = st.converged;
+        stats->residual_norm = st.rnorm;
+        const double sn = std::sqrt(src_sumsq);
+        stats->achieved_tol = sn > 0.0 ? st.rnorm / sn : st.rnorm;
+        stats->solve_ms = ms;
+        stats->fallback_taken = dom->left ? dom->left->fallback : 0;
+        stats->kernel_launches = int64_t(kernels_per_iter) * st.iter;
+        stats->rho = dom->left ? dom->left->rho : -1.0;
+    }
+    return MCLSGPU_OK;
+}
+
 }  // namespace mclsgpu
 
 using namespace mclsgpu;
+
+static int check_mcsa_params(mclsgpu_domain* dom, const mclsgpu_mcsa_params* p,
+                             mclsgpu_mcsa_params* out);
+
+namespace mclsgpu {
+int mcsa_check_params(mclsgpu_domain* dom, const mclsgpu_mcsa_params* p,
+                      mclsgpu_mcsa_params* out) {
+    return check_mcsa_params(dom, p, out);
+}
+}  // namespace mclsgpu
 
 static int check_mcsa_params(mclsgpu_domain* dom, const mclsgpu_mcsa_params* p,
                              mclsgpu_mcsa_params* out) {

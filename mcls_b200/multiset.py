@@ -130,3 +130,34 @@ def solve_anderson(engine, b, x0, group=None, tolerance=1e-8, max_iters=1000, sm
             rnorm, done = float(t[0].item()), bool(t[1].item())
     x, stats = engine.aa_finish()
     return x, steps, rnorm < tolerance * bnorm, rnorm / (bnorm if bnorm > 0.0 else 1.0), stats
+
+
+class _DeviceArray:
+    """A device vector of n doubles at ptr, seen by torch through the CUDA
+    array interface (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 2}
+
+
+def torch_set_params(pg, num_sets: int, device: str, host_copy: bool):
+    """Set params for mclsgpu_mcsa_solve_sets whose reducer is a
+    torch.distributed all-reduce (sum) of the set's correction, issued on the
+    library's stream: over NCCL on the device vector, or with host_copy over
+    a CPU backend (gloo) on a host copy.  The loop then runs from the host;
+    the library's own NCCL communicator (capi.Comm) runs it on the device."""
+    import torch
+
+    def reduce(ptr, n, stream):
+        t = torch.as_tensor(_DeviceArray(ptr, n), device=device)
+        ext = torch.cuda.ExternalStream(stream, device=device)
+        with torch.cuda.stream(ext):
+            if host_copy:
+                h = t.cpu()
+                pg.all_reduce(h)
+                t.copy_(h)
+            else:
+                pg.all_reduce(t)
+
+    return capi.set_params(num_sets, reduce, capturable=False)

@@ -1,0 +1,44 @@
+"""One set of the multi-set MCSA entry point (mclsgpu_mcsa_solve_sets), run
+as one of several processes on one GPU by tests/test_multiset_sets_gpu.py.
+The sets' corrections are summed over gloo on host copies (the host-loop
+form of the entry point; no kernel waits on another process)."""
+import json
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from mcls_b200 import capi, dist, multiset  # noqa: E402
+from mcls_b200 import problems as P  # noqa: E402
+
+
+def main(out):
+    import torch
+
+    world, rank, _, pg = dist.init("gloo", timeout_s=120)
+    A, b = P.diffusion3d_varcoef(10, seed=3)
+    ctx = capi.Context(0)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    seed = capi.rank_seed(99, rank)
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP64, rng_mode=capi.RNG_COUNTER, seed=seed,
+                      estimator=capi.COLLISION, direction=capi.ADJOINT, sample_ratio=1.0,
+                      history_length=10)
+    sets = multiset.torch_set_params(pg, world, "cuda:0", host_copy=True)
+    x, st, on_device = dom.mcsa_solve_sets(sets, b, tolerance=1e-8, max_iters=5000)
+    pg.barrier()
+    with open(out, "w") as f:
+        json.dump({"rank": rank, "seed": seed, "x": x.tolist(), "iters": st["iterations"],
+                   "converged": st["converged"], "device_loop": on_device}, f)
+    dom.close()
+    pc.close()
+    op.close()
+    ctx.close()
+    pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

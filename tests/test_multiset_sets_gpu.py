@@ -1,0 +1,110 @@
+"""Multi-set MCSA through the C ABI (mclsgpu_mcsa_solve_sets), the drop-in
+form of MCSASolverManager on a MultiSetLinearProblem with several sets.
+
+* Two sets in two processes on one GPU, corrections summed over gloo on host
+  copies: both sets end with the same iterate and iteration count, equal
+  bit for bit to the step-wise two-set emulation in one process (the same
+  per-set streams), and the direct solution.
+* One set through the library's NCCL communicator (a one-rank clique): the
+  loop with the ncclAllReduce runs inside the captured device-side WHILE
+  loop and gives the host-loop result bit for bit.
+"""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from mcls_b200 import capi, multiset
+from mcls_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _domain(ctx, op, pc, seed):
+    return capi.Domain(ctx, op, pc, precision=capi.FP64, rng_mode=capi.RNG_COUNTER, seed=seed,
+                       estimator=capi.COLLISION, direction=capi.ADJOINT, sample_ratio=1.0,
+                       history_length=10)
+
+
+def _emulated_two_sets(ctx, A, b):
+    engines = []
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    engines = [multiset.DeviceEngine(_domain(ctx, op, pc, capi.rank_seed(99, r)), A.shape[0])
+               for r in range(2)]
+    params = capi.mcsa_params(tolerance=1e-8, max_iters=5000)
+    norms = [e.begin(b, np.zeros_like(b), params) for e in engines]
+    crit = 1e-8 * norms[0][1]
+    it, rn = 0, norms[0][0]
+    while rn > crit and it < 5000:
+        it += 1
+        d = [e.correction().clone() for e in engines]
+        total = d[0] + d[1]
+        rn = [e.apply(total, 0.5) for e in engines][0]
+    return engines[0].finish()[0].cpu().numpy(), it
+
+
+def test_two_processes_sum_their_corrections(ctx, tmp_path):
+    A, b = P.diffusion3d_varcoef(10, seed=3)
+    port = _free_port()
+    procs, outs = [], []
+    for r in range(2):
+        out = str(tmp_path / f"set{r}.json")
+        outs.append(out)
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK="0", WORLD_SIZE="2",
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.join(ROOT, "tests",
+                                                                    "multiset_sets_worker.py"),
+                                       out], env=env, stdout=subprocess.PIPE,
+                                      stderr=subprocess.STDOUT))
+    logs = []
+    for p in procs:
+        try:
+            o, _ = p.communicate(timeout=600)
+        except subprocess.TimeoutExpired:
+            p.kill()
+            o, _ = p.communicate()
+        logs.append(o.decode(errors="replace"))
+    for p in procs:
+        assert p.returncode == 0, "\n".join(logs)
+    r0, r1 = [json.load(open(o)) for o in outs]
+    assert r0["seed"] != r1["seed"]
+    assert r0["converged"] and r1["converged"] and r0["iters"] == r1["iters"]
+    assert not r0["device_loop"]  # a host reduction runs the loop from the host
+    x0, x1 = np.array(r0["x"]), np.array(r1["x"])
+    assert np.array_equal(x0, x1)
+    xe, ite = _emulated_two_sets(ctx, A, b)
+    assert ite == r0["iters"]
+    assert np.array_equal(x0, xe)
+    xs = spla.spsolve(A.tocsc(), b)
+    assert np.linalg.norm(x0 - xs) <= 1e-6 * np.linalg.norm(xs)
+
+
+def test_nccl_one_rank_runs_on_the_device(ctx):
+    A, b = P.diffusion3d_varcoef(10, seed=5)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    comm = capi.Comm(ctx, 1, 0, capi.Comm.unique_id())
+    sets = comm.set_params()
+    assert sets.num_sets == 1 and sets.capturable == 1
+    x_dev, st_dev, on_device = _domain(ctx, op, pc, 41).mcsa_solve_sets(
+        sets, b, tolerance=1e-8, max_iters=5000)
+    assert on_device and st_dev["converged"] == 1
+    x_host, st_host, on_dev2 = _domain(ctx, op, pc, 41).mcsa_solve_sets(
+        sets, b, tolerance=1e-8, max_iters=5000, host_loop=1)
+    assert not on_dev2
+    assert st_dev["iterations"] == st_host["iterations"]
+    assert np.array_equal(x_dev, x_host)
+    comm.close()
