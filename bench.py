@@ -748,7 +748,9 @@ def workload_config(args, cfgd, n, nnz, world):
             "tolerance": 1e-8, "weight_cutoff": cfgd.get("weight_cutoff", 0.0),
             "stopping_test": "|PL (b - A x)|_2 <= 1e-8 |PL b|_2 (MCSASolverManager's test)",
             "preconditioner": "point Jacobi",
-            "parallelism": f"replicas x{world}" if world > 1 else "single domain",
+            "parallelism": (f"multi-set x{world}: one set of the histories per GPU, "
+                            "corrections summed by an NCCL all-reduce each iteration"
+                            if world > 1 else "single domain"),
             "l2": ("inputs fit in L2 (small latency-bound solve; no flush)"
                    if args.config == "poisson100" else "inputs larger than L2 (no flush)")}
 
@@ -970,10 +972,23 @@ def main():
         tuned = dom.autotune(dt.data_ptr(), reps=2)
         del dt
 
+    # More than one GPU: multi-set MCSA of the one system, one set per GPU,
+    # the sets' corrections summed each iteration by the library's NCCL
+    # communicator inside the device-side loop.
+    sets = None
+    if world > 1:
+        uid = [capi.Comm.unique_id() if rank == 0 else None]
+        pg.broadcast_object_list(uid, src=0)
+        comm = capi.Comm(ctx, world, rank, uid[0])
+        sets = comm.set_params()
+        seed = capi.rank_seed(args.seed, rank)
+
     def device_step():
         dom.reseed(seed)
         xt.zero_()
         torch.cuda.synchronize()
+        if sets is not None:
+            return dom.mcsa_solve_sets_dev(sets, bt.data_ptr(), xt.data_ptr(), params=mp)[0]
         return dom.mcsa_solve_dev(bt.data_ptr(), xt.data_ptr(), params=mp)
 
     for _ in range(args.warmup):
@@ -1003,7 +1018,10 @@ def main():
         dom.reseed(seed)
         x0 = np.zeros(n)
         t1 = time.perf_counter()
-        x, st = dom.mcsa_solve(bh, x0, params=mp)
+        if sets is not None:
+            x, st, _ = dom.mcsa_solve_sets(sets, bh, x0, params=mp)
+        else:
+            x, st = dom.mcsa_solve(bh, x0, params=mp)
         e2e_ms += (time.perf_counter() - t1) * 1e3
         e2e_steps += st["walk_steps"]
     barrier(pg)
@@ -1044,7 +1062,7 @@ def main():
     line = {
         "metric": METRIC, "value": solve_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fp == capi.FP32 else "f64",
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32" if fp == capi.FP32 else "f64",
         "data": "synthetic", "config": config, "results": results,
         "clocks": clk,
         "e2e": {"value": e2e_ms / args.steps / 1e3, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n,

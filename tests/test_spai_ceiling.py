@@ -80,3 +80,25 @@ def test_spectral_gap_gain_is_at_most_2_4():
     # the interior row-sum formula is the matrix's own
     _, W = _gap_and_rowsum(A, _poly_spai(A, *arg))
     assert W.max() <= 1.0 + 1e-12
+
+
+def test_mcsa_iterations_follow_history_length_not_histories():
+    # On the 3D var-coef workload family the MCSA iteration count is set by
+    # rho(H)^(History Length + 1): twice the History Length takes markedly
+    # fewer iterations, four times the histories barely changes the count
+    # (the oracle's FP64 forward expected-value MCSA, 16^3).
+    from oracle import oracle as O
+
+    A, b = P.diffusion3d_varcoef(16, seed=0)
+    Ao = O.Csr.from_scipy(A)
+    PL = O.point_jacobi(Ao)
+
+    def its(L, ratio):
+        r = O.mcsa_solve(Ao, b, PL=PL, tolerance=1e-8, max_iters=5000, estimator=1,
+                         direction=1, sample_ratio=ratio, rng_mode=1, seed=5, history_length=L)
+        assert r["converged"]
+        return r["iters"]
+
+    base = its(10, 2.0)
+    assert its(20, 2.0) < 0.7 * base
+    assert abs(its(10, 8.0) - base) <= 0.1 * base
