@@ -10,6 +10,7 @@
 
 #include <cstdint>
 #include <map>
+#include <cstdio>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -412,6 +413,24 @@ class DeviceProblem {
             auto left = precondFor<Vector, Matrix>(op, problem.getLeftPrec());
             auto right = precondFor<Vector, Matrix>(op, problem.getRightPrec());
             d_domain = std::make_shared<Domain>(op, left, right, mp);
+            // "Compute Convergence Criteria" prints the reference's report of
+            // the new domain (src/MCLS_AlmostOptimalDomain_impl.hpp:95-113,
+            // 530-541).
+            if (flag(pl, "Compute Convergence Criteria", false)) {
+                mclsgpu_criteria c{};
+                c.size = sizeof(c);
+                ctx->check(mclsgpu_domain_convergence_criteria(d_domain->get(), 2000, 1e-6, 7, &c),
+                           "mclsgpu_domain_convergence_criteria");
+                std::printf("\n||H||_inf = %g\nsum|H|_min = %g\n\nH Balance Parameters\n"
+                            "min: %g\nmax: %g\nave: %g\n",
+                            c.row_sum_max, c.row_sum_min, c.balance_min, c.balance_max,
+                            c.balance_ave);
+                std::printf("\nNeumann/Ulam Convergence Criteria\n"
+                            "---------------------------------\n"
+                            "rho(H)  = %g\nrho(H+) = %g\nrho(H*) = %g\n"
+                            "---------------------------------\n\n",
+                            c.rho_h, c.rho_abs, c.rho_star);
+            }
             d_device = device;
             d_mp = mp;
             d_A = problem.getOperator();

@@ -654,6 +654,23 @@ int mclsgpu_domain_spectral_radius(mclsgpu_domain* dom, int which,
                                    int max_iters, double tol, uint64_t seed,
                                    double* rho);
 
+/* Replaces AlmostOptimalDomain::computeConvergenceCriteria and the
+ * "Compute Convergence Criteria" printout (src/MCLS_AlmostOptimalDomain_
+ * impl.hpp:95-113, 437-635): rho(H), rho(H+ = |H|) and rho(H*) by power
+ * iteration, |H|_inf and the smallest row sum of |H|, and the balance
+ * parameters max_j |h_ij| / max_j |h_ji| over the states (min, max, mean;
+ * states that no row transitions into are left out). */
+typedef struct {
+    uint32_t size;            /* sizeof(mclsgpu_criteria) */
+    int32_t reserved0;
+    double rho_h, rho_abs, rho_star;
+    double row_sum_max;       /* ||H||_inf */
+    double row_sum_min;       /* sum|H|_min */
+    double balance_min, balance_max, balance_ave;
+} mclsgpu_criteria;
+int mclsgpu_domain_convergence_criteria(mclsgpu_domain* dom, int max_iters, double tol,
+                                        uint64_t seed, mclsgpu_criteria* out);
+
 #ifdef __cplusplus
 }
 #endif

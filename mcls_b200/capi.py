@@ -140,6 +140,21 @@ class DomainInfo(C.Structure):
     ]
 
 
+class Criteria(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint32),
+        ("reserved0", C.c_int32),
+        ("rho_h", C.c_double),
+        ("rho_abs", C.c_double),
+        ("rho_star", C.c_double),
+        ("row_sum_max", C.c_double),
+        ("row_sum_min", C.c_double),
+        ("balance_min", C.c_double),
+        ("balance_max", C.c_double),
+        ("balance_ave", C.c_double),
+    ]
+
+
 #: Multi-set reducer: (user, data_dev, n, cudaStream_t) -> status.
 SET_REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
 
@@ -182,7 +197,7 @@ EXPORTS = [
     "mclsgpu_debug_device_allocations", "mclsgpu_set_wait_limit",
     "mclsgpu_domain_walk_agreement", "mclsgpu_mcsa_solve_sets", "mclsgpu_mcsa_solve_sets_dev",
     "mclsgpu_comm_unique_id", "mclsgpu_comm_create", "mclsgpu_comm_destroy",
-    "mclsgpu_comm_set_params",
+    "mclsgpu_comm_set_params", "mclsgpu_domain_convergence_criteria",
 ]
 
 _LIB = None
@@ -241,6 +256,8 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_comm_create.argtypes = [P, C.c_int, C.c_int, P, PP]
     L.mclsgpu_comm_destroy.argtypes = [P]
     L.mclsgpu_comm_set_params.argtypes = [P, C.POINTER(SetParams)]
+    L.mclsgpu_domain_convergence_criteria.argtypes = [P, C.c_int, d, C.c_uint64,
+                                                      C.POINTER(Criteria)]
     L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
     L.mclsgpu_domain_set_launch.argtypes = [P, C.c_int, C.c_int]
     L.mclsgpu_domain_autotune.argtypes = [P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -746,6 +763,14 @@ class Domain:
         """Copy the last MCSA solve's preconditioned residual to a device vector."""
         _torch_ready()
         self.ctx.check(self.ctx.L.mclsgpu_domain_residual(self.h, C.c_void_p(rp_dev_ptr)))
+
+    def convergence_criteria(self, max_iters=2000, tol=1e-8, seed=7):
+        """AlmostOptimalDomain::computeConvergenceCriteria's report."""
+        c = Criteria()
+        c.size = C.sizeof(Criteria)
+        self.ctx.check(self.ctx.L.mclsgpu_domain_convergence_criteria(self.h, max_iters, tol,
+                                                                      seed, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in c._fields_ if k not in ("size", "reserved0")}
 
     def spectral_radius(self, which=0, max_iters=2000, tol=1e-8, seed=7):
         rho = C.c_double()

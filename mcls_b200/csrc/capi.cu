@@ -1,5 +1,6 @@
 // capi.cu -- context, operator, preconditioner and domain entry points of the
 // C ABI, plus the error plumbing shared by the other translation units.
+#include <algorithm>
 #include <cstdarg>
 #include <cmath>
 #include <cstring>
@@ -82,6 +83,21 @@ __global__ void k_domain_spmv(const int* rp, const int* ci, const double* h, con
             s = fma(v, x[ci[k]], s);
         }
         y[i] = s;
+    }
+}
+
+// Balance parameters of |H|: rmax[i] = max_j |h_ij|, cmax[j] = max_i |h_ij|
+// (non-negative doubles order like their bit patterns).
+__global__ void k_row_col_max(const int* rp, const double* h, const int* ci, int n, double* rmax,
+                              unsigned long long* cmax) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double m = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const double a = fabs(h[k]);
+            m = fmax(m, a);
+            atomicMax(&cmax[ci[k]], (unsigned long long)__double_as_longlong(a));
+        }
+        rmax[i] = m;
     }
 }
 
@@ -628,6 +644,57 @@ int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed) {
     }
     cudaError_t e = cudaStreamSynchronize(dom->ctx->stream);
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(dom->ctx, e, "reseed");
+}
+
+int mclsgpu_domain_convergence_criteria(mclsgpu_domain* dom, int max_iters, double tol,
+                                        uint64_t seed, mclsgpu_criteria* out) {
+    if (!dom || !out || out->size < sizeof(mclsgpu_criteria)) return MCLSGPU_ERR_INVALID_ARG;
+    double rho[3];
+    for (int which = 0; which < 3; ++which) {
+        int rc = mclsgpu_domain_spectral_radius(dom, which, max_iters, tol, seed, &rho[which]);
+        if (rc) return rc;
+    }
+    mclsgpu_context* ctx = dom->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = dom->n;
+    std::vector<double> w(n), rmax(n);
+    std::vector<unsigned long long> cmax(n);
+    unsigned long long* d_cmax = nullptr;
+    cudaError_t e = dmalloc(&d_cmax, size_t(n));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    cudaMemsetAsync(d_cmax, 0, size_t(n) * sizeof(unsigned long long), s);
+    k_row_col_max<<<grid_for(n), 256, 0, s>>>(dom->D.rp, dom->D.v, dom->D.ci, n, dom->tmp, d_cmax);
+    cudaMemcpyAsync(w.data(), dom->w, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(rmax.data(), dom->tmp, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(cmax.data(), d_cmax, size_t(n) * sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    dfree(d_cmax);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "convergence criteria");
+    out->rho_h = rho[0];
+    out->rho_abs = rho[1];
+    out->rho_star = rho[2];
+    out->row_sum_max = 0.0;
+    out->row_sum_min = std::numeric_limits<double>::max();
+    double bmin = std::numeric_limits<double>::max(), bmax = 0.0, bsum = 0.0;
+    long long rows = 0;
+    for (int i = 0; i < n; ++i) {
+        out->row_sum_max = std::max(out->row_sum_max, w[i]);
+        out->row_sum_min = std::min(out->row_sum_min, w[i]);
+        double c;
+        std::memcpy(&c, &cmax[i], sizeof(c));
+        if (c > 0.0) {  // a state no row transitions into has no column norm
+            const double r = rmax[i] / c;
+            bmin = std::min(bmin, r);
+            bmax = std::max(bmax, r);
+            bsum += r;
+            ++rows;
+        }
+    }
+    out->balance_min = rows ? bmin : 0.0;
+    out->balance_max = bmax;
+    out->balance_ave = rows ? bsum / double(rows) : 0.0;
+    return MCLSGPU_OK;
 }
 
 int mclsgpu_domain_spectral_radius(mclsgpu_domain* dom, int which, int max_iters, double tol,

@@ -269,6 +269,33 @@ def test_spectral_radius_matches_dense_eigensolve(ctx):
         assert abs(rho - want) <= 1e-4 * want, (which, rho, want)
 
 
+@pytest.mark.parametrize("name", ["varcoef3d", "aniso9pt"])
+def test_convergence_criteria_match_dense_computation(ctx, name):
+    # AlmostOptimalDomain::computeConvergenceCriteria
+    # (src/MCLS_AlmostOptimalDomain_impl.hpp:437-635): spectral radii of H,
+    # |H| and H*, |H|_inf, the smallest row sum and the balance parameters
+    # max_j |h_ij| / max_j |h_ji|.
+    A, _ = _systems()[name]
+    dom, op, pc = _gpu_domain(ctx, A, "jacobi", precision=capi.FP64)
+    c = dom.convergence_criteria(max_iters=4000, tol=1e-10)
+    d = dom.export()
+    n = A.shape[0]
+    H = sp.csr_matrix((d["h"], d["col"], d["rowptr"]), shape=(n, n)).toarray()
+    Hp = np.abs(H)
+    for key, M in (("rho_h", H), ("rho_abs", Hp), ("rho_star", Hp * d["weights"][:, None])):
+        want = np.abs(np.linalg.eigvals(M)).max()
+        assert abs(c[key] - want) <= 1e-4 * want, (key, c[key], want)
+    rs = Hp.sum(1)
+    assert c["row_sum_max"] == pytest.approx(rs.max(), rel=1e-14)
+    assert c["row_sum_min"] == pytest.approx(rs.min(), rel=1e-14)
+    colmax = Hp.max(0)
+    keep = colmax > 0
+    ratio = Hp.max(1)[keep] / colmax[keep]
+    assert c["balance_min"] == pytest.approx(ratio.min(), rel=1e-14)
+    assert c["balance_max"] == pytest.approx(ratio.max(), rel=1e-14)
+    assert c["balance_ave"] == pytest.approx(ratio.mean(), rel=1e-12)
+
+
 def test_degenerate_row_is_reported(ctx):
     A = sp.lil_matrix((4, 4))
     A[0, 0] = 1.0
