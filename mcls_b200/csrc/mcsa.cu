@@ -1265,7 +1265,7 @@ int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev) {
 }
 
 int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane, int block_size) {
-    if (!dom || (histories_per_lane != 1 && histories_per_lane != 2) ||
+    if (!dom || (histories_per_lane != 1 && histories_per_lane != 2 && histories_per_lane != 4) ||
         (block_size != 128 && block_size != 256))
         return MCLSGPU_ERR_INVALID_ARG;
     dom->walk_ilp = histories_per_lane;
@@ -1286,10 +1286,14 @@ int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps
     cudaMemcpyAsync(&saved[1], dom->d_pos, sizeof(saved[1]), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "autotune");
-    const int shapes[4][2] = {{1, 256}, {2, 256}, {1, 128}, {2, 128}};
+    // Four histories per lane apply to fixed-length histories on 32-byte
+    // records only.
+    const bool four = dom->slots == 4 && !(dom->p.weight_cutoff > 0.0);
+    const int shapes[6][2] = {{1, 256}, {2, 256}, {1, 128}, {2, 128}, {4, 256}, {4, 128}};
     double best = 1e300;
     int bh = 1, bb = 256;
     for (const auto& sh : shapes) {
+        if (sh[0] == 4 && !four) continue;
         int rc = mclsgpu_domain_set_launch(dom, sh[0], sh[1]);
         if (rc) return rc;
         mclsgpu_stats st{};
