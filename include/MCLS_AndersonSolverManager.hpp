@@ -80,8 +80,9 @@ class AndersonSolverManager : public SolverManager<Vector, Matrix> {
     void setMultiSetProblem(const Teuchos::RCP<MultiSetType>& multiset_problem) {
         if (!Teuchos::nonnull(multiset_problem))
             throw Assertion("AndersonSolverManager: null problem");
-        if (multiset_problem->getNumSets() != 1)
-            throw Assertion("AndersonSolverManager: one set per process on the GPU path");
+        if (multiset_problem->getNumSets() != 1 && !multiset_problem->hasSetReducer())
+            throw Assertion("AndersonSolverManager: a problem of several sets needs a set "
+                            "reducer (MultiSetLinearProblem::setSetReducer)");
         d_multiset = multiset_problem;
         setProblem(multiset_problem->getProblem());
     }
@@ -108,6 +109,19 @@ class AndersonSolverManager : public SolverManager<Vector, Matrix> {
         gpu::Domain& dom = d_device.prepare(left_only, *d_plist, direction());
         d_stats = mclsgpu_stats{};
         d_stats.size = sizeof(d_stats);
+        const int sets = Teuchos::nonnull(d_multiset) ? d_multiset->getNumSets() : 1;
+        if (d_plist->isParameter("Number of Sets") &&
+            int(gpu::numeric(*d_plist, "Number of Sets", 1.0)) != sets)
+            throw Assertion("AndersonSolverManager: \"Number of Sets\" differs from the "
+                            "problem's");
+        if (sets > 1) {
+            dom.context().check(
+                mclsgpu_anderson_solve_sets(dom.get(), &d_multiset->setReducer(),
+                                            VT::view(*d_problem->getRHS()),
+                                            VT::viewNonConst(*d_problem->getLHS()), &ap, &d_stats),
+                "mclsgpu_anderson_solve_sets");
+            return d_stats.converged != 0;
+        }
         dom.context().check(mclsgpu_anderson_solve(dom.get(), VT::view(*d_problem->getRHS()),
                                                    VT::viewNonConst(*d_problem->getLHS()), &ap,
                                                    &d_stats),

@@ -537,6 +537,14 @@ int mclsgpu_mcsa_solve_sets_dev(mclsgpu_domain* dom, const mclsgpu_set_params* s
                                 const double* b_dev, double* x_dev,
                                 const mclsgpu_mcsa_params* params, mclsgpu_stats* stats,
                                 int32_t* device_loop);
+/* The Anderson-accelerated solve of a multi-set problem (AndersonSolverManager
+ * on a MultiSetLinearProblem: the model evaluator sums the sets' corrections
+ * before F, src/MCLS_MCSAModelEvaluator_impl.hpp:338-345), host vectors, the
+ * loop run from the host around mclsgpu_anderson_begin / _correction / the
+ * set reducer / _apply (scale 1 / num_sets) / _finish. */
+int mclsgpu_anderson_solve_sets(mclsgpu_domain* dom, const mclsgpu_set_params* sets,
+                                const double* b, double* x,
+                                const mclsgpu_anderson_params* params, mclsgpu_stats* stats);
 /* An NCCL communicator of nranks sets (no counterpart in the reference, whose
  * sets talk over MPI): the library loads libnccl.so.2 at run time.  One rank
  * makes the 128-byte unique id and the caller sends it to the others (any

@@ -198,6 +198,7 @@ EXPORTS = [
     "mclsgpu_domain_walk_agreement", "mclsgpu_mcsa_solve_sets", "mclsgpu_mcsa_solve_sets_dev",
     "mclsgpu_comm_unique_id", "mclsgpu_comm_create", "mclsgpu_comm_destroy",
     "mclsgpu_comm_set_params", "mclsgpu_domain_convergence_criteria",
+    "mclsgpu_anderson_solve_sets",
 ]
 
 _LIB = None
@@ -256,6 +257,8 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_comm_create.argtypes = [P, C.c_int, C.c_int, P, PP]
     L.mclsgpu_comm_destroy.argtypes = [P]
     L.mclsgpu_comm_set_params.argtypes = [P, C.POINTER(SetParams)]
+    L.mclsgpu_anderson_solve_sets.argtypes = [P, C.POINTER(SetParams), P, P,
+                                              C.POINTER(AndersonParams), C.POINTER(Stats)]
     L.mclsgpu_domain_convergence_criteria.argtypes = [P, C.c_int, d, C.c_uint64,
                                                       C.POINTER(Criteria)]
     L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
@@ -612,6 +615,17 @@ class Domain:
                                                           C.byref(p), C.byref(st),
                                                           C.byref(dl)))
         return x, st.as_dict(), bool(dl.value)
+
+    def anderson_solve_sets(self, sets: "SetParams", b, x0=None,
+                            params: AndersonParams | None = None, **kw):
+        """Multi-set Anderson-accelerated MCSA with host vectors: (x, stats)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+        p = params if params is not None else anderson_params(**kw)
+        st = _stats()
+        self.ctx.check(self.ctx.L.mclsgpu_anderson_solve_sets(self.h, C.byref(sets), _ptr(b),
+                                                              _ptr(x), C.byref(p), C.byref(st)))
+        return x, st.as_dict()
 
     def walk_agreement(self, histories, seed=1):
         """FP32 walk against the FP64 selection on the same draws: (histories

@@ -254,6 +254,45 @@ int mclsgpu_mcsa_solve_sets(mclsgpu_domain* dom, const mclsgpu_set_params* sets,
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "copy x");
 }
 
+int mclsgpu_anderson_solve_sets(mclsgpu_domain* dom, const mclsgpu_set_params* sets,
+                                const double* b, double* x,
+                                const mclsgpu_anderson_params* params, mclsgpu_stats* stats) {
+    if (!dom || !b || !x) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = dom->ctx;
+    if (!sets || sets->size < sizeof(mclsgpu_set_params) || sets->num_sets < 1 || !sets->reduce)
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "set params: num_sets >= 1 and a reducer");
+    const int n = dom->n;
+    cudaStream_t s = ctx->stream;
+    if (!dom->delta) {
+        cudaError_t e = dmalloc(&dom->delta, size_t(n));
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    }
+    // b and x0 go straight into the solver's own vectors.
+    const size_t bytes = size_t(n) * sizeof(double);
+    cudaError_t e = cudaMemcpyAsync(dom->b, b, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dom->x, x, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "copy b, x");
+    double rnorm = 0.0, bnorm = 0.0;
+    int32_t done = 0;
+    int rc = mclsgpu_anderson_begin(dom, dom->b, dom->x, params, &rnorm, &bnorm, &done);
+    const double scale = 1.0 / double(sets->num_sets);
+    while (!rc && !done) {
+        rc = mclsgpu_anderson_correction(dom, dom->delta);
+        if (!rc) {
+            rc = sets->reduce(sets->user, dom->delta, int64_t(n), s);
+            if (rc) set_error(ctx, rc, "multi-set reducer failed (status %d)", rc);
+        }
+        if (!rc) rc = mclsgpu_anderson_apply(dom, dom->delta, scale, &rnorm, &done);
+    }
+    if (rc) return rc;
+    rc = mclsgpu_anderson_finish(dom, dom->x, stats);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(x, dom->x, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "copy x");
+}
+
 int mclsgpu_comm_unique_id(uint8_t* id) {
     if (!id) return MCLSGPU_ERR_INVALID_ARG;
     std::string why;

@@ -170,6 +170,47 @@ int main() {
         }
         EXPECT(std::sqrt(d / nn) < 1e-6);
     }
+    // The Anderson-accelerated manager on the same two sets.
+    {
+        Vec xa[2];
+        bool aconv[2] = {false, false};
+        int aiters[2] = {0, 0};
+        auto run_aa = [&](int set) {
+            try {
+                auto x = Teuchos::rcp(new Vec(n, 0.0));
+                auto b = Teuchos::rcp(new Vec(n, 1.0));
+                auto lp = Teuchos::rcp(new MCLS::LinearProblem<Vec, Mat>(A, x, b));
+                auto ms = Teuchos::rcp(new MCLS::MultiSetLinearProblem<Vec, Mat>(comm, 2, set, lp));
+                mclsgpu_set_params sp{};
+                sp.size = sizeof(sp);
+                sp.num_sets = 2;
+                sp.reduce = &reduce_two;
+                sp.user = &users[set];
+                ms->setSetReducer(sp);
+                auto pl = Teuchos::parameterList();
+                pl->set<double>("Convergence Tolerance", 1e-8);
+                pl->set<int>("Maximum Iterations", 2000);
+                pl->set<double>("Sample Ratio", 1.0);
+                pl->set<int>("Number of Sets", 2);
+                pl->set<double>("Random Seed", 5000.0 + 31.0 * set);
+                pl->sublist("Anderson Parameters").set<int>("Storage Depth", 3);
+                MCLS::AndersonSolverManager<Vec, Mat> sm(ms, pl);
+                aconv[set] = sm.solve();
+                aiters[set] = sm.getNumIters();
+                xa[set] = *x;
+            } catch (const std::exception& e) {
+                errors[set] = e.what();
+            }
+        };
+        std::thread t2(run_aa, 1);
+        run_aa(0);
+        t2.join();
+        for (int s2 = 0; s2 < 2; ++s2)
+            if (!errors[s2].empty()) std::printf("anderson set %d: %s\n", s2, errors[s2].c_str());
+        EXPECT(aconv[0] && aconv[1]);
+        EXPECT(aiters[0] == aiters[1] && aiters[0] > 0);
+        EXPECT(xa[0] == xa[1]);
+    }
     // Two sets without a reducer, or a "Number of Sets" that disagrees.
     {
         auto x = Teuchos::rcp(new Vec(n, 0.0));

@@ -29,10 +29,18 @@ def main(out):
                       history_length=10)
     sets = multiset.torch_set_params(pg, world, "cuda:0", host_copy=True)
     x, st, on_device = dom.mcsa_solve_sets(sets, b, tolerance=1e-8, max_iters=5000)
+    # Anderson-accelerated sets on their own domain and streams.
+    da = capi.Domain(ctx, op, pc, precision=capi.FP64, rng_mode=capi.RNG_COUNTER,
+                     seed=capi.rank_seed(17, rank), estimator=capi.COLLISION,
+                     direction=capi.ADJOINT, sample_ratio=1.0, history_length=10)
+    xa, sa = da.anderson_solve_sets(sets, b, tolerance=1e-10, max_iters=2000, storage_depth=3)
+    da.close()
     pg.barrier()
     with open(out, "w") as f:
         json.dump({"rank": rank, "seed": seed, "x": x.tolist(), "iters": st["iterations"],
-                   "converged": st["converged"], "device_loop": on_device}, f)
+                   "converged": st["converged"], "device_loop": on_device,
+                   "aa_x": xa.tolist(), "aa_iters": sa["iterations"],
+                   "aa_converged": sa["converged"]}, f)
     dom.close()
     pc.close()
     op.close()

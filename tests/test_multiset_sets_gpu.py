@@ -4,7 +4,8 @@ form of MCSASolverManager on a MultiSetLinearProblem with several sets.
 * Two sets in two processes on one GPU, corrections summed over gloo on host
   copies: both sets end with the same iterate and iteration count, equal
   bit for bit to the step-wise two-set emulation in one process (the same
-  per-set streams), and the direct solution.
+  per-set streams), and the direct solution; the same for the
+  Anderson-accelerated solve (mclsgpu_anderson_solve_sets).
 * One set through the library's NCCL communicator (a one-rank clique): the
   loop with the ncclAllReduce runs inside the captured device-side WHILE
   loop and gives the host-loop result bit for bit.
@@ -56,6 +57,22 @@ def _emulated_two_sets(ctx, A, b):
     return engines[0].finish()[0].cpu().numpy(), it
 
 
+def _emulated_two_anderson_sets(ctx, A, b):
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    engines = [multiset.DeviceEngine(_domain(ctx, op, pc, capi.rank_seed(17, r)), A.shape[0])
+               for r in range(2)]
+    params = capi.anderson_params(tolerance=1e-10, max_iters=2000, storage_depth=3)
+    done = [e.aa_begin(b, np.zeros_like(b), params) for e in engines][0][2]
+    steps = 0
+    while not done:
+        steps += 1
+        d = [e.aa_correction().clone() for e in engines]
+        total = d[0] + d[1]
+        done = [e.aa_apply(total, 0.5) for e in engines][0][1]
+    return engines[0].aa_finish()[0].cpu().numpy(), steps
+
+
 def test_two_processes_sum_their_corrections(ctx, tmp_path):
     A, b = P.diffusion3d_varcoef(10, seed=3)
     port = _free_port()
@@ -90,6 +107,13 @@ def test_two_processes_sum_their_corrections(ctx, tmp_path):
     assert np.array_equal(x0, xe)
     xs = spla.spsolve(A.tocsc(), b)
     assert np.linalg.norm(x0 - xs) <= 1e-6 * np.linalg.norm(xs)
+    # Anderson-accelerated sets (mclsgpu_anderson_solve_sets)
+    assert r0["aa_converged"] and r1["aa_converged"] and r0["aa_iters"] == r1["aa_iters"]
+    a0, a1 = np.array(r0["aa_x"]), np.array(r1["aa_x"])
+    assert np.array_equal(a0, a1)
+    xa, steps = _emulated_two_anderson_sets(ctx, A, b)
+    assert steps == r0["aa_iters"] and np.array_equal(a0, xa)
+    assert np.linalg.norm(a0 - xs) <= 1e-5 * np.linalg.norm(xs)
 
 
 def test_nccl_one_rank_runs_on_the_device(ctx):
