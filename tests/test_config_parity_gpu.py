@@ -113,8 +113,8 @@ def _threshold_cases():
     # reference's) is the largest positive off-diagonal entry, not the
     # largest magnitude.
     neg = sp.diags(-1.0 / Aa.diagonal(), format="csr")
-    return [("varcoef_jacobi", A3, "jacobi", 0.2), ("aniso_jacobi", Aa, "jacobi", 0.1),
-            ("aniso_negated_jacobi", Aa, neg, 0.3)]
+    return [("varcoef_jacobi", A3, "jacobi", 0.02), ("aniso_jacobi", Aa, "jacobi", 0.15),
+            ("aniso_negated_jacobi", Aa, neg, 0.5)]
 
 
 @pytest.mark.parametrize("case", range(3))
@@ -138,5 +138,25 @@ def test_composite_threshold_domain_matches_oracle(ctx, case, direction):
     for key in ("rowptr", "col", "h", "cdf", "weights"):
         assert np.array_equal(g[key], o[key]), (name, key)
     dom.close()
+    pc.close()
+    op.close()
+
+
+@pytest.mark.parametrize("direction", [0, 1])
+def test_composite_threshold_that_empties_rows_is_reported(ctx, direction):
+    # Filtering away every off-diagonal entry of a row leaves H's row empty
+    # (H = I - M with M's row reduced to its unit diagonal): the reference
+    # trips MCLS_CHECK(num_entries > 0), the oracle refuses the domain and
+    # the device build reports MCLSGPU_ERR_DEGENERATE.
+    A, _ = P.diffusion3d_varcoef(6, seed=4)
+    Ao = O.Csr.from_scipy(A)
+    with pytest.raises(RuntimeError):
+        O.MC(Ao, PL=O.point_jacobi(Ao), direction=direction, composite_threshold=0.2)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    with pytest.raises(capi.MclsError) as e:
+        capi.Domain(ctx, op, pc, precision=capi.FP64, direction=direction,
+                    composite_threshold=0.2)
+    assert e.value.code == capi.ERR_DEGENERATE
     pc.close()
     op.close()

@@ -345,7 +345,7 @@ def test_mcsa_weight_cutoff_reference_stream_matches_oracle(ctx, direction):
     # iterates (the residual rounds differently, as in the fixed-length test).
     A = P.poisson2d(10)
     b = np.ones(A.shape[0])
-    kw = dict(history_length=40, weight_cutoff=1e-4, sample_ratio=1.0)
+    kw = dict(history_length=20, weight_cutoff=1e-3, sample_ratio=4.0)
     dom, op, pc = _gpu_domain(ctx, A, "jacobi", precision=capi.FP64,
                               rng_mode=capi.RNG_REFERENCE, seed=77, direction=direction, **kw)
     x, st = dom.mcsa_solve(b, tolerance=1e-8, max_iters=400)
