@@ -552,6 +552,12 @@ int64_t orc_mc_solve(orc_mc* mc, const double* rhs, double* x, int internal,
     std::vector<int64_t> starts;
     std::vector<double> w0;
     int64_t nh_total = 0;
+    // Forward histories on the counter stream are independent and walked by
+    // threads over ranges of start states (below).
+    const bool threaded = p.direction == 1 && rng.mode == 1 && !trace_states && !final_weight &&
+                          !events && !start_state && g_threads > 1;
+    const bool fwd_lazy = threaded;
+    int fwd_per = 1;
     if (p.direction == 0) {
         // UniformAdjointSource (src/MCLS_UniformAdjointSource_impl.hpp:58-263)
         int nh_requested = int(double(n) * (p.sample_ratio > 0.0 ? p.sample_ratio : 1.0));
@@ -602,13 +608,16 @@ int64_t orc_mc_solve(orc_mc* mc, const double* rhs, double* x, int internal,
     } else {
         // UniformForwardSource (src/MCLS_UniformForwardSource_impl.hpp:60-148):
         // ceil(Sample Ratio) histories per state in state order, weight 1.
-        int per = p.sample_ratio > 0.0 ? int(std::ceil(p.sample_ratio)) : 1;
-        for (int64_t i = 0; i < n; ++i)
-            for (int c = 0; c < per; ++c) {
-                starts.push_back(i);
-                w0.push_back(1.0);
-            }
-        nh_total = int64_t(starts.size());
+        // (History e starts at state e / per; the threaded walk below uses
+        // that directly instead of the lists.)
+        fwd_per = p.sample_ratio > 0.0 ? int(std::ceil(p.sample_ratio)) : 1;
+        if (!fwd_lazy)
+            for (int64_t i = 0; i < n; ++i)
+                for (int c = 0; c < fwd_per; ++c) {
+                    starts.push_back(i);
+                    w0.push_back(1.0);
+                }
+        nh_total = int64_t(n) * fwd_per;
     }
 
     // Expected-value estimator helper for the forward walk: (H b)_s per row.
@@ -627,21 +636,20 @@ int64_t orc_mc_solve(orc_mc* mc, const double* rhs, double* x, int internal,
     if (p.direction == 1) { fsum.assign(n, 0.0); fcount.assign(n, 0.0); }
 
     // DomainTransporter::transport (src/MCLS_DomainTransporter_impl.hpp:70-119)
-    const int64_t nh = int64_t(starts.size());
-    const bool threaded = p.direction == 1 && rng.mode == 1 && !trace_states && !final_weight &&
-                          !events && !start_state && g_threads > 1;
+    const int64_t nh = fwd_lazy ? nh_total : int64_t(starts.size());
     if (threaded) {
         // Forward histories on the counter stream are independent: threads
         // take contiguous ranges of start states (all histories of a state in
         // one thread, in emission order), so every sum is the one-thread sum.
-        const int per = int(nh / (n > 0 ? n : 1));
+        const int per = fwd_per;
         std::atomic<int64_t> total{0};
         parallel_ranges(n, [&](int64_t lo, int64_t hi) {
             int64_t st = 0;
             for (int64_t e = lo * per; e < hi * per; ++e) {
-                int64_t state = starts[e];
-                double w = w0[e];
-                const double wabs0 = std::abs(w0[e]);
+                const int64_t s0 = e / per;
+                int64_t state = s0;
+                double w = 1.0;
+                const double wabs0 = 1.0;
                 uint64_t cs = counter_state(rng.seed, rng.epoch, 2, uint64_t(e));
                 int steps = 0;
                 double htally = 0.0;
@@ -660,8 +668,8 @@ int64_t orc_mc_solve(orc_mc* mc, const double* rhs, double* x, int internal,
                         break;
                 }
                 st += steps;
-                fsum[starts[e]] += htally;
-                fcount[starts[e]] += 1.0;
+                fsum[s0] += htally;
+                fcount[s0] += 1.0;
             }
             total += st;
         });
