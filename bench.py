@@ -509,7 +509,8 @@ def run_batched(args, world, rank, local, pg):
                    "systems": args.batch_systems, "rows": bt.rows, "rhs_width": bt.width,
                    "pairs": pairs, "kinds": {k: kinds.count(k) for k in sorted(set(kinds))},
                    "parallelism": f"replicas x{world}" if world > 1 else "single batch",
-                   "l2": "inputs larger than L2 (no flush)", "tolerance": 1e-8},
+                   "l2": "inputs larger than L2 (no flush)", "tolerance": 1e-8,
+                   "max_iters": args.max_iters},
         "results": {"walk_launch": tuned, "time_to_1e-8_s": dev_ms_max / args.steps / 1e3,
                     "iterations": s0["iterations"], "pairs_converged": int((it >= 0).sum()),
                     "max_rel_residual": float(rr.max()), "walk_steps_per_s": steps_per_s,
