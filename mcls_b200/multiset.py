@@ -15,6 +15,8 @@ all-reduce of the correction and one of the residual norm per iteration.
 """
 from __future__ import annotations
 
+import os
+
 from . import capi
 
 
@@ -141,23 +143,55 @@ class _DeviceArray:
                                          "data": (ptr, False), "version": 2}
 
 
+def _cudart():
+    """The CUDA runtime the process has loaded (torch's), for the host-copy
+    reducer's stream synchronisation and copies."""
+    import ctypes
+    import glob
+
+    import torch  # noqa: F401  (loads its CUDA runtime)
+
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            return ctypes.CDLL(name)
+        except OSError:
+            pass
+    for path in glob.glob(os.path.join(os.path.dirname(torch.__file__), "..", "nvidia",
+                                       "cuda_runtime", "lib", "libcudart.so*")):
+        return ctypes.CDLL(path)
+    raise OSError("CUDA runtime not found")
+
+
 def torch_set_params(pg, num_sets: int, device: str, host_copy: bool):
     """Set params for mclsgpu_mcsa_solve_sets whose reducer is a
-    torch.distributed all-reduce (sum) of the set's correction, issued on the
-    library's stream: over NCCL on the device vector, or with host_copy over
-    a CPU backend (gloo) on a host copy.  The loop then runs from the host;
+    torch.distributed all-reduce (sum) of the set's correction: with
+    host_copy over a CPU backend (gloo) on a host copy (the library's stream
+    synchronised, the vector copied out and back), otherwise over NCCL on the
+    device vector on the library's stream.  The loop then runs from the host;
     the library's own NCCL communicator (capi.Comm) runs it on the device."""
+    import ctypes
+
+    import numpy as np
     import torch
 
+    rt = _cudart() if host_copy else None
+
     def reduce(ptr, n, stream):
+        if host_copy:
+            h = np.empty(n, np.float64)
+            nbytes = ctypes.c_size_t(8 * n)
+            if rt.cudaStreamSynchronize(ctypes.c_void_p(stream)) != 0:
+                raise RuntimeError("cudaStreamSynchronize")
+            if rt.cudaMemcpy(ctypes.c_void_p(h.ctypes.data), ctypes.c_void_p(ptr), nbytes, 2):
+                raise RuntimeError("cudaMemcpy D2H")
+            t = torch.from_numpy(h)
+            pg.all_reduce(t)
+            if rt.cudaMemcpy(ctypes.c_void_p(ptr), ctypes.c_void_p(h.ctypes.data), nbytes, 1):
+                raise RuntimeError("cudaMemcpy H2D")
+            return
         t = torch.as_tensor(_DeviceArray(ptr, n), device=device)
         ext = torch.cuda.ExternalStream(stream, device=device)
         with torch.cuda.stream(ext):
-            if host_copy:
-                h = t.cpu()
-                pg.all_reduce(h)
-                t.copy_(h)
-            else:
-                pg.all_reduce(t)
+            pg.all_reduce(t)
 
     return capi.set_params(num_sets, reduce, capturable=False)

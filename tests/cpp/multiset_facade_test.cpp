@@ -121,7 +121,7 @@ int main() {
             auto pl = Teuchos::parameterList();
             pl->set<double>("Convergence Tolerance", 1e-8);
             pl->set<int>("Maximum Iterations", 2000);
-            pl->set<double>("Sample Ratio", 1.0);
+            pl->set<double>("Sample Ratio", 4.0);
             pl->set<int>("Number of Sets", 2);
             pl->set<double>("Random Seed", 1000.0 + 17.0 * set);
             MCLS::MCSASolverManager<Vec, Mat> sm(ms, pl);
@@ -190,7 +190,7 @@ int main() {
                 auto pl = Teuchos::parameterList();
                 pl->set<double>("Convergence Tolerance", 1e-8);
                 pl->set<int>("Maximum Iterations", 2000);
-                pl->set<double>("Sample Ratio", 1.0);
+                pl->set<double>("Sample Ratio", 4.0);
                 pl->set<int>("Number of Sets", 2);
                 pl->set<double>("Random Seed", 5000.0 + 31.0 * set);
                 pl->sublist("Anderson Parameters").set<int>("Storage Depth", 3);

@@ -19,7 +19,8 @@ def main(out):
     import torch
 
     world, rank, _, pg = dist.init("gloo", timeout_s=120)
-    A, b = P.diffusion3d_varcoef(10, seed=3)
+    A = P.poisson2d(20)
+    b = np.linspace(0.1, 1.0, A.shape[0])
     ctx = capi.Context(0)
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)

@@ -57,7 +57,7 @@ def _emulated_two_sets(ctx, A, b):
     return engines[0].finish()[0].cpu().numpy(), it
 
 
-def _emulated_two_anderson_sets(ctx, A, b):
+def _emulated_two_anderson_sets(ctx, A, b):  # noqa: D103
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
     engines = [multiset.DeviceEngine(_domain(ctx, op, pc, capi.rank_seed(17, r)), A.shape[0])
@@ -74,7 +74,8 @@ def _emulated_two_anderson_sets(ctx, A, b):
 
 
 def test_two_processes_sum_their_corrections(ctx, tmp_path):
-    A, b = P.diffusion3d_varcoef(10, seed=3)
+    A = P.poisson2d(20)
+    b = np.linspace(0.1, 1.0, A.shape[0])
     port = _free_port()
     procs, outs = [], []
     for r in range(2):
@@ -116,19 +117,47 @@ def test_two_processes_sum_their_corrections(ctx, tmp_path):
     assert np.linalg.norm(a0 - xs) <= 1e-5 * np.linalg.norm(xs)
 
 
+def _one_set_steps(ctx, op, pc, A, b, seed):
+    eng = multiset.DeviceEngine(_domain(ctx, op, pc, seed), A.shape[0])
+    x, it, conv, rel, st = multiset.solve(eng, b, np.zeros_like(b), tolerance=1e-8,
+                                          max_iters=5000)
+    return x.cpu().numpy(), it
+
+
+def test_one_set_with_an_identity_reducer_is_the_step_wise_loop(ctx):
+    # One set whose reducer leaves the correction as it is: the one-call
+    # multi-set loop takes the step-wise loop's steps bit for bit.
+    A = P.poisson2d(20)
+    b = np.linspace(0.1, 1.0, A.shape[0])
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    calls = []
+    sets = capi.set_params(1, lambda ptr, n, stream: calls.append(n))
+    x, st, on_device = _domain(ctx, op, pc, 41).mcsa_solve_sets(sets, b, tolerance=1e-8,
+                                                                max_iters=5000)
+    assert not on_device and st["converged"] == 1
+    assert len(calls) == st["iterations"] and calls[0] == A.shape[0]
+    xs, its = _one_set_steps(ctx, op, pc, A, b, 41)
+    assert its == st["iterations"]
+    assert np.array_equal(x, xs)
+
+
 def test_nccl_one_rank_runs_on_the_device(ctx):
-    A, b = P.diffusion3d_varcoef(10, seed=5)
+    A = P.poisson2d(20)
+    b = np.linspace(0.1, 1.0, A.shape[0])
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
     comm = capi.Comm(ctx, 1, 0, capi.Comm.unique_id())
     sets = comm.set_params()
     assert sets.num_sets == 1 and sets.capturable == 1
+    x_host, st_host, on_dev2 = _domain(ctx, op, pc, 41).mcsa_solve_sets(
+        sets, b, tolerance=1e-8, max_iters=5000, host_loop=1)
+    assert not on_dev2 and st_host["converged"] == 1
     x_dev, st_dev, on_device = _domain(ctx, op, pc, 41).mcsa_solve_sets(
         sets, b, tolerance=1e-8, max_iters=5000)
     assert on_device and st_dev["converged"] == 1
-    x_host, st_host, on_dev2 = _domain(ctx, op, pc, 41).mcsa_solve_sets(
-        sets, b, tolerance=1e-8, max_iters=5000, host_loop=1)
-    assert not on_dev2
     assert st_dev["iterations"] == st_host["iterations"]
     assert np.array_equal(x_dev, x_host)
+    xs, its = _one_set_steps(ctx, op, pc, A, b, 41)
+    assert its == st_dev["iterations"] and np.array_equal(x_dev, xs)
     comm.close()
