@@ -320,6 +320,10 @@ typedef struct {
     int32_t max_row_entries;
     int32_t stencil_offsets;  /* distinct column offsets (stencil records) */
     int32_t operator_dia;     /* operator stored by diagonal offsets */
+    int32_t histories_per_lane;  /* FP32 walk launch shape */
+    int32_t block_size;
+    int32_t record_cache_l1;  /* record loads allocated in L1 */
+    int32_t reserved0;
 } mclsgpu_domain_info;
 int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info);
 
@@ -329,8 +333,12 @@ int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info);
  * threads per block (128 or 256).  No counterpart in the reference. */
 int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane,
                               int block_size);
+/* Record loads of the FP32 walk allocated in L1 (1) or bypassing it (0, the
+ * default).  No counterpart in the reference. */
+int mclsgpu_domain_set_record_cache(mclsgpu_domain* dom, int allocate_l1);
 /* Autotuner: times every launch shape on `reps` Monte Carlo solves of the
- * device vector rhs_dev (n entries), keeps the fastest walk and reports it.
+ * device vector rhs_dev (n entries), with the record loads bypassing and
+ * allocated in L1, keeps the fastest walk and reports it.
  * The random stream position is restored afterwards.  No counterpart in the
  * reference. */
 int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps,

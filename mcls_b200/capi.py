@@ -137,6 +137,10 @@ class DomainInfo(C.Structure):
         ("max_row_entries", C.c_int32),
         ("stencil_offsets", C.c_int32),
         ("operator_dia", C.c_int32),
+        ("histories_per_lane", C.c_int32),
+        ("block_size", C.c_int32),
+        ("record_cache_l1", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
 
 
@@ -198,7 +202,7 @@ EXPORTS = [
     "mclsgpu_domain_walk_agreement", "mclsgpu_mcsa_solve_sets", "mclsgpu_mcsa_solve_sets_dev",
     "mclsgpu_comm_unique_id", "mclsgpu_comm_create", "mclsgpu_comm_destroy",
     "mclsgpu_comm_set_params", "mclsgpu_domain_convergence_criteria",
-    "mclsgpu_anderson_solve_sets",
+    "mclsgpu_anderson_solve_sets", "mclsgpu_domain_set_record_cache",
 ]
 
 _LIB = None
@@ -263,6 +267,7 @@ def load(path: str = LIB_PATH):
                                                       C.POINTER(Criteria)]
     L.mclsgpu_domain_query.argtypes = [P, C.POINTER(DomainInfo)]
     L.mclsgpu_domain_set_launch.argtypes = [P, C.c_int, C.c_int]
+    L.mclsgpu_domain_set_record_cache.argtypes = [P, C.c_int]
     L.mclsgpu_domain_autotune.argtypes = [P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                           C.POINTER(d)]
     L.mclsgpu_rank_seed.argtypes = [C.c_uint64, C.c_int]
@@ -589,7 +594,12 @@ class Domain:
         self.ctx.check(self.ctx.L.mclsgpu_domain_autotune(self.h, C.c_void_p(rhs_dev_ptr), reps,
                                                           C.byref(hpl), C.byref(blk),
                                                           C.byref(ms)))
-        return {"histories_per_lane": hpl.value, "block_size": blk.value, "walk_ms": ms.value}
+        return {"histories_per_lane": hpl.value, "block_size": blk.value, "walk_ms": ms.value,
+                "record_cache_l1": self.info()["record_cache_l1"]}
+
+    def set_record_cache(self, allocate_l1: bool):
+        """FP32 walk record loads allocated in L1 or bypassing it."""
+        self.ctx.check(self.ctx.L.mclsgpu_domain_set_record_cache(self.h, int(bool(allocate_l1))))
 
     def mcsa_solve_sets_dev(self, sets: "SetParams", b_ptr, x_ptr,
                             params: McsaParams | None = None, **kw):

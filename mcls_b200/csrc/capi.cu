@@ -619,6 +619,10 @@ int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info) {
     info->max_row_entries = dom->max_row;
     info->stencil_offsets = dom->stencil_k;
     info->operator_dia = dom->op->dia_k;
+    info->histories_per_lane = dom->walk_ilp;
+    info->block_size = dom->walk_block;
+    info->record_cache_l1 = dom->walk_l1;
+    info->reserved0 = 0;
     return MCLSGPU_OK;
 }
 

@@ -138,6 +138,7 @@ struct mclsgpu_domain {
     // FP32 walk launch shape (autotuned): histories per lane and block size.
     int walk_ilp = 1;
     int walk_block = 256;
+    int walk_l1 = 0;               // record loads allocated in L1
     // Stencil records (stencil_k > 0): row r's slot j is column r + stencil_off[j].
     int stencil_k = 0;
     int rec_q16 = 0;               // stencil records with 16-bit CDF thresholds

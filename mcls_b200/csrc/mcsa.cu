@@ -1275,6 +1275,17 @@ int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane, int b
     return MCLSGPU_OK;
 }
 
+int mclsgpu_domain_set_record_cache(mclsgpu_domain* dom, int allocate_l1) {
+    if (!dom || (allocate_l1 != 0 && allocate_l1 != 1)) return MCLSGPU_ERR_INVALID_ARG;
+    dom->walk_l1 = allocate_l1;
+    dom->graph_key = -1;  // baked into the captured loop
+    if (dom->set_graph) {
+        cudaGraphExecDestroy(dom->set_graph);
+        dom->set_graph = nullptr;
+    }
+    return MCLSGPU_OK;
+}
+
 int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps,
                             int* histories_per_lane, int* block_size, double* walk_ms) {
     if (!dom || !rhs_dev || reps < 1) return MCLSGPU_ERR_INVALID_ARG;
@@ -1289,12 +1300,16 @@ int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps
     // Four histories per lane apply to fixed-length histories on 32-byte
     // records only.
     const bool four = dom->slots == 4 && !(dom->p.weight_cutoff > 0.0);
-    const int shapes[6][2] = {{1, 256}, {2, 256}, {1, 128}, {2, 128}, {4, 256}, {4, 128}};
+    // Each shape with the record loads bypassing L1 and allocated in it.
+    const int shapes[12][3] = {{1, 256, 0}, {2, 256, 0}, {1, 128, 0}, {2, 128, 0},
+                               {4, 256, 0}, {4, 128, 0}, {1, 256, 1}, {2, 256, 1},
+                               {1, 128, 1}, {2, 128, 1}, {4, 256, 1}, {4, 128, 1}};
     double best = 1e300;
-    int bh = 1, bb = 256;
+    int bh = 1, bb = 256, bl = 0;
     for (const auto& sh : shapes) {
         if (sh[0] == 4 && !four) continue;
         int rc = mclsgpu_domain_set_launch(dom, sh[0], sh[1]);
+        if (!rc) rc = mclsgpu_domain_set_record_cache(dom, sh[2]);
         if (rc) return rc;
         mclsgpu_stats st{};
         st.size = sizeof(st);
@@ -1311,9 +1326,11 @@ int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps
             best = tot / reps;
             bh = sh[0];
             bb = sh[1];
+            bl = sh[2];
         }
     }
     int rc = mclsgpu_domain_set_launch(dom, bh, bb);
+    if (!rc) rc = mclsgpu_domain_set_record_cache(dom, bl);
     cudaMemcpyAsync(dom->d_epoch, &saved[0], sizeof(saved[0]), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dom->d_pos, &saved[1], sizeof(saved[1]), cudaMemcpyHostToDevice, s);
     e = cudaStreamSynchronize(s);

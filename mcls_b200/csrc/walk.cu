@@ -61,6 +61,7 @@ struct WalkArgs {
     unsigned long long* d_tim;  // [0] first warp start, [1] last warp end (ns)
     int* status;
     int row0;                   // global index of the first record / tally row
+    int l1;                     // record loads allocate in L1
     int stoff[32];              // stencil records: column offset of each slot
     // variable-length histories on the reference stream (FP64 only): history
     // e's first draw is *d_pos + hoff[e]; hlen[e] receives its length
@@ -83,6 +84,16 @@ constexpr unsigned kFull = 0xffffffffu;
 __device__ __forceinline__ void ld_record256(const void* p, uint32_t* r) {
     asm volatile(
         "ld.global.nc.L1::no_allocate.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7])
+        : "l"(p));
+}
+// The same load allocated in L1: histories of one block start at neighbouring
+// states and step to neighbours, so their records are often fetched again by
+// the block's other warps.
+__device__ __forceinline__ void ld_record256_l1(const void* p, uint32_t* r) {
+    asm volatile(
+        "ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7])
         : "l"(p));
@@ -196,12 +207,18 @@ __device__ __forceinline__ int select64(const WalkArgs& a, int s, double u, int&
 template <int S, int DIR, int ST>
 __device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, int& s, float& w,
                                           uint64_t& x, float& acc, float& comp, int k) {
-    // One record: S/4 256-bit loads that bypass L1 (each step touches exactly
-    // the record's own sectors).
+    // One record: S/4 256-bit loads, bypassing L1 (each step touches exactly
+    // the record's own sectors) or allocated in it (the launch shape says).
     const char* r = rec + size_t(s - a.row0) * (S * 8);
     uint32_t q[2 * S];
 #pragma unroll
-    for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
+    if (a.l1) {
+#pragma unroll
+        for (int t = 0; t < S / 4; ++t) ld_record256_l1(r + 32 * t, q + 8 * t);
+    } else {
+#pragma unroll
+        for (int t = 0; t < S / 4; ++t) ld_record256(r + 32 * t, q + 8 * t);
+    }
     if (DIR == MCLSGPU_ADJOINT) {
         // FP32 weight, FP64 reduction (fire-and-forget RED.ADD.F64).
         if (k > 0) atomicAdd(&a.y64[s - a.row0], double(w));
@@ -657,6 +674,7 @@ static void fill_walk_args(mclsgpu_domain* dom, WalkArgs& a) {
     a.d_steps = dom->d_steps;
     a.d_tim = dom->d_tim;
     a.status = ctx->d_status;
+    a.l1 = dom->walk_l1;
     for (int j = 0; j < 32; ++j) a.stoff[j] = dom->stencil_off[j];
 }
 

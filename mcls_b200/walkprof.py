@@ -27,6 +27,7 @@ def main(argv=None):
     ap.add_argument("--format", choices=["auto", "stencil16"], default="auto")
     ap.add_argument("--histories-per-lane", type=int, default=0,
                     help="0: autotune the launch shape")
+    ap.add_argument("--l1", type=int, default=0, help="record loads allocated in L1 (fixed shape)")
     args = ap.parse_args(argv)
     A, b = P.diffusion3d_varcoef(args.n, seed=1)
     ctx = capi.Context(0)
@@ -41,7 +42,9 @@ def main(argv=None):
     torch.cuda.synchronize()
     if args.histories_per_lane:
         dom.set_launch(args.histories_per_lane, 256)
-        shape = {"histories_per_lane": args.histories_per_lane, "block_size": 256}
+        dom.set_record_cache(args.l1)
+        shape = {"histories_per_lane": args.histories_per_lane, "block_size": 256,
+                 "record_cache_l1": args.l1}
     else:
         shape = dom.autotune(rt.data_ptr(), reps=1)
     ms = steps = launches = 0

@@ -15,10 +15,15 @@ def test_launch_shapes_give_identical_forward_solves(ctx):
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
     xs = []
-    for hpl, blk in ((1, 256), (2, 256), (1, 128), (2, 128), (4, 256), (4, 128)):
+    for hpl, blk, l1 in ((1, 256, 0), (2, 256, 0), (1, 128, 0), (2, 128, 0), (4, 256, 0),
+                         (4, 128, 0), (2, 256, 1), (4, 256, 1)):
         dom = capi.Domain(ctx, op, pc, precision=capi.FP32, direction=capi.FORWARD,
                           estimator=capi.EXPECTED_VALUE, sample_ratio=2.0, seed=9)
         dom.set_launch(hpl, blk)
+        dom.set_record_cache(l1)
+        info = dom.info()
+        assert (info["histories_per_lane"], info["block_size"], info["record_cache_l1"]) == \
+            (hpl, blk, l1)
         x, st = dom.mcsa_solve(b, tolerance=0.0, max_iters=15)
         xs.append(x)
     for x in xs[1:]:
