@@ -78,7 +78,12 @@ HBM_WALK_DRAM_BYTES_PER_LAUNCH = None
 # (FP64 forward expected-value walks on the counter stream, the workload's
 # histories per iteration, seed 1234): its iteration count, which the
 # reference arm multiplies by its timed seconds per iteration.
-CPU_FULL_SOLVE = {}
+CPU_FULL_SOLVE = {
+    "diffusion128": {"iterations": 6002,
+                     "note": "run once to the tolerance on the 8-thread build container in "
+                             "2,843 s: |b - A x|/|b| = 3.40e-8, error against the oracle CG "
+                             "3.94e-8"},
+}
 
 
 def step_bytes(cfg, info):
