@@ -71,9 +71,11 @@ CONFIGS = {
 # dram__bytes_read.sum (83.90 MB) + dram__bytes_write.sum (7.82 MB) for the
 # stencil forward expected-value walk32 launch at 128^3.
 WALK_DRAM_BYTES_PER_LAUNCH = {"diffusion128": 91.72e6}
-# The same for one walk32 launch of the 192^3 roofline domain (records
-# exceed L2); None until an ncu capture supplies it.
-HBM_WALK_DRAM_BYTES_PER_LAUNCH = None
+# The same for one walk32 launch of the 192^3 roofline domain (226 MB of
+# records, more than L2): dram__bytes_read.sum (283.14 MB) +
+# dram__bytes_write.sum (47.17 MB) of the 4-histories-per-lane x 256 launch
+# (python -m mcls_b200.walkprof --n 192 --solves 2 --histories-per-lane 4).
+HBM_WALK_DRAM_BYTES_PER_LAUNCH = 330.31e6
 # The oracle port's whole MCSA solve of a workload, run once to the end
 # (FP64 forward expected-value walks on the counter stream, the workload's
 # histories per iteration, seed 1234): its iteration count, which the

@@ -180,14 +180,19 @@ def torch_set_params(pg, num_sets: int, device: str, host_copy: bool):
         if host_copy:
             h = np.empty(n, np.float64)
             nbytes = ctypes.c_size_t(8 * n)
-            if rt.cudaStreamSynchronize(ctypes.c_void_p(stream)) != 0:
-                raise RuntimeError("cudaStreamSynchronize")
-            if rt.cudaMemcpy(ctypes.c_void_p(h.ctypes.data), ctypes.c_void_p(ptr), nbytes, 2):
-                raise RuntimeError("cudaMemcpy D2H")
+            st = ctypes.c_void_p(stream)
+            # Both copies on the library's stream, each completed before the
+            # host goes on (that stream does not synchronise with the legacy
+            # default stream, so a plain cudaMemcpy could still be landing
+            # when the next kernel reads the vector).
+            if (rt.cudaMemcpyAsync(ctypes.c_void_p(h.ctypes.data), ctypes.c_void_p(ptr), nbytes,
+                                   2, st) or rt.cudaStreamSynchronize(st)):
+                raise RuntimeError("cudaMemcpyAsync D2H")
             t = torch.from_numpy(h)
             pg.all_reduce(t)
-            if rt.cudaMemcpy(ctypes.c_void_p(ptr), ctypes.c_void_p(h.ctypes.data), nbytes, 1):
-                raise RuntimeError("cudaMemcpy H2D")
+            if (rt.cudaMemcpyAsync(ctypes.c_void_p(ptr), ctypes.c_void_p(h.ctypes.data), nbytes,
+                                   1, st) or rt.cudaStreamSynchronize(st)):
+                raise RuntimeError("cudaMemcpyAsync H2D")
             return
         t = torch.as_tensor(_DeviceArray(ptr, n), device=device)
         ext = torch.cuda.ExternalStream(stream, device=device)

@@ -31,7 +31,9 @@ static int g_failures = 0;
         }                                                                  \
     } while (0)
 
-// 2D Poisson 5-point on an n x n grid (unit spacing).
+// 2D Poisson 5-point on an m x m grid with its rows scaled to a unit
+// diagonal (1 on the diagonal, -1/4 beside it), so that the iteration matrix
+// I - A of the unpreconditioned problem has spectral radius cos(pi/(m+1)) < 1.
 static Teuchos::RCP<Mat> poisson(int m) {
     auto A = Teuchos::rcp(new Mat);
     A->n = m * m;
@@ -43,11 +45,11 @@ static Teuchos::RCP<Mat> poisson(int m) {
                 A->colind.push_back(c);
                 A->values.push_back(v);
             };
-            if (y > 0) put(i - m, -1.0);
-            if (x > 0) put(i - 1, -1.0);
-            put(i, 4.0);
-            if (x < m - 1) put(i + 1, -1.0);
-            if (y < m - 1) put(i + m, -1.0);
+            if (y > 0) put(i - m, -0.25);
+            if (x > 0) put(i - 1, -0.25);
+            put(i, 1.0);
+            if (x < m - 1) put(i + 1, -0.25);
+            if (y < m - 1) put(i + m, -0.25);
             A->rowptr.push_back(std::int64_t(A->colind.size()));
         }
     return A;
@@ -84,16 +86,22 @@ static int reduce_two(void* user, double* data, int64_t n, void* stream) {
     SetUser* u = static_cast<SetUser*>(user);
     std::vector<double>& mine = u->sum->slot[u->set];
     mine.resize(size_t(n));
-    if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) return 2;
-    if (cudaMemcpy(mine.data(), data, size_t(n) * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // Both copies on the set's stream, each completed before the host goes on
+    // (the stream does not synchronise with the legacy default stream).
+    if (cudaMemcpyAsync(mine.data(), data, size_t(n) * 8, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
         return 2;
     u->sum->wait_all();
     std::vector<double> total(static_cast<size_t>(n));
     for (int64_t i = 0; i < n; ++i) total[i] = u->sum->slot[0][i] + u->sum->slot[1][i];
     u->sum->wait_all();  // both have read the slots before the next iteration
-    return cudaMemcpy(data, total.data(), size_t(n) * 8, cudaMemcpyHostToDevice) == cudaSuccess
-               ? 0
-               : 2;
+    if (cudaMemcpyAsync(data, total.data(), size_t(n) * 8, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return 2;
+    return 0;
 }
 
 int main() {

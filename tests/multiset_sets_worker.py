@@ -25,15 +25,17 @@ def main(out):
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
     seed = capi.rank_seed(99, rank)
+    # Forward expected-value walks, one history per row (bit-reproducible
+    # corrections; the test compares with an emulation in one process).
     dom = capi.Domain(ctx, op, pc, precision=capi.FP64, rng_mode=capi.RNG_COUNTER, seed=seed,
-                      estimator=capi.COLLISION, direction=capi.ADJOINT, sample_ratio=1.0,
+                      estimator=capi.EXPECTED_VALUE, direction=capi.FORWARD, sample_ratio=1.0,
                       history_length=10)
     sets = multiset.torch_set_params(pg, world, "cuda:0", host_copy=True)
     x, st, on_device = dom.mcsa_solve_sets(sets, b, tolerance=1e-8, max_iters=5000)
     # Anderson-accelerated sets on their own domain and streams.
     da = capi.Domain(ctx, op, pc, precision=capi.FP64, rng_mode=capi.RNG_COUNTER,
-                     seed=capi.rank_seed(17, rank), estimator=capi.COLLISION,
-                     direction=capi.ADJOINT, sample_ratio=1.0, history_length=10)
+                     seed=capi.rank_seed(17, rank), estimator=capi.EXPECTED_VALUE,
+                     direction=capi.FORWARD, sample_ratio=1.0, history_length=10)
     xa, sa = da.anderson_solve_sets(sets, b, tolerance=1e-10, max_iters=2000, storage_depth=3)
     da.close()
     pg.barrier()

@@ -34,8 +34,12 @@ def _free_port():
 
 
 def _domain(ctx, op, pc, seed):
+    # Forward expected-value walks, one history per row: each row's tally is
+    # one addition onto zero, so a set's correction is the same bits on every
+    # run (adjoint tallies of several histories into one row are FP64 atomic
+    # sums whose order, and last bits, vary from run to run).
     return capi.Domain(ctx, op, pc, precision=capi.FP64, rng_mode=capi.RNG_COUNTER, seed=seed,
-                       estimator=capi.COLLISION, direction=capi.ADJOINT, sample_ratio=1.0,
+                       estimator=capi.EXPECTED_VALUE, direction=capi.FORWARD, sample_ratio=1.0,
                        history_length=10)
 
 
