@@ -47,7 +47,8 @@ CONFIGS = {
                                "[0.5,5] and sigma_a in [0.001,0.1] on 8^3 random blocks, Jacobi "
                                "MCSA, forward expected-value estimator, FP32 walks / FP64 "
                                "tallies, residual and update, 2^24 histories per iteration",
-                      n=256, sample_ratio=1.0, estimator=1, history_length=10, direction=1),
+                      n=256, sample_ratio=1.0, estimator=1, history_length=10, direction=1,
+                      max_iters=60000),
     "batched": dict(workload="batched: 1024 systems (2D/3D Poisson and var-coef diffusion, N "
                              "log-uniform in [1e3, nmax] on square/cube grids), 1-16 right-hand "
                              "sides uniform(0,1) each, point-Jacobi forward expected-value MCSA, "
@@ -504,7 +505,10 @@ def run_batched(args, world, rank, local, pg):
     walk_ms = sum(s["walk_ms"] for s in stats)
     launches = sum(s["walk_launches"] for s in stats)
     per_launch = walk_ms / max(launches, 1)
-    bstep = info["record_bytes"] + 4 * bt.width  # record + one FP32 tally-source row
+    # A step reads the record and its state's FP32 tally-source row (the
+    # history's width class): the mean over histories of the row widths.
+    mean_w = float((bt.n * bt.widths).sum()) / bt.rows
+    bstep = info["record_bytes"] + 4 * mean_w
     walk_steps = sum(s["walk_steps"] for s in stats)
     achieved = (bstep * walk_steps / max(launches, 1)) / (per_launch * 1e-3) / 1e9
     line = {
@@ -513,7 +517,8 @@ def run_batched(args, world, rank, local, pg):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": cfgd["workload"].replace("nmax", f"{args.batch_nmax:g}"),
-                   "systems": args.batch_systems, "rows": bt.rows, "rhs_width": bt.width,
+                   "systems": args.batch_systems, "rows": bt.rows, "elements": bt.elements,
+                   "max_rhs_width": bt.width, "mean_row_width": mean_w,
                    "pairs": pairs, "kinds": {k: kinds.count(k) for k in sorted(set(kinds))},
                    "parallelism": f"replicas x{world}" if world > 1 else "single batch",
                    "l2": "inputs larger than L2 (no flush)", "tolerance": 1e-8,
@@ -535,6 +540,8 @@ def run_batched(args, world, rank, local, pg):
                      "walk_share_of_solve": walk_ms / dev_ms if dev_ms else None},
         "wall_s": wall,
     }
+    if rank == 0 and world == 1:
+        line["results"]["err_vs_oracle"] = batch_oracle_error(bt, systems, rhs, X.cpu().numpy())
     if rank == 0:
         print(json.dumps(line))
     bt.close()
@@ -558,6 +565,34 @@ def oracle_error(A, b, x):
                       "|b - A x_o|_2 <= 1e-12 |b|_2",
             "oracle_rel_residual": r["rel_residual"], "oracle_iterations": r["iters"],
             "oracle_s": secs}
+
+
+def batch_oracle_error(bt, systems, rhs, X, sample_systems=8, sample_rhs=4):
+    """Relative errors of the batch's solutions against the oracle's FP64
+    solves of a sample of its pairs: `sample_systems` systems spaced evenly
+    through the batch, their first `sample_rhs` right-hand sides each
+    (diagonal-preconditioned conjugate gradients to 1e-12, all host threads;
+    every system of the batch is symmetric positive definite)."""
+    from oracle import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    blocks = bt.unpack(X)
+    pick = sorted(set(np.linspace(0, len(systems) - 1, sample_systems).round().astype(int)))
+    errs, rows = [], 0
+    t0 = time.perf_counter()
+    for s in pick:
+        A = O.Csr.from_scipy(systems[s])
+        rs = np.asarray(rhs[s]).reshape(systems[s].shape[0], -1)
+        for r in range(min(sample_rhs, rs.shape[1])):
+            xo = O.pcg(A, rs[:, r], tolerance=1e-12)["x"]
+            errs.append(float(np.linalg.norm(blocks[s][:, r] - xo) / np.linalg.norm(xo)))
+        rows += systems[s].shape[0]
+    return {"max_rel_error": max(errs), "median_rel_error": float(np.median(errs)),
+            "pairs_checked": len(errs), "systems_checked": len(pick), "rows_checked": rows,
+            "sample": f"{len(pick)} systems spaced evenly through the batch, their first "
+                      f"{sample_rhs} right-hand sides",
+            "oracle": "FP64 diagonal-preconditioned conjugate gradients (oracle/), "
+                      "|b - A x_o|_2 <= 1e-12 |b|_2", "oracle_s": time.perf_counter() - t0}
 
 
 def walk_agreement(dom, histories, seed):
@@ -628,14 +663,26 @@ def _aniso_solve(args, ctx, op, A, b, kind, cfgd, net=None, block=4, rho_fallbac
     from mcls_b200 import capi
 
     pc = capi.Precond(ctx, op, kind, block_size=block, net=net, rho_fallback=rho_fallback)
-    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=args.seed,
-                      estimator=cfgd["estimator"], sample_ratio=cfgd["sample_ratio"],
-                      direction=cfgd["direction"], history_length=cfgd["history_length"],
-                      record_format=record_format)
+
+    def domain(fmt):
+        return capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER,
+                           seed=args.seed, estimator=cfgd["estimator"],
+                           sample_ratio=cfgd["sample_ratio"], direction=cfgd["direction"],
+                           history_length=cfgd["history_length"], record_format=fmt)
+
+    try:
+        dom = domain(record_format)
+    except capi.MclsError as e:
+        # More column offsets than 16-bit stencil records hold: the library's
+        # own choice (FP32 stencil or packed records).
+        if e.code != capi.ERR_UNSUPPORTED or record_format == capi.RECORD_AUTO:
+            raise
+        dom = domain(capi.RECORD_AUTO)
     mp = capi.mcsa_params(tolerance=1e-8, max_iters=args.max_iters)
     bt = torch.tensor(b, device=ctx_device(), dtype=torch.float64)
     xt = torch.zeros_like(bt)
-    out = {"record_bytes": dom.info()["record_bytes"]}
+    info = dom.info()
+    out = {"record_bytes": info["record_bytes"], "record_format": info["record_format"]}
     try:
         for _ in range(2):
             dom.reseed(args.seed)
@@ -892,7 +939,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-hbm-roofline", action="store_true",
                     help="skip the walk roofline on the 192^3 domain whose records exceed L2")
-    ap.add_argument("--max-iters", type=int, default=20000)
+    ap.add_argument("--max-iters", type=int, default=None,
+                    help="iteration limit (default: the workload's own, else 20000)")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-SPAI arm (training + learned MCSA solves)")
@@ -928,6 +976,8 @@ def main():
     ap.add_argument("--batch-nmax", type=float, default=1e4,
                     help="largest system of the batched workload (5e5 for the full size)")
     args = ap.parse_args()
+    if args.max_iters is None:
+        args.max_iters = CONFIGS.get(args.config, {}).get("max_iters", 20000)
     world, rank, local, pg = dist_init(args)
     if args.impl == "mcls_b200" and args.config == "aniso512":
         run_aniso(args, world, rank, local, pg)

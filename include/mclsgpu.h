@@ -577,31 +577,38 @@ int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev);
  * 278-432).  m square systems (host int64 CSR each) with 1..16 right-hand
  * sides each are solved in one MCSA loop: one block-diagonal point-Jacobi
  * domain, one shared set of forward FP32 walks per iteration whose histories
- * carry a tally per right-hand side, and a separate convergence test
- * |rp|_2 <= tol |D^-1 b|_2 for every (system, right-hand side) pair.  The
- * loop (six kernels per iteration) runs in a captured CUDA graph.  params
- * must ask for forward FP32 walks without a weight cutoff. */
+ * carry a tally per right-hand side of their system, and a separate
+ * convergence test |rp|_2 <= tol |D^-1 b|_2 for every (system, right-hand
+ * side) pair.  The loop (four kernels per iteration) runs in a captured CUDA
+ * graph.  params must ask for forward FP32 walks without a weight cutoff. */
 typedef struct mclsgpu_batch mclsgpu_batch;
 int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
                         const int64_t* const* rowptr, const int64_t* const* colind,
                         const double* const* values, const int32_t* nrhs,
                         const mclsgpu_mc_params* params, mclsgpu_batch** out);
 int mclsgpu_batch_destroy(mclsgpu_batch* b);
-/* Vector layout: [rows][width] row-major FP64; system s owns rows
- * row_offsets[s] .. row_offsets[s+1]-1 and columns 0 .. nrhs[s]-1 (the other
- * columns are ignored).  row_offsets has nsys+1 entries (may be NULL). */
-int mclsgpu_batch_layout(mclsgpu_batch* b, int64_t* row_offsets, int32_t* width);
+/* Vector layout: FP64 arrays of `elements` entries.  System s owns the
+ * row-major [n_s][widths[s]] block starting at elem_offsets[s]; widths[s] is
+ * nrhs[s] rounded up to a power of two, and columns nrhs[s] .. widths[s]-1
+ * are ignored.  Systems are placed grouped by width (not in argument order),
+ * with unused padding elements between the groups.  Per-pair outputs are
+ * [nsys][max_width].  elem_offsets and widths have nsys entries; any output
+ * may be NULL. */
+int mclsgpu_batch_layout(mclsgpu_batch* b, int64_t* elem_offsets, int32_t* widths,
+                         int64_t* elements, int32_t* max_width);
 /* The batch's block-diagonal domain (for mclsgpu_domain_query/reseed). */
 int mclsgpu_batch_domain(mclsgpu_batch* b, mclsgpu_domain** dom);
-/* Walk threads per block (128 or 256); the autotuner times both on `reps`
- * iterations of b_dev (x_dev is overwritten) and keeps the faster. */
-int mclsgpu_batch_set_launch(mclsgpu_batch* b, int block_size);
+/* Walk launch shape: threads per block (128 or 256) and the work-queue grab
+ * (each warp takes 32 * grab histories per grab, 1..8).  The autotuner times
+ * block sizes {256, 128} x grabs {1, 2, 4} on `reps` iterations of b_dev
+ * (x_dev is overwritten) and keeps the fastest walk. */
+int mclsgpu_batch_set_launch(mclsgpu_batch* b, int block_size, int grab);
 int mclsgpu_batch_autotune(mclsgpu_batch* b, const double* b_dev, double* x_dev, int reps,
-                           int* block_size, double* walk_ms);
+                           int* block_size, int* grab, double* walk_ms);
 /* x_dev holds the initial guesses and receives the solutions.  Optional host
- * outputs, [nsys][width]: conv_iters = the iteration at which each pair first
- * met the tolerance (-1: never, or an unused column), rel_resid = the final
- * |rp|_2 / |D^-1 b|_2.  params->smoother_steps must be 1. */
+ * outputs, [nsys][max_width]: conv_iters = the iteration at which each pair
+ * first met the tolerance (-1: never, or an unused column), rel_resid = the
+ * final |rp|_2 / |D^-1 b|_2.  params->smoother_steps must be 1. */
 int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* x_dev,
                                  const mclsgpu_mcsa_params* params, int32_t* conv_iters,
                                  double* rel_resid, mclsgpu_stats* stats);

@@ -318,10 +318,11 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_spai_set_penalty.argtypes = [P, d, d]
     L.mclsgpu_batch_build.argtypes = [P, C.c_int, P, P, P, P, P, C.POINTER(McParams), PP]
     L.mclsgpu_batch_destroy.argtypes = [P]
-    L.mclsgpu_batch_layout.argtypes = [P, P, C.POINTER(C.c_int32)]
+    L.mclsgpu_batch_layout.argtypes = [P, P, P, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
     L.mclsgpu_batch_domain.argtypes = [P, PP]
-    L.mclsgpu_batch_set_launch.argtypes = [P, C.c_int]
-    L.mclsgpu_batch_autotune.argtypes = [P, P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(d)]
+    L.mclsgpu_batch_set_launch.argtypes = [P, C.c_int, C.c_int]
+    L.mclsgpu_batch_autotune.argtypes = [P, P, P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(d)]
     L.mclsgpu_batch_mcsa_solve_dev.argtypes = [P, P, P, C.POINTER(McsaParams), P, P,
                                                C.POINTER(Stats)]
     _LIB = L
@@ -889,7 +890,10 @@ class SpaiNet:
 
 class Batch:
     """Many systems with 1..16 right-hand sides each in one MCSA loop
-    (forward FP32 walks shared by every right-hand side)."""
+    (forward FP32 walks shared by every right-hand side).  Device vectors are
+    flat FP64 arrays of `elements` entries: system s owns the row-major
+    [n_s, widths[s]] block at elem_offsets[s] (widths[s] = its right-hand-side
+    count rounded up to a power of two); pack/unpack convert."""
 
     def __init__(self, ctx: Context, systems, nrhs, params: McParams | None = None, **kw):
         self.ctx = ctx
@@ -906,24 +910,33 @@ class Batch:
                                             _ptr(self.nrhs), C.byref(p), C.byref(h)))
         del mats
         self.h = h
-        off = np.empty(self.nsys + 1, np.int64)
-        w = C.c_int32()
-        ctx.check(ctx.L.mclsgpu_batch_layout(self.h, _ptr(off), C.byref(w)))
-        self.offsets, self.width = off, w.value
-        self.rows = int(off[-1])
+        off = np.empty(self.nsys, np.int64)
+        wid = np.empty(self.nsys, np.int32)
+        ne, w = C.c_int64(), C.c_int32()
+        ctx.check(ctx.L.mclsgpu_batch_layout(self.h, _ptr(off), _ptr(wid), C.byref(ne),
+                                             C.byref(w)))
+        self.elem_offsets, self.widths, self.elements, self.width = off, wid, ne.value, w.value
+        self.n = n
+        self.rows = int(n.sum())
         ctx._adopt(self)
 
+    def block(self, X, s):
+        """System s's [n_s, widths[s]] view of a flat element array."""
+        o = int(self.elem_offsets[s])
+        return X[o:o + int(self.n[s]) * int(self.widths[s])].reshape(int(self.n[s]),
+                                                                      int(self.widths[s]))
+
     def pack(self, vectors):
-        """[rows, width] array from per-system [n_s, nrhs_s] blocks."""
-        out = np.zeros((self.rows, self.width))
+        """Flat element array from per-system [n_s, nrhs_s] blocks."""
+        out = np.zeros(self.elements)
         for s, v in enumerate(vectors):
-            v = np.asarray(v, np.float64).reshape(self.offsets[s + 1] - self.offsets[s], -1)
-            out[self.offsets[s]:self.offsets[s + 1], : v.shape[1]] = v
+            v = np.asarray(v, np.float64).reshape(int(self.n[s]), -1)
+            self.block(out, s)[:, : v.shape[1]] = v
         return out
 
     def unpack(self, X):
-        X = np.asarray(X)
-        return [X[self.offsets[s]:self.offsets[s + 1], : self.nrhs[s]] for s in range(self.nsys)]
+        X = np.asarray(X).reshape(-1)
+        return [self.block(X, s)[:, : self.nrhs[s]] for s in range(self.nsys)]
 
     def domain_info(self):
         hd = C.c_void_p()
@@ -938,21 +951,21 @@ class Batch:
         self.ctx.check(self.ctx.L.mclsgpu_batch_domain(self.h, C.byref(hd)))
         self.ctx.check(self.ctx.L.mclsgpu_domain_reseed(hd, seed))
 
-    def set_launch(self, block_size):
-        self.ctx.check(self.ctx.L.mclsgpu_batch_set_launch(self.h, block_size))
+    def set_launch(self, block_size, grab=1):
+        self.ctx.check(self.ctx.L.mclsgpu_batch_set_launch(self.h, block_size, grab))
 
     def autotune(self, b_ptr, x_ptr, reps=3):
         _torch_ready()
-        blk, ms = C.c_int(), C.c_double()
+        blk, grab, ms = C.c_int(), C.c_int(), C.c_double()
         self.ctx.check(self.ctx.L.mclsgpu_batch_autotune(self.h, C.c_void_p(b_ptr),
                                                          C.c_void_p(x_ptr), reps, C.byref(blk),
-                                                         C.byref(ms)))
-        return {"block_size": blk.value, "walk_ms": ms.value}
+                                                         C.byref(grab), C.byref(ms)))
+        return {"block_size": blk.value, "grab": grab.value, "walk_ms": ms.value}
 
     def mcsa_solve_dev(self, b_ptr, x_ptr, params: McsaParams | None = None, **kw):
-        """Solve in place on device [rows, width] arrays; returns (stats,
-        per-pair convergence iterations [nsys, width], final relative
-        preconditioned residuals [nsys, width])."""
+        """Solve in place on device element arrays; returns (stats, per-pair
+        convergence iterations [nsys, width], final relative preconditioned
+        residuals [nsys, width]), width the widest system's."""
         _torch_ready()
         p = params if params is not None else mcsa_params(**kw)
         st = Stats()

@@ -2,29 +2,31 @@
 //
 // m systems A_s (uneven sizes) with R_s right-hand sides each are solved
 // together: the block-diagonal operator S = diag(A_1..A_m) carries one
-// point-Jacobi domain H = I - D^-1 S (walks never leave a block), and the
-// right-hand sides are the columns of an [rows][R] row-major matrix, R the
-// largest R_s rounded up to a power of two (columns r >= R_s of system s are
-// zero and ignored).  Forward walks do not depend on the source, so one set
-// of histories per iteration serves every right-hand side of every system:
-// each history carries R tallies (walk32_multi).  Every (system, rhs) pair has
-// its own convergence test |rp_{s,r}|_2 <= tol |D^-1 b_{s,r}|_2 (the
+// point-Jacobi domain H = I - D^-1 S (walks never leave a block).  System s
+// gets W_s = R_s rounded up to a power of two columns; the systems are
+// grouped by W_s into five width classes (1, 2, 4, 8, 16 columns), each a
+// contiguous range of rows whose vectors are row-major [rows][W] blocks of
+// the element arrays (BatchClasses), so a system with one right-hand side
+// costs one column, not the widest system's sixteen.  Forward walks do not
+// depend on the source, so one set of histories per iteration serves every
+// right-hand side of every system: each history carries one tally per column
+// of its row's class (walk32_batch).  Every (system, rhs) pair has its own
+// convergence test |rp_{s,r}|_2 <= tol |D^-1 b_{s,r}|_2 (the
 // MCSASolverManager criterion, src/MCLS_MCSASolverManager_impl.hpp:299-318);
-// the loop ends when every pair has met it or at the iteration limit.  One
-// iteration is six kernels (Richardson + residual, tally source, the shared
-// walk, correction, residual + per-pair norms, convergence test) captured in a
-// CUDA graph whose WHILE node the last kernel controls.
+// a system whose pairs have all met it stops (its rows and walks are
+// skipped), and the loop ends when every pair has met it or at the iteration
+// limit.  One iteration is four kernels in a CUDA graph whose WHILE node the
+// last one controls: Richardson step + residual, tally source, the shared
+// walk, and correction + residual + per-pair norms, whose last block to
+// finish runs the convergence test.
 #include <cmath>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
 #include "internal.h"
 
 namespace mclsgpu {
-
-int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y, const int* rsys,
-                      const int* sys_done);
-
 namespace {
 
 struct BatchState {
@@ -46,9 +48,11 @@ inline int grid_for(long long work, int threads = kThreads, int cap = 148 * 8) {
 }
 
 struct BatchArgs {
-    int n;
+    BatchClasses cls;
+    long long ne;        // elements (padding included)
     int nsys;
-    const int* rp;      // S (CSR)
+    int pw;              // per-pair row width: pair (s, r) is s * pw + r
+    const int* rp;       // S (CSR)
     const int* ci;
     const double* v;
     const double* dinv;  // D^-1
@@ -63,13 +67,14 @@ struct BatchArgs {
     double* RP2;
     double* Y;
     float* cR;
-    double* norm2;       // [nsys][R]
+    double* norm2;       // [nsys][pw]
     double* bnorm2;
-    int* conv_iter;      // [nsys][R]
+    int* conv_iter;      // [nsys][pw]
     const int* nrhs;
     int* sys_done;       // per system: every right-hand side converged
     int skip;            // skip the rows of finished systems
     BatchState* st;
+    unsigned* blocks_done;
     double omega;        // Richardson relaxation
     double nomega;       // Neumann relaxation (1 when absent)
     double inv_per;      // 1 / histories per state
@@ -80,51 +85,63 @@ struct BatchArgs {
     int* status;
 };
 
-// All per-row kernels below run one thread per (row, column) element: with
-// the [rows][R] row-major layout a warp then reads whole 8R-byte rows of X,
-// RP and B at every matrix entry, so every load and store is coalesced.
-template <int R>
-__device__ __forceinline__ void elem_rc(long long t, int& i, int& r) {
-    i = int(t / R);
-    r = int(t % R);
+// Element t -> row i, column r and width class c (false for the padding
+// between classes).
+__device__ __forceinline__ bool elem_map(const BatchClasses& k, long long t, int& i, int& r,
+                                         int& c) {
+    c = 0;
+    while (c < 4 && t >= k.cel[c + 1]) ++c;
+    const long long local = t - k.cel[c];
+    const long long row = k.crow[c] + (local >> c);
+    if (row >= k.crow[c + 1]) return false;
+    i = int(row);
+    r = int(local & ((1 << c) - 1));
+    return true;
 }
+
+// The element of row j, column r, in class c (j in c's rows).
+__device__ __forceinline__ size_t elem_of(const BatchClasses& k, int c, int j, int r) {
+    return size_t(k.cel[c] + ((long long)(j - k.crow[c]) << c) + r);
+}
+
+// Every per-element kernel runs one thread per (row, column) element: with
+// the row-major class blocks a warp reads whole rows of X, RP and B at every
+// matrix entry, so loads and stores are coalesced.
 
 // x2 = x + w rp;  rp2 = D^-1 (b - S x2), with x2 at the neighbours formed on
 // the fly (RichardsonIteration::doOneIteration then updatePrecResidual,
-// src/MCLS_RichardsonIteration_impl.hpp:134-147).
-template <int R>
+// src/MCLS_RichardsonIteration_impl.hpp:134-147); the walk tallies Y are
+// cleared for this iteration's walk.
 __global__ void __launch_bounds__(kThreads) k_b_richardson_residual(BatchArgs a) {
-    const long long total = (long long)a.n * R;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.ne;
          t += (long long)gridDim.x * blockDim.x) {
-        int i, r;
-        elem_rc<R>(t, i, r);
+        int i, r, c;
+        if (!elem_map(a.cls, t, i, r, c)) continue;
         if (a.skip && a.sys_done[a.rsys[i]]) continue;
         double acc = 0.0;
         for (int p = a.rp[i]; p < a.rp[i + 1]; ++p) {
-            const size_t k = size_t(a.ci[p]) * R + r;
+            const size_t k = elem_of(a.cls, c, a.ci[p], r);
             acc = fma(a.v[p], __dadd_rn(a.X[k], __dmul_rn(a.omega, a.RP[k])), acc);
         }
         a.X2[t] = __dadd_rn(a.X[t], __dmul_rn(a.omega, a.RP[t]));
         a.RP2[t] = a.dinv[i] * (a.B[t] - acc);
+        a.Y[t] = 0.0;
     }
 }
 
 // Tally source of every right-hand side: expected value c = H (w rp2),
 // collision c = w rp2 (FP32).
-template <int R>
 __global__ void __launch_bounds__(kThreads) k_b_source(BatchArgs a) {
-    const long long total = (long long)a.n * R;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.ne;
          t += (long long)gridDim.x * blockDim.x) {
-        int i, r;
-        elem_rc<R>(t, i, r);
+        int i, r, c;
+        if (!elem_map(a.cls, t, i, r, c)) continue;
         if (a.skip && a.sys_done[a.rsys[i]]) continue;  // walks skip these rows too
         double v;
         if (a.ev) {
             v = 0.0;
             for (int p = a.hrp[i]; p < a.hrp[i + 1]; ++p)
-                v = fma(a.hv[p], a.RP2[size_t(a.hci[p]) * R + r], v);
+                v = fma(a.hv[p], a.RP2[elem_of(a.cls, c, a.hci[p], r)], v);
         } else {
             v = a.RP2[t];
         }
@@ -132,65 +149,19 @@ __global__ void __launch_bounds__(kThreads) k_b_source(BatchArgs a) {
     }
 }
 
-// x = x2 + delta: delta = Y / per (+ w rp2 for the expected value, the
-// estimator's source term); Y cleared for the next iteration
-// (ForwardTally::finalize, src/MCLS_ForwardTally_impl.hpp:180-209).
-template <int R>
-__global__ void __launch_bounds__(kThreads) k_b_correction(BatchArgs a) {
-    const long long total = (long long)a.n * R;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        if (a.skip && a.sys_done[a.rsys[int(t / R)]]) continue;
-        double d = a.Y[t] * a.inv_per;
-        if (a.ev) d += a.nomega * a.RP2[t];
-        a.X[t] = a.X2[t] + d;
-        a.Y[t] = 0.0;
-    }
-}
-
-// rp = D^-1 (b - S x) and the per-(system, rhs) sums of squares.  A warp
-// covers 32/R rows: when they all belong to one system the lanes of each
-// column reduce with shuffles and one lane per column adds the sum,
-// otherwise every lane adds its own square.
-template <int R>
-__global__ void __launch_bounds__(kThreads) k_b_residual_norm(BatchArgs a, const double* Xin) {
-    const unsigned full = 0xffffffffu;
-    const long long total = (long long)a.n * R;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < total;
-         base += (long long)gridDim.x * blockDim.x) {
-        const long long t = base + threadIdx.x;
-        const bool live = t < total;
-        double sq = 0.0;
-        int sys = -1, r = 0;
-        if (live) {
-            int i;
-            elem_rc<R>(t, i, r);
-            sys = a.rsys[i];
-            if (!(a.skip && a.sys_done[sys])) {
-                double acc = 0.0;
-                for (int p = a.rp[i]; p < a.rp[i + 1]; ++p)
-                    acc = fma(a.v[p], Xin[size_t(a.ci[p]) * R + r], acc);
-                const double rv = a.dinv[i] * (a.B[t] - acc);
-                a.RP[t] = rv;
-                sq = rv * rv;
-            }
-        }
-        const int s0 = __shfl_sync(full, sys, 0);
-        const bool uniform = __all_sync(full, sys == s0) && s0 >= 0;
-        if (uniform) {
-            double v = sq;
-#pragma unroll
-            for (int d = 16; d >= R; d >>= 1) v += __shfl_xor_sync(full, v, d);
-            if ((threadIdx.x & 31) < R && v != 0.0) atomicAdd(&a.norm2[size_t(s0) * R + r], v);
-        } else if (live && sq != 0.0) {
-            atomicAdd(&a.norm2[size_t(sys) * R + r], sq);
-        }
-    }
+// The corrected iterate at element k: x2 + Y / per (+ w rp2 for the expected
+// value, the estimator's source term; ForwardTally::finalize,
+// src/MCLS_ForwardTally_impl.hpp:180-209).
+__device__ __forceinline__ double corrected(const BatchArgs& a, size_t k) {
+    double d = a.Y[k] * a.inv_per;
+    if (a.ev) d += a.nomega * a.RP2[k];
+    return a.X2[k] + d;
 }
 
 // Per-pair convergence, loop control and the per-iteration bookkeeping (new
-// stream epoch, work-queue reset, walk timing, norms cleared).
-__global__ void k_b_check(BatchArgs a, int R, int use_cond, cudaGraphConditionalHandle handle) {
+// stream epoch, work-queue reset, walk timing, norms cleared), run by one
+// block.
+__device__ void batch_check(const BatchArgs& a, int use_cond, cudaGraphConditionalHandle handle) {
     __shared__ int s_conv;
     if (threadIdx.x == 0) s_conv = 0;
     __syncthreads();
@@ -198,10 +169,10 @@ __global__ void k_b_check(BatchArgs a, int R, int use_cond, cudaGraphConditional
     const int it = st.iter + 1;
     const bool check = (it % st.check_freq) == 0 || it >= st.max_iters;
     int conv = 0;
-    for (int q = threadIdx.x; q < a.nsys * R; q += blockDim.x) {
-        const int s = q / R, r = q % R;
+    for (int q = threadIdx.x; q < a.nsys * a.pw; q += blockDim.x) {
+        const int s = q / a.pw, r = q % a.pw;
         if (r >= a.nrhs[s]) continue;
-        const double nr = a.norm2[q];
+        const double nr = __ldcg(&a.norm2[q]);
         if (!isfinite(nr)) atomicOr(a.status, DEV_ERR_NONFINITE);
         if (a.conv_iter[q] < 0 && check && sqrt(nr) <= st.tol * sqrt(a.bnorm2[q]))
             a.conv_iter[q] = it;
@@ -213,7 +184,7 @@ __global__ void k_b_check(BatchArgs a, int R, int use_cond, cudaGraphConditional
     // Systems whose every right-hand side has converged stop iterating.
     for (int s = threadIdx.x; s < a.nsys; s += blockDim.x) {
         int all = 1;
-        for (int r = 0; r < a.nrhs[s]; ++r) all &= a.conv_iter[size_t(s) * R + r] >= 0;
+        for (int r = 0; r < a.nrhs[s]; ++r) all &= a.conv_iter[size_t(s) * a.pw + r] >= 0;
         a.sys_done[s] = all;
     }
     if (threadIdx.x == 0) {
@@ -233,16 +204,70 @@ __global__ void k_b_check(BatchArgs a, int R, int use_cond, cudaGraphConditional
     }
 }
 
+// rp = D^-1 (b - S x) and the per-(system, rhs) sums of squares.  CORR: x is
+// this iteration's corrected iterate (formed on the fly at the neighbours
+// and written to X), otherwise Xin.  A warp covers 32/W rows of one class:
+// when they all belong to one system the lanes of each column reduce with
+// shuffles and one lane per column adds the sum, otherwise every lane adds
+// its own square.  CHECK: the last block to finish runs the convergence
+// test (the other blocks' sums are complete and visible by then).
+template <bool CORR, bool CHECK>
+__global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double* Xin, int use_cond,
+                                                       cudaGraphConditionalHandle handle) {
+    const unsigned full = 0xffffffffu;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < a.ne;
+         base += (long long)gridDim.x * blockDim.x) {
+        const long long t = base + threadIdx.x;
+        double sq = 0.0;
+        int sys = -1, r = 0, c = 0, i = 0;
+        if (t < a.ne && elem_map(a.cls, t, i, r, c)) {
+            sys = a.rsys[i];
+            if (!(a.skip && a.sys_done[sys])) {
+                double acc = 0.0;
+                for (int p = a.rp[i]; p < a.rp[i + 1]; ++p) {
+                    const size_t k = elem_of(a.cls, c, a.ci[p], r);
+                    acc = fma(a.v[p], CORR ? corrected(a, k) : Xin[k], acc);
+                }
+                if (CORR) a.X[t] = corrected(a, size_t(t));
+                const double rv = a.dinv[i] * (a.B[t] - acc);
+                a.RP[t] = rv;
+                sq = rv * rv;
+            }
+        }
+        const int s0 = __shfl_sync(full, sys, 0);
+        const int c0 = __shfl_sync(full, c, 0);
+        const bool uniform = __all_sync(full, sys == s0) && s0 >= 0;
+        if (uniform) {
+            double v = sq;
+            for (int d = 16; d >= (1 << c0); d >>= 1) v += __shfl_xor_sync(full, v, d);
+            if ((threadIdx.x & 31) < (1 << c0) && v != 0.0)
+                atomicAdd(&a.norm2[size_t(s0) * a.pw + r], v);
+        } else if (sys >= 0 && sq != 0.0) {
+            atomicAdd(&a.norm2[size_t(sys) * a.pw + r], sq);
+        }
+    }
+    if (CHECK) {
+        __shared__ bool s_last;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = atomicAdd(a.blocks_done, 1u) == gridDim.x - 1;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            batch_check(a, use_cond, handle);
+            if (threadIdx.x == 0) *a.blocks_done = 0u;
+        }
+    }
+}
+
 // Before the loop: sums of squares of D^-1 b per pair.
-template <int R>
 __global__ void k_b_init_norms(BatchArgs a) {
-    const long long total = (long long)a.n * R;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.ne;
          t += (long long)gridDim.x * blockDim.x) {
-        int i, r;
-        elem_rc<R>(t, i, r);
+        int i, r, c;
+        if (!elem_map(a.cls, t, i, r, c)) continue;
         const double v = a.dinv[i] * a.B[t];
-        if (v != 0.0) atomicAdd(&a.bnorm2[size_t(a.rsys[i]) * R + r], v * v);
+        if (v != 0.0) atomicAdd(&a.bnorm2[size_t(a.rsys[i]) * a.pw + r], v * v);
     }
 }
 
@@ -272,9 +297,13 @@ __global__ void k_b_forward_nh(int* d_nh, int nh) { *d_nh = nh; }
 struct mclsgpu_batch {
     mclsgpu_context* ctx = nullptr;
     int nsys = 0;
-    int R = 1;
-    int n = 0;
-    std::vector<int64_t> off;
+    int pw = 1;                    // widest system's width (per-pair arrays)
+    int n = 0;                     // rows
+    long long ne = 0;              // elements (padding included)
+    mclsgpu::BatchClasses cls{};
+    std::vector<int64_t> row0;     // system -> its first row (placement order)
+    std::vector<int64_t> eoff;     // system -> its first element
+    std::vector<int> width;        // system -> its width (power of two)
     std::vector<int> nrhs;
     mclsgpu_operator* op = nullptr;
     mclsgpu_precond* pc = nullptr;
@@ -287,12 +316,14 @@ struct mclsgpu_batch {
     double* bnorm2 = nullptr;
     int* conv_iter = nullptr;
     int* sys_done = nullptr;
+    unsigned* blocks_done = nullptr;
     mclsgpu::BatchState* d_state = nullptr;
     mclsgpu::BatchState* h_state = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int graph_key = -1;
+    long long graph_key = -1;
     int body_kernels = 0;
     int per = 1;
+    int grab = 1;                  // walk work-queue grab, in 32-history chunks
 };
 
 namespace mclsgpu {
@@ -316,6 +347,7 @@ void batch_release(mclsgpu_batch* b) {
     dfree(b->bnorm2);
     dfree(b->conv_iter);
     dfree(b->sys_done);
+    dfree(b->blocks_done);
     dfree(b->d_state);
     if (b->h_state) cudaFreeHost(b->h_state);
     delete b;
@@ -324,8 +356,10 @@ void batch_release(mclsgpu_batch* b) {
 BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     const mclsgpu_mc_params& p = b->dom->p;
     BatchArgs a{};
-    a.n = b->n;
+    a.cls = b->cls;
+    a.ne = b->ne;
     a.nsys = b->nsys;
+    a.pw = b->pw;
     a.rp = b->op->A.rp;
     a.ci = b->op->A.ci;
     a.v = b->op->A.v;
@@ -348,6 +382,7 @@ BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     a.sys_done = b->sys_done;
     a.skip = 1;
     a.st = b->d_state;
+    a.blocks_done = b->blocks_done;
     a.omega = mp ? mp->richardson_omega : 1.0;
     a.nomega = p.neumann_relaxation > 0.0 ? p.neumann_relaxation : 1.0;
     a.inv_per = 1.0 / double(b->per);
@@ -359,97 +394,31 @@ BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     return a;
 }
 
-#define MCLSGPU_BATCH_R(R, CALL) \
-    switch (R) {                 \
-        case 1: CALL(1); break;  \
-        case 2: CALL(2); break;  \
-        case 4: CALL(4); break;  \
-        case 8: CALL(8); break;  \
-        default: CALL(16); break; \
-    }
-
-// One batched MCSA iteration (6 kernels).
+// One batched MCSA iteration (4 kernels).
 int enqueue_batch_iteration(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp, int use_cond,
                             cudaGraphConditionalHandle handle) {
     cudaStream_t s = b->ctx->stream;
     BatchArgs a = batch_args(b, mp);
-    const int grid = grid_for((long long)b->n * b->R);
-#define K1(R) k_b_richardson_residual<R><<<grid, kThreads, 0, s>>>(a)
-    MCLSGPU_BATCH_R(b->R, K1)
-#undef K1
-#define K2(R) k_b_source<R><<<grid, kThreads, 0, s>>>(a)
-    MCLSGPU_BATCH_R(b->R, K2)
-#undef K2
-    int rc = launch_walk_multi(b->dom, b->R, b->cR, b->Y, b->d_rsys, b->sys_done);
+    const int grid = grid_for(b->ne);
+    k_b_richardson_residual<<<grid, kThreads, 0, s>>>(a);
+    k_b_source<<<grid, kThreads, 0, s>>>(a);
+    int rc = launch_walk_batch(b->dom, b->cls, b->cR, b->Y, b->d_rsys, b->sys_done, b->grab);
     if (rc) return rc;
-#define K3(R) k_b_correction<R><<<grid, kThreads, 0, s>>>(a)
-    MCLSGPU_BATCH_R(b->R, K3)
-#undef K3
-#define K4(R) k_b_residual_norm<R><<<grid, kThreads, 0, s>>>(a, b->X)
-    MCLSGPU_BATCH_R(b->R, K4)
-#undef K4
-    k_b_check<<<1, 1024, 0, s>>>(a, b->R, use_cond, handle);
+    k_b_update<true, true><<<grid, kThreads, 0, s>>>(a, nullptr, use_cond, handle);
     return MCLSGPU_OK;
 }
 
 int build_batch_graph(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     mclsgpu_context* ctx = b->ctx;
-    cudaStream_t s = ctx->stream;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
-    cudaGraph_t g;
-    cudaError_t e = cudaGraphCreate(&g, 0);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphCreate");
-    cudaGraphConditionalHandle handle;
-    e = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(g);
-        return cuda_fail(ctx, e, "cudaGraphConditionalHandleCreate");
-    }
-    cudaGraphNodeParams np = {};
-    np.type = cudaGraphNodeTypeConditional;
-    np.conditional.handle = handle;
-    np.conditional.type = cudaGraphCondTypeWhile;
-    np.conditional.size = 1;
-    cudaGraphNode_t node;
-    e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(g);
-        return cuda_fail(ctx, e, "cudaGraphAddNode(conditional)");
-    }
-    cudaGraph_t body = np.conditional.phGraph_out[0];
-    e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
-                                      cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(g);
-        return cuda_fail(ctx, e, "cudaStreamBeginCaptureToGraph");
-    }
-    int rc = enqueue_batch_iteration(b, mp, 1, handle);
-    cudaGraph_t captured = body;
-    e = cudaStreamEndCapture(s, &captured);
-    if (rc || e != cudaSuccess) {
-        cudaGraphDestroy(g);
-        return rc ? rc : cuda_fail(ctx, e, "cudaStreamEndCapture");
-    }
-    size_t nn = 0;
-    cudaGraphGetNodes(body, nullptr, &nn);
-    std::vector<cudaGraphNode_t> nodes(nn);
-    if (nn) cudaGraphGetNodes(body, nodes.data(), &nn);
-    b->body_kernels = 0;
-    for (size_t k = 0; k < nn; ++k) {
-        cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
-            ++b->body_kernels;
-    }
-    e = cudaGraphInstantiate(&b->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-        b->graph = nullptr;
-        return cuda_fail(ctx, e, "cudaGraphInstantiate");
-    }
-    return MCLSGPU_OK;
+    int red = MCLSGPU_OK;
+    const int rc = build_while_graph(
+        ctx, [&](cudaGraphConditionalHandle h) { red = enqueue_batch_iteration(b, mp, 1, h); },
+        &b->graph, &b->body_kernels);
+    return rc ? rc : red;
 }
 
 }  // namespace
@@ -472,49 +441,79 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
         params->weight_cutoff > 0.0)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
                          "batched MCSA runs forward FP32 walks of fixed length");
-    // Concatenate the systems into the block-diagonal operator.
-    std::vector<int64_t> off(nsys + 1, 0);
-    int maxr = 1;
+    // Width classes: system s gets W_s = nrhs_s rounded up to a power of two;
+    // the systems are placed class by class (in argument order within a class).
+    std::vector<int> width(nsys), cls_of(nsys);
+    int pw = 1;
     for (int s = 0; s < nsys; ++s) {
         if (n[s] < 1 || !rowptr[s] || !colind[s] || !values[s] || nrhs[s] < 1 || nrhs[s] > 16)
             return set_error(ctx, MCLSGPU_ERR_INVALID_ARG,
                              "batch system %d: empty, missing arrays or 1..16 right-hand sides", s);
-        off[s + 1] = off[s] + n[s];
-        if (nrhs[s] > maxr) maxr = nrhs[s];
+        int c = 0;
+        while ((1 << c) < nrhs[s]) ++c;
+        cls_of[s] = c;
+        width[s] = 1 << c;
+        if (width[s] > pw) pw = width[s];
     }
-    const int64_t N = off[nsys];
+    std::vector<int> order;
+    for (int c = 0; c < 5; ++c)
+        for (int s = 0; s < nsys; ++s)
+            if (cls_of[s] == c) order.push_back(s);
+    BatchClasses cls{};
+    std::vector<int64_t> row0(nsys), eoff(nsys);
+    int64_t N = 0, NE = 0;
+    size_t k = 0;
+    for (int c = 0; c < 5; ++c) {
+        cls.crow[c] = int(std::min<int64_t>(N, int64_t(1) << 30));
+        NE = (NE + 15) / 16 * 16;  // class blocks start on 16-element boundaries
+        cls.cel[c] = NE;
+        for (; k < order.size() && cls_of[order[k]] == c; ++k) {
+            const int s = order[k];
+            row0[s] = N;
+            eoff[s] = NE;
+            N += n[s];
+            NE += n[s] << c;
+        }
+    }
+    cls.crow[5] = int(std::min<int64_t>(N, int64_t(1) << 30));
+    NE = (NE + 15) / 16 * 16;
+    cls.cel[5] = NE;
     if (N >= (int64_t(1) << 30))
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batch too large (%lld rows)", (long long)N);
     int64_t nnz = 0;
     for (int s = 0; s < nsys; ++s) nnz += rowptr[s][n[s]] - rowptr[s][0];
     if (nnz >= (int64_t(1) << 31) - 1)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batch too large (%lld entries)", (long long)nnz);
+    // The block-diagonal operator in placement order.
     std::vector<int64_t> rp(N + 1), ci(nnz);
     std::vector<double> v(nnz);
     std::vector<int> rsys(N);
     int64_t pos = 0;
-    for (int s = 0; s < nsys; ++s) {
+    for (int s : order) {
+        const int64_t o = row0[s];
         for (int64_t i = 0; i < n[s]; ++i) {
-            rp[off[s] + i] = pos;
-            rsys[off[s] + i] = s;
+            rp[o + i] = pos;
+            rsys[o + i] = s;
             for (int64_t p = rowptr[s][i]; p < rowptr[s][i + 1]; ++p, ++pos) {
                 if (colind[s][p] < 0 || colind[s][p] >= n[s])
                     return set_error(ctx, MCLSGPU_ERR_INVALID_ARG,
                                      "batch system %d: column index out of range", s);
-                ci[pos] = colind[s][p] + off[s];
+                ci[pos] = colind[s][p] + o;
                 v[pos] = values[s][p];
             }
         }
     }
     rp[N] = pos;
-    int R = 1;
-    while (R < maxr) R <<= 1;
     mclsgpu_batch* b = new mclsgpu_batch;
     b->ctx = ctx;
     b->nsys = nsys;
-    b->R = R;
+    b->pw = pw;
     b->n = int(N);
-    b->off = off;
+    b->ne = NE;
+    b->cls = cls;
+    b->row0 = row0;
+    b->eoff = eoff;
+    b->width = width;
     b->nrhs.assign(nrhs, nrhs + nsys);
     b->per = params->sample_ratio > 0.0 ? int(std::ceil(params->sample_ratio)) : 1;
     int rc = mclsgpu_operator_upload(ctx, N, rp.data(), ci.data(), v.data(), &b->op);
@@ -531,27 +530,34 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
         pk.record_format = MCLSGPU_RECORD_PACKED;
         rc = mclsgpu_domain_build(ctx, b->op, b->pc, nullptr, &pk, &b->dom);
     }
-    if (!rc && b->dom->slots > 16)
+    if (!rc && (b->dom->slots > 16 || b->dom->rec_q16))
         rc = set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
                        "batched walks: rows of at most 15 retained entries");
-    const size_t NR = size_t(N) * R, PR = size_t(nsys) * R;
+    const size_t PR = size_t(nsys) * pw;
     cudaError_t e = cudaSuccess;
     if (!rc &&
         ((e = dmalloc(&b->d_rsys, N)) != cudaSuccess || (e = dmalloc(&b->d_nrhs, nsys)) != cudaSuccess ||
-         (e = dmalloc(&b->X, NR)) != cudaSuccess || (e = dmalloc(&b->X2, NR)) != cudaSuccess ||
-         (e = dmalloc(&b->RP, NR)) != cudaSuccess || (e = dmalloc(&b->RP2, NR)) != cudaSuccess ||
-         (e = dmalloc(&b->B, NR)) != cudaSuccess || (e = dmalloc(&b->Y, NR)) != cudaSuccess ||
-         (e = dmalloc(&b->cR, NR)) != cudaSuccess || (e = dmalloc(&b->norm2, PR)) != cudaSuccess ||
+         (e = dmalloc(&b->X, NE)) != cudaSuccess || (e = dmalloc(&b->X2, NE)) != cudaSuccess ||
+         (e = dmalloc(&b->RP, NE)) != cudaSuccess || (e = dmalloc(&b->RP2, NE)) != cudaSuccess ||
+         (e = dmalloc(&b->B, NE)) != cudaSuccess || (e = dmalloc(&b->Y, NE)) != cudaSuccess ||
+         (e = dmalloc(&b->cR, NE)) != cudaSuccess || (e = dmalloc(&b->norm2, PR)) != cudaSuccess ||
          (e = dmalloc(&b->bnorm2, PR)) != cudaSuccess ||
          (e = dmalloc(&b->conv_iter, PR)) != cudaSuccess || (e = dmalloc(&b->sys_done, nsys)) != cudaSuccess ||
-         (e = dmalloc(&b->d_state, 1)) != cudaSuccess ||
+         (e = dmalloc(&b->blocks_done, 1)) != cudaSuccess || (e = dmalloc(&b->d_state, 1)) != cudaSuccess ||
          (e = cudaMallocHost(reinterpret_cast<void**>(&b->h_state), sizeof(BatchState))) != cudaSuccess))
         rc = cuda_fail(ctx, e, "cudaMalloc batch");
     if (!rc) {
         cudaStream_t s = ctx->stream;
         cudaMemcpyAsync(b->d_rsys, rsys.data(), sizeof(int) * N, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(b->d_nrhs, b->nrhs.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
-        cudaMemsetAsync(b->Y, 0, sizeof(double) * NR, s);
+        // Padding elements are never written by the loop: zero every array once.
+        cudaMemsetAsync(b->X, 0, sizeof(double) * NE, s);
+        cudaMemsetAsync(b->X2, 0, sizeof(double) * NE, s);
+        cudaMemsetAsync(b->RP, 0, sizeof(double) * NE, s);
+        cudaMemsetAsync(b->RP2, 0, sizeof(double) * NE, s);
+        cudaMemsetAsync(b->Y, 0, sizeof(double) * NE, s);
+        cudaMemsetAsync(b->cR, 0, sizeof(float) * NE, s);
+        cudaMemsetAsync(b->blocks_done, 0, sizeof(unsigned), s);
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch build");
     }
@@ -569,11 +575,15 @@ int mclsgpu_batch_destroy(mclsgpu_batch* b) {
     return MCLSGPU_OK;
 }
 
-int mclsgpu_batch_layout(mclsgpu_batch* b, int64_t* row_offsets, int32_t* width) {
+int mclsgpu_batch_layout(mclsgpu_batch* b, int64_t* elem_offsets, int32_t* widths,
+                         int64_t* elements, int32_t* max_width) {
     if (!b) return MCLSGPU_ERR_INVALID_ARG;
-    if (row_offsets)
-        for (int s = 0; s <= b->nsys; ++s) row_offsets[s] = b->off[s];
-    if (width) *width = b->R;
+    for (int s = 0; s < b->nsys; ++s) {
+        if (elem_offsets) elem_offsets[s] = b->eoff[s];
+        if (widths) widths[s] = b->width[s];
+    }
+    if (elements) *elements = b->ne;
+    if (max_width) *max_width = b->pw;
     return MCLSGPU_OK;
 }
 
@@ -583,15 +593,17 @@ int mclsgpu_batch_domain(mclsgpu_batch* b, mclsgpu_domain** dom) {
     return MCLSGPU_OK;
 }
 
-int mclsgpu_batch_set_launch(mclsgpu_batch* b, int block_size) {
-    if (!b || (block_size != 128 && block_size != 256)) return MCLSGPU_ERR_INVALID_ARG;
+int mclsgpu_batch_set_launch(mclsgpu_batch* b, int block_size, int grab) {
+    if (!b || (block_size != 128 && block_size != 256) || grab < 1 || grab > 8)
+        return MCLSGPU_ERR_INVALID_ARG;
     b->dom->walk_block = block_size;
+    b->grab = grab;
     b->graph_key = -1;  // the captured loop bakes the launch shape in
     return MCLSGPU_OK;
 }
 
 int mclsgpu_batch_autotune(mclsgpu_batch* b, const double* b_dev, double* x_dev, int reps,
-                           int* block_size, double* walk_ms) {
+                           int* block_size, int* grab, double* walk_ms) {
     if (!b || !b_dev || !x_dev || reps < 1) return MCLSGPU_ERR_INVALID_ARG;
     mclsgpu_mcsa_params p{};
     p.size = sizeof(p);
@@ -601,25 +613,31 @@ int mclsgpu_batch_autotune(mclsgpu_batch* b, const double* b_dev, double* x_dev,
     p.smoother_steps = 1;
     p.richardson_omega = 1.0;
     p.host_loop = 1;
-    const int shapes[2] = {256, 128};
-    int best = 256;
+    const int blocks[2] = {256, 128};
+    const int grabs[3] = {1, 2, 4};
+    int best_b = 256, best_g = 1;
     double best_ms = 1e300;
-    for (int blk : shapes) {
-        b->dom->walk_block = blk;
-        cudaMemsetAsync(x_dev, 0, sizeof(double) * size_t(b->n) * b->R, b->ctx->stream);
-        mclsgpu_stats st{};
-        st.size = sizeof(st);
-        int rc = mclsgpu_batch_mcsa_solve_dev(b, b_dev, x_dev, &p, nullptr, nullptr, &st);
-        if (rc) return rc;
-        const double per = st.walk_launches ? st.walk_ms / double(st.walk_launches) : 1e300;
-        if (per < best_ms) {
-            best_ms = per;
-            best = blk;
+    for (int blk : blocks)
+        for (int g : grabs) {
+            b->dom->walk_block = blk;
+            b->grab = g;
+            cudaMemsetAsync(x_dev, 0, sizeof(double) * size_t(b->ne), b->ctx->stream);
+            mclsgpu_stats st{};
+            st.size = sizeof(st);
+            int rc = mclsgpu_batch_mcsa_solve_dev(b, b_dev, x_dev, &p, nullptr, nullptr, &st);
+            if (rc) return rc;
+            const double per = st.walk_launches ? st.walk_ms / double(st.walk_launches) : 1e300;
+            if (per < best_ms) {
+                best_ms = per;
+                best_b = blk;
+                best_g = g;
+            }
         }
-    }
-    b->dom->walk_block = best;
+    b->dom->walk_block = best_b;
+    b->grab = best_g;
     b->graph_key = -1;
-    if (block_size) *block_size = best;
+    if (block_size) *block_size = best_b;
+    if (grab) *grab = best_g;
     if (walk_ms) *walk_ms = best_ms;
     return MCLSGPU_OK;
 }
@@ -634,10 +652,11 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         return set_error(ctx, MCLSGPU_ERR_INVALID_ARG,
                          "batch mcsa params out of range (one smoother step)");
     cudaStream_t s = ctx->stream;
-    const size_t NR = size_t(b->n) * b->R, PR = size_t(b->nsys) * b->R;
+    const size_t NE = size_t(b->ne), PR = size_t(b->nsys) * b->pw;
     int pairs = 0;
     for (int q = 0; q < b->nsys; ++q) pairs += b->nrhs[q];
-    const int key = int(params->richardson_omega * 1e6);
+    const long long key = (long long)(params->richardson_omega * 1e6) * 64 +
+                          (long long)b->grab * 2 + (b->dom->walk_block == 128 ? 1 : 0);
     if (!params->host_loop && (!b->graph || b->graph_key != key)) {
         int rc = build_batch_graph(b, params);
         if (rc) return rc;
@@ -649,25 +668,23 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
     cudaMemsetAsync(b->dom->d_counter, 0, sizeof(int), s);
     cudaMemsetAsync(b->dom->d_steps, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(b->blocks_done, 0, sizeof(unsigned), s);
     {
         unsigned long long tim0[4] = {~0ULL, 0ULL, 0ULL, 0ULL};
         cudaMemcpyAsync(b->dom->d_tim, tim0, sizeof(tim0), cudaMemcpyHostToDevice, s);
     }
     cudaEventRecord(e0, s);
-    cudaMemcpyAsync(b->B, b_dev, sizeof(double) * NR, cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(b->X, x_dev, sizeof(double) * NR, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b->B, b_dev, sizeof(double) * NE, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(b->X, x_dev, sizeof(double) * NE, cudaMemcpyDeviceToDevice, s);
     cudaMemsetAsync(b->bnorm2, 0, sizeof(double) * PR, s);
     k_b_forward_nh<<<1, 1, 0, s>>>(b->dom->d_nh, b->n * b->per);
     k_b_state_init<<<1, 1024, 0, s>>>(b->d_state, params->max_iters, params->check_freq,
                                        params->tolerance, pairs, b->conv_iter, int(PR), b->norm2,
                                        b->sys_done, b->nsys);
     BatchArgs a = batch_args(b, params);
-    const int grid = grid_for((long long)b->n * b->R);
-#define KI(R)                                                 \
-    k_b_init_norms<R><<<grid, kThreads, 0, s>>>(a);           \
-    k_b_residual_norm<R><<<grid, kThreads, 0, s>>>(a, b->X)
-    MCLSGPU_BATCH_R(b->R, KI)
-#undef KI
+    const int grid = grid_for(b->ne);
+    k_b_init_norms<<<grid, kThreads, 0, s>>>(a);
+    k_b_update<false, false><<<grid, kThreads, 0, s>>>(a, b->X, 0, cudaGraphConditionalHandle(0));
     cudaMemsetAsync(b->norm2, 0, sizeof(double) * PR, s);
     cudaError_t e = cudaSuccess;
     int rc = MCLSGPU_OK;
@@ -683,7 +700,7 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
     }
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) {
-        cudaMemcpyAsync(x_dev, b->X, sizeof(double) * NR, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(x_dev, b->X, sizeof(double) * NE, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(b->h_state, b->d_state, sizeof(BatchState), cudaMemcpyDeviceToHost, s);
         e = cudaStreamSynchronize(s);
     }
@@ -701,16 +718,14 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         std::vector<int> ci(PR);
         cudaMemsetAsync(b->norm2, 0, sizeof(double) * PR, s);
         a.skip = 0;  // every system's final residual
-#define KF(R) k_b_residual_norm<R><<<grid, kThreads, 0, s>>>(a, b->X)
-        MCLSGPU_BATCH_R(b->R, KF)
-#undef KF
+        k_b_update<false, false><<<grid, kThreads, 0, s>>>(a, b->X, 0, cudaGraphConditionalHandle(0));
         cudaMemcpyAsync(nr.data(), b->norm2, sizeof(double) * PR, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(bn.data(), b->bnorm2, sizeof(double) * PR, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(ci.data(), b->conv_iter, sizeof(int) * PR, cudaMemcpyDeviceToHost, s);
         e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "batch residuals");
         for (size_t q = 0; q < PR; ++q) {
-            const bool valid = int(q % b->R) < b->nrhs[q / b->R];
+            const bool valid = int(q % b->pw) < b->nrhs[q / b->pw];
             if (conv_iters) conv_iters[q] = valid ? ci[q] : -1;
             if (rel_resid)
                 rel_resid[q] = valid ? (bn[q] > 0.0 ? std::sqrt(nr[q] / bn[q]) : std::sqrt(nr[q])) : 0.0;
@@ -731,7 +746,7 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         out.solve_ms = ms;
         out.walk_ms = double(tim[2]) * 1e-6;
         out.walk_launches = int64_t(tim[3]);
-        out.kernel_launches = int64_t(b->body_kernels ? b->body_kernels : 6) * st.iter + 4;
+        out.kernel_launches = int64_t(b->body_kernels ? b->body_kernels : 4) * st.iter + 4;
         out.rho = -1.0;
         *stats = out;
     }

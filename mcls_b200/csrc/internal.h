@@ -278,6 +278,26 @@ int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
                         mclsgpu_domain* dom, int row0 = 0);
 
+// ---- batched walks (walk.cu, batch.cu) -------------------------------------------
+// Width classes of a batch: the rows [crow[c], crow[c+1]) belong to systems
+// with 2^c right-hand-side columns, and their elements occupy
+// [cel[c], cel[c] + (crow[c+1] - crow[c]) * 2^c) of every element array,
+// row-major [rows][2^c]; cel[c] is a multiple of 16 (aligned vector loads),
+// cel[5] the element count (padding included).
+struct BatchClasses {
+    int crow[6];
+    long long cel[6];
+};
+// Forward walks shared by the right-hand sides of a batch: every history
+// carries one Kahan-compensated FP32 tally per column of its start row's
+// class, reading the tally source cR at each state's elements and adding into
+// Y at the start row's elements.  Histories whose start row belongs to a
+// finished system (done[rsys[row]]) are skipped.  Each warp takes 32 * grab
+// histories per work-queue grab.  The work-queue counter must be zero on
+// entry; the caller resets it afterwards.
+int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const float* cR, double* Y,
+                      const int* rsys, const int* done, int grab);
+
 // ---- MCSA helpers (mcsa.cu) ----------------------------------------------------
 // rp_out = PL (b - A PR x)   (LinearProblem::updatePrecResidual)
 void prec_residual(mclsgpu_domain* dom, const double* x, const double* b, double* rp_out);

@@ -211,7 +211,6 @@ __device__ __forceinline__ void walk_step(const WalkArgs& a, const char* rec, in
     // the record's own sectors) or allocated in it (the launch shape says).
     const char* r = rec + size_t(s - a.row0) * (S * 8);
     uint32_t q[2 * S];
-#pragma unroll
     if (a.l1) {
 #pragma unroll
         for (int t = 0; t < S / 4; ++t) ld_record256_l1(r + 32 * t, q + 8 * t);
@@ -538,21 +537,78 @@ void prepare_walk(mclsgpu_domain* dom) {
 
 namespace {
 
-// Forward walks shared by R right-hand sides (batched MCSA): the walk does
-// not depend on the source, so each history carries R Kahan-compensated FP32
-// sums of w * c_r(state) (cR is row-major [n][R], the tally source of every
-// right-hand side at a state) and adds them into Y[start][r] in FP64.
-// Fixed-length histories only.
-// Histories that start in a row whose system is finished (done[rsys[row]])
-// are skipped; rsys / done may be null.
-struct MultiSkip {
+// Forward walks shared by the right-hand sides of a batch (batched MCSA): the
+// walk does not depend on the source, so each history carries one
+// Kahan-compensated FP32 sum of w * c_r(state) per column r of its start
+// row's width class (cR holds the tally source of every column at every
+// state, in the batch's element layout) and adds them into Y at the start
+// row's elements in FP64.  Fixed-length histories only; a history never
+// leaves its system, so every state it visits has its start row's width.
+struct BatchWalk {
+    const float* cR;
+    double* Y;
     const int* rsys;
     const int* done;
+    BatchClasses cls;
+    int grab;
 };
 
-template <int S, bool ST, int R>
-__global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* __restrict__ cR,
-                                                       double* __restrict__ Y, MultiSkip skip) {
+// The tally-source row of state s in class c (W = 2^c columns).
+template <int W>
+__device__ __forceinline__ void load_source_row(const float* p, float (&c)[W]) {
+    if constexpr (W >= 4) {
+#pragma unroll
+        for (int r = 0; r < W; r += 4) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(p + r));
+            c[r] = q.x;
+            c[r + 1] = q.y;
+            c[r + 2] = q.z;
+            c[r + 3] = q.w;
+        }
+    } else if constexpr (W == 2) {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(p));
+        c[0] = q.x;
+        c[1] = q.y;
+    } else {
+        c[0] = __ldg(p);
+    }
+}
+
+// One history of a row of class C (2^C columns), returns its steps.
+template <int S, bool ST, int C>
+__device__ __forceinline__ unsigned batch_history(const WalkArgs& a, const char* rec,
+                                                  const BatchWalk& m, int s, float w,
+                                                  uint64_t x) {
+    constexpr int W = 1 << C;
+    const int r0 = m.cls.crow[C];
+    const float* cbase = m.cR + m.cls.cel[C];
+    const int s0 = s;
+    float acc[W], comp[W];
+#pragma unroll
+    for (int r = 0; r < W; ++r) acc[r] = comp[r] = 0.f;
+    const int L = a.L;
+    for (int k = 0; k < L; ++k) {
+        float c[W];
+        load_source_row<W>(cbase + size_t(s - r0) * W, c);
+#pragma unroll
+        for (int r = 0; r < W; ++r) {
+            const float term = w * c[r] - comp[r];
+            const float t = acc[r] + term;
+            comp[r] = (t - acc[r]) - term;
+            acc[r] = t;
+        }
+        float da = 0.f, dc = 0.f;  // the record header's own tally is unused here
+        walk_step<S, MCLSGPU_FORWARD, ST ? kStencil : kPacked>(a, rec, s, w, x, da, dc, k);
+    }
+    double* y = m.Y + m.cls.cel[C] + size_t(s0 - r0) * W;
+#pragma unroll
+    for (int r = 0; r < W; ++r)
+        if (acc[r] != 0.f || comp[r] != 0.f) atomicAdd(&y[r], double(acc[r]) - double(comp[r]));
+    return unsigned(L);
+}
+
+template <int S, bool ST>
+__global__ void __launch_bounds__(256, 3) walk32_batch(WalkArgs a, BatchWalk m) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
     __shared__ int s_nh;
@@ -565,56 +621,30 @@ __global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* 
     const char* rec = reinterpret_cast<const char*>(a.rec);
     if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
     unsigned steps = 0;
-    const int L = a.L;
+    const int chunk = 32 * m.grab;
     while (true) {
         int base = 0;
-        if (lane == 0) base = atomicAdd(a.d_counter, 32);
+        if (lane == 0) base = atomicAdd(a.d_counter, chunk);
         base = __shfl_sync(kFull, base, 0);
         const int nh = s_nh;
         if (base >= nh) break;
-        const int e = base + lane;
-        bool alive = e < nh;
-        int s = 0;
-        float w = 0.f;
-        uint64_t x = 0;
-        if (alive) walk_start<MCLSGPU_FORWARD>(a, e, s_ekey, 1.f, s, w, x);
-        if (alive && skip.done && skip.done[skip.rsys[s]]) alive = false;
-        const int s0 = s;
-        float acc[R], comp[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) acc[r] = comp[r] = 0.f;
-        if (alive) {
-            for (int k = 0; k < L; ++k) {
-                float c[R];
-                const float* cs = cR + size_t(s) * R;
-                if constexpr (R % 4 == 0) {
-#pragma unroll
-                    for (int r = 0; r < R; r += 4) {
-                        const float4 q = __ldg(reinterpret_cast<const float4*>(cs + r));
-                        c[r] = q.x;
-                        c[r + 1] = q.y;
-                        c[r + 2] = q.z;
-                        c[r + 3] = q.w;
-                    }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < R; ++r) c[r] = __ldg(cs + r);
-                }
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const float term = w * c[r] - comp[r];
-                    const float t = acc[r] + term;
-                    comp[r] = (t - acc[r]) - term;
-                    acc[r] = t;
-                }
-                float da = 0.f, dc = 0.f;  // the record header's own tally is unused here
-                walk_step<S, MCLSGPU_FORWARD, ST ? kStencil : kPacked>(a, rec, s, w, x, da, dc, k);
+        for (int g = 0; g < m.grab; ++g) {
+            const int e = base + 32 * g + lane;
+            if (e >= nh) break;
+            int s;
+            float w;
+            uint64_t x;
+            walk_start<MCLSGPU_FORWARD>(a, e, s_ekey, 1.f, s, w, x);
+            if (m.done && m.done[m.rsys[s]]) continue;
+            int c = 0;
+            while (c < 4 && s >= m.cls.crow[c + 1]) ++c;
+            switch (c) {
+                case 0: steps += batch_history<S, ST, 0>(a, rec, m, s, w, x); break;
+                case 1: steps += batch_history<S, ST, 1>(a, rec, m, s, w, x); break;
+                case 2: steps += batch_history<S, ST, 2>(a, rec, m, s, w, x); break;
+                case 3: steps += batch_history<S, ST, 3>(a, rec, m, s, w, x); break;
+                default: steps += batch_history<S, ST, 4>(a, rec, m, s, w, x); break;
             }
-            steps += L;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (acc[r] != 0.f || comp[r] != 0.f)
-                    atomicAdd(&Y[size_t(s0) * R + r], double(acc[r]) - double(comp[r]));
         }
     }
 #pragma unroll
@@ -625,30 +655,16 @@ __global__ void __launch_bounds__(256, 4) walk32_multi(WalkArgs a, const float* 
     }
 }
 
-template <int S, bool ST, int R>
-void launch_multi_sr(const WalkArgs& a, const float* cR, double* Y, MultiSkip sk, int sms,
-                     int block, cudaStream_t st) {
+template <int S, bool ST>
+void launch_batch_s(const WalkArgs& a, const BatchWalk& m, int sms, int block, cudaStream_t st) {
     static int cached[2] = {0, 0};
     const int slot = block == 128 ? 0 : 1;
     if (!cached[slot]) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32_multi<S, ST, R>, block, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, walk32_batch<S, ST>, block, 0);
         cached[slot] = b > 0 ? b : 1;
     }
-    walk32_multi<S, ST, R><<<sms * cached[slot], block, 0, st>>>(a, cR, Y, sk);
-}
-
-template <int S, bool ST>
-bool launch_multi_s(int R, const WalkArgs& a, const float* cR, double* Y, MultiSkip sk, int sms,
-                    int block, cudaStream_t st) {
-    switch (R) {
-        case 1: launch_multi_sr<S, ST, 1>(a, cR, Y, sk, sms, block, st); return true;
-        case 2: launch_multi_sr<S, ST, 2>(a, cR, Y, sk, sms, block, st); return true;
-        case 4: launch_multi_sr<S, ST, 4>(a, cR, Y, sk, sms, block, st); return true;
-        case 8: launch_multi_sr<S, ST, 8>(a, cR, Y, sk, sms, block, st); return true;
-        case 16: launch_multi_sr<S, ST, 16>(a, cR, Y, sk, sms, block, st); return true;
-        default: return false;
-    }
+    walk32_batch<S, ST><<<sms * cached[slot], block, 0, st>>>(a, m);
 }
 
 }  // namespace
@@ -678,41 +694,41 @@ static void fill_walk_args(mclsgpu_domain* dom, WalkArgs& a) {
     for (int j = 0; j < 32; ++j) a.stoff[j] = dom->stencil_off[j];
 }
 
-// Multi-right-hand-side forward walks over the domain's FP32 records (R in
-// {1, 2, 4, 8, 16}; records of at most 16 slots).  The work-queue counter must
-// be zero on entry; the caller resets it afterwards.
-int launch_walk_multi(mclsgpu_domain* dom, int R, const float* cR, double* Y, const int* rsys,
-                      const int* sys_done) {
+// Batched forward walks over the domain's FP32 records (records of at most
+// 16 slots; see launch_walk_batch in internal.h).
+int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const float* cR, double* Y,
+                      const int* rsys, const int* done, int grab) {
     mclsgpu_context* ctx = dom->ctx;
     if (dom->p.precision != MCLSGPU_FP32 || dom->p.direction != MCLSGPU_FORWARD || !dom->slots ||
         dom->rec_q16)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
                          "batched walks need FP32 forward packed or stencil records");
+    if (grab < 1 || grab > 8)
+        return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "batched walks: grab %d not in 1..8", grab);
     WalkArgs a{};
     fill_walk_args(dom, a);
     const int sms = ctx->num_sms;
     const int block = dom->walk_block;
     cudaStream_t st = ctx->stream;
-    const MultiSkip sk{rsys, sys_done};
-    bool ok = false;
+    const BatchWalk m{cR, Y, rsys, done, cls, grab};
+    bool ok = true;
     if (dom->stencil_k) {
         switch (dom->slots) {
-            case 4: ok = launch_multi_s<4, true>(R, a, cR, Y, sk, sms, block, st); break;
-            case 8: ok = launch_multi_s<8, true>(R, a, cR, Y, sk, sms, block, st); break;
+            case 4: launch_batch_s<4, true>(a, m, sms, block, st); break;
+            case 8: launch_batch_s<8, true>(a, m, sms, block, st); break;
             default: ok = false;
         }
     } else {
         switch (dom->slots) {
-            case 4: ok = launch_multi_s<4, false>(R, a, cR, Y, sk, sms, block, st); break;
-            case 8: ok = launch_multi_s<8, false>(R, a, cR, Y, sk, sms, block, st); break;
-            case 12: ok = launch_multi_s<12, false>(R, a, cR, Y, sk, sms, block, st); break;
-            case 16: ok = launch_multi_s<16, false>(R, a, cR, Y, sk, sms, block, st); break;
+            case 4: launch_batch_s<4, false>(a, m, sms, block, st); break;
+            case 8: launch_batch_s<8, false>(a, m, sms, block, st); break;
+            case 12: launch_batch_s<12, false>(a, m, sms, block, st); break;
+            case 16: launch_batch_s<16, false>(a, m, sms, block, st); break;
             default: ok = false;
         }
     }
     if (!ok)
-        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
-                         "batched walks: %d right-hand sides on %d-slot records not supported", R,
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batched walks: %d-slot records not supported",
                          dom->slots);
     return MCLSGPU_OK;
 }

@@ -2,12 +2,14 @@
 for profiling the FP32 walk kernel alone (ncu captures one walk32 launch).
 
     python -m mcls_b200.walkprof [--n 192] [--solves 4] [--format auto|stencil16]
-        [--histories-per-lane 0|1|2|4]
+        [--histories-per-lane 0|1|2|4] [--direction forward|adjoint]
 
-Point-Jacobi forward expected-value walks, 2 histories per row of 10 steps;
-prints the walk's device time per launch and its algorithmic bandwidth (the
-record bytes of every step).  At n = 192 the records (32 bytes x n^3 = 226 MB)
-exceed the 126 MB L2, so the walk is served from HBM.
+Point-Jacobi walks of 10 steps, 2 histories per row: forward expected-value
+(each history starts at its own row, neighbouring rows in neighbouring lanes)
+or adjoint collision (start states drawn from the right-hand side, so
+neighbouring lanes start at unrelated rows).  Prints the walk's device time
+per launch and its algorithmic bandwidth (the record bytes of every step).
+At n = 192 the records (32 bytes x n^3 = 226 MB) exceed the 126 MB L2.
 """
 from __future__ import annotations
 
@@ -28,14 +30,17 @@ def main(argv=None):
     ap.add_argument("--histories-per-lane", type=int, default=0,
                     help="0: autotune the launch shape")
     ap.add_argument("--l1", type=int, default=0, help="record loads allocated in L1 (fixed shape)")
+    ap.add_argument("--direction", choices=["forward", "adjoint"], default="forward")
     args = ap.parse_args(argv)
     A, b = P.diffusion3d_varcoef(args.n, seed=1)
     ctx = capi.Context(0)
     op = capi.Operator(ctx, A)
     pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
     fmt = capi.RECORD_STENCIL16 if args.format == "stencil16" else capi.RECORD_AUTO
+    fwd = args.direction == "forward"
     dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=3,
-                      estimator=capi.EXPECTED_VALUE, sample_ratio=2.0, direction=capi.FORWARD,
+                      estimator=capi.EXPECTED_VALUE if fwd else capi.COLLISION,
+                      sample_ratio=2.0, direction=capi.FORWARD if fwd else capi.ADJOINT,
                       history_length=10, record_format=fmt)
     rt = torch.tensor((1.0 / A.diagonal()) * b, device="cuda:0", dtype=torch.float64)
     xt = torch.zeros_like(rt)
@@ -55,11 +60,15 @@ def main(argv=None):
         launches += st["walk_launches"]
     info = dom.info()
     per = ms / max(launches, 1)
-    print(json.dumps({"n": A.shape[0], "record_bytes": info["record_bytes"],
+    # A forward step reads its record (the tally source rides in it); an
+    # adjoint step also reads and writes one FP64 tally.
+    step_b = info["record_bytes"] + (0 if fwd else 16)
+    print(json.dumps({"n": A.shape[0], "direction": args.direction, "record_bytes": info["record_bytes"],
                       "records_mb": info["record_bytes"] * A.shape[0] / 1e6,
                       "walk_ms_per_launch": per, "steps_per_launch": steps / max(launches, 1),
-                      "algorithmic_gbs": info["record_bytes"] * steps / max(launches, 1) /
-                      (per * 1e-3) / 1e9, "launch": shape}))
+                      "step_bytes": step_b,
+                      "algorithmic_gbs": step_b * steps / max(launches, 1) / (per * 1e-3) / 1e9,
+                      "launch": shape}))
     dom.close()
     pc.close()
     op.close()

@@ -78,16 +78,53 @@ def test_batch_matches_single_system_iterations(ctx):
 def test_batch_autotune_and_layout(ctx):
     import torch
 
-    systems, nrhs = _systems()
+    systems, nrhs = _systems()  # right-hand sides 1, 3, 2, 4 -> widths 1, 4, 2, 4
     bt = capi.Batch(ctx, systems, nrhs, direction=capi.FORWARD, estimator=capi.EXPECTED_VALUE,
                     precision=capi.FP32, sample_ratio=1.0, history_length=10)
     assert bt.width == 4 and bt.rows == sum(A.shape[0] for A in systems)
-    assert list(np.diff(bt.offsets)) == [A.shape[0] for A in systems]
-    B = torch.ones((bt.rows, bt.width), dtype=torch.float64, device="cuda:0")
+    assert list(bt.widths) == [1, 4, 2, 4]
+    # Grouped by width: the one-column system first, then the two-column one,
+    # then the four-column ones in argument order; groups start on 16-element
+    # boundaries and the blocks do not overlap.
+    order = np.argsort(bt.elem_offsets)
+    assert list(order) == [0, 2, 1, 3]
+    ends = bt.elem_offsets + bt.n * bt.widths
+    assert np.all(bt.elem_offsets[order][1:] >= ends[order][:-1])
+    assert bt.elem_offsets[2] % 16 == 0 and bt.elem_offsets[1] % 16 == 0
+    assert bt.elements >= ends.max() and bt.elements % 16 == 0
+    B = torch.ones(bt.elements, dtype=torch.float64, device="cuda:0")
     X = torch.zeros_like(B)
     tuned = bt.autotune(B.data_ptr(), X.data_ptr(), reps=2)
-    assert tuned["block_size"] in (128, 256) and tuned["walk_ms"] > 0
+    assert tuned["block_size"] in (128, 256) and tuned["grab"] in (1, 2, 4)
+    assert tuned["walk_ms"] > 0
     bt.close()
+
+
+@pytest.mark.parametrize("grab", [1, 4])
+def test_batch_launch_shapes_agree(ctx, grab):
+    # The walk's queue grab changes which warp runs a history, not its draws:
+    # every shape gives the same solutions up to the order of the FP64 tally
+    # additions.
+    import torch
+
+    systems, nrhs = _systems()
+    rng = np.random.default_rng(1)
+    Bb = [rng.uniform(0, 1, (A.shape[0], r)) for A, r in zip(systems, nrhs)]
+    out = []
+    for blk in (256, 128):
+        bt = capi.Batch(ctx, systems, nrhs, direction=capi.FORWARD,
+                        estimator=capi.EXPECTED_VALUE, precision=capi.FP32, sample_ratio=2.0,
+                        history_length=10, seed=3)
+        bt.set_launch(blk, grab)
+        B = torch.tensor(bt.pack(Bb), device="cuda:0")
+        X = torch.zeros_like(B)
+        st, it, rr = bt.mcsa_solve_dev(B.data_ptr(), X.data_ptr(), tolerance=1e-8,
+                                       max_iters=20000)
+        assert st["converged"] == 1
+        out.append(bt.unpack(X.cpu().numpy()))
+        bt.close()
+    for a, b in zip(*out):
+        np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-10 * np.abs(b).max())
 
 
 def test_batch_rejects_adjoint_and_too_many_rhs(ctx):
