@@ -274,6 +274,11 @@ int mclsgpu_spai_set_params(mclsgpu_spai* net, const float* host);
 /* Inference on every row of op: raw outputs out[n][16] and/or the values of
  * M on A's CSR pattern (either may be NULL, not both). */
 int mclsgpu_spai_infer(mclsgpu_spai* net, mclsgpu_operator* op, float* out, double* mvals);
+/* The same into device arrays (out_dev [n][16] FP32, mvals_dev [nnz] FP64;
+ * either may be NULL, not both); *ms (may be NULL) receives the forward
+ * kernel's device time. */
+int mclsgpu_spai_infer_dev(mclsgpu_spai* net, mclsgpu_operator* op, float* out_dev,
+                           double* mvals_dev, float* ms);
 /* Loss and parameter gradient (host, may be NULL) for nvec device vectors
  * stored one after another (v_dev[k*n + i]). */
 int mclsgpu_spai_gradient(mclsgpu_spai* net, mclsgpu_operator* op, const double* v_dev,

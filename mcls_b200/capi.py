@@ -187,7 +187,7 @@ EXPORTS = [
     "mclsgpu_domain_query", "mclsgpu_domain_set_launch", "mclsgpu_domain_autotune",
     "mclsgpu_operator_apply_static", "mclsgpu_spai_num_params", "mclsgpu_spai_create",
     "mclsgpu_spai_destroy", "mclsgpu_spai_get_params", "mclsgpu_spai_set_params",
-    "mclsgpu_spai_infer", "mclsgpu_spai_gradient", "mclsgpu_spai_train_step", "mclsgpu_spai_rho",
+    "mclsgpu_spai_infer", "mclsgpu_spai_infer_dev", "mclsgpu_spai_gradient", "mclsgpu_spai_train_step", "mclsgpu_spai_rho",
     "mclsgpu_domain_residual", "mclsgpu_spai_smooth_vectors", "mclsgpu_spai_set_penalty",
     "mclsgpu_batch_build", "mclsgpu_batch_destroy", "mclsgpu_batch_layout",
     "mclsgpu_batch_domain", "mclsgpu_batch_set_launch", "mclsgpu_batch_autotune",
@@ -311,6 +311,7 @@ def load(path: str = LIB_PATH):
     L.mclsgpu_spai_get_params.argtypes = [P, P]
     L.mclsgpu_spai_set_params.argtypes = [P, P]
     L.mclsgpu_spai_infer.argtypes = [P, P, P, P]
+    L.mclsgpu_spai_infer_dev.argtypes = [P, P, P, P, C.POINTER(C.c_float)]
     L.mclsgpu_spai_gradient.argtypes = [P, P, P, C.c_int, C.POINTER(d), P]
     L.mclsgpu_spai_train_step.argtypes = [P, P, P, C.c_int, C.POINTER(SpaiAdam), C.POINTER(d)]
     L.mclsgpu_spai_rho.argtypes = [P, P, C.c_int, C.POINTER(d), C.POINTER(d)]
@@ -846,6 +847,16 @@ class SpaiNet:
         m = np.empty(nnz, np.float64)
         self.ctx.check(self.ctx.L.mclsgpu_spai_infer(self.h, op.h, _ptr(out), _ptr(m)))
         return out, m
+
+    def infer_dev(self, op: Operator, out_ptr=None, mvals_ptr=None):
+        """Inference into device arrays; returns the forward kernel's device
+        time in ms."""
+        _torch_ready()
+        ms = C.c_float()
+        self.ctx.check(self.ctx.L.mclsgpu_spai_infer_dev(
+            self.h, op.h, C.c_void_p(out_ptr) if out_ptr else None,
+            C.c_void_p(mvals_ptr) if mvals_ptr else None, C.byref(ms)))
+        return ms.value
 
     def gradient(self, op: Operator, v_dev_ptr, nvec):
         """(loss, FP32 parameter gradient) for nvec device vectors."""

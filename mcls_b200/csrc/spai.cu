@@ -1213,6 +1213,33 @@ int mclsgpu_spai_infer(mclsgpu_spai* net, mclsgpu_operator* op, float* out, doub
     return rc;
 }
 
+int mclsgpu_spai_infer_dev(mclsgpu_spai* net, mclsgpu_operator* op, float* out_dev,
+                           double* mvals_dev, float* ms) {
+    if (!net || !op || (!out_dev && !mvals_dev)) return MCLSGPU_ERR_INVALID_ARG;
+    mclsgpu_context* ctx = net->ctx;
+    SlotTable t;
+    int rc = slot_table(ctx, op, net->slots, t);
+    if (rc) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, ctx->stream);
+    }
+    rc = launch_forward(net, op, t, mvals_dev, out_dev);
+    if (ms) cudaEventRecord(e1, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "spai infer");
+    if (ms) {
+        *ms = 0.f;
+        if (!rc) cudaEventElapsedTime(ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (!rc) rc = check_device_status(ctx);
+    return rc;
+}
+
 int mclsgpu_spai_gradient(mclsgpu_spai* net, mclsgpu_operator* op, const double* v_dev, int nvec,
                           double* loss, float* grad) {
     if (!net || !op || !v_dev) return MCLSGPU_ERR_INVALID_ARG;

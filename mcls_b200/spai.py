@@ -15,6 +15,8 @@ a library kernel).
 """
 from __future__ import annotations
 
+import json
+
 import numpy as np
 
 from . import capi
@@ -101,6 +103,38 @@ def train(net, samples, steps, lr=2e-3, lr_final=2e-4, grad_clip=0.0, log_every=
     return losses
 
 
+def time_inference(ctx, net, grid, reps, device=0):
+    """Device time of the forward MLP kernel over every row of a grid^3
+    variable-coefficient diffusion operator (M values on A's pattern and the
+    raw outputs into device arrays), after two warm-up launches."""
+    import torch
+
+    from . import problems as P
+
+    A, _ = P.diffusion3d_varcoef(grid, seed=1)
+    op = capi.Operator(ctx, A)
+    n, nnz = A.shape[0], A.nnz
+    dev = f"cuda:{device}"
+    mv = torch.empty(nnz, dtype=torch.float64, device=dev)
+    out = torch.empty((n, 16), dtype=torch.float32, device=dev)
+    for _ in range(2):
+        net.infer_dev(op, out.data_ptr(), mv.data_ptr())
+    ms = [net.infer_dev(op, out.data_ptr(), mv.data_ptr()) for _ in range(reps)]
+    per = float(np.mean(ms))
+    # Bytes a row must move: its stencil values by diagonal (K x 8) and CSR
+    # row pointer and columns (4 + 4 per entry) in, M on its pattern (8 per
+    # entry) and the raw outputs (16 x 4) out.
+    k = nnz / n
+    row_bytes = 8 * k + 4 + 4 * k + 8 * k + 64
+    flops = 2 * (16 * 64 + 64 * 64 + 64 * 16)
+    op.close()
+    return {"rows": n, "forward_ms": per, "rows_per_s": n / (per * 1e-3),
+            "tflops": flops * n / (per * 1e-3) / 1e12, "bytes_per_row": row_bytes,
+            "algorithmic_gbs": row_bytes * n / (per * 1e-3) / 1e9,
+            "what": f"k_spai_forward over a {grid}^3 var-coef diffusion operator, mean of {reps} "
+                    "launches after 2 warm-up launches"}
+
+
 def main(argv=None):
     """Train a learned-SPAI network on seeded systems of one family and save
     its parameters (numpy .npy, FP32, the flat order of mclsgpu_spai_*)."""
@@ -120,6 +154,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=1000)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=None, help="where to save the parameters (.npy)")
+    ap.add_argument("--infer-grid", type=int, default=0,
+                    help="after training, time inference on an N^3 var-coef diffusion system")
+    ap.add_argument("--infer-reps", type=int, default=10)
     args = ap.parse_args(argv)
     ctx = capi.Context(args.device)
     samples, slots = [], None
@@ -152,6 +189,9 @@ def main(argv=None):
           f"loss {np.mean(losses[:8]):.4f} -> {np.mean(losses[-8:]):.4f}", flush=True)
     if args.out:
         np.save(args.out, net.params)
+    if args.infer_grid:
+        print(json.dumps(time_inference(ctx, net, args.infer_grid, args.infer_reps, args.device)),
+              flush=True)
     net.close()
     ctx.close()
 
