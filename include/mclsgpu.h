@@ -627,27 +627,35 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
  * src/MCLS_History_impl.hpp:56-89) for systems whose domain does not fit one
  * GPU.  A part holds rows [bounds[part], bounds[part+1]) of the domain (FP32
  * records, FP64 domain, tallies).  Histories that step into another part's
- * rows with steps left are written to that part's outbox as 24-byte
- * mclsgpu_history_wire records and continue there in the next round on the
- * same random stream, so every transition and tally is the one the
- * whole-domain walk makes.  The caller runs the rounds and moves outboxes to
- * inboxes (NCCL all-to-all between GPUs, device copies within one GPU) until
- * no part has departures; no kernel waits on another part. */
+ * rows and go on (steps left, weight above the cutoff) are written to that
+ * part's outbox as 32-byte mclsgpu_history_wire records and continue there in
+ * the next round on the same random stream, so every transition and tally is
+ * the one the whole-domain walk makes.  Adjoint histories tally where they
+ * stand; a forward history's sum belongs to its start row, so when it ends
+ * outside the part that owns that row, the sum goes there as a tally return
+ * (state -1) in the next round.  The caller runs the rounds and moves outboxes
+ * to inboxes (NCCL all-to-all between GPUs, device copies within one GPU)
+ * until no part has departures; no kernel waits on another part. */
 typedef struct {
     uint64_t rng;     /* Xorshift state after the last draw */
-    int32_t state;    /* the global state the history moved to */
+    int32_t state;    /* the global state the history moved to; -1: a forward
+                         tally return */
     int32_t step;     /* transitions taken */
     float weight;
     int32_t id;       /* its index in the global source */
+    float acc;        /* forward: the history's Kahan-compensated sum so far */
+    float comp;       /* forward: its compensation */
 } mclsgpu_history_wire;
 int32_t mclsgpu_history_wire_size(void);
 
 typedef struct mclsgpu_subdomain mclsgpu_subdomain;
 /* Part `part` of nparts (<= 64).  bounds: nparts + 1 global row bounds from
- * 0 to n_global.  The part's rows of the transposed composite operator
- * (PL A PR)^T as a host CSR (bounds[part+1] - bounds[part] rows, global
- * column indices), filtered by params->composite_threshold.  params: FP32
- * adjoint collision walks of fixed length on the counter-based stream; all
+ * 0 to n_global.  The part's rows of the composite operator the walks
+ * follow -- (PL A PR)^T for adjoint walks, PL A PR for forward walks -- as a
+ * host CSR (bounds[part+1] - bounds[part] rows, global column indices),
+ * filtered by params->composite_threshold.  params: FP32 walks on the
+ * counter-based stream, adjoint collision or forward (collision or expected
+ * value), of History Length steps or ended earlier by the Weight Cutoff; all
  * parts of one solve take the same params (seed included). */
 int mclsgpu_subdomain_build(mclsgpu_context* ctx, int64_t n_global, int32_t nparts,
                             const int64_t* bounds, int32_t part, const int64_t* rowptr,
@@ -657,10 +665,12 @@ int mclsgpu_subdomain_destroy(mclsgpu_subdomain* sd);
 int mclsgpu_subdomain_info(const mclsgpu_subdomain* sd, int64_t* row_begin, int64_t* rows,
                            int32_t* record_bytes);
 /* Start of one Monte Carlo solve of rhs_dev (the whole source vector,
- * n_global, device; already left preconditioned as an MCSA residual is):
- * the global adjoint source is built as the whole-domain solve builds it and
- * the part keeps the histories starting in its rows.  *n_start = those,
- * *n_total = histories in the solve. */
+ * n_global, device; already left preconditioned as an MCSA residual is).
+ * Adjoint: the global source is built as the whole-domain solve builds it
+ * and the part keeps the histories starting in its rows.  Forward: history e
+ * starts at row e / ceil(Sample Ratio), and the part's records take the tally
+ * source of its rows.  *n_start = the part's starting histories, *n_total =
+ * histories in the solve. */
 int mclsgpu_subdomain_begin(mclsgpu_subdomain* sd, const double* rhs_dev, int64_t* n_start,
                             int64_t* n_total);
 /* One round: walk the part's starting histories (inbox_dev NULL) or the
@@ -670,8 +680,10 @@ int mclsgpu_subdomain_begin(mclsgpu_subdomain* sd, const double* rhs_dev, int64_
 int mclsgpu_subdomain_transport(mclsgpu_subdomain* sd, const mclsgpu_history_wire* inbox_dev,
                                 int64_t n_in, mclsgpu_history_wire* outbox_dev,
                                 int64_t capacity, int64_t* out_counts);
-/* End of the solve: x_part_dev (the part's rows, device) = tallies / total
- * histories; stats->walk_steps = steps walked in this part. */
+/* End of the solve: x_part_dev (the part's rows, device) = the normalised
+ * tallies (adjoint: / total histories; forward: / histories per row, plus the
+ * source for the expected-value estimator); stats->walk_steps = steps walked
+ * in this part. */
 int mclsgpu_subdomain_finish(mclsgpu_subdomain* sd, double* x_part_dev, mclsgpu_stats* stats);
 
 /* ---- spectral radius ------------------------------------------------------- */

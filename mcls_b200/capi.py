@@ -998,10 +998,11 @@ class Batch:
 
 
 class Subdomain:
-    """One part of a row-partitioned adjoint domain (mclsgpu_subdomain_*).
+    """One part of a row-partitioned domain (mclsgpu_subdomain_*).
 
-    `rows` is the part's rows of the transposed composite operator
-    (PL A PR)^T with global column indices (scipy CSR, n_global columns)."""
+    `rows` is the part's rows of the composite operator the walks follow --
+    (PL A PR)^T for adjoint walks, PL A PR for forward walks -- with global
+    column indices (scipy CSR, n_global columns)."""
 
     def __init__(self, ctx: Context, n_global: int, bounds, part: int, rows,
                  params: McParams | None = None, **kw):

@@ -342,12 +342,14 @@ constexpr int kMaxParts = 64;
 // mclsgpu_history_wire).
 struct HistoryWire {
     uint64_t rng;     // Xorshift state after the last draw
-    int32_t state;    // the global state it moved to
+    int32_t state;    // the global state it moved to; -1: a forward tally return
     int32_t step;     // transitions taken
     float weight;
     int32_t id;       // its index in the global source
+    float acc;        // forward: the history's Kahan-compensated sum so far
+    float comp;       //          and its compensation
 };
-static_assert(sizeof(HistoryWire) == 24, "history wire format");
+static_assert(sizeof(HistoryWire) == 32, "history wire format");
 
 struct PartWalk {
     const uint2* rec;       // packed FP32 records of rows [row0, row0 + n)
@@ -355,10 +357,14 @@ struct PartWalk {
     int row0;
     int n;
     int L;
+    int dir;                // MCLSGPU_ADJOINT or MCLSGPU_FORWARD
+    int per;                // forward: histories per start row
+    float cutoff;           // relative weight cutoff (0: fixed length)
     // first round: the histories e_begin <= e < e_end of the global source
+    // (adjoint: its start list; forward: history e starts at row e / per)
     const int* start;
     long long e_begin, e_end;
-    const double* sc;       // [0] = starting weight |b|_1
+    const double* sc;       // [0] = adjoint starting weight |b|_1
     uint64_t seed;
     const unsigned long long* d_epoch;
     // later rounds: histories handed over by other parts

@@ -68,6 +68,40 @@ __global__ void k_part_finish(const double* y, const double* sc, int n, double* 
         x[i] = __dmul_rn(y[i], inv);  // AdjointTally::normalize
 }
 
+// Forward solve, once per solve: the tally source of the part's rows into
+// their records' headers, c_i = (H v)_i for the expected-value estimator or
+// v_i for collision (the whole-domain build's arithmetic, over the part's
+// FP64 rows with global columns), the part's slice of v kept for the
+// finalisation, and the tallies cleared.
+__global__ void k_part_forward_rec(const double* v, int row0, int n, double omega, int has,
+                                   int ev, const int* rp, const int* ci, const double* h,
+                                   int slots, uint2* rec, double* y, double* srcp) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double c;
+        if (!ev) {
+            c = has ? v[row0 + i] * omega : v[row0 + i];
+        } else {
+            c = 0.0;
+            for (int k = rp[i]; k < rp[i + 1]; ++k)
+                c = fma(h[k], has ? v[ci[k]] * omega : v[ci[k]], c);
+        }
+        rec[size_t(i) * slots].y = __float_as_uint(__double2float_rn(c));
+        y[i] = 0.0;
+        srcp[i] = v[row0 + i];
+    }
+}
+
+// ForwardTally::finalize (src/MCLS_ForwardTally_impl.hpp:194-208): sum /
+// count, plus the source term for the expected-value estimator.
+__global__ void k_part_finish_forward(const double* y, const double* srcp, int n, int per,
+                                      int ev, double omega, int has, double* x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = __ddiv_rn(y[i], per);
+        if (ev) d = __dadd_rn(d, has ? srcp[i] * omega : srcp[i]);
+        x[i] = d;
+    }
+}
+
 __global__ void k_epoch_next(unsigned long long* e) { *e += 1ULL; }
 
 void release_source(mclsgpu_domain* d) {
@@ -110,6 +144,8 @@ struct mclsgpu_subdomain {
     mclsgpu_domain src;    // the global source: N states, no records
     mclsgpu_domain recs;   // the part's rows: records and FP64 domain
     double* y = nullptr;   // tallies of the part's rows
+    double* srcp = nullptr;  // forward: the part's slice of the source
+    int per = 1;             // forward: histories per start row
     unsigned long long* d_out_cnt = nullptr;
     unsigned long long* d_steps = nullptr;
     long long* d_range = nullptr;
@@ -120,6 +156,7 @@ struct mclsgpu_subdomain {
         release_records(&recs);
         dfree(d_bounds);
         dfree(y);
+        dfree(srcp);
         dfree(d_out_cnt);
         dfree(d_steps);
         dfree(d_range);
@@ -147,12 +184,13 @@ int mclsgpu_subdomain_build(mclsgpu_context* ctx, int64_t n_global, int32_t npar
         if (bounds[q + 1] <= bounds[q])
             return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "parts: empty or decreasing part %d",
                              q);
-    if (p->direction != MCLSGPU_ADJOINT || p->estimator != MCLSGPU_COLLISION ||
-        p->precision != MCLSGPU_FP32 || p->rng_mode != MCLSGPU_RNG_COUNTER ||
-        p->weight_cutoff > 0.0 || p->history_length < 1)
+    const bool adjoint = p->direction == MCLSGPU_ADJOINT;
+    if ((adjoint && p->estimator != MCLSGPU_COLLISION) ||
+        (!adjoint && p->direction != MCLSGPU_FORWARD) || p->precision != MCLSGPU_FP32 ||
+        p->rng_mode != MCLSGPU_RNG_COUNTER || p->weight_cutoff < 0.0 || p->history_length < 1)
         return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED,
-                         "partitioned domains take FP32 adjoint collision walks of fixed length "
-                         "on the counter-based stream");
+                         "partitioned domains take FP32 walks on the counter-based stream: "
+                         "adjoint collision or forward (collision or expected value)");
     cudaSetDevice(ctx->device);
     mclsgpu_subdomain* sd = new mclsgpu_subdomain;
     sd->ctx = ctx;
@@ -163,6 +201,11 @@ int mclsgpu_subdomain_build(mclsgpu_context* ctx, int64_t n_global, int32_t npar
     sd->part = part;
     sd->row0 = int(bounds[part]);
     sd->n = int(bounds[part + 1] - bounds[part]);
+    sd->per = p->sample_ratio > 0.0 ? int(std::ceil(p->sample_ratio)) : 1;
+    if (!adjoint && double(n_global) * sd->per >= double(int64_t(1) << 31)) {
+        delete sd;
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "too many histories per solve");
+    }
     cudaStream_t s = ctx->stream;
     const int N = int(n_global);
     int rc = MCLSGPU_OK;
@@ -211,6 +254,7 @@ int mclsgpu_subdomain_build(mclsgpu_context* ctx, int64_t n_global, int32_t npar
              (e = dmalloc(&g.ipart, parts)) != cudaSuccess ||
              (e = dmalloc(&g.d_epoch, 1)) != cudaSuccess || (e = dmalloc(&g.d_pos, 1)) != cudaSuccess ||
              (e = dmalloc(&sd->y, sd->n)) != cudaSuccess ||
+             (e = dmalloc(&sd->srcp, sd->n)) != cudaSuccess ||
              (e = dmalloc(&sd->d_bounds, nparts + 1)) != cudaSuccess ||
              (e = dmalloc(&sd->d_out_cnt, nparts)) != cudaSuccess ||
              (e = dmalloc(&sd->d_steps, 1)) != cudaSuccess ||
@@ -261,13 +305,24 @@ int mclsgpu_subdomain_begin(mclsgpu_subdomain* sd, const double* rhs_dev, int64_
     cudaSetDevice(ctx->device);
     cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s);
     const double omega = sd->p.neumann_relaxation;
-    launch_adjoint_source(&sd->src, rhs_dev, omega, omega > 0.0);
-    k_part_range<<<1, 1, 0, s>>>(sd->src.start, sd->src.d_nh, sd->row0, sd->row0 + sd->n,
-                                 sd->d_range);
-    // Step-0 tallies of the part's rows (counts x starting weight).
-    cudaMemcpyAsync(sd->y, sd->src.y64 + sd->row0, size_t(sd->n) * sizeof(double),
-                    cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(sd->range, sd->d_range, sizeof(sd->range), cudaMemcpyDeviceToHost, s);
+    if (sd->p.direction == MCLSGPU_FORWARD) {
+        // History e starts at row e / per: the part's are a contiguous range.
+        const mclsgpu_domain& r = sd->recs;
+        k_part_forward_rec<<<grid_for(sd->n), 256, 0, s>>>(
+            rhs_dev, sd->row0, sd->n, omega, omega > 0.0, sd->p.estimator == MCLSGPU_EXPECTED_VALUE,
+            r.D.rp, r.D.ci, r.D.v, r.slots, r.rec, sd->y, sd->srcp);
+        sd->range[0] = (long long)sd->row0 * sd->per;
+        sd->range[1] = (long long)(sd->row0 + sd->n) * sd->per;
+        sd->range[2] = (long long)sd->N * sd->per;
+    } else {
+        launch_adjoint_source(&sd->src, rhs_dev, omega, omega > 0.0);
+        k_part_range<<<1, 1, 0, s>>>(sd->src.start, sd->src.d_nh, sd->row0, sd->row0 + sd->n,
+                                     sd->d_range);
+        // Step-0 tallies of the part's rows (counts x starting weight).
+        cudaMemcpyAsync(sd->y, sd->src.y64 + sd->row0, size_t(sd->n) * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(sd->range, sd->d_range, sizeof(sd->range), cudaMemcpyDeviceToHost, s);
+    }
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "subdomain begin");
     int rc = check_device_status(ctx);
@@ -295,6 +350,9 @@ int mclsgpu_subdomain_transport(mclsgpu_subdomain* sd, const mclsgpu_history_wir
     w.row0 = sd->row0;
     w.n = sd->n;
     w.L = sd->p.history_length;
+    w.dir = sd->p.direction;
+    w.per = sd->per;
+    w.cutoff = float(sd->p.weight_cutoff);
     w.start = sd->src.start;
     w.e_begin = sd->range[0];
     w.e_end = sd->range[1];
@@ -332,7 +390,15 @@ int mclsgpu_subdomain_finish(mclsgpu_subdomain* sd, double* x_part_dev, mclsgpu_
     if (!sd->ready) return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "mclsgpu_subdomain_begin first");
     cudaStream_t s = ctx->stream;
     cudaSetDevice(ctx->device);
-    k_part_finish<<<grid_for(sd->n), 256, 0, s>>>(sd->y, sd->src.d_scalars, sd->n, x_part_dev);
+    if (sd->p.direction == MCLSGPU_FORWARD) {
+        const double omega = sd->p.neumann_relaxation;
+        k_part_finish_forward<<<grid_for(sd->n), 256, 0, s>>>(
+            sd->y, sd->srcp, sd->n, sd->per, sd->p.estimator == MCLSGPU_EXPECTED_VALUE, omega,
+            omega > 0.0, x_part_dev);
+    } else {
+        k_part_finish<<<grid_for(sd->n), 256, 0, s>>>(sd->y, sd->src.d_scalars, sd->n,
+                                                      x_part_dev);
+    }
     k_epoch_next<<<1, 1, 0, s>>>(sd->src.d_epoch);
     unsigned long long steps = 0;
     cudaMemcpyAsync(&steps, sd->d_steps, sizeof(steps), cudaMemcpyDeviceToHost, s);

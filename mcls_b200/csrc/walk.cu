@@ -849,13 +849,35 @@ void launch_walk(mclsgpu_domain* dom, long long max_trace, long long* tr_states,
 //
 // One part holds the records and tallies of rows [row0, row0 + n).  A
 // history walks while its state stays in the part; when a transition takes
-// it to another part's row with steps left, it is written to that part's
-// outbox (HistoryWire: Xorshift state, state, step, weight) and continues
-// there in a later round, on the same random stream.  Every transition and
-// tally is therefore the one the whole-domain walk would make.
+// it to another part's row and the history goes on (steps left, weight above
+// the cutoff), it is written to that part's outbox (HistoryWire: Xorshift
+// state, state, step, weight and, forward, its running sum) and continues
+// there in a later round, on the same random stream.  An adjoint history
+// tallies where it stands, so its tallies land in the parts it visits.  A
+// forward history's sum belongs to its start row: when it ends outside the
+// part that owns that row, the sum travels there as a tally return (state
+// -1).  Every transition and tally is therefore the one the whole-domain walk
+// would make.
 namespace {
 
-template <int S>
+__device__ __forceinline__ int part_owner(const int* sb, int nparts, int s) {
+    int lo = 0, up = nparts;  // sb[lo] <= s < sb[lo + 1]
+    while (up - lo > 1) {
+        const int mid = (lo + up) >> 1;
+        if (sb[mid] <= s) lo = mid; else up = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void part_send(const PartWalk& p, int q, const HistoryWire& h) {
+    const unsigned long long slot = atomicAdd(&p.out_cnt[q], 1ULL);
+    if (slot < (unsigned long long)p.cap)
+        p.out[size_t(q) * size_t(p.cap) + slot] = h;
+    else
+        atomicOr(p.status, DEV_ERR_CAPACITY);
+}
+
+template <int S, int DIR>
 __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
     __shared__ int sb[kMaxParts + 1];
     for (int t = threadIdx.x; t <= p.nparts; t += blockDim.x) sb[t] = p.bounds[t];
@@ -864,7 +886,8 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
     a.y64 = p.y;
     a.row0 = p.row0;
     const uint64_t ekey = epoch_key(p.seed, *p.d_epoch);
-    const float wnorm = float(p.sc[0]);
+    const float wnorm = DIR == MCLSGPU_ADJOINT ? float(p.sc[0]) : 1.f;
+    const float wcut = p.cutoff * wnorm;
     const long long nwork = p.in ? p.n_in : p.e_end - p.e_begin;
     const char* rec = reinterpret_cast<const char*>(p.rec);
     const int hi = p.row0 + p.n;
@@ -872,20 +895,35 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nwork;
          t += (long long)gridDim.x * blockDim.x) {
         int s, k, id;
-        float w;
+        float w, acc = 0.f, comp = 0.f;
         uint64_t x;
         if (p.in) {
             const HistoryWire h = p.in[t];
+            if (DIR == MCLSGPU_FORWARD && h.state < 0) {  // a tally return
+                const int s0 = h.id / p.per;
+                if (s0 < p.row0 || s0 >= hi)
+                    atomicOr(p.status, DEV_ERR_BOUNDS);
+                else
+                    atomicAdd(&p.y[s0 - p.row0], double(h.acc) - double(h.comp));
+                continue;
+            }
             s = h.state;
             k = h.step;
             w = h.weight;
             x = h.rng;
             id = h.id;
+            acc = h.acc;
+            comp = h.comp;
         } else {
             const long long e = p.e_begin + t;
-            const int sv = p.start[e];
-            s = sv & 0x7fffffff;
-            w = sv < 0 ? -wnorm : wnorm;
+            if (DIR == MCLSGPU_ADJOINT) {
+                const int sv = p.start[e];
+                s = sv & 0x7fffffff;
+                w = sv < 0 ? -wnorm : wnorm;
+            } else {
+                s = int(e / p.per);
+                w = 1.f;
+            }
             x = counter_state(ekey, 2, uint64_t(e));
             k = 0;
             id = int(e);
@@ -894,29 +932,39 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
             atomicOr(p.status, DEV_ERR_BOUNDS);
             continue;
         }
-        float acc = 0.f, comp = 0.f;
-        while (k < p.L) {
-            walk_step<S, MCLSGPU_ADJOINT, kPacked>(a, rec, s, w, x, acc, comp, k);
+        while (true) {
+            walk_step<S, DIR, kPacked>(a, rec, s, w, x, acc, comp, k);
             ++k;
             ++steps;
-            if (k < p.L && (s < p.row0 || s >= hi)) {
-                int lo = 0, up = p.nparts;  // owner: sb[lo] <= s < sb[lo + 1]
-                while (up - lo > 1) {
-                    const int mid = (lo + up) >> 1;
-                    if (sb[mid] <= s) lo = mid; else up = mid;
+            if (k >= p.L || fabsf(w) < wcut) {
+                if (DIR == MCLSGPU_FORWARD) {
+                    const int s0 = id / p.per;
+                    if (s0 >= p.row0 && s0 < hi) {
+                        atomicAdd(&p.y[s0 - p.row0], double(acc) - double(comp));
+                    } else {
+                        HistoryWire h;
+                        h.rng = 0;
+                        h.state = -1;
+                        h.step = k;
+                        h.weight = w;
+                        h.id = id;
+                        h.acc = acc;
+                        h.comp = comp;
+                        part_send(p, part_owner(sb, p.nparts, s0), h);
+                    }
                 }
-                const unsigned long long slot = atomicAdd(&p.out_cnt[lo], 1ULL);
-                if (slot < (unsigned long long)p.cap) {
-                    HistoryWire h;
-                    h.rng = x;
-                    h.state = s;
-                    h.step = k;
-                    h.weight = w;
-                    h.id = id;
-                    p.out[size_t(lo) * size_t(p.cap) + slot] = h;
-                } else {
-                    atomicOr(p.status, DEV_ERR_CAPACITY);
-                }
+                break;
+            }
+            if (s < p.row0 || s >= hi) {
+                HistoryWire h;
+                h.rng = x;
+                h.state = s;
+                h.step = k;
+                h.weight = w;
+                h.id = id;
+                h.acc = acc;
+                h.comp = comp;
+                part_send(p, part_owner(sb, p.nparts, s), h);
                 break;
             }
         }
@@ -1050,14 +1098,21 @@ void launch_walk_part(const PartWalk& p, mclsgpu_context* ctx) {
     long long g = (nwork + 255) / 256;
     const int grid = int(g < ctx->num_sms * 8 ? g : ctx->num_sms * 8);
     cudaStream_t st = ctx->stream;
-    switch (p.slots) {
-        case 4: walk32_part<4><<<grid, 256, 0, st>>>(p); break;
-        case 8: walk32_part<8><<<grid, 256, 0, st>>>(p); break;
-        case 12: walk32_part<12><<<grid, 256, 0, st>>>(p); break;
-        case 16: walk32_part<16><<<grid, 256, 0, st>>>(p); break;
-        case 24: walk32_part<24><<<grid, 256, 0, st>>>(p); break;
-        default: walk32_part<32><<<grid, 256, 0, st>>>(p); break;
+#define MCLSGPU_PART_SLOTS(D)                                   \
+    switch (p.slots) {                                          \
+        case 4: walk32_part<4, D><<<grid, 256, 0, st>>>(p); break;   \
+        case 8: walk32_part<8, D><<<grid, 256, 0, st>>>(p); break;   \
+        case 12: walk32_part<12, D><<<grid, 256, 0, st>>>(p); break; \
+        case 16: walk32_part<16, D><<<grid, 256, 0, st>>>(p); break; \
+        case 24: walk32_part<24, D><<<grid, 256, 0, st>>>(p); break; \
+        default: walk32_part<32, D><<<grid, 256, 0, st>>>(p); break; \
     }
+    if (p.dir == MCLSGPU_FORWARD) {
+        MCLSGPU_PART_SLOTS(MCLSGPU_FORWARD)
+    } else {
+        MCLSGPU_PART_SLOTS(MCLSGPU_ADJOINT)
+    }
+#undef MCLSGPU_PART_SLOTS
 }
 
 }  // namespace mclsgpu

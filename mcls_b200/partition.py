@@ -7,13 +7,17 @@ leave a rank's rows to the owning rank through buffered messages
 src/MCLS_DomainCommunicator_impl.hpp, src/MCLS_SourceTransporter_impl.hpp).
 Here a part is a `capi.Subdomain`; one Monte Carlo solve is
 
-    begin       every part builds the global source of the residual and
-                keeps the histories that start in its rows
+    begin       adjoint: every part builds the global source of the
+                residual and keeps the histories that start in its rows;
+                forward: every part takes the histories of its own rows and
+                the tally source of its rows
     rounds      every part walks its histories until they end or cross;
-                the departures (24-byte history records) are exchanged
-                -- all-to-all between ranks, device copies between the parts
-                of one process -- and walked by their new owners, until no
-                part has departures in a round
+                the departures (32-byte history records; forward sums of
+                histories that ended away from their start row go home as
+                tally returns) are exchanged -- all-to-all between ranks,
+                device copies between the parts of one process -- and
+                walked by their new owners, until no part has departures in
+                a round
     finish      every part normalises the tallies of its rows.
 
 Every rank takes the same collective steps in the same order (two
@@ -29,9 +33,9 @@ import scipy.sparse as sp
 
 from . import capi
 
-#: mclsgpu_history_wire (24 bytes).
+#: mclsgpu_history_wire (32 bytes).
 WIRE_DTYPE = np.dtype([("rng", "<u8"), ("state", "<i4"), ("step", "<i4"), ("weight", "<f4"),
-                       ("id", "<i4")])
+                       ("id", "<i4"), ("acc", "<f4"), ("comp", "<f4")])
 WIRE_BYTES = WIRE_DTYPE.itemsize
 
 
@@ -49,6 +53,17 @@ def transposed_composite(A, left_diag_inv=None):
         T = sp.csr_matrix(T.multiply(np.asarray(left_diag_inv)[None, :]))
     T.sort_indices()
     return T
+
+
+def composite(A, left_diag_inv=None):
+    """PL A on the host as the library's forward domain build forms it: with
+    a point-Jacobi PL (left_diag_inv = 1 / diag(A)) row i is scaled,
+    entry (i, j) = (1 / A_ii) * A_ij."""
+    M = sp.csr_matrix(A, copy=True)
+    if left_diag_inv is not None:
+        M = sp.csr_matrix(sp.diags(np.asarray(left_diag_inv)) @ M)
+    M.sort_indices()
+    return M
 
 
 class DevicePart:

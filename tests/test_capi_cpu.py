@@ -58,6 +58,7 @@ int main(void) {
   F(mclsgpu_anderson_params, host_loop)
   F(mclsgpu_history_wire, state) F(mclsgpu_history_wire, step)
   F(mclsgpu_history_wire, weight) F(mclsgpu_history_wire, id)
+  F(mclsgpu_history_wire, acc) F(mclsgpu_history_wire, comp)
   return 0;
 }
 """)
@@ -86,7 +87,7 @@ int main(void) {
     from mcls_b200 import partition
 
     assert int(out["wire"]) == partition.WIRE_BYTES == capi.load().mclsgpu_history_wire_size()
-    for f in ("state", "step", "weight", "id"):
+    for f in ("state", "step", "weight", "id", "acc", "comp"):
         assert int(out["mclsgpu_history_wire." + f]) == partition.WIRE_DTYPE.fields[f][1]
 
 

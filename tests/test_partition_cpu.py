@@ -1,7 +1,9 @@
 """Domain-decomposed transport host logic across processes over gloo (CPU).
 
 Two and three ranks each own a block of rows and walk a deterministic toy
-history set in the library's 24-byte history records; the product's driver
+history set (adjoint tallies where the history stands; forward sums that go
+home to their start row) in the library's 32-byte history records; the
+product's driver
 (mcls_b200.partition.solve_distributed) runs the rounds, the all-to-all
 exchanges and the termination test.  The ranks' tallies, put together, must
 equal the same walk done in one piece, and histories must have crossed.
@@ -24,8 +26,9 @@ def _free_port():
         return s.getsockname()[1]
 
 
+@pytest.mark.parametrize("mode", ["adjoint", "forward"])
 @pytest.mark.parametrize("world", [2, 3])
-def test_partitioned_walk_equals_whole_walk(tmp_path, world):
+def test_partitioned_walk_equals_whole_walk(tmp_path, world, mode):
     port = _free_port()
     procs, outs = [], []
     for r in range(world):
@@ -34,7 +37,7 @@ def test_partitioned_walk_equals_whole_walk(tmp_path, world):
         env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(world),
                    MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
         procs.append(subprocess.Popen([sys.executable, os.path.join(ROOT, "tests",
-                                                                    "partition_worker.py"), out],
+                                                                    "partition_worker.py"), out, mode],
                                       env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
     logs = []
     for p in procs:
