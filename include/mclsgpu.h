@@ -332,9 +332,9 @@ typedef struct {
 } mclsgpu_domain_info;
 int mclsgpu_domain_query(mclsgpu_domain* dom, mclsgpu_domain_info* info);
 
-/* FP32 walk launch shape: histories carried per lane (1, 2 or 4; 2 applies
- * to fixed-length histories on records of at most 64 bytes, 4 to
- * fixed-length histories on 32-byte records, others fall back to fewer) and
+/* FP32 walk launch shape: histories carried per lane (1, 2, 4 or 8; 2
+ * applies to fixed-length histories on records of at most 64 bytes, 4 and 8
+ * to fixed-length histories on 32-byte records, others fall back to fewer) and
  * threads per block (128 or 256).  No counterpart in the reference. */
 int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane,
                               int block_size);

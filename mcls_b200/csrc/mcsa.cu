@@ -1265,7 +1265,9 @@ int mclsgpu_domain_residual(mclsgpu_domain* dom, double* rp_dev) {
 }
 
 int mclsgpu_domain_set_launch(mclsgpu_domain* dom, int histories_per_lane, int block_size) {
-    if (!dom || (histories_per_lane != 1 && histories_per_lane != 2 && histories_per_lane != 4) ||
+    if (!dom ||
+        (histories_per_lane != 1 && histories_per_lane != 2 && histories_per_lane != 4 &&
+         histories_per_lane != 8) ||
         (block_size != 128 && block_size != 256))
         return MCLSGPU_ERR_INVALID_ARG;
     dom->walk_ilp = histories_per_lane;
@@ -1297,17 +1299,18 @@ int mclsgpu_domain_autotune(mclsgpu_domain* dom, const double* rhs_dev, int reps
     cudaMemcpyAsync(&saved[1], dom->d_pos, sizeof(saved[1]), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(dom->ctx, e, "autotune");
-    // Four histories per lane apply to fixed-length histories on 32-byte
-    // records only.
+    // Four or eight histories per lane apply to fixed-length histories on
+    // 32-byte records only.
     const bool four = dom->slots == 4 && !(dom->p.weight_cutoff > 0.0);
     // Each shape with the record loads bypassing L1 and allocated in it.
-    const int shapes[12][3] = {{1, 256, 0}, {2, 256, 0}, {1, 128, 0}, {2, 128, 0},
-                               {4, 256, 0}, {4, 128, 0}, {1, 256, 1}, {2, 256, 1},
-                               {1, 128, 1}, {2, 128, 1}, {4, 256, 1}, {4, 128, 1}};
+    const int shapes[16][3] = {{1, 256, 0}, {2, 256, 0}, {1, 128, 0}, {2, 128, 0},
+                               {4, 256, 0}, {4, 128, 0}, {8, 256, 0}, {8, 128, 0},
+                               {1, 256, 1}, {2, 256, 1}, {1, 128, 1}, {2, 128, 1},
+                               {4, 256, 1}, {4, 128, 1}, {8, 256, 1}, {8, 128, 1}};
     double best = 1e300;
     int bh = 1, bb = 256, bl = 0;
     for (const auto& sh : shapes) {
-        if (sh[0] == 4 && !four) continue;
+        if (sh[0] >= 4 && !four) continue;
         int rc = mclsgpu_domain_set_launch(dom, sh[0], sh[1]);
         if (!rc) rc = mclsgpu_domain_set_record_cache(dom, sh[2]);
         if (rc) return rc;

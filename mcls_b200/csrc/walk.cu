@@ -257,8 +257,10 @@ __device__ __forceinline__ void walk_start(const WalkArgs& a, int e, uint64_t ek
 // termination checks.  Otherwise lanes refill one by one from the queue as
 // their histories terminate.
 template <int S, int DIR, int ST, bool FIXED, int ILP = 1>
-__global__ void __launch_bounds__(256, ILP == 1 ? WalkOccupancy<S>::kMinBlocks
-                                                 : (ILP == 2 ? 5 : 4))
+__global__ void __launch_bounds__(256, ILP == 1   ? WalkOccupancy<S>::kMinBlocks
+                                      : ILP == 2 ? 5
+                                      : ILP == 4 ? 4
+                                                 : 3)
     walk32(WalkArgs a) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
@@ -463,8 +465,8 @@ void launch32_slots(int slots, const WalkArgs& a, int sms, int block, cudaStream
         else                                                                              \
             blocks_per_sm<SL, DIR, ST, FX, ILP>(block);                                   \
         break;
-    if constexpr (ILP == 4) {
-        // four histories per lane: 32-byte records only
+    if constexpr (ILP >= 4) {
+        // four or eight histories per lane: 32-byte records only
         switch (slots) {
             default:
                 MCLSGPU_WALK_CASE(4)
@@ -503,12 +505,14 @@ void dispatch_walk32(const mclsgpu_domain* dom, const WalkArgs& a, bool launch) 
     const bool fixed = !(dom->p.weight_cutoff > 0.0);
     // Several histories per lane only for fixed-length histories: two on
     // records of at most 8 slots (the register budget of 5 blocks per SM),
-    // four on 32-byte records (4 blocks per SM).
-    const bool ilp4 = fixed && dom->walk_ilp == 4 && dom->slots == 4;
-    const bool ilp2 = fixed && dom->walk_ilp >= 2 && dom->slots <= 8 && !ilp4;
+    // four or eight on 32-byte records (4 or 3 blocks per SM).
+    const bool ilp8 = fixed && dom->walk_ilp == 8 && dom->slots == 4;
+    const bool ilp4 = fixed && dom->walk_ilp >= 4 && dom->slots == 4 && !ilp8;
+    const bool ilp2 = fixed && dom->walk_ilp >= 2 && dom->slots <= 8 && !ilp4 && !ilp8;
     const int block = dom->walk_block;
 #define MCLSGPU_WALK_DIR(DIRV, STV)                                                           \
-    (ilp4   ? launch32_slots<DIRV, STV, true, 4>(dom->slots, a, sms, block, st, launch)       \
+    (ilp8   ? launch32_slots<DIRV, STV, true, 8>(dom->slots, a, sms, block, st, launch)       \
+     : ilp4 ? launch32_slots<DIRV, STV, true, 4>(dom->slots, a, sms, block, st, launch)       \
      : ilp2 ? launch32_slots<DIRV, STV, true, 2>(dom->slots, a, sms, block, st, launch)       \
      : fixed ? launch32_slots<DIRV, STV, true, 1>(dom->slots, a, sms, block, st, launch)      \
              : launch32_slots<DIRV, STV, false, 1>(dom->slots, a, sms, block, st, launch))
