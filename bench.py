@@ -66,7 +66,8 @@ CONFIGS = {
                               "histories per row per iteration: point Jacobi vs block Jacobi "
                               "(4 along x) vs learned SPAI (network trained on 2,000 seeded "
                               "systems of the family)",
-                     n=512, sample_ratio=2.0, estimator=1, history_length=10, direction=1),
+                     n=512, sample_ratio=2.0, estimator=1, history_length=10, direction=1,
+                     max_iters=100000),
 }
 # DRAM bytes (read + write) of one walk launch on each workload: ncu's
 # dram__bytes_read.sum (83.90 MB) + dram__bytes_write.sum (7.82 MB) for the
@@ -654,9 +655,10 @@ def hbm_walk_roofline(args, ctx, n=192, reps=10):
 
 
 def _aniso_solve(args, ctx, op, A, b, kind, cfgd, net=None, block=4, rho_fallback=2.0,
-                 record_format=0):
+                 record_format=0, anderson_depth=0):
     """One timed MCSA solve of the anisotropic system (after one warm-up
-    solve); divergence (non-finite weights or residual) is reported, not
+    solve), and with anderson_depth the Anderson-accelerated solve on the same
+    domain; divergence (non-finite weights or residual) is reported, not
     raised."""
     import torch
 
@@ -696,6 +698,15 @@ def _aniso_solve(args, ctx, op, A, b, kind, cfgd, net=None, block=4, rho_fallbac
                     "rel_residual_b_minus_Ax": float(np.linalg.norm(b - A @ x) /
                                                      np.linalg.norm(b)),
                     "walk_ms_per_launch": st["walk_ms"] / max(st["walk_launches"], 1)})
+        if anderson_depth:
+            try:
+                aa = anderson_arm(args, anderson_depth, dom, bt, xt, A, b, args.seed,
+                                  st["solve_ms"] if st["converged"] else float("nan"),
+                                  PL=pc.to_scipy(A.shape[0]))
+                aa["speedup_vs_this_mcsa"] = aa.pop("speedup_vs_jacobi_mcsa")
+            except capi.MclsError as e:
+                aa = {"converged": False, "storage_depth": anderson_depth, "error": str(e)}
+            out["anderson"] = aa
     except capi.MclsError as e:
         out.update({"converged": False, "diverged": e.code == capi.ERR_DIVERGED,
                     "error": str(e), "time_to_1e-8_s": None})
@@ -753,7 +764,8 @@ def run_aniso(args, world, rank, local, pg):
             "block_jacobi": _aniso_solve(args, ctx, op, A, b, capi.PREC_BLOCK_JACOBI, cfgd,
                                          record_format=capi.RECORD_STENCIL16),
             "learned_spai": _aniso_solve(args, ctx, op, A, b, capi.PREC_LEARNED_SPAI, cfgd,
-                                         net=net, record_format=capi.RECORD_STENCIL16)}
+                                         net=net, record_format=capi.RECORD_STENCIL16,
+                                         anderson_depth=0 if args.no_anderson else 6)}
     from oracle import oracle as O
 
     O.set_threads(os.cpu_count() or 1)

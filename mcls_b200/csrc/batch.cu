@@ -48,18 +48,32 @@ inline int grid_for(long long work, int threads = kThreads, int cap = 148 * 8) {
 }
 
 struct BatchArgs {
-    BatchClasses cls;
-    long long ne;        // elements (padding included)
     int nsys;
     int pw;              // per-pair row width: pair (s, r) is s * pw + r
+    int per;             // histories per row
     const int* rp;       // S (CSR)
     const int* ci;
     const double* v;
     const double* dinv;  // D^-1
-    const int* rsys;     // row -> system
     const int* hrp;      // H rows (forward domain, FP64)
     const int* hci;
     const double* hv;
+    // Per system: first row, first element, log2 of its width, rows.
+    const int* srow0;
+    const long long* seoff;
+    const int* slog;
+    const int* sn;
+    const int* sorder;   // the systems in placement order
+    // The systems this launch works on: lsys[k] for k < *lcount, their
+    // elements at [lecum[k], lecum[k+1]) of the launch's element space.
+    const int* lsys;
+    const long long* lecum;
+    const int* lcount;
+    // The active list the convergence test rebuilds (the iteration's list).
+    int* act_sys;
+    long long* act_ecum;
+    int* act_hcum;
+    int* act_count;
     const double* B;
     double* X;
     double* X2;
@@ -72,7 +86,6 @@ struct BatchArgs {
     int* conv_iter;      // [nsys][pw]
     const int* nrhs;
     int* sys_done;       // per system: every right-hand side converged
-    int skip;            // skip the rows of finished systems
     BatchState* st;
     unsigned* blocks_done;
     double omega;        // Richardson relaxation
@@ -85,68 +98,97 @@ struct BatchArgs {
     int* status;
 };
 
-// Element t -> row i, column r and width class c (false for the padding
-// between classes).
-__device__ __forceinline__ bool elem_map(const BatchClasses& k, long long t, int& i, int& r,
-                                         int& c) {
-    c = 0;
-    while (c < 4 && t >= k.cel[c + 1]) ++c;
-    const long long local = t - k.cel[c];
-    const long long row = k.crow[c] + (local >> c);
-    if (row >= k.crow[c + 1]) return false;
-    i = int(row);
-    r = int(local & ((1 << c) - 1));
-    return true;
+// One element of a launch's element space: system s, row i, column r, log2
+// width c, its index e in the element arrays and the element index of its
+// row's column 0 minus the row times the width (so that the element of row j,
+// column r of the same system is base + (j << c) + r).
+struct Elem {
+    int s, i, r, c;
+    size_t e;
+    long long base;
+};
+
+// The list entry k with lecum[k] <= t < lecum[k+1] (count >= 1 entries).
+__device__ __forceinline__ int elem_entry(const long long* lecum, int count, long long t) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (lecum[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
 }
 
-// The element of row j, column r, in class c (j in c's rows).
-__device__ __forceinline__ size_t elem_of(const BatchClasses& k, int c, int j, int r) {
-    return size_t(k.cel[c] + ((long long)(j - k.crow[c]) << c) + r);
+// Element t of the launch (t < lecum[count]), starting the entry search at
+// k0 (the entry of the block's first element).
+__device__ __forceinline__ Elem elem_at(const BatchArgs& a, int count, int k0, long long t) {
+    int k = k0;
+    while (k + 1 < count && t >= a.lecum[k + 1]) ++k;
+    Elem q;
+    q.s = a.lsys[k];
+    q.c = a.slog[q.s];
+    const long long local = t - a.lecum[k];
+    q.i = a.srow0[q.s] + int(local >> q.c);
+    q.r = int(local & ((1 << q.c) - 1));
+    q.e = size_t(a.seoff[q.s] + local);
+    q.base = a.seoff[q.s] - ((long long)a.srow0[q.s] << q.c);
+    return q;
 }
 
-// Every per-element kernel runs one thread per (row, column) element: with
-// the row-major class blocks a warp reads whole rows of X, RP and B at every
-// matrix entry, so loads and stores are coalesced.
+// Grid-stride loop over the launch's elements, block by block: the block's
+// first thread finds the list entry of the block's first element.  body(live,
+// q) runs on every thread of the block for every block-sized tile (block-
+// uniform trip count, so body may use warp collectives).
+template <class Body>
+__device__ __forceinline__ void for_elements(const BatchArgs& a, Body body) {
+    __shared__ int s_k0;
+    const int count = *a.lcount;
+    const long long total = count > 0 ? a.lecum[count] : 0;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < total;
+         base += (long long)gridDim.x * blockDim.x) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_k0 = elem_entry(a.lecum, count, base);
+        __syncthreads();
+        const long long t = base + threadIdx.x;
+        const bool live = t < total;
+        Elem q{};
+        if (live) q = elem_at(a, count, s_k0, t);
+        body(live, q);
+    }
+}
 
 // x2 = x + w rp;  rp2 = D^-1 (b - S x2), with x2 at the neighbours formed on
 // the fly (RichardsonIteration::doOneIteration then updatePrecResidual,
 // src/MCLS_RichardsonIteration_impl.hpp:134-147); the walk tallies Y are
 // cleared for this iteration's walk.
 __global__ void __launch_bounds__(kThreads) k_b_richardson_residual(BatchArgs a) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.ne;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i, r, c;
-        if (!elem_map(a.cls, t, i, r, c)) continue;
-        if (a.skip && a.sys_done[a.rsys[i]]) continue;
+    for_elements(a, [&](bool live, const Elem& q) {
+        if (!live) return;
         double acc = 0.0;
-        for (int p = a.rp[i]; p < a.rp[i + 1]; ++p) {
-            const size_t k = elem_of(a.cls, c, a.ci[p], r);
+        for (int p = a.rp[q.i]; p < a.rp[q.i + 1]; ++p) {
+            const size_t k = size_t(q.base + ((long long)a.ci[p] << q.c) + q.r);
             acc = fma(a.v[p], __dadd_rn(a.X[k], __dmul_rn(a.omega, a.RP[k])), acc);
         }
-        a.X2[t] = __dadd_rn(a.X[t], __dmul_rn(a.omega, a.RP[t]));
-        a.RP2[t] = a.dinv[i] * (a.B[t] - acc);
-        a.Y[t] = 0.0;
-    }
+        a.X2[q.e] = __dadd_rn(a.X[q.e], __dmul_rn(a.omega, a.RP[q.e]));
+        a.RP2[q.e] = a.dinv[q.i] * (a.B[q.e] - acc);
+        a.Y[q.e] = 0.0;
+    });
 }
 
 // Tally source of every right-hand side: expected value c = H (w rp2),
 // collision c = w rp2 (FP32).
 __global__ void __launch_bounds__(kThreads) k_b_source(BatchArgs a) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.ne;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i, r, c;
-        if (!elem_map(a.cls, t, i, r, c)) continue;
-        if (a.skip && a.sys_done[a.rsys[i]]) continue;  // walks skip these rows too
+    for_elements(a, [&](bool live, const Elem& q) {
+        if (!live) return;
         double v;
         if (a.ev) {
             v = 0.0;
-            for (int p = a.hrp[i]; p < a.hrp[i + 1]; ++p)
-                v = fma(a.hv[p], a.RP2[elem_of(a.cls, c, a.hci[p], r)], v);
+            for (int p = a.hrp[q.i]; p < a.hrp[q.i + 1]; ++p)
+                v = fma(a.hv[p], a.RP2[size_t(q.base + ((long long)a.hci[p] << q.c) + q.r)], v);
         } else {
-            v = a.RP2[t];
+            v = a.RP2[q.e];
         }
-        a.cR[t] = __double2float_rn(a.nomega * v);
-    }
+        a.cR[q.e] = __double2float_rn(a.nomega * v);
+    });
 }
 
 // The corrected iterate at element k: x2 + Y / per (+ w rp2 for the expected
@@ -158,9 +200,65 @@ __device__ __forceinline__ double corrected(const BatchArgs& a, size_t k) {
     return a.X2[k] + d;
 }
 
+// The active list from sys_done, in placement order, by one block: each
+// thread counts a contiguous run of systems, a block scan places the runs.
+__device__ void build_active(const BatchArgs& a) {
+    __shared__ int s_cnt[1024];
+    __shared__ long long s_el[1024];
+    __shared__ int s_h[1024];
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int seg = (a.nsys + T - 1) / T;
+    const int j0 = min(tid * seg, a.nsys), j1 = min(j0 + seg, a.nsys);
+    int cnt = 0, hs = 0;
+    long long el = 0;
+    for (int j = j0; j < j1; ++j) {
+        const int s = a.sorder[j];
+        if (a.sys_done[s]) continue;
+        ++cnt;
+        el += (long long)a.sn[s] << a.slog[s];
+        hs += a.sn[s] * a.per;
+    }
+    s_cnt[tid] = cnt;
+    s_el[tid] = el;
+    s_h[tid] = hs;
+    __syncthreads();
+    for (int d = 1; d < T; d <<= 1) {  // inclusive scan (Hillis-Steele)
+        int c2 = 0, h2 = 0;
+        long long e2 = 0;
+        if (tid >= d) {
+            c2 = s_cnt[tid - d];
+            e2 = s_el[tid - d];
+            h2 = s_h[tid - d];
+        }
+        __syncthreads();
+        s_cnt[tid] += c2;
+        s_el[tid] += e2;
+        s_h[tid] += h2;
+        __syncthreads();
+    }
+    int k = s_cnt[tid] - cnt;
+    long long eo = s_el[tid] - el;
+    int ho = s_h[tid] - hs;
+    for (int j = j0; j < j1; ++j) {
+        const int s = a.sorder[j];
+        if (a.sys_done[s]) continue;
+        a.act_sys[k] = s;
+        a.act_ecum[k] = eo;
+        a.act_hcum[k] = ho;
+        eo += (long long)a.sn[s] << a.slog[s];
+        ho += a.sn[s] * a.per;
+        ++k;
+    }
+    if (tid == T - 1) {
+        *a.act_count = s_cnt[tid];
+        a.act_ecum[s_cnt[tid]] = s_el[tid];
+        a.act_hcum[s_cnt[tid]] = s_h[tid];
+    }
+}
+
 // Per-pair convergence, loop control and the per-iteration bookkeeping (new
-// stream epoch, work-queue reset, walk timing, norms cleared), run by one
-// block.
+// stream epoch, work-queue reset, walk timing, norms cleared, the active
+// list rebuilt), run by one block.
 __device__ void batch_check(const BatchArgs& a, int use_cond, cudaGraphConditionalHandle handle) {
     __shared__ int s_conv;
     if (threadIdx.x == 0) s_conv = 0;
@@ -187,6 +285,8 @@ __device__ void batch_check(const BatchArgs& a, int use_cond, cudaGraphCondition
         for (int r = 0; r < a.nrhs[s]; ++r) all &= a.conv_iter[size_t(s) * a.pw + r] >= 0;
         a.sys_done[s] = all;
     }
+    __syncthreads();
+    build_active(a);
     if (threadIdx.x == 0) {
         st.iter = it;
         st.converged = s_conv;
@@ -206,46 +306,41 @@ __device__ void batch_check(const BatchArgs& a, int use_cond, cudaGraphCondition
 
 // rp = D^-1 (b - S x) and the per-(system, rhs) sums of squares.  CORR: x is
 // this iteration's corrected iterate (formed on the fly at the neighbours
-// and written to X), otherwise Xin.  A warp covers 32/W rows of one class:
-// when they all belong to one system the lanes of each column reduce with
-// shuffles and one lane per column adds the sum, otherwise every lane adds
-// its own square.  CHECK: the last block to finish runs the convergence
-// test (the other blocks' sums are complete and visible by then).
+// and written to X), otherwise Xin.  A warp covers 32/W rows: when they all
+// belong to one system the lanes of each column reduce with shuffles and one
+// lane per column adds the sum, otherwise every lane adds its own square.
+// CHECK: the last block to finish runs the convergence test (the other
+// blocks' sums are complete and visible by then).
 template <bool CORR, bool CHECK>
 __global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double* Xin, int use_cond,
                                                        cudaGraphConditionalHandle handle) {
     const unsigned full = 0xffffffffu;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < a.ne;
-         base += (long long)gridDim.x * blockDim.x) {
-        const long long t = base + threadIdx.x;
+    for_elements(a, [&](bool live, const Elem& q) {
         double sq = 0.0;
-        int sys = -1, r = 0, c = 0, i = 0;
-        if (t < a.ne && elem_map(a.cls, t, i, r, c)) {
-            sys = a.rsys[i];
-            if (!(a.skip && a.sys_done[sys])) {
-                double acc = 0.0;
-                for (int p = a.rp[i]; p < a.rp[i + 1]; ++p) {
-                    const size_t k = elem_of(a.cls, c, a.ci[p], r);
-                    acc = fma(a.v[p], CORR ? corrected(a, k) : Xin[k], acc);
-                }
-                if (CORR) a.X[t] = corrected(a, size_t(t));
-                const double rv = a.dinv[i] * (a.B[t] - acc);
-                a.RP[t] = rv;
-                sq = rv * rv;
+        const int sys = live ? q.s : -1;
+        if (live) {
+            double acc = 0.0;
+            for (int p = a.rp[q.i]; p < a.rp[q.i + 1]; ++p) {
+                const size_t k = size_t(q.base + ((long long)a.ci[p] << q.c) + q.r);
+                acc = fma(a.v[p], CORR ? corrected(a, k) : Xin[k], acc);
             }
+            if (CORR) a.X[q.e] = corrected(a, q.e);
+            const double rv = a.dinv[q.i] * (a.B[q.e] - acc);
+            a.RP[q.e] = rv;
+            sq = rv * rv;
         }
         const int s0 = __shfl_sync(full, sys, 0);
-        const int c0 = __shfl_sync(full, c, 0);
+        const int c0 = __shfl_sync(full, q.c, 0);
         const bool uniform = __all_sync(full, sys == s0) && s0 >= 0;
         if (uniform) {
             double v = sq;
             for (int d = 16; d >= (1 << c0); d >>= 1) v += __shfl_xor_sync(full, v, d);
             if ((threadIdx.x & 31) < (1 << c0) && v != 0.0)
-                atomicAdd(&a.norm2[size_t(s0) * a.pw + r], v);
+                atomicAdd(&a.norm2[size_t(s0) * a.pw + q.r], v);
         } else if (sys >= 0 && sq != 0.0) {
-            atomicAdd(&a.norm2[size_t(sys) * a.pw + r], sq);
+            atomicAdd(&a.norm2[size_t(sys) * a.pw + q.r], sq);
         }
-    }
+    });
     if (CHECK) {
         __shared__ bool s_last;
         __threadfence();
@@ -260,39 +355,40 @@ __global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double
     }
 }
 
-// Before the loop: sums of squares of D^-1 b per pair.
+// Before the loop: sums of squares of D^-1 b per pair (every system).
 __global__ void k_b_init_norms(BatchArgs a) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.ne;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i, r, c;
-        if (!elem_map(a.cls, t, i, r, c)) continue;
-        const double v = a.dinv[i] * a.B[t];
-        if (v != 0.0) atomicAdd(&a.bnorm2[size_t(a.rsys[i]) * a.pw + r], v * v);
-    }
+    for_elements(a, [&](bool live, const Elem& q) {
+        if (!live) return;
+        const double v = a.dinv[q.i] * a.B[q.e];
+        if (v != 0.0) atomicAdd(&a.bnorm2[size_t(q.s) * a.pw + q.r], v * v);
+    });
 }
 
-__global__ void k_b_state_init(BatchState* st, int max_iters, int check_freq, double tol, int pairs,
-                               int* conv_iter, int count, double* norm2, int* sys_done,
-                               int nsys) {
+// Loop state, per-pair bookkeeping and the active list (every system), by
+// one block.
+__global__ void k_b_state_init(BatchArgs a, int max_iters, int check_freq, double tol,
+                               int pairs) {
+    const int count = a.nsys * a.pw;
     for (int q = threadIdx.x; q < count; q += blockDim.x) {
-        conv_iter[q] = -1;
-        norm2[q] = 0.0;
+        a.conv_iter[q] = -1;
+        a.norm2[q] = 0.0;
     }
-    for (int q = threadIdx.x; q < nsys; q += blockDim.x) sys_done[q] = 0;
+    for (int q = threadIdx.x; q < a.nsys; q += blockDim.x) a.sys_done[q] = 0;
+    __syncthreads();
+    build_active(a);
     if (threadIdx.x == 0) {
         BatchState s{};
         s.max_iters = max_iters;
         s.check_freq = check_freq;
         s.tol = tol;
         s.pairs = pairs;
-        *st = s;
+        *a.st = s;
     }
 }
 
-__global__ void k_b_forward_nh(int* d_nh, int nh) { *d_nh = nh; }
-
 }  // namespace
 }  // namespace mclsgpu
+
 
 struct mclsgpu_batch {
     mclsgpu_context* ctx = nullptr;
@@ -308,8 +404,22 @@ struct mclsgpu_batch {
     mclsgpu_operator* op = nullptr;
     mclsgpu_precond* pc = nullptr;
     mclsgpu_domain* dom = nullptr;
-    int* d_rsys = nullptr;
     int* d_nrhs = nullptr;
+    // Per system (device): first row, first element, log2 width, rows, and
+    // the systems in placement order.
+    int* d_srow0 = nullptr;
+    long long* d_seoff = nullptr;
+    int* d_slog = nullptr;
+    int* d_sn = nullptr;
+    int* d_sorder = nullptr;
+    // The active list (rebuilt every iteration) and the list of every system.
+    int* act_sys = nullptr;
+    long long* act_ecum = nullptr;
+    int* act_hcum = nullptr;
+    int* act_count = nullptr;
+    int* all_sys = nullptr;
+    long long* all_ecum = nullptr;
+    int* all_count = nullptr;
     double *X = nullptr, *X2 = nullptr, *RP = nullptr, *RP2 = nullptr, *B = nullptr, *Y = nullptr;
     float* cR = nullptr;
     double* norm2 = nullptr;
@@ -334,8 +444,19 @@ void batch_release(mclsgpu_batch* b) {
     if (b->dom) mclsgpu_domain_destroy(b->dom);
     if (b->pc) mclsgpu_precond_destroy(b->pc);
     if (b->op) mclsgpu_operator_destroy(b->op);
-    dfree(b->d_rsys);
     dfree(b->d_nrhs);
+    dfree(b->d_srow0);
+    dfree(b->d_seoff);
+    dfree(b->d_slog);
+    dfree(b->d_sn);
+    dfree(b->d_sorder);
+    dfree(b->act_sys);
+    dfree(b->act_ecum);
+    dfree(b->act_hcum);
+    dfree(b->act_count);
+    dfree(b->all_sys);
+    dfree(b->all_ecum);
+    dfree(b->all_count);
     dfree(b->X);
     dfree(b->X2);
     dfree(b->RP);
@@ -353,21 +474,32 @@ void batch_release(mclsgpu_batch* b) {
     delete b;
 }
 
-BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
+// Kernel arguments over the active list (all = false) or every system.
+BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp, bool all) {
     const mclsgpu_mc_params& p = b->dom->p;
     BatchArgs a{};
-    a.cls = b->cls;
-    a.ne = b->ne;
     a.nsys = b->nsys;
     a.pw = b->pw;
+    a.per = b->per;
     a.rp = b->op->A.rp;
     a.ci = b->op->A.ci;
     a.v = b->op->A.v;
     a.dinv = b->pc->diag;
-    a.rsys = b->d_rsys;
     a.hrp = b->dom->D.rp;
     a.hci = b->dom->D.ci;
     a.hv = b->dom->D.v;
+    a.srow0 = b->d_srow0;
+    a.seoff = b->d_seoff;
+    a.slog = b->d_slog;
+    a.sn = b->d_sn;
+    a.sorder = b->d_sorder;
+    a.lsys = all ? b->all_sys : b->act_sys;
+    a.lecum = all ? b->all_ecum : b->act_ecum;
+    a.lcount = all ? b->all_count : b->act_count;
+    a.act_sys = b->act_sys;
+    a.act_ecum = b->act_ecum;
+    a.act_hcum = b->act_hcum;
+    a.act_count = b->act_count;
     a.B = b->B;
     a.X = b->X;
     a.X2 = b->X2;
@@ -380,7 +512,6 @@ BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     a.conv_iter = b->conv_iter;
     a.nrhs = b->d_nrhs;
     a.sys_done = b->sys_done;
-    a.skip = 1;
     a.st = b->d_state;
     a.blocks_done = b->blocks_done;
     a.omega = mp ? mp->richardson_omega : 1.0;
@@ -394,15 +525,16 @@ BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp) {
     return a;
 }
 
-// One batched MCSA iteration (4 kernels).
+// One batched MCSA iteration (4 kernels) over the active systems.
 int enqueue_batch_iteration(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp, int use_cond,
                             cudaGraphConditionalHandle handle) {
     cudaStream_t s = b->ctx->stream;
-    BatchArgs a = batch_args(b, mp);
+    BatchArgs a = batch_args(b, mp, false);
     const int grid = grid_for(b->ne);
     k_b_richardson_residual<<<grid, kThreads, 0, s>>>(a);
     k_b_source<<<grid, kThreads, 0, s>>>(a);
-    int rc = launch_walk_batch(b->dom, b->cls, b->cR, b->Y, b->d_rsys, b->sys_done, b->grab);
+    const BatchList list{b->act_sys, b->act_hcum, b->act_count, b->d_srow0};
+    int rc = launch_walk_batch(b->dom, b->cls, list, b->cR, b->Y, b->grab);
     if (rc) return rc;
     k_b_update<true, true><<<grid, kThreads, 0, s>>>(a, nullptr, use_cond, handle);
     return MCLSGPU_OK;
@@ -487,13 +619,11 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
     // The block-diagonal operator in placement order.
     std::vector<int64_t> rp(N + 1), ci(nnz);
     std::vector<double> v(nnz);
-    std::vector<int> rsys(N);
     int64_t pos = 0;
     for (int s : order) {
         const int64_t o = row0[s];
         for (int64_t i = 0; i < n[s]; ++i) {
             rp[o + i] = pos;
-            rsys[o + i] = s;
             for (int64_t p = rowptr[s][i]; p < rowptr[s][i + 1]; ++p, ++pos) {
                 if (colind[s][p] < 0 || colind[s][p] >= n[s])
                     return set_error(ctx, MCLSGPU_ERR_INVALID_ARG,
@@ -516,6 +646,22 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
     b->width = width;
     b->nrhs.assign(nrhs, nrhs + nsys);
     b->per = params->sample_ratio > 0.0 ? int(std::ceil(params->sample_ratio)) : 1;
+    if (double(N) * b->per >= double(int64_t(1) << 31)) {
+        delete b;
+        return set_error(ctx, MCLSGPU_ERR_UNSUPPORTED, "batch too large (histories per iteration)");
+    }
+    // Per-system tables and the list of every system (placement order).
+    std::vector<int> srow0(nsys), sn(nsys), all_count(1, nsys);
+    std::vector<long long> seoff(nsys), all_ecum(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+        srow0[s] = int(row0[s]);
+        seoff[s] = eoff[s];
+        sn[s] = int(n[s]);
+    }
+    for (int k = 0; k < nsys; ++k) {
+        const int s = order[k];
+        all_ecum[k + 1] = all_ecum[k] + ((long long)n[s] << cls_of[s]);
+    }
     int rc = mclsgpu_operator_upload(ctx, N, rp.data(), ci.data(), v.data(), &b->op);
     mclsgpu_precond_params pp{};
     pp.size = sizeof(pp);
@@ -536,7 +682,18 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
     const size_t PR = size_t(nsys) * pw;
     cudaError_t e = cudaSuccess;
     if (!rc &&
-        ((e = dmalloc(&b->d_rsys, N)) != cudaSuccess || (e = dmalloc(&b->d_nrhs, nsys)) != cudaSuccess ||
+        ((e = dmalloc(&b->d_nrhs, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->d_srow0, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->d_seoff, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->d_slog, nsys)) != cudaSuccess || (e = dmalloc(&b->d_sn, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->d_sorder, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->act_sys, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->act_ecum, nsys + 1)) != cudaSuccess ||
+         (e = dmalloc(&b->act_hcum, nsys + 1)) != cudaSuccess ||
+         (e = dmalloc(&b->act_count, 1)) != cudaSuccess ||
+         (e = dmalloc(&b->all_sys, nsys)) != cudaSuccess ||
+         (e = dmalloc(&b->all_ecum, nsys + 1)) != cudaSuccess ||
+         (e = dmalloc(&b->all_count, 1)) != cudaSuccess ||
          (e = dmalloc(&b->X, NE)) != cudaSuccess || (e = dmalloc(&b->X2, NE)) != cudaSuccess ||
          (e = dmalloc(&b->RP, NE)) != cudaSuccess || (e = dmalloc(&b->RP2, NE)) != cudaSuccess ||
          (e = dmalloc(&b->B, NE)) != cudaSuccess || (e = dmalloc(&b->Y, NE)) != cudaSuccess ||
@@ -548,8 +705,17 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
         rc = cuda_fail(ctx, e, "cudaMalloc batch");
     if (!rc) {
         cudaStream_t s = ctx->stream;
-        cudaMemcpyAsync(b->d_rsys, rsys.data(), sizeof(int) * N, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(b->d_nrhs, b->nrhs.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->d_srow0, srow0.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->d_seoff, seoff.data(), sizeof(long long) * nsys, cudaMemcpyHostToDevice,
+                        s);
+        cudaMemcpyAsync(b->d_slog, cls_of.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->d_sn, sn.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->d_sorder, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->all_sys, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->all_ecum, all_ecum.data(), sizeof(long long) * (nsys + 1),
+                        cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(b->all_count, all_count.data(), sizeof(int), cudaMemcpyHostToDevice, s);
         // Padding elements are never written by the loop: zero every array once.
         cudaMemsetAsync(b->X, 0, sizeof(double) * NE, s);
         cudaMemsetAsync(b->X2, 0, sizeof(double) * NE, s);
@@ -677,11 +843,9 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
     cudaMemcpyAsync(b->B, b_dev, sizeof(double) * NE, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(b->X, x_dev, sizeof(double) * NE, cudaMemcpyDeviceToDevice, s);
     cudaMemsetAsync(b->bnorm2, 0, sizeof(double) * PR, s);
-    k_b_forward_nh<<<1, 1, 0, s>>>(b->dom->d_nh, b->n * b->per);
-    k_b_state_init<<<1, 1024, 0, s>>>(b->d_state, params->max_iters, params->check_freq,
-                                       params->tolerance, pairs, b->conv_iter, int(PR), b->norm2,
-                                       b->sys_done, b->nsys);
-    BatchArgs a = batch_args(b, params);
+    BatchArgs a = batch_args(b, params, true);  // every system
+    k_b_state_init<<<1, 1024, 0, s>>>(a, params->max_iters, params->check_freq,
+                                       params->tolerance, pairs);
     const int grid = grid_for(b->ne);
     k_b_init_norms<<<grid, kThreads, 0, s>>>(a);
     k_b_update<false, false><<<grid, kThreads, 0, s>>>(a, b->X, 0, cudaGraphConditionalHandle(0));
@@ -717,7 +881,6 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         std::vector<double> nr(PR), bn(PR);
         std::vector<int> ci(PR);
         cudaMemsetAsync(b->norm2, 0, sizeof(double) * PR, s);
-        a.skip = 0;  // every system's final residual
         k_b_update<false, false><<<grid, kThreads, 0, s>>>(a, b->X, 0, cudaGraphConditionalHandle(0));
         cudaMemcpyAsync(nr.data(), b->norm2, sizeof(double) * PR, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(bn.data(), b->bnorm2, sizeof(double) * PR, cudaMemcpyDeviceToHost, s);
@@ -746,7 +909,7 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         out.solve_ms = ms;
         out.walk_ms = double(tim[2]) * 1e-6;
         out.walk_launches = int64_t(tim[3]);
-        out.kernel_launches = int64_t(b->body_kernels ? b->body_kernels : 4) * st.iter + 4;
+        out.kernel_launches = int64_t(b->body_kernels ? b->body_kernels : 4) * st.iter + 3;
         out.rho = -1.0;
         *stats = out;
     }

@@ -288,15 +288,25 @@ struct BatchClasses {
     int crow[6];
     long long cel[6];
 };
+// The systems a batched iteration works on: lsys[k] for k < *lcount, whose
+// histories occupy [hcum[k], hcum[k+1]) of the iteration's history space
+// (n_s * per each, hcum[*lcount] in all).
+struct BatchList {
+    const int* lsys;
+    const int* hcum;
+    const int* lcount;
+    const int* srow0;   // system -> its first row
+};
 // Forward walks shared by the right-hand sides of a batch: every history
 // carries one Kahan-compensated FP32 tally per column of its start row's
 // class, reading the tally source cR at each state's elements and adding into
-// Y at the start row's elements.  Histories whose start row belongs to a
-// finished system (done[rsys[row]]) are skipped.  Each warp takes 32 * grab
-// histories per work-queue grab.  The work-queue counter must be zero on
-// entry; the caller resets it afterwards.
-int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const float* cR, double* Y,
-                      const int* rsys, const int* done, int grab);
+// Y at the start row's elements.  Only the listed systems' histories run;
+// history h of system s is history srow0[s] * per + (h - hcum[k]) of the
+// whole batch, on that history's own random stream, whatever the list.
+// Each warp takes 32 * grab histories per work-queue grab.  The work-queue
+// counter must be zero on entry; the caller resets it afterwards.
+int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const BatchList& list,
+                      const float* cR, double* Y, int grab);
 
 // ---- MCSA helpers (mcsa.cu) ----------------------------------------------------
 // rp_out = PL (b - A PR x)   (LinearProblem::updatePrecResidual)

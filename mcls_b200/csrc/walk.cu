@@ -551,11 +551,21 @@ namespace {
 struct BatchWalk {
     const float* cR;
     double* Y;
-    const int* rsys;
-    const int* done;
+    BatchList list;
     BatchClasses cls;
     int grab;
+    int per;
 };
+
+// The list entry k with hcum[k] <= h < hcum[k+1] (count entries).
+__device__ __forceinline__ int list_entry(const int* hcum, int count, int h) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (hcum[mid] <= h) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
 
 // The tally-source row of state s in class c (W = 2^c columns).
 template <int W>
@@ -615,31 +625,41 @@ template <int S, bool ST>
 __global__ void __launch_bounds__(256, 3) walk32_batch(WalkArgs a, BatchWalk m) {
     static_assert(S % 4 == 0, "records are whole 32-byte halves");
     __shared__ uint64_t s_ekey;
-    __shared__ int s_nh;
+    __shared__ int s_nh, s_count;
     const int lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         s_ekey = epoch_key(a.seed, *a.d_epoch);
-        s_nh = *a.d_nh;
+        s_count = *m.list.lcount;
+        s_nh = s_count > 0 ? m.list.hcum[s_count] : 0;
     }
     __syncthreads();
     const char* rec = reinterpret_cast<const char*>(a.rec);
     if (lane == 0) atomicMin(&a.d_tim[0], global_ns());
     unsigned steps = 0;
     const int chunk = 32 * m.grab;
+    const int count = s_count;
     while (true) {
         int base = 0;
         if (lane == 0) base = atomicAdd(a.d_counter, chunk);
         base = __shfl_sync(kFull, base, 0);
         const int nh = s_nh;
         if (base >= nh) break;
+        // The list entry of the grab's first history (one search per warp);
+        // the lanes step forward from it.
+        int k0 = 0;
+        if (lane == 0) k0 = list_entry(m.list.hcum, count, base);
+        k0 = __shfl_sync(kFull, k0, 0);
         for (int g = 0; g < m.grab; ++g) {
-            const int e = base + 32 * g + lane;
-            if (e >= nh) break;
+            const int h = base + 32 * g + lane;
+            if (h >= nh) break;
+            int k = k0;
+            while (k + 1 < count && h >= m.list.hcum[k + 1]) ++k;
+            const int sys = m.list.lsys[k];
+            const int e = m.list.srow0[sys] * m.per + (h - m.list.hcum[k]);
             int s;
             float w;
             uint64_t x;
             walk_start<MCLSGPU_FORWARD>(a, e, s_ekey, 1.f, s, w, x);
-            if (m.done && m.done[m.rsys[s]]) continue;
             int c = 0;
             while (c < 4 && s >= m.cls.crow[c + 1]) ++c;
             switch (c) {
@@ -700,8 +720,8 @@ static void fill_walk_args(mclsgpu_domain* dom, WalkArgs& a) {
 
 // Batched forward walks over the domain's FP32 records (records of at most
 // 16 slots; see launch_walk_batch in internal.h).
-int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const float* cR, double* Y,
-                      const int* rsys, const int* done, int grab) {
+int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const BatchList& list,
+                      const float* cR, double* Y, int grab) {
     mclsgpu_context* ctx = dom->ctx;
     if (dom->p.precision != MCLSGPU_FP32 || dom->p.direction != MCLSGPU_FORWARD || !dom->slots ||
         dom->rec_q16)
@@ -714,7 +734,7 @@ int launch_walk_batch(mclsgpu_domain* dom, const BatchClasses& cls, const float*
     const int sms = ctx->num_sms;
     const int block = dom->walk_block;
     cudaStream_t st = ctx->stream;
-    const BatchWalk m{cR, Y, rsys, done, cls, grab};
+    const BatchWalk m{cR, Y, list, cls, grab, a.per};
     bool ok = true;
     if (dom->stencil_k) {
         switch (dom->slots) {
