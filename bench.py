@@ -78,6 +78,11 @@ WALK_DRAM_BYTES_PER_LAUNCH = {"diffusion128": 91.72e6}
 # dram__bytes_write.sum (47.17 MB) of the 4-histories-per-lane x 256 launch
 # (python -m mcls_b200.walkprof --n 192 --solves 2 --histories-per-lane 4).
 HBM_WALK_DRAM_BYTES_PER_LAUNCH = 330.31e6
+# The same capture's L2 and DRAM figures: what binds the walk (L2 throughput
+# and latency, the records read from HBM about once per launch).
+HBM_WALK_NCU = {"lts_throughput_pct_of_peak": 64.1, "lts_sector_hit_pct": 87.3,
+                "dram_throughput_pct_of_peak": 8.8, "top_stall": "long scoreboard (L2 loads)",
+                "capture": "ncu --set full, one walk32 launch, 192^3, 4 histories per lane x 256"}
 # The oracle port's whole MCSA solve of a workload, run once to the end
 # (FP64 forward expected-value walks on the counter stream, the workload's
 # histories per iteration, seed 1234): its iteration count, which the
@@ -362,14 +367,31 @@ def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None):
         torch.cuda.synchronize()
         st = dom.anderson_solve_dev(bt.data_ptr(), xt.data_ptr(), tolerance=tol,
                                     max_iters=args.max_iters,
-                                    storage_depth=depth,
+                                    storage_depth=depth, mixing=args.anderson_mixing,
                                     host_loop=1 if args.host_loop else 0)
         if k >= 1:
             stats.append(st)
     ms = sum(s["solve_ms"] for s in stats) / len(stats)
     rel = float(np.linalg.norm(b - A @ xt.cpu().numpy()) / np.linalg.norm(b))
+    sweep = []
+    for sd in [int(v) for v in args.anderson_seeds.split(",") if v]:
+        # One solve per further seed of the random stream: the spread of the
+        # stochastic fixed-point map's acceleration.
+        dom.reseed(sd)
+        xs = torch.zeros_like(xt)
+        torch.cuda.synchronize()
+        sst = dom.anderson_solve_dev(bt.data_ptr(), xs.data_ptr(), tolerance=tol,
+                                     max_iters=args.max_iters, storage_depth=depth,
+                                     mixing=args.anderson_mixing,
+                                     host_loop=1 if args.host_loop else 0)
+        sweep.append({"seed": sd, "iterations": sst["iterations"],
+                      "converged": bool(sst["converged"]),
+                      "time_to_1e-8_s": sst["solve_ms"] / 1e3,
+                      "speedup_vs_jacobi_mcsa": jacobi_ms / sst["solve_ms"] if jacobi_ms else None})
+    out_seeds = {"seeds": sweep} if sweep else {}
     return {"time_to_1e-8_s": ms / 1e3, "iterations": stats[-1]["iterations"],
             "converged": bool(stats[-1]["converged"]), "storage_depth": depth,
+            "mixing": args.anderson_mixing, **out_seeds,
             "criterion": "|PL (b - A x)|_2 < tol |b|_2, tol = 1e-8 |PL b|_2 / |b|_2 "
                          "(the MCSA arm's |PL (b - A x)|_2 <= 1e-8 |PL b|_2)",
             "tolerance": tol,
@@ -377,7 +399,8 @@ def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None):
                                        np.linalg.norm(apply_pl(b))),
             "walk_steps_per_s": sum(s["walk_steps"] for s in stats) /
                                 (sum(s["solve_ms"] for s in stats) * 1e-3),
-            "rel_residual_b_minus_Ax": rel, "speedup_vs_jacobi_mcsa": jacobi_ms / ms}
+            "rel_residual_b_minus_Ax": rel,
+            "speedup_vs_jacobi_mcsa": jacobi_ms / ms if jacobi_ms else None}
 
 
 def partition_arm(args, ctx, A, b):
@@ -701,7 +724,7 @@ def _aniso_solve(args, ctx, op, A, b, kind, cfgd, net=None, block=4, rho_fallbac
         if anderson_depth:
             try:
                 aa = anderson_arm(args, anderson_depth, dom, bt, xt, A, b, args.seed,
-                                  st["solve_ms"] if st["converged"] else float("nan"),
+                                  st["solve_ms"] if st["converged"] else None,
                                   PL=pc.to_scipy(A.shape[0]))
                 aa["speedup_vs_this_mcsa"] = aa.pop("speedup_vs_jacobi_mcsa")
             except capi.MclsError as e:
@@ -963,6 +986,10 @@ def main():
                          "inside conditional graph nodes)")
     ap.add_argument("--no-anderson", action="store_true",
                     help="skip the Anderson-accelerated MCSA arm")
+    ap.add_argument("--anderson-mixing", type=float, default=1.0,
+                    help="Anderson mixing parameter beta (NOX's default 1)")
+    ap.add_argument("--anderson-seeds", default="",
+                    help="comma-separated further seeds: one Anderson solve each")
     ap.add_argument("--anderson-depth", default="2,6",
                     help="Anderson storage depths to time, comma separated (NOX's default "
                          "is 2)")
@@ -1153,7 +1180,10 @@ def main():
         line["roofline"] = {
             "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
             "traffic": tr, "kernel": "walk32", "peak_kind": peak_kind,
-            "dram_gbs": tr / (hr["per_launch_ms"] * 1e-3) / 1e9 if tr else None, **hr}
+            "dram_gbs": tr / (hr["per_launch_ms"] * 1e-3) / 1e9 if tr else None,
+            "binding": "L2: the algorithmic bytes exceed the HBM peak because each record is "
+                       "read from HBM about once per launch and its later reads hit L2",
+            "ncu": HBM_WALK_NCU, **hr}
     else:
         line["roofline"] = dict(roofline_workload, frac=roofline_workload["frac_of_hbm_peak"])
     if world == 1 and args.partition_parts > 1:

@@ -134,22 +134,32 @@ __device__ __forceinline__ Elem elem_at(const BatchArgs& a, int count, int k0, l
     return q;
 }
 
-// Grid-stride loop over the launch's elements, block by block: the block's
-// first thread finds the list entry of the block's first element.  body(live,
-// q) runs on every thread of the block for every block-sized tile (block-
-// uniform trip count, so body may use warp collectives).
+// Loop over the launch's elements: each block takes one contiguous range in
+// tiles of blockDim elements.  The block's first thread finds the list entry
+// of the range's first element once and steps it forward tile by tile (the
+// entries only increase along the range).  body(live, q) runs on every
+// thread of the block for every tile (block-uniform trip count, so body may
+// use warp collectives).
 template <class Body>
 __device__ __forceinline__ void for_elements(const BatchArgs& a, Body body) {
     __shared__ int s_k0;
     const int count = *a.lcount;
     const long long total = count > 0 ? a.lecum[count] : 0;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < total;
-         base += (long long)gridDim.x * blockDim.x) {
+    const long long T = blockDim.x;
+    const long long span = ((total + gridDim.x - 1) / gridDim.x + T - 1) / T * T;
+    const long long beg = (long long)blockIdx.x * span;
+    const long long end = beg + span < total ? beg + span : total;
+    if (threadIdx.x == 0 && beg < end) s_k0 = elem_entry(a.lecum, count, beg);
+    for (long long base = beg; base < end; base += T) {
         __syncthreads();
-        if (threadIdx.x == 0) s_k0 = elem_entry(a.lecum, count, base);
+        if (threadIdx.x == 0) {
+            int k = s_k0;
+            while (k + 1 < count && base >= a.lecum[k + 1]) ++k;
+            s_k0 = k;
+        }
         __syncthreads();
         const long long t = base + threadIdx.x;
-        const bool live = t < total;
+        const bool live = t < end;
         Elem q{};
         if (live) q = elem_at(a, count, s_k0, t);
         body(live, q);
