@@ -97,14 +97,14 @@ __global__ void k_pack_records(const int* drp, const int* dcol, const double* dh
 // Distinct column offsets (col - row) into a max_k-slot table; an offset
 // takes the first free slot it meets scanning from slot 0, so each offset
 // owns one slot.  More than max_k distinct offsets sets *overflow.
-__global__ void k_collect_offsets(const int* rp, const int* ci, int n, int max_k, int* tab,
-                                  int* overflow) {
+__global__ void k_collect_offsets(const int* rp, const int* ci, int n, int row0, int max_k,
+                                  int* tab, int* overflow) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         // Once the table has overflowed the answer is known: stop early
         // instead of contending on the full table.
         if (*reinterpret_cast<volatile int*>(overflow)) return;
         for (int k = rp[i]; k < rp[i + 1]; ++k) {
-            const int d = ci[k] - i;
+            const int d = ci[k] - (row0 + i);
             bool placed = false;
             for (int t = 0; t < max_k && !placed; ++t) {
                 int cur = tab[t];
@@ -120,7 +120,7 @@ __global__ void k_collect_offsets(const int* rp, const int* ci, int n, int max_k
 // word 2 + j = CDF value at offset off[j] with the sign of h in its sign bit,
 // or NaN when the row has no entry at that offset (never selected).
 __global__ void k_pack_stencil(const int* drp, const int* dcol, const double* dh,
-                               const double* dcdf, const double* dw, int n, int K,
+                               const double* dcdf, const double* dw, int n, int row0, int K,
                                const int* off, int words, uint32_t* rec) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* r = rec + size_t(i) * words;
@@ -128,7 +128,7 @@ __global__ void k_pack_stencil(const int* drp, const int* dcol, const double* dh
         r[1] = 0u;
         for (int j = 2; j < words; ++j) r[j] = 0x7fc00000u;
         for (int k = drp[i]; k < drp[i + 1]; ++k) {
-            const int d = dcol[k] - i;
+            const int d = dcol[k] - (row0 + i);
             int j = 0;
             while (j < K && off[j] != d) ++j;
             if (j == K) continue;  // cannot happen: every offset is in the table
@@ -143,7 +143,7 @@ __global__ void k_pack_stencil(const int* drp, const int* dcol, const double* dh
 // round(65536 cdf_j) (65535 for the row's last entry; 0, never selected, for
 // offsets the row lacks) in the 16-bit half j of words 3...
 __global__ void k_pack_stencil16(const int* drp, const int* dcol, const double* dh,
-                                 const double* dcdf, const double* dw, int n, int K,
+                                 const double* dcdf, const double* dw, int n, int row0, int K,
                                  const int* off, int words, uint32_t* rec) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* r = rec + size_t(i) * words;
@@ -152,7 +152,7 @@ __global__ void k_pack_stencil16(const int* drp, const int* dcol, const double* 
         for (int j = 2; j < words; ++j) r[j] = 0u;
         const int last = drp[i + 1] - 1;
         for (int k = drp[i]; k <= last; ++k) {
-            const int d = dcol[k] - i;
+            const int d = dcol[k] - (row0 + i);
             int j = 0;
             while (j < K && off[j] != d) ++j;
             if (j == K) continue;  // cannot happen: every offset is in the table
@@ -173,7 +173,8 @@ __global__ void k_to_float(const double* a, float* b, int n) {
 
 // Sorted distinct column offsets of D (at most max_k <= 32; *K = 0 when
 // there are more).
-int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int max_k, int* offsets, int* K) {
+int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int max_k, int* offsets, int* K,
+                    int row0) {
     cudaStream_t s = ctx->stream;
     if (max_k < 1 || max_k > 32) return set_error(ctx, MCLSGPU_ERR_INVALID_ARG, "offset table size");
     int* tab = nullptr;
@@ -182,7 +183,8 @@ int collect_offsets(mclsgpu_context* ctx, const DevCsr& D, int max_k, int* offse
     std::vector<int> init(max_k + 1, INT_MIN);
     init[max_k] = 0;
     cudaMemcpyAsync(tab, init.data(), (max_k + 1) * sizeof(int), cudaMemcpyHostToDevice, s);
-    k_collect_offsets<<<grid_for(D.n), 256, 0, s>>>(D.rp, D.ci, D.n, max_k, tab, tab + max_k);
+    k_collect_offsets<<<grid_for(D.n), 256, 0, s>>>(D.rp, D.ci, D.n, row0, max_k, tab,
+                                                    tab + max_k);
     std::vector<int> h(max_k + 1);
     cudaMemcpyAsync(h.data(), tab, (max_k + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
@@ -258,9 +260,9 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
     // for offsets the row lacks: 2 + K words instead of 2 + 2 * row length.
     dom->stencil_k = 0;
     const int fmt = dom->p.record_format;
-    if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED && row0 == 0) {
+    if (dom->p.precision == MCLSGPU_FP32 && fmt != MCLSGPU_RECORD_PACKED) {
         int K = 0;
-        if ((rc = collect_offsets(ctx, D, 30, dom->stencil_off, &K))) return rc;
+        if ((rc = collect_offsets(ctx, D, 30, dom->stencil_off, &K, row0))) return rc;
         // 32-, 64- or 128-byte records; stencil16: 3 words + K halves in 32 or
         // 64 bytes.
         const bool q16 = fmt == MCLSGPU_RECORD_STENCIL16;
@@ -288,12 +290,12 @@ int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
             cudaMemcpyAsync(doff, dom->stencil_off, 32 * sizeof(int), cudaMemcpyHostToDevice, s);
             if (dom->rec_q16)
                 k_pack_stencil16<<<grid_for(n), 256, 0, s>>>(
-                    D.rp, D.ci, D.v, dom->cdf, dom->w, n, dom->stencil_k, doff, 2 * slots,
+                    D.rp, D.ci, D.v, dom->cdf, dom->w, n, row0, dom->stencil_k, doff, 2 * slots,
                     reinterpret_cast<uint32_t*>(dom->rec));
             else
-                k_pack_stencil<<<grid_for(n), 256, 0, s>>>(D.rp, D.ci, D.v, dom->cdf, dom->w, n,
-                                                           dom->stencil_k, doff, 2 * slots,
-                                                           reinterpret_cast<uint32_t*>(dom->rec));
+                k_pack_stencil<<<grid_for(n), 256, 0, s>>>(
+                    D.rp, D.ci, D.v, dom->cdf, dom->w, n, row0, dom->stencil_k, doff, 2 * slots,
+                    reinterpret_cast<uint32_t*>(dom->rec));
             e = cudaStreamSynchronize(s);
             dfree(doff);
             if (e != cudaSuccess) return cuda_fail(ctx, e, "stencil records");

@@ -258,7 +258,9 @@ int point_jacobi_csr(mclsgpu_context* ctx, int n, const double* dinv,
 int csr_to_sell(mclsgpu_context* ctx, const DevCsr& A, DevSell& S);
 // Sorted distinct column offsets (col - row) of A, at most max_k <= 32
 // (*K = 0 if more).
-int collect_offsets(mclsgpu_context* ctx, const DevCsr& A, int max_k, int* offsets, int* K);
+// row0: global index of A's first row (column offsets are col - global row).
+int collect_offsets(mclsgpu_context* ctx, const DevCsr& A, int max_k, int* offsets, int* K,
+                    int row0 = 0);
 // Diagonal-offset values of a stencil matrix (K offsets): val[j*n + r].
 int csr_to_dia(mclsgpu_context* ctx, const DevCsr& A, int K, const int* offsets,
                double** val);
@@ -277,6 +279,13 @@ int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int
 // domain; its columns are global).
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
                         mclsgpu_domain* dom, int row0 = 0);
+
+// FP32 forward walks: the tally source of v into the domain's records (H v
+// for the expected-value estimator, v for collision, with the Neumann
+// relaxation when has_omega) and the tallies y cleared.  row0: the global
+// index of the domain's first row (v is the whole vector).
+void launch_forward_records(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
+                            int row0, double* y);
 
 // ---- batched walks (walk.cu, batch.cu) -------------------------------------------
 // Width classes of a batch: the rows [crow[c], crow[c+1]) belong to systems
@@ -362,12 +371,14 @@ struct HistoryWire {
 static_assert(sizeof(HistoryWire) == 32, "history wire format");
 
 struct PartWalk {
-    const uint2* rec;       // packed FP32 records of rows [row0, row0 + n)
+    const uint2* rec;       // FP32 records of rows [row0, row0 + n)
     int slots;
     int row0;
     int n;
     int L;
     int dir;                // MCLSGPU_ADJOINT or MCLSGPU_FORWARD
+    int kind;               // records: 0 packed, 1 stencil, 2 stencil16
+    int stoff[32];          // stencil records: column offset of each slot
     int per;                // forward: histories per start row
     float cutoff;           // relative weight cutoff (0: fixed length)
     // first round: the histories e_begin <= e < e_end of the global source

@@ -198,16 +198,17 @@ __global__ void k_forward_c(const double* v, int n, double omega, int has, int e
 // FP32 forward walk: the tally source of each state goes into its record's
 // header word (slot 0, second word) so that a step reads one record only;
 // the history-sum tallies are cleared in the same pass.
-__global__ void __launch_bounds__(256) k_forward_rec(const double* v, int n, double omega,
-                                                     int has, int ev, const int* off,
-                                                     const int* col, const double* h, int slots,
-                                                     uint2* rec, double* y) {
+__global__ void __launch_bounds__(256) k_forward_rec(const double* v, int n, int row0,
+                                                     double omega, int has, int ev,
+                                                     const int* off, const int* col,
+                                                     const double* h, int slots, uint2* rec,
+                                                     double* y) {
     // H over SELL-32: a warp owns one slice, every entry column is one
     // coalesced access.
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double c;
         if (!ev) {
-            c = load_src(v, i, omega, has);
+            c = load_src(v, row0 + i, omega, has);
         } else {
             c = 0.0;
             const int o = off[i >> 5] + (i & 31), w = (off[(i >> 5) + 1] - off[i >> 5]) >> 5;
@@ -295,24 +296,25 @@ __device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, const d
                  : "memory");
 }
 
-__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, double omega,
-                                                             int has, int ev, int K,
-                                                             StencilOffsets so, int words,
+__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, int row0,
+                                                             double omega, int has, int ev,
+                                                             int K, StencilOffsets so, int words,
                                                              int q16, uint32_t* rec, double* y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* r = rec + size_t(i) * words;
+        const int g = row0 + i;  // the state's index in v
         if (!ev) {
-            r[1] = __float_as_uint(__double2float_rn(load_src(v, i, omega, has)));
+            r[1] = __float_as_uint(__double2float_rn(load_src(v, g, omega, has)));
         } else if (q16 && words == 8) {
-            rec_stencil16_source<8>(r, i, v, omega, has, K, so);
+            rec_stencil16_source<8>(r, g, v, omega, has, K, so);
         } else if (q16) {
-            rec_stencil16_source<16>(r, i, v, omega, has, K, so);
+            rec_stencil16_source<16>(r, g, v, omega, has, K, so);
         } else if (words == 8) {
-            rec_stencil_source<8>(r, i, v, omega, has, K, so);
+            rec_stencil_source<8>(r, g, v, omega, has, K, so);
         } else if (words == 16) {
-            rec_stencil_source<16>(r, i, v, omega, has, K, so);
+            rec_stencil_source<16>(r, g, v, omega, has, K, so);
         } else {
-            rec_stencil_source<32>(r, i, v, omega, has, K, so);
+            rec_stencil_source<32>(r, g, v, omega, has, K, so);
         }
         y[i] = 0.0;
     }
@@ -579,6 +581,25 @@ void launch_forward_setup(mclsgpu_domain* dom) {
     k_forward_nh<<<1, 1, 0, dom->ctx->stream>>>(dom->d_nh, dom->n * per, dom->d_scalars);
 }
 
+void launch_forward_records(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
+                            int row0, double* y) {
+    cudaStream_t s = dom->ctx->stream;
+    const int n = dom->n;
+    const int ev = dom->p.estimator == MCLSGPU_EXPECTED_VALUE;
+    if (dom->stencil_k) {
+        StencilOffsets so{};
+        for (int j = 0; j < 32; ++j) so.off[j] = dom->stencil_off[j];
+        k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
+            v, n, row0, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots, dom->rec_q16,
+            reinterpret_cast<uint32_t*>(dom->rec), y);
+    } else {
+        k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, row0, omega, has_omega, ev,
+                                                               dom->DS.off, dom->DS.col,
+                                                               dom->DS.val, dom->slots, dom->rec,
+                                                               y);
+    }
+}
+
 // `fused`: the history count was set once by launch_forward_setup.
 void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
                            bool fused) {
@@ -590,18 +611,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     const int ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
     if (!fused) k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
     if (p.precision == MCLSGPU_FP32) {
-        if (dom->stencil_k) {
-            StencilOffsets so{};
-            for (int j = 0; j < 32; ++j) so.off[j] = dom->stencil_off[j];
-            k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
-                v, n, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots, dom->rec_q16,
-                reinterpret_cast<uint32_t*>(dom->rec), dom->y64);
-        } else {
-            k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, omega, has_omega, ev,
-                                                                   dom->DS.off, dom->DS.col,
-                                                                   dom->DS.val, dom->slots,
-                                                                   dom->rec, dom->y64);
-        }
+        launch_forward_records(dom, v, omega, has_omega, 0, dom->y64);
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);

@@ -68,29 +68,6 @@ __global__ void k_part_finish(const double* y, const double* sc, int n, double* 
         x[i] = __dmul_rn(y[i], inv);  // AdjointTally::normalize
 }
 
-// Forward solve, once per solve: the tally source of the part's rows into
-// their records' headers, c_i = (H v)_i for the expected-value estimator or
-// v_i for collision (the whole-domain build's arithmetic, over the part's
-// FP64 rows with global columns), the part's slice of v kept for the
-// finalisation, and the tallies cleared.
-__global__ void k_part_forward_rec(const double* v, int row0, int n, double omega, int has,
-                                   int ev, const int* rp, const int* ci, const double* h,
-                                   int slots, uint2* rec, double* y, double* srcp) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double c;
-        if (!ev) {
-            c = has ? v[row0 + i] * omega : v[row0 + i];
-        } else {
-            c = 0.0;
-            for (int k = rp[i]; k < rp[i + 1]; ++k)
-                c = fma(h[k], has ? v[ci[k]] * omega : v[ci[k]], c);
-        }
-        rec[size_t(i) * slots].y = __float_as_uint(__double2float_rn(c));
-        y[i] = 0.0;
-        srcp[i] = v[row0 + i];
-    }
-}
-
 // ForwardTally::finalize (src/MCLS_ForwardTally_impl.hpp:194-208): sum /
 // count, plus the source term for the expected-value estimator.
 __global__ void k_part_finish_forward(const double* y, const double* srcp, int n, int per,
@@ -195,7 +172,6 @@ int mclsgpu_subdomain_build(mclsgpu_context* ctx, int64_t n_global, int32_t npar
     mclsgpu_subdomain* sd = new mclsgpu_subdomain;
     sd->ctx = ctx;
     sd->p = *p;
-    sd->p.record_format = MCLSGPU_RECORD_PACKED;
     sd->N = n_global;
     sd->nparts = nparts;
     sd->part = part;
@@ -307,10 +283,12 @@ int mclsgpu_subdomain_begin(mclsgpu_subdomain* sd, const double* rhs_dev, int64_
     const double omega = sd->p.neumann_relaxation;
     if (sd->p.direction == MCLSGPU_FORWARD) {
         // History e starts at row e / per: the part's are a contiguous range.
-        const mclsgpu_domain& r = sd->recs;
-        k_part_forward_rec<<<grid_for(sd->n), 256, 0, s>>>(
-            rhs_dev, sd->row0, sd->n, omega, omega > 0.0, sd->p.estimator == MCLSGPU_EXPECTED_VALUE,
-            r.D.rp, r.D.ci, r.D.v, r.slots, r.rec, sd->y, sd->srcp);
+        // The part's rows' tally source into their records (the whole-domain
+        // build's kernels, over the part's rows), the tallies cleared, and the
+        // part's slice of the source kept for the finalisation.
+        launch_forward_records(&sd->recs, rhs_dev, omega, omega > 0.0, sd->row0, sd->y);
+        cudaMemcpyAsync(sd->srcp, rhs_dev + sd->row0, size_t(sd->n) * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s);
         sd->range[0] = (long long)sd->row0 * sd->per;
         sd->range[1] = (long long)(sd->row0 + sd->n) * sd->per;
         sd->range[2] = (long long)sd->N * sd->per;
@@ -347,6 +325,8 @@ int mclsgpu_subdomain_transport(mclsgpu_subdomain* sd, const mclsgpu_history_wir
     PartWalk w{};
     w.rec = sd->recs.rec;
     w.slots = sd->recs.slots;
+    w.kind = !sd->recs.stencil_k ? 0 : (sd->recs.rec_q16 ? 2 : 1);
+    for (int j = 0; j < 32; ++j) w.stoff[j] = sd->recs.stencil_off[j];
     w.row0 = sd->row0;
     w.n = sd->n;
     w.L = sd->p.history_length;

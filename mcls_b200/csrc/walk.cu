@@ -901,7 +901,7 @@ __device__ __forceinline__ void part_send(const PartWalk& p, int q, const Histor
         atomicOr(p.status, DEV_ERR_CAPACITY);
 }
 
-template <int S, int DIR>
+template <int S, int DIR, int ST>
 __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
     __shared__ int sb[kMaxParts + 1];
     for (int t = threadIdx.x; t <= p.nparts; t += blockDim.x) sb[t] = p.bounds[t];
@@ -909,6 +909,10 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
     WalkArgs a{};
     a.y64 = p.y;
     a.row0 = p.row0;
+    if constexpr (ST != kPacked) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) a.stoff[j] = p.stoff[j];
+    }
     const uint64_t ekey = epoch_key(p.seed, *p.d_epoch);
     const float wnorm = DIR == MCLSGPU_ADJOINT ? float(p.sc[0]) : 1.f;
     const float wcut = p.cutoff * wnorm;
@@ -957,7 +961,7 @@ __global__ void __launch_bounds__(256) walk32_part(PartWalk p) {
             continue;
         }
         while (true) {
-            walk_step<S, DIR, kPacked>(a, rec, s, w, x, acc, comp, k);
+            walk_step<S, DIR, ST>(a, rec, s, w, x, acc, comp, k);
             ++k;
             ++steps;
             if (k >= p.L || fabsf(w) < wcut) {
@@ -1122,14 +1126,25 @@ void launch_walk_part(const PartWalk& p, mclsgpu_context* ctx) {
     long long g = (nwork + 255) / 256;
     const int grid = int(g < ctx->num_sms * 8 ? g : ctx->num_sms * 8);
     cudaStream_t st = ctx->stream;
-#define MCLSGPU_PART_SLOTS(D)                                   \
-    switch (p.slots) {                                          \
-        case 4: walk32_part<4, D><<<grid, 256, 0, st>>>(p); break;   \
-        case 8: walk32_part<8, D><<<grid, 256, 0, st>>>(p); break;   \
-        case 12: walk32_part<12, D><<<grid, 256, 0, st>>>(p); break; \
-        case 16: walk32_part<16, D><<<grid, 256, 0, st>>>(p); break; \
-        case 24: walk32_part<24, D><<<grid, 256, 0, st>>>(p); break; \
-        default: walk32_part<32, D><<<grid, 256, 0, st>>>(p); break; \
+#define MCLSGPU_PART_SLOTS(D)                                                 \
+    if (p.kind == kStencil16) {                                               \
+        if (p.slots == 4) walk32_part<4, D, kStencil16><<<grid, 256, 0, st>>>(p);  \
+        else walk32_part<8, D, kStencil16><<<grid, 256, 0, st>>>(p);            \
+    } else if (p.kind == kStencil) {                                          \
+        switch (p.slots) {                                                    \
+            case 4: walk32_part<4, D, kStencil><<<grid, 256, 0, st>>>(p); break;   \
+            case 8: walk32_part<8, D, kStencil><<<grid, 256, 0, st>>>(p); break;   \
+            default: walk32_part<16, D, kStencil><<<grid, 256, 0, st>>>(p); break; \
+        }                                                                     \
+    } else {                                                                  \
+        switch (p.slots) {                                                    \
+            case 4: walk32_part<4, D, kPacked><<<grid, 256, 0, st>>>(p); break;   \
+            case 8: walk32_part<8, D, kPacked><<<grid, 256, 0, st>>>(p); break;   \
+            case 12: walk32_part<12, D, kPacked><<<grid, 256, 0, st>>>(p); break; \
+            case 16: walk32_part<16, D, kPacked><<<grid, 256, 0, st>>>(p); break; \
+            case 24: walk32_part<24, D, kPacked><<<grid, 256, 0, st>>>(p); break; \
+            default: walk32_part<32, D, kPacked><<<grid, 256, 0, st>>>(p); break; \
+        }                                                                     \
     }
     if (p.dir == MCLSGPU_FORWARD) {
         MCLSGPU_PART_SLOTS(MCLSGPU_FORWARD)

@@ -52,6 +52,13 @@ WALKS = {
     "forward_collision": dict(direction=capi.FORWARD, estimator=capi.COLLISION),
     "forward_ev_cutoff": dict(direction=capi.FORWARD, estimator=capi.EXPECTED_VALUE,
                               weight_cutoff=0.6),
+    # Stencil records: column offsets from the global row, on the whole domain
+    # and in every part.
+    "adjoint_stencil": dict(record_format=capi.RECORD_STENCIL),
+    "forward_ev_stencil": dict(direction=capi.FORWARD, estimator=capi.EXPECTED_VALUE,
+                               record_format=capi.RECORD_STENCIL),
+    "forward_ev_stencil16": dict(direction=capi.FORWARD, estimator=capi.EXPECTED_VALUE,
+                                 record_format=capi.RECORD_STENCIL16),
 }
 
 
@@ -77,6 +84,7 @@ def test_parts_give_the_whole_domain_solve(ctx, nparts, name, walks):
         xp = xp.cpu().numpy()
         assert rounds >= 2 and moved > 0
         assert np.allclose(xp, xw, rtol=0, atol=1e-12 * np.abs(xw).max()), solve
+        assert parts[0].sub.record_bytes == dom.info()["record_bytes"]
         assert steps == st["walk_steps"]
         if "weight_cutoff" in kw:
             assert steps < st["histories"] * 10  # some histories ended early
