@@ -839,6 +839,14 @@ int anderson_solve(mclsgpu_domain* dom, const double* b_dev, double* x_dev,
 }
 
 }  // namespace
+
+void anderson_drop_graph(mclsgpu_domain* dom) {
+    if (dom->aa && dom->aa->graph) {
+        cudaGraphExecDestroy(dom->aa->graph);
+        dom->aa->graph = nullptr;
+    }
+}
+
 }  // namespace mclsgpu
 
 using namespace mclsgpu;

@@ -118,28 +118,41 @@ __device__ __forceinline__ int elem_entry(const long long* lecum, int count, lon
     return lo;
 }
 
-// Element t of the launch (t < lecum[count]), starting the entry search at
-// k0 (the entry of the block's first element).
-__device__ __forceinline__ Elem elem_at(const BatchArgs& a, int count, int k0, long long t) {
-    int k = k0;
-    while (k + 1 < count && t >= a.lecum[k + 1]) ++k;
-    Elem q;
-    q.s = a.lsys[k];
-    q.c = a.slog[q.s];
-    const long long local = t - a.lecum[k];
-    q.i = a.srow0[q.s] + int(local >> q.c);
-    q.r = int(local & ((1 << q.c) - 1));
-    q.e = size_t(a.seoff[q.s] + local);
-    q.base = a.seoff[q.s] - ((long long)a.srow0[q.s] << q.c);
-    return q;
-}
+// A thread's position in the launch's list: entry k and its system's fields,
+// reloaded only when the thread's element crosses into the next entry (the
+// elements a thread visits only increase).
+struct Cursor {
+    int k, s, c, row0;
+    long long lo, hi, eoff;
+    __device__ __forceinline__ void load(const BatchArgs& a, int kk) {
+        k = kk;
+        s = a.lsys[k];
+        c = a.slog[s];
+        row0 = a.srow0[s];
+        eoff = a.seoff[s];
+        lo = a.lecum[k];
+        hi = a.lecum[k + 1];
+    }
+    // Element t (lo <= t after the first call; t < lecum[count]).
+    __device__ __forceinline__ Elem at(const BatchArgs& a, long long t) {
+        while (t >= hi) load(a, k + 1);
+        Elem q;
+        q.s = s;
+        q.c = c;
+        const long long local = t - lo;
+        q.i = row0 + int(local >> c);
+        q.r = int(local & ((1 << c) - 1));
+        q.e = size_t(eoff + local);
+        q.base = eoff - ((long long)row0 << c);
+        return q;
+    }
+};
 
 // Loop over the launch's elements: each block takes one contiguous range in
-// tiles of blockDim elements.  The block's first thread finds the list entry
-// of the range's first element once and steps it forward tile by tile (the
-// entries only increase along the range).  body(live, q) runs on every
-// thread of the block for every tile (block-uniform trip count, so body may
-// use warp collectives).
+// tiles of blockDim elements; the block's first thread finds the list entry
+// of the range's first element, and every thread steps its own cursor
+// forward from there.  body(live, q) runs on every thread of the block for
+// every tile (block-uniform trip count, so body may use warp collectives).
 template <class Body>
 __device__ __forceinline__ void for_elements(const BatchArgs& a, Body body) {
     __shared__ int s_k0;
@@ -149,19 +162,16 @@ __device__ __forceinline__ void for_elements(const BatchArgs& a, Body body) {
     const long long span = ((total + gridDim.x - 1) / gridDim.x + T - 1) / T * T;
     const long long beg = (long long)blockIdx.x * span;
     const long long end = beg + span < total ? beg + span : total;
-    if (threadIdx.x == 0 && beg < end) s_k0 = elem_entry(a.lecum, count, beg);
+    if (beg >= end) return;  // the whole block
+    if (threadIdx.x == 0) s_k0 = elem_entry(a.lecum, count, beg);
+    __syncthreads();
+    Cursor cur;
+    cur.load(a, s_k0);
     for (long long base = beg; base < end; base += T) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int k = s_k0;
-            while (k + 1 < count && base >= a.lecum[k + 1]) ++k;
-            s_k0 = k;
-        }
-        __syncthreads();
         const long long t = base + threadIdx.x;
         const bool live = t < end;
         Elem q{};
-        if (live) q = elem_at(a, count, s_k0, t);
+        if (live) q = cur.at(a, t);
         body(live, q);
     }
 }
@@ -441,6 +451,7 @@ struct mclsgpu_batch {
     mclsgpu::BatchState* h_state = nullptr;
     cudaGraphExec_t graph = nullptr;
     long long graph_key = -1;
+    uint64_t graph_seed = 0;       // the domain seed the captured walks carry
     int body_kernels = 0;
     int per = 1;
     int grab = 1;                  // walk work-queue grab, in 32-history chunks
@@ -833,10 +844,11 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
     for (int q = 0; q < b->nsys; ++q) pairs += b->nrhs[q];
     const long long key = (long long)(params->richardson_omega * 1e6) * 64 +
                           (long long)b->grab * 2 + (b->dom->walk_block == 128 ? 1 : 0);
-    if (!params->host_loop && (!b->graph || b->graph_key != key)) {
+    if (!params->host_loop && (!b->graph || b->graph_key != key || b->graph_seed != b->dom->seed)) {
         int rc = build_batch_graph(b, params);
         if (rc) return rc;
         b->graph_key = key;
+        b->graph_seed = b->dom->seed;
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

@@ -642,10 +642,16 @@ int mclsgpu_domain_reseed(mclsgpu_domain* dom, uint64_t seed) {
     dom->seed = seed;
     cudaMemsetAsync(dom->d_pos, 0, sizeof(unsigned long long), dom->ctx->stream);
     cudaMemsetAsync(dom->d_epoch, 0, sizeof(unsigned long long), dom->ctx->stream);
-    if (dom->graph) {  // the seed is baked into the captured iteration
+    // The seed is baked into the walk launches of every captured loop.
+    if (dom->graph) {
         cudaGraphExecDestroy(dom->graph);
         dom->graph = nullptr;
     }
+    if (dom->set_graph) {
+        cudaGraphExecDestroy(dom->set_graph);
+        dom->set_graph = nullptr;
+    }
+    anderson_drop_graph(dom);
     cudaError_t e = cudaStreamSynchronize(dom->ctx->stream);
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(dom->ctx, e, "reseed");
 }

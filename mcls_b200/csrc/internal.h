@@ -280,6 +280,9 @@ int exclusive_scan_counts_dev(mclsgpu_context* ctx, const int* d_cnt, int n, int
 int build_domain_arrays(mclsgpu_context* ctx, const DevCsr& M, double relax,
                         mclsgpu_domain* dom, int row0 = 0);
 
+// Releases the domain's captured Anderson loop (rebuilt on the next solve).
+void anderson_drop_graph(mclsgpu_domain* dom);
+
 // FP32 forward walks: the tally source of v into the domain's records (H v
 // for the expected-value estimator, v for collision, with the Neumann
 // relaxation when has_omega) and the tallies y cleared.  row0: the global

@@ -133,3 +133,29 @@ def test_anderson_parameter_checks(ctx):
     with pytest.raises(capi.MclsError) as e:
         dr.anderson_solve(np.ones(36))
     assert e.value.code == capi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("solver", ["anderson", "mcsa"])
+def test_reseed_reaches_the_captured_loop(ctx, solver):
+    # The seed is baked into the walk launches of the captured device-side
+    # loop: a reseed must rebuild it.  Forward expected-value walks with one
+    # history per row (every tally one addition onto zero) give the same bits
+    # for the same seed, so a second seed must differ and the first seed,
+    # set again, must come back exactly.
+    A, b = P.diffusion3d_varcoef(10, seed=6)
+    op = capi.Operator(ctx, A)
+    pc = capi.Precond(ctx, op, capi.PREC_POINT_JACOBI)
+    dom = capi.Domain(ctx, op, pc, precision=capi.FP32, rng_mode=capi.RNG_COUNTER, seed=5,
+                      direction=capi.FORWARD, estimator=capi.EXPECTED_VALUE, sample_ratio=1.0)
+
+    def run(seed):
+        dom.reseed(seed)
+        if solver == "anderson":
+            return dom.anderson_solve(b, tolerance=0.0, max_iters=12, storage_depth=3)[0]
+        return dom.mcsa_solve(b, tolerance=0.0, max_iters=12)[0]
+
+    x1 = run(11)
+    x2 = run(12)
+    x1b = run(11)
+    assert not np.array_equal(x1, x2)
+    assert np.array_equal(x1, x1b)
