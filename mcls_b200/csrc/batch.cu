@@ -324,20 +324,54 @@ __device__ void batch_check(const BatchArgs& a, int use_cond, cudaGraphCondition
     }
 }
 
+// Per-(system, column) sums of squares of one tile: a warp whose 32
+// elements all belong to one system reduces the lanes of each column with
+// shuffles and its lanes r < W keep the column sums in registers (a lane's
+// column stays the same from tile to tile while its system does), adding
+// them into the global sums only when the lane's system changes or the loop
+// ends; a warp that straddles systems adds each lane's square directly.
+struct PairSums {
+    double* sums;   // [nsys][pw]
+    int pw;
+    int s = -1, r = 0;
+    double v = 0.0;
+    __device__ __forceinline__ void flush() {
+        if (s >= 0 && v != 0.0) atomicAdd(&sums[size_t(s) * pw + r], v);
+        s = -1;
+        v = 0.0;
+    }
+    __device__ __forceinline__ void add(int sys, int c, int rr, double sq) {
+        const unsigned full = 0xffffffffu;
+        const int s0 = __shfl_sync(full, sys, 0);
+        const int c0 = __shfl_sync(full, c, 0);
+        if (__all_sync(full, sys == s0) && s0 >= 0) {
+            double x = sq;
+            for (int d = 16; d >= (1 << c0); d >>= 1) x += __shfl_xor_sync(full, x, d);
+            if ((threadIdx.x & 31) < (1 << c0)) {
+                if (s != s0 || r != rr) {
+                    flush();
+                    s = s0;
+                    r = rr;
+                }
+                v += x;
+            }
+        } else if (sys >= 0 && sq != 0.0) {
+            atomicAdd(&sums[size_t(sys) * pw + rr], sq);
+        }
+    }
+};
+
 // rp = D^-1 (b - S x) and the per-(system, rhs) sums of squares.  CORR: x is
 // this iteration's corrected iterate (formed on the fly at the neighbours
-// and written to X), otherwise Xin.  A warp covers 32/W rows: when they all
-// belong to one system the lanes of each column reduce with shuffles and one
-// lane per column adds the sum, otherwise every lane adds its own square.
-// CHECK: the last block to finish runs the convergence test (the other
-// blocks' sums are complete and visible by then).
+// and written to X), otherwise Xin.  CHECK: the last block to finish runs
+// the convergence test (the other blocks' sums are complete and visible by
+// then).
 template <bool CORR, bool CHECK>
 __global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double* Xin, int use_cond,
                                                        cudaGraphConditionalHandle handle) {
-    const unsigned full = 0xffffffffu;
+    PairSums ps{a.norm2, a.pw};
     for_elements(a, [&](bool live, const Elem& q) {
         double sq = 0.0;
-        const int sys = live ? q.s : -1;
         if (live) {
             double acc = 0.0;
             for (int p = a.rp[q.i]; p < a.rp[q.i + 1]; ++p) {
@@ -349,18 +383,9 @@ __global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double
             a.RP[q.e] = rv;
             sq = rv * rv;
         }
-        const int s0 = __shfl_sync(full, sys, 0);
-        const int c0 = __shfl_sync(full, q.c, 0);
-        const bool uniform = __all_sync(full, sys == s0) && s0 >= 0;
-        if (uniform) {
-            double v = sq;
-            for (int d = 16; d >= (1 << c0); d >>= 1) v += __shfl_xor_sync(full, v, d);
-            if ((threadIdx.x & 31) < (1 << c0) && v != 0.0)
-                atomicAdd(&a.norm2[size_t(s0) * a.pw + q.r], v);
-        } else if (sys >= 0 && sq != 0.0) {
-            atomicAdd(&a.norm2[size_t(sys) * a.pw + q.r], sq);
-        }
+        ps.add(live ? q.s : -1, q.c, q.r, sq);
     });
+    ps.flush();
     if (CHECK) {
         __shared__ bool s_last;
         __threadfence();
@@ -377,11 +402,12 @@ __global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double
 
 // Before the loop: sums of squares of D^-1 b per pair (every system).
 __global__ void k_b_init_norms(BatchArgs a) {
+    PairSums ps{a.bnorm2, a.pw};
     for_elements(a, [&](bool live, const Elem& q) {
-        if (!live) return;
-        const double v = a.dinv[q.i] * a.B[q.e];
-        if (v != 0.0) atomicAdd(&a.bnorm2[size_t(q.s) * a.pw + q.r], v * v);
+        const double v = live ? a.dinv[q.i] * a.B[q.e] : 0.0;
+        ps.add(live ? q.s : -1, q.c, q.r, v * v);
     });
+    ps.flush();
 }
 
 // Loop state, per-pair bookkeeping and the active list (every system), by
