@@ -41,12 +41,6 @@ struct BatchState {
 
 constexpr int kThreads = 256;
 
-inline int grid_for(long long work, int threads = kThreads, int cap = 148 * 8) {
-    long long g = (work + threads - 1) / threads;
-    if (g < 1) g = 1;
-    return int(g > cap ? cap : g);
-}
-
 struct BatchArgs {
     int nsys;
     int pw;              // per-pair row width: pair (s, r) is s * pw + r
@@ -481,6 +475,9 @@ struct mclsgpu_batch {
     int body_kernels = 0;
     int per = 1;
     int grab = 1;                  // walk work-queue grab, in 32-history chunks
+    // Grids of the element kernels: every block resident at once (each block
+    // takes one contiguous range, so a second wave would double the time).
+    int g_rich = 1, g_src = 1, g_upd = 1, g_upd0 = 1, g_init = 1;
 };
 
 namespace mclsgpu {
@@ -572,18 +569,24 @@ BatchArgs batch_args(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp, bool all) 
     return a;
 }
 
+template <class K>
+int resident_grid(K kernel, int sms) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, 0);
+    return sms * (b > 0 ? b : 1);
+}
+
 // One batched MCSA iteration (4 kernels) over the active systems.
 int enqueue_batch_iteration(mclsgpu_batch* b, const mclsgpu_mcsa_params* mp, int use_cond,
                             cudaGraphConditionalHandle handle) {
     cudaStream_t s = b->ctx->stream;
     BatchArgs a = batch_args(b, mp, false);
-    const int grid = grid_for(b->ne);
-    k_b_richardson_residual<<<grid, kThreads, 0, s>>>(a);
-    k_b_source<<<grid, kThreads, 0, s>>>(a);
+    k_b_richardson_residual<<<b->g_rich, kThreads, 0, s>>>(a);
+    k_b_source<<<b->g_src, kThreads, 0, s>>>(a);
     const BatchList list{b->act_sys, b->act_hcum, b->act_count, b->d_srow0};
     int rc = launch_walk_batch(b->dom, b->cls, list, b->cR, b->Y, b->grab);
     if (rc) return rc;
-    k_b_update<true, true><<<grid, kThreads, 0, s>>>(a, nullptr, use_cond, handle);
+    k_b_update<true, true><<<b->g_upd, kThreads, 0, s>>>(a, nullptr, use_cond, handle);
     return MCLSGPU_OK;
 }
 
@@ -751,6 +754,12 @@ int mclsgpu_batch_build(mclsgpu_context* ctx, int nsys, const int64_t* n,
          (e = cudaMallocHost(reinterpret_cast<void**>(&b->h_state), sizeof(BatchState))) != cudaSuccess))
         rc = cuda_fail(ctx, e, "cudaMalloc batch");
     if (!rc) {
+        const int sms = ctx->num_sms;
+        b->g_rich = resident_grid(k_b_richardson_residual, sms);
+        b->g_src = resident_grid(k_b_source, sms);
+        b->g_upd = resident_grid(k_b_update<true, true>, sms);
+        b->g_upd0 = resident_grid(k_b_update<false, false>, sms);
+        b->g_init = resident_grid(k_b_init_norms, sms);
         cudaStream_t s = ctx->stream;
         cudaMemcpyAsync(b->d_nrhs, b->nrhs.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(b->d_srow0, srow0.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, s);
@@ -894,9 +903,9 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
     BatchArgs a = batch_args(b, params, true);  // every system
     k_b_state_init<<<1, 1024, 0, s>>>(a, params->max_iters, params->check_freq,
                                        params->tolerance, pairs);
-    const int grid = grid_for(b->ne);
-    k_b_init_norms<<<grid, kThreads, 0, s>>>(a);
-    k_b_update<false, false><<<grid, kThreads, 0, s>>>(a, b->X, 0, cudaGraphConditionalHandle(0));
+    k_b_init_norms<<<b->g_init, kThreads, 0, s>>>(a);
+    k_b_update<false, false><<<b->g_upd0, kThreads, 0, s>>>(a, b->X, 0,
+                                                          cudaGraphConditionalHandle(0));
     cudaMemsetAsync(b->norm2, 0, sizeof(double) * PR, s);
     cudaError_t e = cudaSuccess;
     int rc = MCLSGPU_OK;
@@ -929,7 +938,8 @@ int mclsgpu_batch_mcsa_solve_dev(mclsgpu_batch* b, const double* b_dev, double* 
         std::vector<double> nr(PR), bn(PR);
         std::vector<int> ci(PR);
         cudaMemsetAsync(b->norm2, 0, sizeof(double) * PR, s);
-        k_b_update<false, false><<<grid, kThreads, 0, s>>>(a, b->X, 0, cudaGraphConditionalHandle(0));
+        k_b_update<false, false><<<b->g_upd0, kThreads, 0, s>>>(a, b->X, 0,
+                                                              cudaGraphConditionalHandle(0));
         cudaMemcpyAsync(nr.data(), b->norm2, sizeof(double) * PR, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(bn.data(), b->bnorm2, sizeof(double) * PR, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(ci.data(), b->conv_iter, sizeof(int) * PR, cudaMemcpyDeviceToHost, s);
