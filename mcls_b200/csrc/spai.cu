@@ -265,17 +265,14 @@ constexpr int kFwdW3 = kFwdW2 + kH * kH * 2;       // 16 x 64
 constexpr int kFwdX = kFwdW3 + kO * kH * 2;        // 128 x 16
 constexpr int kFwdH = kFwdX + kTileRows * kF * 2;  // 128 x 64
 constexpr int kFwdBar = kFwdH + kTileRows * kH * 2;
-// Requested dynamic shared memory: the tiles and weights (32 KB) and the
-// barrier; six CTAs fit an SM's shared memory, and their 6 x 64
-// tensor-memory columns its 512.
-constexpr int kFwdSmem = 33 * 1024;
-constexpr int kFwdTmemCols = 64;
+// Requested dynamic shared memory: at most 4 CTAs per SM, so that their
+// 4 x 128 tensor-memory columns fit the SM's 512.
+constexpr int kFwdSmem = 56 * 1024;
 static_assert(kFwdBar + 64 <= kFwdSmem, "forward shared memory");
 
 // Forward pass: one CTA (4 warps, one row per thread) per 128-row tile,
-// persistent over tiles.  TMEM: columns 0-63 hold each layer's accumulator
-// in turn (a layer's MMAs are issued after every thread has read the
-// previous layer's accumulator out, across the fenced barrier).
+// persistent over tiles.  TMEM: columns 0-63 layer-1 and layer-3
+// accumulators, 64-127 layer 2.
 __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -286,7 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
     stage_weights(smem + kFwdW2, a.params + kW2, kH, kH);
     stage_weights(smem + kFwdW3, a.params + kW3, kO, kH);
     if (tid == 0) mbar_init(mbar);
-    if (warp == 0) tmem_alloc(smem_u32(tslot), kFwdTmemCols);
+    if (warp == 0) tmem_alloc(smem_u32(tslot), 128);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
@@ -351,24 +348,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
         if (tid == 0 && ok) {
             fence_after_sync();
             for (int ks = 0; ks < kH / 16; ++ks)
-                mma_bf16(tmem, desc_kmajor(sH, kTileRows, ks), desc_kmajor(sW2, kH, ks),
+                mma_bf16(tmem + 64, desc_kmajor(sH, kTileRows, ks), desc_kmajor(sW2, kH, ks),
                          idesc_bf16(128, kH, 0, 0), ks > 0);
             mma_commit(mbar);
         }
         wait_mma();
         // H2 overwrites H1: layer 2's operands are consumed (its MMAs are
-        // complete once the barrier phase has flipped), so the epilogue can
-        // write each 16-column chunk as soon as it is read (a thread writes
-        // only its own row).
-#pragma unroll 1
-        for (int c = 0; c < kH; c += 16) {
-            float z[16];
-            tmem_ld16(lane_base + c, z);
+        // complete once the barrier phase has flipped).
+        float h2[kH];
 #pragma unroll
-            for (int k = 0; k < 16; ++k) z[k] = fmaxf(z[k] + b2[c + k], 0.f);
-            store8(smem + kFwdH, tid, c, kTileRows, z);
-            store8(smem + kFwdH, tid, c + 8, kTileRows, z + 8);
-        }
+        for (int c = 0; c < kH; c += 16) tmem_ld16(lane_base + 64 + c, h2 + c);
+#pragma unroll
+        for (int k = 0; k < kH; ++k) h2[k] = fmaxf(h2[k] + b2[k], 0.f);
+#pragma unroll
+        for (int c = 0; c < kH; c += 8) store8(smem + kFwdH, tid, c, kTileRows, h2 + c);
         fence_async_smem();
         fence_before_sync();
         __syncthreads();
@@ -413,7 +406,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spai_forward(SpaiFwdArgs a) {
     __syncthreads();
     if (warp == 0) {
         fence_after_sync();
-        tmem_dealloc(tmem, kFwdTmemCols);
+        tmem_dealloc(tmem, 128);
     }
 }
 
@@ -897,15 +890,8 @@ int launch_forward(mclsgpu_spai* net, mclsgpu_operator* op, const SlotTable& t, 
     a.out = out;
     a.status = ctx->d_status;
     const int ntiles = (op->A.n + kTileRows - 1) / kTileRows;
-    // As many CTAs as fit an SM at once (at most 512 / 64 by tensor memory).
-    static int per_sm = 0;
-    if (!per_sm) {
-        int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spai_forward, kThreads, kFwdSmem);
-        per_sm = b < 1 ? 1 : (b > 512 / kFwdTmemCols ? 512 / kFwdTmemCols : b);
-    }
-    const int cap = ctx->num_sms * per_sm;
-    const int grid = ntiles < cap ? ntiles : cap;
+    // Up to 4 CTAs per SM (4 x 128 TMEM columns).
+    const int grid = ntiles < ctx->num_sms * 4 ? ntiles : ctx->num_sms * 4;
     k_spai_forward<<<grid, kThreads, kFwdSmem, ctx->stream>>>(a);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? MCLSGPU_OK : cuda_fail(ctx, e, "spai forward launch");
