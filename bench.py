@@ -341,15 +341,19 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
         out["threshold_sweep"] = sweep
     if not args.no_anderson:
         M = pc.to_scipy(A.shape[0])
-        out["anderson"] = [anderson_arm(args, int(d), dom, bt, xt, A, b, args.seed, jacobi_ms,
-                                        PL=M) for d in args.anderson_depth.split(",")]
+        depths = [int(d) for d in args.anderson_depth.split(",")]
+        # The further seeds for the deepest store only (the accelerated arm).
+        out["anderson"] = [anderson_arm(args, d, dom, bt, xt, A, b, args.seed, jacobi_ms, PL=M,
+                                        seeds=args.learned_anderson_seeds
+                                        if d == max(depths) else "")
+                           for d in depths]
     dom.close()
     pc.close()
     net.close()
     return out
 
 
-def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None):
+def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None, seeds=None):
     """Anderson-accelerated MCSA (the "Adjoint/Forward Anderson" managers) on
     an MCSA arm's domain and right-hand side: one untimed warm-up solve, then
     the timed solves, each from x = 0 on the same random stream.  PL: the
@@ -374,7 +378,7 @@ def anderson_arm(args, depth, dom, bt, xt, A, b, seed, jacobi_ms, PL=None):
     ms = sum(s["solve_ms"] for s in stats) / len(stats)
     rel = float(np.linalg.norm(b - A @ xt.cpu().numpy()) / np.linalg.norm(b))
     sweep = []
-    for sd in [int(v) for v in args.anderson_seeds.split(",") if v]:
+    for sd in [int(v) for v in (args.anderson_seeds if seeds is None else seeds).split(",") if v]:
         # One solve per further seed of the random stream: the spread of the
         # stochastic fixed-point map's acceleration.
         dom.reseed(sd)
@@ -990,6 +994,8 @@ def main():
                     help="Anderson mixing parameter beta (NOX's default 1)")
     ap.add_argument("--anderson-seeds", default="",
                     help="comma-separated further seeds: one Anderson solve each")
+    ap.add_argument("--learned-anderson-seeds", default="777,4242,99,2024",
+                    help="further seeds for the Anderson solves on the learned domain")
     ap.add_argument("--anderson-depth", default="2,6",
                     help="Anderson storage depths to time, comma separated (NOX's default "
                          "is 2)")
