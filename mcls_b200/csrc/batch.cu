@@ -170,96 +170,38 @@ __device__ __forceinline__ void for_elements(const BatchArgs& a, Body body) {
     }
 }
 
-// The same loop two elements per thread and tile (t and t + blockDim): each
-// thread keeps two independent gathers in flight.
-template <class Body>
-__device__ __forceinline__ void for_elements2(const BatchArgs& a, Body body) {
-    __shared__ int s_k0;
-    const int count = *a.lcount;
-    const long long total = count > 0 ? a.lecum[count] : 0;
-    const long long T = blockDim.x, T2 = 2 * T;
-    const long long span = ((total + gridDim.x - 1) / gridDim.x + T2 - 1) / T2 * T2;
-    const long long beg = (long long)blockIdx.x * span;
-    const long long end = beg + span < total ? beg + span : total;
-    if (beg >= end) return;  // the whole block
-    if (threadIdx.x == 0) s_k0 = elem_entry(a.lecum, count, beg);
-    __syncthreads();
-    Cursor cur;
-    cur.load(a, s_k0);
-    for (long long base = beg; base < end; base += T2) {
-        const long long t0 = base + threadIdx.x, t1 = t0 + T;
-        const bool l0 = t0 < end, l1 = t1 < end;
-        Elem q0{}, q1{};
-        if (l0) q0 = cur.at(a, t0);
-        if (l1) q1 = cur.at(a, t1);
-        body(l0, q0, l1, q1);
-    }
-}
-
-// Row products of two elements, interleaved: acc_e = sum_p val[p] * f(element
-// of (col[p], r_e)) over row i_e of the CSR (rp, col, val), in column order
-// (the one-element products' order, so the same sums).
-template <class F>
-__device__ __forceinline__ void gather2(const int* rp, const int* col, const double* val,
-                                        bool l0, const Elem& q0, bool l1, const Elem& q1, F f,
-                                        double& acc0, double& acc1) {
-    const int p0 = l0 ? rp[q0.i] : 0, n0 = l0 ? rp[q0.i + 1] - p0 : 0;
-    const int p1 = l1 ? rp[q1.i] : 0, n1 = l1 ? rp[q1.i + 1] - p1 : 0;
-    const int nm = n0 > n1 ? n0 : n1;
-    for (int u = 0; u < nm; ++u) {
-        double w0 = 0.0, x0 = 0.0, w1 = 0.0, x1 = 0.0;
-        if (u < n0) {
-            w0 = val[p0 + u];
-            x0 = f(size_t(q0.base + ((long long)col[p0 + u] << q0.c) + q0.r));
-        }
-        if (u < n1) {
-            w1 = val[p1 + u];
-            x1 = f(size_t(q1.base + ((long long)col[p1 + u] << q1.c) + q1.r));
-        }
-        if (u < n0) acc0 = fma(w0, x0, acc0);
-        if (u < n1) acc1 = fma(w1, x1, acc1);
-    }
-}
-
 // x2 = x + w rp;  rp2 = D^-1 (b - S x2), with x2 at the neighbours formed on
 // the fly (RichardsonIteration::doOneIteration then updatePrecResidual,
 // src/MCLS_RichardsonIteration_impl.hpp:134-147); the walk tallies Y are
 // cleared for this iteration's walk.
 __global__ void __launch_bounds__(kThreads) k_b_richardson_residual(BatchArgs a) {
-    for_elements2(a, [&](bool l0, const Elem& q0, bool l1, const Elem& q1) {
-        double acc0 = 0.0, acc1 = 0.0;
-        gather2(a.rp, a.ci, a.v, l0, q0, l1, q1,
-                [&](size_t k) { return __dadd_rn(a.X[k], __dmul_rn(a.omega, a.RP[k])); }, acc0,
-                acc1);
-        if (l0) {
-            a.X2[q0.e] = __dadd_rn(a.X[q0.e], __dmul_rn(a.omega, a.RP[q0.e]));
-            a.RP2[q0.e] = a.dinv[q0.i] * (a.B[q0.e] - acc0);
-            a.Y[q0.e] = 0.0;
+    for_elements(a, [&](bool live, const Elem& q) {
+        if (!live) return;
+        double acc = 0.0;
+        for (int p = a.rp[q.i]; p < a.rp[q.i + 1]; ++p) {
+            const size_t k = size_t(q.base + ((long long)a.ci[p] << q.c) + q.r);
+            acc = fma(a.v[p], __dadd_rn(a.X[k], __dmul_rn(a.omega, a.RP[k])), acc);
         }
-        if (l1) {
-            a.X2[q1.e] = __dadd_rn(a.X[q1.e], __dmul_rn(a.omega, a.RP[q1.e]));
-            a.RP2[q1.e] = a.dinv[q1.i] * (a.B[q1.e] - acc1);
-            a.Y[q1.e] = 0.0;
-        }
+        a.X2[q.e] = __dadd_rn(a.X[q.e], __dmul_rn(a.omega, a.RP[q.e]));
+        a.RP2[q.e] = a.dinv[q.i] * (a.B[q.e] - acc);
+        a.Y[q.e] = 0.0;
     });
 }
 
 // Tally source of every right-hand side: expected value c = H (w rp2),
 // collision c = w rp2 (FP32).
 __global__ void __launch_bounds__(kThreads) k_b_source(BatchArgs a) {
-    for_elements2(a, [&](bool l0, const Elem& q0, bool l1, const Elem& q1) {
-        double v0, v1;
+    for_elements(a, [&](bool live, const Elem& q) {
+        if (!live) return;
+        double v;
         if (a.ev) {
-            v0 = 0.0;
-            v1 = 0.0;
-            gather2(a.hrp, a.hci, a.hv, l0, q0, l1, q1, [&](size_t k) { return a.RP2[k]; }, v0,
-                    v1);
+            v = 0.0;
+            for (int p = a.hrp[q.i]; p < a.hrp[q.i + 1]; ++p)
+                v = fma(a.hv[p], a.RP2[size_t(q.base + ((long long)a.hci[p] << q.c) + q.r)], v);
         } else {
-            v0 = l0 ? a.RP2[q0.e] : 0.0;
-            v1 = l1 ? a.RP2[q1.e] : 0.0;
+            v = a.RP2[q.e];
         }
-        if (l0) a.cR[q0.e] = __double2float_rn(a.nomega * v0);
-        if (l1) a.cR[q1.e] = __double2float_rn(a.nomega * v1);
+        a.cR[q.e] = __double2float_rn(a.nomega * v);
     });
 }
 
@@ -422,24 +364,20 @@ template <bool CORR, bool CHECK>
 __global__ void __launch_bounds__(kThreads) k_b_update(BatchArgs a, const double* Xin, int use_cond,
                                                        cudaGraphConditionalHandle handle) {
     PairSums ps{a.norm2, a.pw};
-    for_elements2(a, [&](bool l0, const Elem& q0, bool l1, const Elem& q1) {
-        double acc0 = 0.0, acc1 = 0.0, sq0 = 0.0, sq1 = 0.0;
-        gather2(a.rp, a.ci, a.v, l0, q0, l1, q1,
-                [&](size_t k) { return CORR ? corrected(a, k) : Xin[k]; }, acc0, acc1);
-        if (l0) {
-            if (CORR) a.X[q0.e] = corrected(a, q0.e);
-            const double rv = a.dinv[q0.i] * (a.B[q0.e] - acc0);
-            a.RP[q0.e] = rv;
-            sq0 = rv * rv;
+    for_elements(a, [&](bool live, const Elem& q) {
+        double sq = 0.0;
+        if (live) {
+            double acc = 0.0;
+            for (int p = a.rp[q.i]; p < a.rp[q.i + 1]; ++p) {
+                const size_t k = size_t(q.base + ((long long)a.ci[p] << q.c) + q.r);
+                acc = fma(a.v[p], CORR ? corrected(a, k) : Xin[k], acc);
+            }
+            if (CORR) a.X[q.e] = corrected(a, q.e);
+            const double rv = a.dinv[q.i] * (a.B[q.e] - acc);
+            a.RP[q.e] = rv;
+            sq = rv * rv;
         }
-        if (l1) {
-            if (CORR) a.X[q1.e] = corrected(a, q1.e);
-            const double rv = a.dinv[q1.i] * (a.B[q1.e] - acc1);
-            a.RP[q1.e] = rv;
-            sq1 = rv * rv;
-        }
-        ps.add(l0 ? q0.s : -1, q0.c, q0.r, sq0);
-        ps.add(l1 ? q1.s : -1, q1.c, q1.r, sq1);
+        ps.add(live ? q.s : -1, q.c, q.r, sq);
     });
     ps.flush();
     if (CHECK) {
