@@ -215,21 +215,22 @@ struct SlotTable {
     int pcentre;
 };
 
-// Features of row i from the diagonal-offset storage of A (FP64).
+// Features of row i from the diagonal-offset storage of A (FP64 values,
+// features formed in FP32: the network reads them in BF16).
 __device__ __forceinline__ void row_features(const double* dia, int n, const SlotTable& t, int i,
                                              float* f) {
 #pragma unroll
     for (int k = 0; k < kF; ++k) f[k] = 0.f;
     if (i >= n) return;
-    const double aii = dia[size_t(t.centre) * n + i];
+    const float aii = float(dia[size_t(t.centre) * n + i]);
     int q = 0;
     for (int s = 0; s < t.K; ++s) {
         if (s == t.centre) continue;
         const double a = dia[size_t(s) * n + i];
         const int j = i + t.off[s];
         if (a != 0.0 && j >= 0 && j < n) {
-            f[2 * q] = float(a / aii);
-            f[2 * q + 1] = float(log(dia[size_t(t.centre) * n + j] / aii));
+            f[2 * q] = float(a) / aii;
+            f[2 * q + 1] = logf(float(dia[size_t(t.centre) * n + j]) / aii);
         }
         ++q;
     }
