@@ -149,7 +149,7 @@ def main(argv=None):
     ap.add_argument("--family", choices=["diffusion3d", "anisotropic2d"], default="diffusion3d")
     ap.add_argument("--grid", type=int, default=32, help="grid points per axis of each system")
     ap.add_argument("--systems", type=int, default=8)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=2000, help="0: no training (the initial network)")
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--seed", type=int, default=1000)
     ap.add_argument("--device", type=int, default=0)
@@ -181,12 +181,13 @@ def main(argv=None):
                             generator=g)
         samples.append((op, V))
     net = capi.SpaiNet(ctx, slots, seed=0)
-    losses = train(net, samples, steps=args.steps, lr=args.lr, lr_final=args.lr / 10,
-                   refresh=25 if args.steps >= 100 else 0, adv_count=8, adv_iters=50,
-                   device=args.device)
-    torch.cuda.synchronize()
-    print(f"{len(samples)} systems, {args.steps} steps, {time.perf_counter() - t0:.1f} s, "
-          f"loss {np.mean(losses[:8]):.4f} -> {np.mean(losses[-8:]):.4f}", flush=True)
+    if args.steps > 0:
+        losses = train(net, samples, steps=args.steps, lr=args.lr, lr_final=args.lr / 10,
+                       refresh=25 if args.steps >= 100 else 0, adv_count=8, adv_iters=50,
+                       device=args.device)
+        torch.cuda.synchronize()
+        print(f"{len(samples)} systems, {args.steps} steps, {time.perf_counter() - t0:.1f} s, "
+              f"loss {np.mean(losses[:8]):.4f} -> {np.mean(losses[-8:]):.4f}", flush=True)
     if args.out:
         np.save(args.out, net.params)
     if args.infer_grid:
