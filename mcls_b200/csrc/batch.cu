@@ -174,7 +174,7 @@ __device__ __forceinline__ void for_elements(const BatchArgs& a, Body body) {
 // the fly (RichardsonIteration::doOneIteration then updatePrecResidual,
 // src/MCLS_RichardsonIteration_impl.hpp:134-147); the walk tallies Y are
 // cleared for this iteration's walk.
-__global__ void __launch_bounds__(kThreads, 6) k_b_richardson_residual(BatchArgs a) {
+__global__ void __launch_bounds__(kThreads, 8) k_b_richardson_residual(BatchArgs a) {
     for_elements(a, [&](bool live, const Elem& q) {
         if (!live) return;
         double acc = 0.0;
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_b_richardson_residual(BatchArgs
 
 // Tally source of every right-hand side: expected value c = H (w rp2),
 // collision c = w rp2 (FP32).
-__global__ void __launch_bounds__(kThreads, 6) k_b_source(BatchArgs a) {
+__global__ void __launch_bounds__(kThreads, 8) k_b_source(BatchArgs a) {
     for_elements(a, [&](bool live, const Elem& q) {
         if (!live) return;
         double v;
