@@ -231,28 +231,10 @@ struct StencilOffsets {
 // v[i + off_j] with |h_j| = W (|cdf_j| - |cdf_prev|) and the sign of slot j.
 // The record is read with 256-bit loads and its first 32 bytes (W, c and the
 // first CDF slots) written back with one 256-bit store.
-// The source at the K stencil neighbours of state i, loaded before the
-// record so that both round trips overlap (an index outside [0, n) -- a
-// neighbour the row does not have -- is clamped and its value never used).
-template <int SLOTS>
-__device__ __forceinline__ void prefetch_neighbours(const double* v, int i, int n, double omega,
-                                                    int has, int K, const StencilOffsets& so,
-                                                    double (&vs)[SLOTS]) {
-#pragma unroll
-    for (int j = 0; j < SLOTS; ++j) {
-        if (j >= K) break;
-        int g = i + so.off[j];
-        g = g < 0 ? 0 : (g >= n ? n - 1 : g);
-        vs[j] = load_src(v, g, omega, has);
-    }
-}
-
 template <int WORDS>
-__device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, int n, const double* v,
+__device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, const double* v,
                                                    double omega, int has, int K,
                                                    const StencilOffsets& so) {
-    double vs[WORDS - 2];
-    prefetch_neighbours<WORDS - 2>(v, i, n, omega, has, K, so, vs);
     uint32_t q[WORDS];
 #pragma unroll
     for (int t = 0; t < WORDS / 8; ++t)
@@ -272,7 +254,7 @@ __device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, int n, co
         const float a = fabsf(qv);
         const float h = W * (a - prev);
         prev = a;
-        c = fma(double(qv < 0.f ? -h : h), vs[j], c);
+        c = fma(double(qv < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
     }
     q[1] = __float_as_uint(__double2float_rn(c));
     asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
@@ -284,11 +266,9 @@ __device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, int n, co
 // 65536 (the last entry's 65535 standing for 65536), the transition
 // probabilities the walk samples, and the sign in bit j of word 2.
 template <int WORDS>
-__device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, int n, const double* v,
+__device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, const double* v,
                                                      double omega, int has, int K,
                                                      const StencilOffsets& so) {
-    double vs[2 * (WORDS - 3)];
-    prefetch_neighbours<2 * (WORDS - 3)>(v, i, n, omega, has, K, so, vs);
     uint32_t q[WORDS];
 #pragma unroll
     for (int t = 0; t < WORDS / 8; ++t)
@@ -308,7 +288,7 @@ __device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, int n, 
         if (t == 65535u) t = 65536u;
         const float h = W * (float(t - prev) * 0x1p-16f);
         prev = t;
-        c = fma(double(((q[2] >> j) & 1u) ? -h : h), vs[j], c);
+        c = fma(double(((q[2] >> j) & 1u) ? -h : h), load_src(v, i + so.off[j], omega, has), c);
     }
     q[1] = __float_as_uint(__double2float_rn(c));
     asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
@@ -316,26 +296,25 @@ __device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, int n, 
                  : "memory");
 }
 
-__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int nv, int n,
-                                                             int row0, double omega, int has,
-                                                             int ev, int K, StencilOffsets so,
-                                                             int words, int q16, uint32_t* rec,
-                                                             double* y) {
+__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, int row0,
+                                                             double omega, int has, int ev,
+                                                             int K, StencilOffsets so, int words,
+                                                             int q16, uint32_t* rec, double* y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* r = rec + size_t(i) * words;
         const int g = row0 + i;  // the state's index in v
         if (!ev) {
             r[1] = __float_as_uint(__double2float_rn(load_src(v, g, omega, has)));
         } else if (q16 && words == 8) {
-            rec_stencil16_source<8>(r, g, nv, v, omega, has, K, so);
+            rec_stencil16_source<8>(r, g, v, omega, has, K, so);
         } else if (q16) {
-            rec_stencil16_source<16>(r, g, nv, v, omega, has, K, so);
+            rec_stencil16_source<16>(r, g, v, omega, has, K, so);
         } else if (words == 8) {
-            rec_stencil_source<8>(r, g, nv, v, omega, has, K, so);
+            rec_stencil_source<8>(r, g, v, omega, has, K, so);
         } else if (words == 16) {
-            rec_stencil_source<16>(r, g, nv, v, omega, has, K, so);
+            rec_stencil_source<16>(r, g, v, omega, has, K, so);
         } else {
-            rec_stencil_source<32>(r, g, nv, v, omega, has, K, so);
+            rec_stencil_source<32>(r, g, v, omega, has, K, so);
         }
         y[i] = 0.0;
     }
@@ -602,8 +581,8 @@ void launch_forward_setup(mclsgpu_domain* dom) {
     k_forward_nh<<<1, 1, 0, dom->ctx->stream>>>(dom->d_nh, dom->n * per, dom->d_scalars);
 }
 
-void launch_forward_records(mclsgpu_domain* dom, const double* v, int nv, double omega,
-                            int has_omega, int row0, double* y) {
+void launch_forward_records(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
+                            int row0, double* y) {
     cudaStream_t s = dom->ctx->stream;
     const int n = dom->n;
     const int ev = dom->p.estimator == MCLSGPU_EXPECTED_VALUE;
@@ -611,7 +590,7 @@ void launch_forward_records(mclsgpu_domain* dom, const double* v, int nv, double
         StencilOffsets so{};
         for (int j = 0; j < 32; ++j) so.off[j] = dom->stencil_off[j];
         k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
-            v, nv, n, row0, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots, dom->rec_q16,
+            v, n, row0, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots, dom->rec_q16,
             reinterpret_cast<uint32_t*>(dom->rec), y);
     } else {
         k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, row0, omega, has_omega, ev,
@@ -632,7 +611,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     const int ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
     if (!fused) k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
     if (p.precision == MCLSGPU_FP32) {
-        launch_forward_records(dom, v, n, omega, has_omega, 0, dom->y64);
+        launch_forward_records(dom, v, omega, has_omega, 0, dom->y64);
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);
