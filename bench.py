@@ -267,7 +267,8 @@ def learned_arm(args, ctx, op, A, b, cfgd, jacobi_ms):
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     rl, rj = net.rho(op, iters=300)
-    pc = capi.Precond(ctx, op, capi.PREC_LEARNED_SPAI, net=net)
+    gate = {} if args.learned_rho_fallback is None else {"rho_fallback": args.learned_rho_fallback}
+    pc = capi.Precond(ctx, op, capi.PREC_LEARNED_SPAI, net=net, **gate)
     thresholds = [float(t) for t in args.learned_threshold.split(",")]
     sweep = []
     for thr in thresholds[1:]:
@@ -994,6 +995,9 @@ def main():
                     help="Anderson mixing parameter beta (NOX's default 1)")
     ap.add_argument("--anderson-seeds", default="",
                     help="comma-separated further seeds: one Anderson solve each")
+    ap.add_argument("--learned-rho-fallback", type=float, default=None,
+                    help="the learned preconditioner's rho gate (default: the library's 0.95; "
+                         "2 disables it)")
     ap.add_argument("--learned-anderson-seeds", default="777,4242,99,2024",
                     help="further seeds for the Anderson solves on the learned domain")
     ap.add_argument("--anderson-depth", default="2,6",
