@@ -286,9 +286,9 @@ void anderson_drop_graph(mclsgpu_domain* dom);
 // FP32 forward walks: the tally source of v into the domain's records (H v
 // for the expected-value estimator, v for collision, with the Neumann
 // relaxation when has_omega) and the tallies y cleared.  row0: the global
-// index of the domain's first row (v is the whole vector).
-void launch_forward_records(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
-                            int row0, double* y);
+// index of the domain's first row (v is the whole vector, nv entries).
+void launch_forward_records(mclsgpu_domain* dom, const double* v, int nv, double omega,
+                            int has_omega, int row0, double* y);
 
 // ---- batched walks (walk.cu, batch.cu) -------------------------------------------
 // Width classes of a batch: the rows [crow[c], crow[c+1]) belong to systems

@@ -231,10 +231,33 @@ struct StencilOffsets {
 // v[i + off_j] with |h_j| = W (|cdf_j| - |cdf_prev|) and the sign of slot j.
 // The record is read with 256-bit loads and its first 32 bytes (W, c and the
 // first CDF slots) written back with one 256-bit store.
+// The source at the stencil neighbours of state i, loaded before the record
+// so that both round trips overlap (an index outside [0, n) -- a neighbour
+// the row does not have -- is clamped and its value never used).
+template <int SLOTS>
+__device__ __forceinline__ void prefetch_neighbours(const double* v, int i, int n, double omega,
+                                                    int has, int K, const StencilOffsets& so,
+                                                    double (&vs)[SLOTS]) {
+    // Every slot is loaded (a slot past K has offset 0: the state itself), so
+    // the loop unrolls and vs stays in registers.
+#pragma unroll
+    for (int j = 0; j < SLOTS; ++j) {
+        int g = i + so.off[j];
+        g = g < 0 ? 0 : (g >= n ? n - 1 : g);
+        vs[j] = load_src(v, g, omega, has);
+    }
+}
+
 template <int WORDS>
-__device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, const double* v,
+__device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, int n, const double* v,
                                                    double omega, int has, int K,
                                                    const StencilOffsets& so) {
+    // 32-byte records: the neighbours' source loaded before the record; larger
+    // records load it slot by slot after the record (their slot counts would
+    // cost the registers of several resident blocks).
+    constexpr bool kPre = WORDS == 8;
+    double vs[kPre ? WORDS - 2 : 1];
+    if constexpr (kPre) prefetch_neighbours<WORDS - 2>(v, i, n, omega, has, K, so, vs);
     uint32_t q[WORDS];
 #pragma unroll
     for (int t = 0; t < WORDS / 8; ++t)
@@ -254,7 +277,10 @@ __device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, const dou
         const float a = fabsf(qv);
         const float h = W * (a - prev);
         prev = a;
-        c = fma(double(qv < 0.f ? -h : h), load_src(v, i + so.off[j], omega, has), c);
+        double src;
+        if constexpr (kPre) src = vs[j];
+        else src = load_src(v, i + so.off[j], omega, has);
+        c = fma(double(qv < 0.f ? -h : h), src, c);
     }
     q[1] = __float_as_uint(__double2float_rn(c));
     asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
@@ -266,9 +292,12 @@ __device__ __forceinline__ void rec_stencil_source(uint32_t* r, int i, const dou
 // 65536 (the last entry's 65535 standing for 65536), the transition
 // probabilities the walk samples, and the sign in bit j of word 2.
 template <int WORDS>
-__device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, const double* v,
+__device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, int n, const double* v,
                                                      double omega, int has, int K,
                                                      const StencilOffsets& so) {
+    constexpr bool kPre = WORDS == 8;
+    double vs[kPre ? 2 * (WORDS - 3) : 1];
+    if constexpr (kPre) prefetch_neighbours<2 * (WORDS - 3)>(v, i, n, omega, has, K, so, vs);
     uint32_t q[WORDS];
 #pragma unroll
     for (int t = 0; t < WORDS / 8; ++t)
@@ -288,7 +317,10 @@ __device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, const d
         if (t == 65535u) t = 65536u;
         const float h = W * (float(t - prev) * 0x1p-16f);
         prev = t;
-        c = fma(double(((q[2] >> j) & 1u) ? -h : h), load_src(v, i + so.off[j], omega, has), c);
+        double src;
+        if constexpr (kPre) src = vs[j];
+        else src = load_src(v, i + so.off[j], omega, has);
+        c = fma(double(((q[2] >> j) & 1u) ? -h : h), src, c);
     }
     q[1] = __float_as_uint(__double2float_rn(c));
     asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"(q[0]),
@@ -296,26 +328,23 @@ __device__ __forceinline__ void rec_stencil16_source(uint32_t* r, int i, const d
                  : "memory");
 }
 
-__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int n, int row0,
-                                                             double omega, int has, int ev,
-                                                             int K, StencilOffsets so, int words,
-                                                             int q16, uint32_t* rec, double* y) {
+// One kernel per record layout (WORDS 32-bit words, Q16: 16-bit
+// thresholds), so that each keeps only its own slots' prefetched source in
+// registers.
+template <int WORDS, bool Q16>
+__global__ void __launch_bounds__(256) k_forward_rec_stencil(const double* v, int nv, int n,
+                                                             int row0, double omega, int has,
+                                                             int ev, int K, StencilOffsets so,
+                                                             uint32_t* rec, double* y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t* r = rec + size_t(i) * words;
+        uint32_t* r = rec + size_t(i) * WORDS;
         const int g = row0 + i;  // the state's index in v
-        if (!ev) {
+        if (!ev)
             r[1] = __float_as_uint(__double2float_rn(load_src(v, g, omega, has)));
-        } else if (q16 && words == 8) {
-            rec_stencil16_source<8>(r, g, v, omega, has, K, so);
-        } else if (q16) {
-            rec_stencil16_source<16>(r, g, v, omega, has, K, so);
-        } else if (words == 8) {
-            rec_stencil_source<8>(r, g, v, omega, has, K, so);
-        } else if (words == 16) {
-            rec_stencil_source<16>(r, g, v, omega, has, K, so);
-        } else {
-            rec_stencil_source<32>(r, g, v, omega, has, K, so);
-        }
+        else if constexpr (Q16)
+            rec_stencil16_source<WORDS>(r, g, nv, v, omega, has, K, so);
+        else
+            rec_stencil_source<WORDS>(r, g, nv, v, omega, has, K, so);
         y[i] = 0.0;
     }
 }
@@ -581,17 +610,31 @@ void launch_forward_setup(mclsgpu_domain* dom) {
     k_forward_nh<<<1, 1, 0, dom->ctx->stream>>>(dom->d_nh, dom->n * per, dom->d_scalars);
 }
 
-void launch_forward_records(mclsgpu_domain* dom, const double* v, double omega, int has_omega,
-                            int row0, double* y) {
+void launch_forward_records(mclsgpu_domain* dom, const double* v, int nv, double omega,
+                            int has_omega, int row0, double* y) {
     cudaStream_t s = dom->ctx->stream;
     const int n = dom->n;
     const int ev = dom->p.estimator == MCLSGPU_EXPECTED_VALUE;
     if (dom->stencil_k) {
         StencilOffsets so{};
         for (int j = 0; j < 32; ++j) so.off[j] = dom->stencil_off[j];
-        k_forward_rec_stencil<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(
-            v, n, row0, omega, has_omega, ev, dom->stencil_k, so, 2 * dom->slots, dom->rec_q16,
-            reinterpret_cast<uint32_t*>(dom->rec), y);
+        const int grid = grid_for(n, 256, 148 * 8);
+        uint32_t* rec = reinterpret_cast<uint32_t*>(dom->rec);
+        const int K = dom->stencil_k, words = 2 * dom->slots;
+#define MCLSGPU_SRC(W, Q)                                                                 \
+    k_forward_rec_stencil<W, Q><<<grid, 256, 0, s>>>(v, nv, n, row0, omega, has_omega, ev, K, \
+                                                     so, rec, y)
+        if (dom->rec_q16) {
+            if (words == 8) MCLSGPU_SRC(8, true);
+            else MCLSGPU_SRC(16, true);
+        } else if (words == 8) {
+            MCLSGPU_SRC(8, false);
+        } else if (words == 16) {
+            MCLSGPU_SRC(16, false);
+        } else {
+            MCLSGPU_SRC(32, false);
+        }
+#undef MCLSGPU_SRC
     } else {
         k_forward_rec<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(v, n, row0, omega, has_omega, ev,
                                                                dom->DS.off, dom->DS.col,
@@ -611,7 +654,7 @@ void launch_forward_source(mclsgpu_domain* dom, const double* v, double omega, i
     const int ev = p.estimator == MCLSGPU_EXPECTED_VALUE;
     if (!fused) k_forward_nh<<<1, 1, 0, s>>>(dom->d_nh, n * per, dom->d_scalars);
     if (p.precision == MCLSGPU_FP32) {
-        launch_forward_records(dom, v, omega, has_omega, 0, dom->y64);
+        launch_forward_records(dom, v, n, omega, has_omega, 0, dom->y64);
     } else {
         k_forward_c<double><<<grid_for(n), 256, 0, s>>>(v, n, omega, has_omega, ev, dom->D.rp,
                                                         dom->D.ci, dom->D.v, dom->c64);

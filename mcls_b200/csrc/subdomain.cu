@@ -286,7 +286,8 @@ int mclsgpu_subdomain_begin(mclsgpu_subdomain* sd, const double* rhs_dev, int64_
         // The part's rows' tally source into their records (the whole-domain
         // build's kernels, over the part's rows), the tallies cleared, and the
         // part's slice of the source kept for the finalisation.
-        launch_forward_records(&sd->recs, rhs_dev, omega, omega > 0.0, sd->row0, sd->y);
+        launch_forward_records(&sd->recs, rhs_dev, int(sd->N), omega, omega > 0.0, sd->row0,
+                               sd->y);
         cudaMemcpyAsync(sd->srcp, rhs_dev + sd->row0, size_t(sd->n) * sizeof(double),
                         cudaMemcpyDeviceToDevice, s);
         sd->range[0] = (long long)sd->row0 * sd->per;
